@@ -1,0 +1,400 @@
+#!/usr/bin/env python
+"""Louvain benchmark: R-MAT scale 24 (plain method) on one B200 per rank.
+
+One step = one complete Louvain run (all levels, gain threshold 1e-6) from
+singleton communities on the seeded R-MAT-24 graph (a=.57 b=.19 c=.19,
+edge factor 16, float32 weights uniform in [0.5, 1.5)).
+
+  value : edge-sweeps/s with the graph resident in HBM (lv_create_device once,
+          lv_reset + lv_run per step), timed with CUDA events between barriers,
+          max over ranks; whole-job value = sum of all ranks' edge-sweeps.
+  e2e   : the same metric through the public C ABI with host buffers: each
+          step creates the engine from pinned host CSR (host->device copies
+          inside lv_create), runs, and reads the original->community map back.
+  roofline: the dominant kernel class (most device time), its algorithmic
+          bytes (8 + weight bytes per edge, 20 per vertex) over its
+          event-timed duration, against the measured HBM copy bandwidth.
+  cpu_baseline: the CPU oracle (OpenMP, exact same rule) on the box's host
+          cores, sample = the first level-0 sweep(s) of the same graph.
+
+--impl reference: the reference has no CPU implementation of the path, so
+the reference arm times the CPU restatement of its rule (the oracle, all host
+threads) on the same workload; each step is one level-0 sweep.
+
+Multi-GPU: the path does not shard (one graph per GPU); --gpus N runs N
+independent replicas under torchrun (weak scaling, no collective on the
+data path; the only collectives are the timing barrier and max/sum).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "Louvain wall-time + edge-sweeps/s at RMAT-24; learned vs plain at ΔQ≤1e-3"
+UNIT = "edge-sweeps/s"
+SEED = 1
+EDGE_FACTOR = 16
+MIN_GAIN = 1e-6
+FALLBACK_HBM_GBS = 6650.0
+CLASS_NAMES = ["b0_deg4", "b1_deg8", "b2_deg16", "b3_deg32", "b4_deg84", "b5_deg319",
+               "h1_deg1024", "h2_deg4096", "hg_global"]
+
+
+def load_pkg():
+    import importlib.util
+    if "gpu_louvain_b200" in sys.modules:
+        return sys.modules["gpu_louvain_b200"]
+    d = os.path.join(ROOT, "gpu-louvain_b200")
+    spec = importlib.util.spec_from_file_location("gpu_louvain_b200", os.path.join(d, "__init__.py"),
+                                                  submodule_search_locations=[d])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["gpu_louvain_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    return oracle
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# rank plumbing (torch.distributed; gloo on CPU for tests, nccl on GPUs)
+# ---------------------------------------------------------------------------
+class Ranks:
+    def __init__(self, backend=None):
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group(backend or "nccl", timeout=datetime.timedelta(seconds=600))
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def reduce(self, x: float, op: str) -> float:
+        if not self.pg:
+            return x
+        import torch
+        import torch.distributed as dist
+        dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+def combine(ranks: Ranks, local_units: float, local_seconds: float):
+    """Whole-job throughput: all ranks' units over the slowest rank's time."""
+    units = ranks.reduce(local_units, "sum")
+    secs = ranks.reduce(local_seconds, "max")
+    return units, secs, (units / secs if secs > 0 else 0.0)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gpu_index_for(local_rank: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x.strip() for x in vis.split(",") if x.strip()]
+        if local_rank < len(ids) and ids[local_rank].isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(cls_name: str):
+    """DRAM bytes per launch of a kernel class from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d.get(cls_name)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (the oracle, OpenMP)
+# ---------------------------------------------------------------------------
+def cpu_sweeps(rowptr, col, w, sweeps: int, warmup: int = 0):
+    orc = load_oracle()
+    nt = host_threads()
+    o = orc.Oracle(rowptr, col, w, nt)
+    for _ in range(warmup):
+        o.sweep()
+    t0 = time.perf_counter()
+    for _ in range(sweeps):
+        o.sweep()
+    dt = time.perf_counter() - t0
+    E = len(col)
+    o.close()
+    return E * sweeps / dt, dt, nt
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, ranks: Ranks):
+    import numpy as np
+    import torch
+    lvb = load_pkg()
+    dev = ranks.local
+    torch.cuda.set_device(dev)
+    scale = args.scale
+    dg = lvb.gen_rmat_device(scale, EDGE_FACTOR, SEED, device=dev)
+    V, E = dg.V, dg.E
+    # --- value: resident inputs ---
+    eng = lvb.Louvain(device_csr=(dg.rowptr, dg.col, dg.w, V, E), device=dev, profile=True)
+    for _ in range(args.warmup):
+        eng.reset()
+        eng.run(MIN_GAIN)
+    eng.reset()
+    eng.clear_stats()
+    sampler = ClockSampler(gpu_index_for(dev))
+    ranks.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    qs = []
+    for k in range(args.steps):
+        if k:
+            eng.reset()
+        qs.append(eng.run(MIN_GAIN))
+    ev1.record()
+    torch.cuda.synchronize()
+    ranks.barrier()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    st = eng.stats()
+    cs = eng.class_stats()
+    o2c, ncomm = eng.original_to_community()
+    units, secs, value = combine(ranks, float(st["edge_sweeps"]), ms / 1e3)
+    # roofline of the dominant kernel class
+    dom = max(range(len(CLASS_NAMES)), key=lambda c: cs["ms"][c])
+    peak, peak_kind = measured_peak()
+    achieved = cs["bytes"][dom] / (cs["ms"][dom] * 1e-3) / 1e9 if cs["ms"][dom] > 0 else 0.0
+    per_launch_bytes = cs["bytes"][dom] / max(cs["launches"][dom], 1)
+    sweep_gbs = st["move_bytes"] / (st["move_ms"] * 1e-3) / 1e9 if st["move_ms"] > 0 else 0.0
+    class_table = {CLASS_NAMES[c]: {"launches": cs["launches"][c], "ms": round(cs["ms"][c], 3),
+                                    "GB/s": round(cs["bytes"][c] / (cs["ms"][c] * 1e-3) / 1e9, 1)
+                                    if cs["ms"][c] > 0 else None}
+                   for c in range(len(CLASS_NAMES))}
+    eng.close()
+    # --- e2e: host buffers through the C ABI ---
+    def dev_tensor(ptr, n, dtype):
+        class W:
+            __cuda_array_interface__ = {"shape": (n,), "typestr": dtype, "data": (ptr, False), "version": 3}
+        return torch.as_tensor(W(), device=f"cuda:{dev}")
+    h_rp = torch.empty(V + 1, dtype=torch.int32, pin_memory=True)
+    h_cl = torch.empty(E, dtype=torch.int32, pin_memory=True)
+    h_w = torch.empty(E, dtype=torch.float32, pin_memory=True)
+    h_rp.copy_(dev_tensor(dg.rowptr, V + 1, "<i4"))
+    h_cl.copy_(dev_tensor(dg.col, E, "<i4"))
+    h_w.copy_(dev_tensor(dg.w, E, "<f4"))
+    torch.cuda.synchronize()
+    dg.free()
+    host_graph = lvb.Graph(h_rp.numpy(), h_cl.numpy(), h_w.numpy())
+    out_map = torch.empty(V, dtype=torch.int32, pin_memory=True).numpy()
+    e2e_steps = max(1, args.steps)
+
+    def e2e_step():
+        with lvb.Louvain(host_graph, device=dev) as e:
+            e.run(MIN_GAIN)
+            m, nc = e.original_to_community()
+            out_map[:] = m
+            return e.stats()["edge_sweeps"]
+
+    e2e_step()   # warm-up (allocator, module load)
+    ranks.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_units = 0
+    for _ in range(e2e_steps):
+        e2e_units += e2e_step()
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    ranks.barrier()
+    _, _, e2e_value = combine(ranks, float(e2e_units), t_e2e)
+    assert np.array_equal(out_map, o2c), "e2e partition differs from the resident run"
+    # --- CPU baseline on rank 0 at N=1 ---
+    cpu = None
+    if ranks.world == 1 and ranks.rank == 0 and not args.no_cpu_baseline:
+        cpu_val, cpu_dt, nt = cpu_sweeps(host_graph.rowptr, host_graph.col, host_graph.w, args.cpu_sweeps)
+        cpu = {"value": cpu_val, "unit": UNIT, "cores": nt, "kind": "port",
+               "sample": f"oracle (OpenMP, exact rule) level-0 sweep x{args.cpu_sweeps} of the same "
+                         f"R-MAT-{scale} graph (E={E}), {cpu_dt:.2f} s"}
+    ms_per_step = secs * 1e3 / args.steps
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded R-MAT generated on device)",
+        "config": {"workload": f"rmat{scale}_plain", "scale": scale, "edge_factor": EDGE_FACTOR,
+                   "a_b_c": [0.57, 0.19, 0.19], "seed": SEED, "V": V, "E_csr": E,
+                   "weights": "fp32 uniform [0.5,1.5) (exact on the 2^-24 grid)",
+                   "min_gain": MIN_GAIN, "parallelism": f"replicas{ranks.world}",
+                   "l2": "inputs larger than L2 (CSR %.2f GB vs 126 MB L2)" % ((8 * E + 4 * V) / 1e9)},
+        "wall_time_s": ms_per_step / 1e3,
+        "modularity": qs[-1], "communities": ncomm, "levels": st["levels"] // args.steps,
+        "sweeps": st["sweeps"] // args.steps, "edge_sweeps_per_run": st["edge_sweeps"] // args.steps,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * (V + 1) + 8 * E,
+                "d2h_bytes_per_step": 4 * V, "seconds_per_step": t_e2e / e2e_steps},
+        "gpu_launches": st["kernel_launches"],
+        "roofline": {"bound": "hbm", "kernel": CLASS_NAMES[dom], "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "bytes_per_launch": per_launch_bytes,
+                     "traffic": ncu_traffic(CLASS_NAMES[dom]),
+                     "sweep_achieved": sweep_gbs, "sweep_frac": sweep_gbs / peak},
+        "phases_ms_per_step": {k: round(st[k] / args.steps, 3)
+                               for k in ("move_ms", "modularity_ms", "aggregate_ms", "setup_ms")},
+        "classes": class_table,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    return line
+
+
+def run_reference(args, ranks: Ranks):
+    """The reference arm: CPU restatement of the reference's rule, all host
+    threads, rank 0 only."""
+    if ranks.rank != 0:
+        return None
+    lvb = load_pkg()
+    g = lvb.gen_rmat(args.scale, EDGE_FACTOR, SEED)
+    orc = load_oracle()
+    nt = host_threads()
+    o = orc.Oracle(g.rowptr, g.col, g.w, nt)
+    for _ in range(args.warmup):
+        o.sweep()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.sweep()
+    dt = time.perf_counter() - t0
+    value = g.E * args.steps / dt
+    sample = (f"level-0 sweeps {args.warmup + 1}..{args.warmup + args.steps} of R-MAT-{args.scale} "
+              f"(E={g.E}) by the CPU restatement of the reference rule, {nt} threads")
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded R-MAT generated on the host)",
+        "config": {"workload": f"rmat{args.scale}_plain", "scale": args.scale,
+                   "edge_factor": EDGE_FACTOR, "seed": SEED, "V": g.V, "E_csr": g.E,
+                   "min_gain": MIN_GAIN, "parallelism": "cpu"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--cpu-sweeps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        ranks = Ranks(backend="gloo")
+        line = run_reference(args, ranks)
+    else:
+        ranks = Ranks()
+        line = run_ours(args, ranks)
+    if ranks.rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    ranks.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,401 @@
+"""gpu-louvain_b200 -- Python host mirror of the B200 Louvain engine.
+
+The engine is the C-ABI library ``lib/liblouvain_b200.so`` (CUDA kernels for
+sm_100a, see ``include/louvain_b200.h``).  This module binds it with ctypes and
+mirrors the reference's operator surface for the level loop:
+
+    Louvain.optimise_modularity(min_gain)  <- optimiseModularity
+                                             (modularity_optimisation.cuh:28)
+    Louvain.aggregate_communities()        <- aggregateCommunities
+                                             (community_aggregation.cuh:11)
+    Louvain.calculate_modularity()         <- calculateModularity
+                                             (modularity_optimisation.cuh:30)
+    Louvain.run(min_gain)                  <- the level loop of main()
+                                             (gpulouvain.cu:30-37)
+    read_mtx(path)                         <- readInputData (utils.cu:9-62)
+    print_communities(...)                 <- printOriginalToCommunity
+                                             (modularity_optimisation.cu:403-418)
+
+Errors raise LouvainError carrying the lv_status code (the reference exits
+the process instead, utils.cuh:92-98).  There is no CPU fallback: when the
+library or a CUDA device is missing the calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "liblouvain_b200.so")
+CLI_PATH = os.path.join(_HERE, "bin", "gpulouvain")
+
+LV_OK = 0
+LV_ERR_INVALID = 1
+LV_ERR_WEIGHT = 2
+LV_ERR_TOO_LARGE = 3
+LV_ERR_NOMEM = 4
+LV_ERR_CUDA = 5
+LV_ERR_DEVICE = 6
+LV_ERR_IO = 7
+LV_ERR_NO_DEVICE = 8
+
+NUM_CLASSES = 9
+CLASS_NAMES = ["b0_deg4", "b1_deg8", "b2_deg16", "b3_deg32", "b4_deg84", "b5_deg319",
+               "h1_deg1024", "h2_deg4096", "hg_global"]
+
+
+class LouvainError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        self.status = status
+        super().__init__(f"lv_status {status}: {msg}")
+
+
+class _Opts(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("device", C.c_int32), ("max_sweeps", C.c_int32),
+                ("profile", C.c_int32), ("reserved", C.c_int32 * 12)]
+
+
+class _Stats(C.Structure):
+    _fields_ = [("levels", C.c_int32), ("final_vertices", C.c_int32), ("sweeps", C.c_int64),
+                ("edge_sweeps", C.c_int64), ("moves", C.c_int64), ("move_ms", C.c_double),
+                ("modularity_ms", C.c_double), ("aggregate_ms", C.c_double),
+                ("setup_ms", C.c_double), ("move_bytes", C.c_double),
+                ("kernel_launches", C.c_int64)]
+
+
+class _ClassStats(C.Structure):
+    _fields_ = [("launches", C.c_int64 * NUM_CLASSES), ("vertices", C.c_int64 * NUM_CLASSES),
+                ("edges", C.c_int64 * NUM_CLASSES), ("ms", C.c_double * NUM_CLASSES),
+                ("bytes", C.c_double * NUM_CLASSES)]
+
+
+EXPORTED = [
+    "lv_default_opts", "lv_status_string", "lv_version", "lv_create", "lv_create_device",
+    "lv_reset", "lv_destroy", "lv_last_error", "lv_optimise_level", "lv_aggregate",
+    "lv_modularity", "lv_run", "lv_sweep", "lv_get_original_to_community", "lv_get_communities",
+    "lv_set_communities", "lv_get_level_info", "lv_get_csr", "lv_get_scale", "lv_get_stats",
+    "lv_get_class_stats", "lv_clear_stats", "lv_read_mtx", "lv_write_mtx", "lv_free_host",
+    "lv_print_communities", "lv_gen_rmat", "lv_gen_planted", "lv_gen_rmat_device",
+    "lv_free_device",
+]
+
+_lib = None
+
+P32 = C.POINTER(C.c_int32)
+P64 = C.POINTER(C.c_int64)
+PF = C.POINTER(C.c_float)
+
+
+def build(verbose: bool = False) -> None:
+    """Compile the CUDA library and CLI in-tree (nvcc, sm_100a)."""
+    r = subprocess.run(["make", "-C", _HERE, "-j8"], capture_output=True, text=True)
+    if verbose or r.returncode != 0:
+        print(r.stdout[-4000:], r.stderr[-4000:])
+    if r.returncode != 0:
+        raise RuntimeError("building liblouvain_b200.so failed")
+
+
+def lib() -> C.CDLL:
+    """Load the engine library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build the CUDA extension first")
+    L = C.CDLL(LIB_PATH)
+    L.lv_status_string.restype = C.c_char_p
+    L.lv_version.restype = C.c_char_p
+    L.lv_last_error.restype = C.c_char_p
+    L.lv_last_error.argtypes = [C.c_void_p]
+    L.lv_default_opts.argtypes = [C.POINTER(_Opts)]
+    L.lv_create.argtypes = [P32, P32, PF, C.c_int32, C.c_int64, C.POINTER(_Opts), C.POINTER(C.c_void_p)]
+    L.lv_create_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64,
+                                   C.POINTER(_Opts), C.POINTER(C.c_void_p)]
+    for name in ["lv_reset", "lv_destroy", "lv_aggregate", "lv_clear_stats"]:
+        getattr(L, name).argtypes = [C.c_void_p]
+    L.lv_optimise_level.argtypes = [C.c_void_p, C.c_float, P32]
+    L.lv_modularity.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    L.lv_run.argtypes = [C.c_void_p, C.c_float, C.POINTER(C.c_double)]
+    L.lv_sweep.argtypes = [C.c_void_p, P64]
+    L.lv_get_original_to_community.argtypes = [C.c_void_p, P32, P32]
+    L.lv_get_communities.argtypes = [C.c_void_p, P32]
+    L.lv_set_communities.argtypes = [C.c_void_p, P32]
+    L.lv_get_level_info.argtypes = [C.c_void_p, P32, P64, P32]
+    L.lv_get_csr.argtypes = [C.c_void_p, P32, P32, P64]
+    L.lv_get_scale.argtypes = [C.c_void_p, P32, C.POINTER(C.c_uint64), P32]
+    L.lv_get_stats.argtypes = [C.c_void_p, C.POINTER(_Stats)]
+    L.lv_get_class_stats.argtypes = [C.c_void_p, C.POINTER(_ClassStats)]
+    L.lv_read_mtx.argtypes = [C.c_char_p, P32, P64, C.POINTER(P32), C.POINTER(P32), C.POINTER(PF), PF]
+    L.lv_write_mtx.argtypes = [C.c_char_p, C.c_int32, C.c_int64, P32, P32, PF]
+    L.lv_free_host.argtypes = [C.c_void_p]
+    L.lv_print_communities.argtypes = [C.c_char_p, P32, C.c_int32, C.c_int32]
+    L.lv_gen_rmat.argtypes = [C.c_int32, C.c_int32, C.c_uint64, C.c_double, C.c_double, C.c_double,
+                              C.c_int32, P32, P64, C.POINTER(P32), C.POINTER(P32), C.POINTER(PF)]
+    L.lv_gen_planted.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_uint64, C.c_int32,
+                                 P64, C.POINTER(P32), C.POINTER(P32), C.POINTER(PF)]
+    L.lv_gen_rmat_device.argtypes = [C.c_int32, C.c_int32, C.c_uint64, C.c_double, C.c_double,
+                                     C.c_double, C.c_int32, C.c_int32, P32, P64,
+                                     C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                     C.POINTER(C.c_void_p)]
+    L.lv_free_device.argtypes = [C.c_void_p]
+    _lib = L
+    return L
+
+
+def status_string(code: int) -> str:
+    return lib().lv_status_string(code).decode()
+
+
+def _check(code: int, handle=None) -> None:
+    if code != LV_OK:
+        msg = status_string(code)
+        if handle:
+            detail = lib().lv_last_error(handle)
+            if detail:
+                msg += f" ({detail.decode()})"
+        raise LouvainError(code, msg)
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _ptr(a: np.ndarray, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def _take_host(ptr, n: int, dtype) -> np.ndarray:
+    """Copy a malloc'd C array into numpy and free it."""
+    L = lib()
+    if n > 0:
+        buf = np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype, copy=True)
+    else:
+        buf = np.zeros(0, dtype=dtype)
+    L.lv_free_host(C.cast(ptr, C.c_void_p))
+    return buf
+
+
+class Graph:
+    """A CSR graph on the host: rowptr int32[V+1], col int32[E], w float32[E]."""
+
+    def __init__(self, rowptr, col, w, m_ref: float | None = None):
+        self.rowptr = _i32(rowptr)
+        self.col = _i32(col)
+        self.w = np.ascontiguousarray(w, dtype=np.float32)
+        self.m_ref = m_ref
+
+    @property
+    def V(self) -> int:
+        return int(self.rowptr.shape[0] - 1)
+
+    @property
+    def E(self) -> int:
+        return int(self.col.shape[0])
+
+    def edges(self):
+        """Undirected edge list (u > v, plus self-loops) with weights."""
+        row = np.repeat(np.arange(self.V, dtype=np.int32), np.diff(self.rowptr))
+        m = row >= self.col
+        return row[m], self.col[m], self.w[m]
+
+
+def read_mtx(path: str) -> Graph:
+    L = lib()
+    V = C.c_int32()
+    E = C.c_int64()
+    rp, cl, w = P32(), P32(), PF()
+    m = C.c_float()
+    _check(L.lv_read_mtx(path.encode(), C.byref(V), C.byref(E), C.byref(rp), C.byref(cl), C.byref(w),
+                         C.byref(m)))
+    return Graph(_take_host(rp, V.value + 1, np.int32), _take_host(cl, E.value, np.int32),
+                 _take_host(w, E.value, np.float32), m_ref=m.value)
+
+
+def write_mtx(path: str, g: Graph) -> None:
+    u, v, w = g.edges()
+    u, v, w = _i32(u), _i32(v), np.ascontiguousarray(w, dtype=np.float32)
+    _check(lib().lv_write_mtx(path.encode(), g.V, len(u), _ptr(u, C.c_int32), _ptr(v, C.c_int32),
+                              _ptr(w, C.c_float)))
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, seed: int = 1, a: float = 0.57, b: float = 0.19,
+             c: float = 0.19, weights: str = "uniform") -> Graph:
+    L = lib()
+    V = C.c_int32()
+    E = C.c_int64()
+    rp, cl, w = P32(), P32(), PF()
+    _check(L.lv_gen_rmat(scale, edge_factor, seed, a, b, c, 1 if weights == "uniform" else 0,
+                         C.byref(V), C.byref(E), C.byref(rp), C.byref(cl), C.byref(w)))
+    return Graph(_take_host(rp, V.value + 1, np.int32), _take_host(cl, E.value, np.int32),
+                 _take_host(w, E.value, np.float32))
+
+
+def gen_planted(V: int = 10000, blocks: int = 64, d_in: float = 16.0, d_out: float = 2.0,
+                seed: int = 0, weights: str = "unit") -> Graph:
+    L = lib()
+    E = C.c_int64()
+    rp, cl, w = P32(), P32(), PF()
+    _check(L.lv_gen_planted(V, blocks, d_in, d_out, seed, 1 if weights == "uniform" else 0,
+                            C.byref(E), C.byref(rp), C.byref(cl), C.byref(w)))
+    return Graph(_take_host(rp, V + 1, np.int32), _take_host(cl, E.value, np.int32),
+                 _take_host(w, E.value, np.float32))
+
+
+class DeviceGraph:
+    """A CSR graph drawn on the device (owned device buffers)."""
+
+    def __init__(self, V, E, rowptr, col, w, device):
+        self.V, self.E = V, E
+        self.rowptr, self.col, self.w = rowptr, col, w
+        self.device = device
+
+    def free(self) -> None:
+        L = lib()
+        for p in (self.rowptr, self.col, self.w):
+            if p:
+                L.lv_free_device(C.c_void_p(p))
+        self.rowptr = self.col = self.w = 0
+
+
+def gen_rmat_device(scale: int, edge_factor: int = 16, seed: int = 1, a: float = 0.57,
+                    b: float = 0.19, c: float = 0.19, weights: str = "uniform",
+                    device: int = 0) -> DeviceGraph:
+    L = lib()
+    V = C.c_int32()
+    E = C.c_int64()
+    rp, cl, w = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    _check(L.lv_gen_rmat_device(scale, edge_factor, seed, a, b, c, 1 if weights == "uniform" else 0,
+                                device, C.byref(V), C.byref(E), C.byref(rp), C.byref(cl), C.byref(w)))
+    return DeviceGraph(V.value, E.value, rp.value, cl.value, w.value, device)
+
+
+def print_communities(orig2comm: np.ndarray, num_communities: int, path: str | None = None) -> None:
+    o = _i32(orig2comm)
+    _check(lib().lv_print_communities(path.encode() if path else None, _ptr(o, C.c_int32), len(o),
+                                      num_communities))
+
+
+class Louvain:
+    """One engine handle: a graph resident on one GPU plus its Louvain state."""
+
+    def __init__(self, graph: Graph | None = None, *, device: int = 0, max_sweeps: int = 0,
+                 profile: bool = False, device_csr: tuple | None = None):
+        L = lib()
+        opts = _Opts()
+        L.lv_default_opts(C.byref(opts))
+        opts.device = device
+        opts.max_sweeps = max_sweeps
+        opts.profile = 1 if profile else 0
+        h = C.c_void_p()
+        if device_csr is not None:
+            rp, cl, w, V, E = device_csr
+            _check(L.lv_create_device(C.c_void_p(rp), C.c_void_p(cl), C.c_void_p(w), V, E,
+                                      C.byref(opts), C.byref(h)))
+            self.V0 = V
+        else:
+            g = graph
+            self._keep = g
+            _check(L.lv_create(_ptr(g.rowptr, C.c_int32), _ptr(g.col, C.c_int32),
+                               _ptr(g.w, C.c_float), g.V, g.E, C.byref(opts), C.byref(h)))
+            self.V0 = g.V
+        self._h = h
+
+    # -- lifecycle --
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            lib().lv_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, code: int) -> None:
+        _check(code, self._h)
+
+    def reset(self) -> None:
+        self._c(lib().lv_reset(self._h))
+
+    # -- reference operators --
+    def optimise_modularity(self, min_gain: float) -> bool:
+        ch = C.c_int32()
+        self._c(lib().lv_optimise_level(self._h, min_gain, C.byref(ch)))
+        return bool(ch.value)
+
+    def aggregate_communities(self) -> None:
+        self._c(lib().lv_aggregate(self._h))
+
+    def calculate_modularity(self) -> float:
+        q = C.c_double()
+        self._c(lib().lv_modularity(self._h, C.byref(q)))
+        return q.value
+
+    def run(self, min_gain: float) -> float:
+        q = C.c_double()
+        self._c(lib().lv_run(self._h, min_gain, C.byref(q)))
+        return q.value
+
+    def sweep(self) -> int:
+        m = C.c_int64()
+        self._c(lib().lv_sweep(self._h, C.byref(m)))
+        return m.value
+
+    # -- state access --
+    def level_info(self):
+        V, E, lvl = C.c_int32(), C.c_int64(), C.c_int32()
+        self._c(lib().lv_get_level_info(self._h, C.byref(V), C.byref(E), C.byref(lvl)))
+        return V.value, E.value, lvl.value
+
+    def original_to_community(self):
+        out = np.empty(self.V0, np.int32)
+        nc = C.c_int32()
+        self._c(lib().lv_get_original_to_community(self._h, _ptr(out, C.c_int32), C.byref(nc)))
+        return out, nc.value
+
+    def communities(self) -> np.ndarray:
+        V, _, _ = self.level_info()
+        out = np.empty(V, np.int32)
+        self._c(lib().lv_get_communities(self._h, _ptr(out, C.c_int32)))
+        return out
+
+    def set_communities(self, comm) -> None:
+        c = _i32(comm)
+        self._c(lib().lv_set_communities(self._h, _ptr(c, C.c_int32)))
+
+    def csr(self):
+        """(rowptr int32, col int32, wfix int64) of the current level."""
+        V, E, _ = self.level_info()
+        rp = np.empty(V + 1, np.int32)
+        cl = np.empty(E, np.int32)
+        wf = np.empty(E, np.int64)
+        self._c(lib().lv_get_csr(self._h, _ptr(rp, C.c_int32), _ptr(cl, C.c_int32), _ptr(wf, C.c_int64)))
+        return rp, cl, wf
+
+    def scale(self):
+        s, t, ex = C.c_int32(), C.c_uint64(), C.c_int32()
+        self._c(lib().lv_get_scale(self._h, C.byref(s), C.byref(t), C.byref(ex)))
+        return s.value, t.value, bool(ex.value)
+
+    def stats(self) -> dict:
+        st = _Stats()
+        self._c(lib().lv_get_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in _Stats._fields_}
+
+    def class_stats(self) -> dict:
+        st = _ClassStats()
+        self._c(lib().lv_get_class_stats(self._h, C.byref(st)))
+        return {k: list(getattr(st, k)) for k, _ in _ClassStats._fields_}
+
+    def clear_stats(self) -> None:
+        self._c(lib().lv_clear_stats(self._h))

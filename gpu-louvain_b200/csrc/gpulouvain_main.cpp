@@ -1,0 +1,89 @@
+// gpulouvain_main.cpp -- the `gpulouvain -f file.mtx -g min-gain [-v]` CLI.
+//
+// Same flags and stdout as the reference's main (gpulouvain.cu:6-46,
+// utils.cu:161-186): line 1 the final modularity ("%f"), line 2
+// "algorithmTime totalTime" in milliseconds, then with -v the map of
+// printOriginalToCommunity (modularity_optimisation.cu:403-418).  Timing
+// scopes follow the reference: totalTime adds the device set-up (allocation,
+// host->device copy, M) to the algorithm time (level loop + final modularity);
+// reading the file is not timed.
+#include <getopt.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+
+#include "../../include/louvain_b200.h"
+
+static void usage() {
+    std::printf("Usage: ./gpulouvain -f mtx-matrix-file -g min-gain [-v]\n");
+    std::exit(1);
+}
+
+int main(int argc, char *argv[]) {
+    const char *file = nullptr;
+    float min_gain = 0;
+    bool have_f = false, have_g = false, verbose = false;
+    int device = 0;
+    int opt;
+    while ((opt = getopt(argc, argv, "f:g:vd:")) != -1) {
+        switch (opt) {
+        case 'g': have_g = true; min_gain = std::strtof(optarg, nullptr); break;
+        case 'v': verbose = true; break;
+        case 'f': have_f = true; file = optarg; break;
+        case 'd': device = std::atoi(optarg); break;
+        default: usage();
+        }
+    }
+    if (!have_f || !have_g) usage();
+
+    int32_t V = 0;
+    int64_t E = 0;
+    int32_t *rowptr = nullptr, *col = nullptr;
+    float *w = nullptr;
+    int rc = lv_read_mtx(file, &V, &E, &rowptr, &col, &w, nullptr);
+    if (rc != LV_OK) {
+        std::fprintf(stderr, "gpulouvain: cannot read %s: %s\n", file, lv_status_string(rc));
+        return EXIT_FAILURE;
+    }
+    lv_opts opts;
+    lv_default_opts(&opts);
+    opts.device = device;
+    using clk = std::chrono::steady_clock;
+    lv_handle *h = nullptr;
+    auto t0 = clk::now();
+    rc = lv_create(rowptr, col, w, V, E, &opts, &h);
+    auto t1 = clk::now();
+    if (rc != LV_OK) {
+        std::fprintf(stderr, "gpulouvain: %s\n", lv_status_string(rc));
+        return EXIT_FAILURE;
+    }
+    double q = 0;
+    auto t2 = clk::now();
+    rc = lv_run(h, min_gain, &q);
+    auto t3 = clk::now();
+    if (rc != LV_OK) {
+        std::fprintf(stderr, "gpulouvain: %s: %s\n", lv_status_string(rc), lv_last_error(h));
+        lv_destroy(h);
+        return EXIT_FAILURE;
+    }
+    const double memory_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    const double algo_ms = std::chrono::duration<double, std::milli>(t3 - t2).count();
+    std::printf("%f\n", q);
+    std::printf("%f %f\n", algo_ms, algo_ms + memory_ms);
+    if (verbose) {
+        int32_t *o2c = (int32_t *)std::malloc(sizeof(int32_t) * (size_t)(V > 0 ? V : 1));
+        int32_t nc = 0;
+        rc = lv_get_original_to_community(h, o2c, &nc);
+        if (rc == LV_OK) {
+            std::fflush(stdout);
+            rc = lv_print_communities(nullptr, o2c, V, nc);
+        }
+        std::free(o2c);
+    }
+    lv_destroy(h);
+    lv_free_host(rowptr);
+    lv_free_host(col);
+    lv_free_host(w);
+    return rc == LV_OK ? 0 : EXIT_FAILURE;
+}

@@ -1,0 +1,461 @@
+// lv_agg.cu -- community aggregation kernels.
+//
+// Replaces fillArrays / orderVertices / mergeCommunity{Shared,Global} /
+// compressEdges / updateOriginalToCommunity of community_aggregation.cu
+// (:47-74, :76-228).  The result is the same graph as the reference's
+// aggregateCommunities (:248-347): non-empty communities are renumbered in
+// ascending old id, each new vertex's row holds one entry per neighbouring
+// new community with the summed weight (intra-community weight becomes a
+// self-loop counting both directions), and the new vertex weight equals
+// Sigma_tot.  Sums are exact uint64, so the rows are identical whatever the
+// order of the atomic additions; only the order of entries inside a row is
+// unspecified (it is in the reference too).
+//
+// Pipeline (all on the device, three small host reads per level):
+//   flag/newid scan -> lab[v] = newid[C(v)] -> members grouped by community
+//   -> member-order prefix P of degrees -> permute every row into the
+//   community-grouped "virtual edge" array (key = lab[neighbour], weight)
+//   -> per-community hash merge written back in place -> scan of the
+//   distinct counts -> compaction into the next level's CSR.
+#include "lv_internal.h"
+
+namespace lv {
+
+namespace {
+
+inline unsigned grid_for(int64_t n, int64_t cap = 148 * 16) {
+    int64_t b = (n + 255) / 256;
+    if (b < 1) b = 1;
+    return (unsigned)(b < cap ? b : cap);
+}
+inline unsigned nblocks(int64_t items, int per_block) {
+    return (unsigned)((items + per_block - 1) / per_block);
+}
+
+__global__ void flag_kernel(const int32_t *__restrict__ size, int32_t V, int32_t *flag) {
+    for (int32_t c = blockIdx.x * 256 + threadIdx.x; c < V; c += gridDim.x * 256)
+        flag[c] = size[c] > 0 ? 1 : 0;
+}
+
+__global__ void label_kernel(const int32_t *__restrict__ comm, const int32_t *__restrict__ newid,
+                             int32_t V, int32_t *lab) {
+    for (int32_t v = blockIdx.x * 256 + threadIdx.x; v < V; v += gridDim.x * 256)
+        lab[v] = newid[comm[v]];
+}
+
+__global__ void members_kernel(const int32_t *__restrict__ comm, const int32_t *__restrict__ mstart,
+                               const int32_t *__restrict__ rowptr, int32_t V, int32_t *cursor,
+                               int32_t *members, int32_t *mslot, int32_t *degm) {
+    for (int32_t v = blockIdx.x * 256 + threadIdx.x; v < V; v += gridDim.x * 256) {
+        const int32_t c = comm[v];
+        const int32_t m = mstart[c] + atomicAdd(cursor + c, 1);
+        members[m] = v;
+        mslot[v] = m;
+        degm[m] = rowptr[v + 1] - rowptr[v];
+    }
+}
+
+// Permute vertex rows into community-grouped order.
+template <int G, typename WT>
+__global__ void __launch_bounds__(256) permute_group_kernel(GraphView<WT> g,
+                                                            const int32_t *__restrict__ lab,
+                                                            const int32_t *__restrict__ mslot,
+                                                            const int32_t *__restrict__ P,
+                                                            const int32_t *__restrict__ list,
+                                                            int32_t n, int32_t *vkey, u64 *vw) {
+    const int grp = threadIdx.x / G, lane = threadIdx.x % G;
+    const int32_t idx = blockIdx.x * (256 / G) + grp;
+    if (idx >= n) return;
+    const int32_t v = list[idx];
+    const int32_t r0 = g.rowptr[v], r1 = g.rowptr[v + 1];
+    const int32_t dst = P[mslot[v]] - r0;
+    for (int32_t e = r0 + lane; e < r1; e += G) {
+        vkey[dst + e] = lab[__ldg(g.col + e)];
+        vw[dst + e] = wfix(g.w, e, g.scale);
+    }
+}
+
+template <int T, typename WT>
+__global__ void __launch_bounds__(T) permute_cta_kernel(GraphView<WT> g,
+                                                        const int32_t *__restrict__ lab,
+                                                        const int32_t *__restrict__ mslot,
+                                                        const int32_t *__restrict__ P,
+                                                        const int32_t *__restrict__ list,
+                                                        int32_t n, int32_t *vkey, u64 *vw) {
+    for (int32_t idx = blockIdx.x; idx < n; idx += gridDim.x) {
+        const int32_t v = list[idx];
+        const int32_t r0 = g.rowptr[v], r1 = g.rowptr[v + 1];
+        const int32_t dst = P[mslot[v]] - r0;
+        for (int32_t e = r0 + threadIdx.x; e < r1; e += T) {
+            vkey[dst + e] = lab[__ldg(g.col + e)];
+            vw[dst + e] = wfix(g.w, e, g.scale);
+        }
+    }
+}
+
+// Merge classes of communities by degree bound (sum of member degrees).
+enum AggClass { AC1 = 0, AC2, AC3, AC4, AC5, NAC };
+__device__ __forceinline__ int agg_class(int32_t d) {
+    if (d <= 0) return -1;
+    if (d <= 32) return AC1;
+    if (d <= 128) return AC2;
+    if (d <= 1024) return AC3;
+    if (d <= 4096) return AC4;
+    return AC5;
+}
+
+__global__ void __launch_bounds__(256) agg_class_count_kernel(const int32_t *__restrict__ size,
+                                                              const int32_t *__restrict__ mstart,
+                                                              const int32_t *__restrict__ P,
+                                                              int32_t V, int32_t *counts) {
+    __shared__ int32_t c[NAC];
+    if (threadIdx.x < NAC) c[threadIdx.x] = 0;
+    __syncthreads();
+    for (int32_t x = blockIdx.x * 256 + threadIdx.x; x < V; x += gridDim.x * 256) {
+        if (size[x] <= 0) continue;
+        const int cls = agg_class(P[mstart[x + 1]] - P[mstart[x]]);
+        if (cls >= 0) atomicAdd(c + cls, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < NAC && c[threadIdx.x]) atomicAdd(counts + threadIdx.x, c[threadIdx.x]);
+}
+
+struct AggOffsets {
+    int32_t off[NAC];
+};
+
+__global__ void __launch_bounds__(256) agg_class_scatter_kernel(
+    const int32_t *__restrict__ size, const int32_t *__restrict__ mstart,
+    const int32_t *__restrict__ P, int32_t V, AggOffsets offs, int32_t *cursors, int32_t *clist) {
+    const int lane = threadIdx.x & 31;
+    for (int32_t base = blockIdx.x * 256; base < V; base += gridDim.x * 256) {
+        const int32_t x = base + threadIdx.x;
+        int cls = -1;
+        if (x < V && size[x] > 0) cls = agg_class(P[mstart[x + 1]] - P[mstart[x]]);
+        const unsigned peers = __match_any_sync(FULL, cls);
+        const int leader = __ffs(peers) - 1;
+        int32_t pos = 0;
+        if (lane == leader && cls >= 0) pos = atomicAdd(cursors + cls, __popc(peers));
+        pos = __shfl_sync(FULL, pos, leader);
+        if (cls >= 0) clist[offs.off[cls] + pos + __popc(peers & ((1u << lane) - 1u))] = x;
+    }
+}
+
+// New vertex weights and the rows of communities without edges.
+__global__ void new_vertex_kernel(const int32_t *__restrict__ size,
+                                  const int32_t *__restrict__ newid,
+                                  const int32_t *__restrict__ mstart,
+                                  const int32_t *__restrict__ P, const u64 *__restrict__ S,
+                                  int32_t V, u64 *knew, int32_t *newdeg, int32_t *epos_new) {
+    for (int32_t c = blockIdx.x * 256 + threadIdx.x; c < V; c += gridDim.x * 256) {
+        if (size[c] <= 0) continue;
+        const int32_t nid = newid[c];
+        knew[nid] = S[c];
+        const int32_t a = P[mstart[c]], b = P[mstart[c + 1]];
+        if (a == b) {
+            newdeg[nid] = 0;
+            epos_new[nid] = a;
+        }
+    }
+}
+
+template <int G, int CAP>
+__global__ void __launch_bounds__(256) merge_group_kernel(const int32_t *__restrict__ clist,
+                                                          int32_t n, const int32_t *__restrict__ mstart,
+                                                          const int32_t *__restrict__ P,
+                                                          const int32_t *__restrict__ newid,
+                                                          int32_t *vkey, u64 *vw, int32_t *newdeg,
+                                                          int32_t *epos_new, int *err) {
+    constexpr int GPB = 256 / G;
+    constexpr int LG = (CAP == 64) ? 6 : (CAP == 128) ? 7 : 8;
+    static_assert((1 << LG) == CAP, "CAP");
+    __shared__ u64 svals[GPB * CAP];
+    __shared__ int32_t skeys[GPB * CAP];
+    const int grp = threadIdx.x / G, lane = threadIdx.x % G;
+    const int32_t idx = blockIdx.x * GPB + grp;
+    int32_t *keys = skeys + grp * CAP;
+    u64 *vals = svals + grp * CAP;
+#pragma unroll
+    for (int s = lane; s < CAP; s += G) { keys[s] = -1; vals[s] = 0; }
+    __syncwarp();
+    const bool active = idx < n;
+    int32_t c = 0, a = 0, b = 0;
+    if (active) {
+        c = clist[idx];
+        a = P[mstart[c]];
+        b = P[mstart[c + 1]];
+        for (int32_t i = a + lane; i < b; i += G) table_insert(keys, vals, LG, vkey[i], vw[i], err);
+    }
+    __syncwarp();
+    // write the distinct entries back at the start of the range, in slot order
+    const int wl = threadIdx.x & 31;
+    const unsigned gmask = (G == 32) ? FULL : (((1u << G) - 1u) << (wl & ~(G - 1)));
+    int32_t cnt = 0;
+#pragma unroll
+    for (int s0 = 0; s0 < CAP; s0 += G) {
+        const int s = s0 + lane;
+        const bool occ = active && keys[s] >= 0;
+        const unsigned bal = __ballot_sync(FULL, occ) & gmask;
+        if (occ) {
+            const int32_t pos = a + cnt + __popc(bal & ((1u << wl) - 1u));
+            vkey[pos] = keys[s];
+            vw[pos] = vals[s];
+        }
+        cnt += __popc(bal);
+    }
+    if (active && lane == 0) {
+        const int32_t nid = newid[c];
+        newdeg[nid] = cnt;
+        epos_new[nid] = a;
+    }
+}
+
+template <int T, int CAPMAX>
+__global__ void __launch_bounds__(T) merge_cta_kernel(const int32_t *__restrict__ clist, int32_t n,
+                                                      const int32_t *__restrict__ mstart,
+                                                      const int32_t *__restrict__ P,
+                                                      const int32_t *__restrict__ newid,
+                                                      int32_t *vkey, u64 *vw, int32_t *newdeg,
+                                                      int32_t *epos_new, int *err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    u64 *vals = reinterpret_cast<u64 *>(smem_raw);
+    int32_t *keys = reinterpret_cast<int32_t *>(vals + CAPMAX);
+    __shared__ int32_t cnt;
+    for (int s = threadIdx.x; s < CAPMAX; s += T) { keys[s] = -1; vals[s] = 0; }
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    for (int32_t idx = blockIdx.x; idx < n; idx += gridDim.x) {
+        const int32_t c = clist[idx];
+        const int32_t a = P[mstart[c]], b = P[mstart[c + 1]];
+        int lg = ceil_log2_i(2 * (int64_t)(b - a));
+        lg = lg < 3 ? 3 : lg;
+        const int cap = 1 << lg;
+        for (int32_t i = a + threadIdx.x; i < b; i += T) table_insert(keys, vals, lg, vkey[i], vw[i], err);
+        __syncthreads();
+        for (int s = threadIdx.x; s < cap; s += T) {
+            const int32_t key = keys[s];
+            if (key >= 0) {
+                const int32_t pos = a + atomicAdd(&cnt, 1);
+                vkey[pos] = key;
+                vw[pos] = vals[s];
+                keys[s] = -1;
+                vals[s] = 0;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int32_t nid = newid[c];
+            newdeg[nid] = cnt;
+            epos_new[nid] = a;
+            cnt = 0;
+        }
+        __syncthreads();
+    }
+}
+
+// Global-table merge for communities whose degree bound exceeds 4096.
+__global__ void __launch_bounds__(256) mergeg_insert_kernel(HubGlobal hg,
+                                                            const int32_t *__restrict__ mstart,
+                                                            const int32_t *__restrict__ P,
+                                                            const int32_t *__restrict__ vkey,
+                                                            const u64 *__restrict__ vw, int *err) {
+    const int32_t h = hg.echunk_hub[blockIdx.x];
+    const int32_t c = hg.hubs[h];
+    const int32_t b = P[mstart[c + 1]];
+    const int32_t i0 = P[mstart[c]] + hg.echunk_e0[blockIdx.x];
+    const int32_t i1 = min(i0 + HG_EDGE_CHUNK, b);
+    int32_t *keys = hg.keys + hg.tbl_off[h];
+    u64 *vals = hg.vals + hg.tbl_off[h];
+    const int lg = hg.tbl_lg[h];
+    for (int32_t i = i0 + threadIdx.x; i < i1; i += 256) table_insert(keys, vals, lg, vkey[i], vw[i], err);
+}
+
+__global__ void __launch_bounds__(256) mergeg_emit_kernel(HubGlobal hg,
+                                                          const int32_t *__restrict__ mstart,
+                                                          const int32_t *__restrict__ P,
+                                                          const int32_t *__restrict__ newid,
+                                                          int32_t *vkey, u64 *vw, int32_t *rowcnt) {
+    const int32_t bidx = blockIdx.x;
+    const int32_t h = hg.schunk_hub[bidx];
+    const int32_t c = hg.hubs[h];
+    const int32_t a = P[mstart[c]];
+    const int32_t nid = newid[c];
+    int32_t *keys = hg.keys + hg.tbl_off[h];
+    u64 *vals = hg.vals + hg.tbl_off[h];
+    const int32_t cap = 1 << hg.tbl_lg[h];
+    const int32_t s0 = hg.schunk_s0[bidx];
+    const int32_t s1 = min(s0 + HG_SLOT_CHUNK, cap);
+    for (int32_t s = s0 + threadIdx.x; s < s1; s += 256) {
+        const int32_t key = keys[s];
+        if (key >= 0) {
+            const int32_t pos = a + atomicAdd(rowcnt + nid, 1);
+            vkey[pos] = key;
+            vw[pos] = vals[s];
+            keys[s] = -1;
+            vals[s] = 0;
+        }
+    }
+}
+
+__global__ void mergeg_finish_kernel(HubGlobal hg, const int32_t *__restrict__ mstart,
+                                     const int32_t *__restrict__ P, const int32_t *__restrict__ newid,
+                                     const int32_t *__restrict__ rowcnt, int32_t *newdeg,
+                                     int32_t *epos_new) {
+    for (int32_t h = blockIdx.x * 256 + threadIdx.x; h < hg.nhubs; h += gridDim.x * 256) {
+        const int32_t c = hg.hubs[h];
+        const int32_t nid = newid[c];
+        newdeg[nid] = rowcnt[nid];
+        epos_new[nid] = P[mstart[c]];
+    }
+}
+
+__global__ void zero_rowcnt_kernel(HubGlobal hg, const int32_t *__restrict__ newid, int32_t *rowcnt) {
+    for (int32_t h = blockIdx.x * 256 + threadIdx.x; h < hg.nhubs; h += gridDim.x * 256)
+        rowcnt[newid[hg.hubs[h]]] = 0;
+}
+
+// Compaction: each thread copies 8 consecutive output entries; the row of
+// the first is found by binary search over the new offsets.
+__global__ void __launch_bounds__(256) compact_kernel(const int32_t *__restrict__ rowptr_new,
+                                                      int32_t Vn, int64_t En,
+                                                      const int32_t *__restrict__ epos_new,
+                                                      const int32_t *__restrict__ vkey,
+                                                      const u64 *__restrict__ vw, int32_t *col_out,
+                                                      u64 *w_out) {
+    const int64_t t = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    int64_t i = t * 8;
+    if (i >= En) return;
+    // largest r with rowptr_new[r] <= i
+    int32_t lo = 0, hi = Vn;
+    while (hi - lo > 1) {
+        const int32_t mid = (lo + hi) >> 1;
+        if ((int64_t)rowptr_new[mid] <= i) lo = mid; else hi = mid;
+    }
+    int32_t r = lo;
+    const int64_t iend = min(i + 8, En);
+    for (; i < iend; ++i) {
+        while ((int64_t)rowptr_new[r + 1] <= i) ++r;
+        const int64_t src = (int64_t)epos_new[r] + (i - rowptr_new[r]);
+        col_out[i] = vkey[src];
+        w_out[i] = vw[src];
+    }
+}
+
+}  // namespace
+
+constexpr int A3_T = 256, A3_CAP = 2048;
+constexpr int A4_T = 512, A4_CAP = 8192;
+static int g_occ_a3 = 4, g_occ_a4 = 2;
+
+void init_agg_attributes() {
+    cudaFuncSetAttribute(merge_cta_kernel<A3_T, A3_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         A3_CAP * 12);
+    cudaFuncSetAttribute(merge_cta_kernel<A4_T, A4_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         A4_CAP * 12);
+    int o3 = 0, o4 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, merge_cta_kernel<A3_T, A3_CAP>, A3_T, A3_CAP * 12);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o4, merge_cta_kernel<A4_T, A4_CAP>, A4_T, A4_CAP * 12);
+    g_occ_a3 = o3 > 0 ? o3 : 1;
+    g_occ_a4 = o4 > 0 ? o4 : 1;
+}
+
+// Steps up to the member prefix and the merge classification.
+//   flag -> newid (scan, total in scalars[0]), lab, mstart (scan of size),
+//   members / mslot / degm, P (scan of degm, total in scalars[1]),
+//   class counts in scalars[2..2+NAC).
+void agg_prepare(const int32_t *rowptr, const int32_t *comm, const int32_t *size, int32_t V,
+                 AggBuffers &ab, int32_t *mslot, int32_t *degm, int32_t *P, cudaStream_t s) {
+    flag_kernel<<<grid_for(V), 256, 0, s>>>(size, V, ab.flag); note_launches(1);
+    scan_exclusive_i32(ab.flag, ab.flag, V, ab.scalars + 0, ab.scan_tmp, s);
+    label_kernel<<<grid_for(V), 256, 0, s>>>(comm, ab.flag, V, ab.lab); note_launches(1);
+    scan_exclusive_i32(size, ab.mstart, V, ab.mstart + V, ab.scan_tmp, s);
+    cudaMemsetAsync(ab.cursor, 0, sizeof(int32_t) * (size_t)V, s);
+    members_kernel<<<grid_for(V), 256, 0, s>>>(comm, ab.mstart, rowptr, V, ab.cursor, ab.members,
+                                                mslot, degm); note_launches(1);
+    scan_exclusive_i32(degm, P, V, P + V, ab.scan_tmp, s);
+    cudaMemsetAsync(ab.scalars + 2, 0, sizeof(int32_t) * NAC, s);
+    agg_class_count_kernel<<<grid_for(V), 256, 0, s>>>(size, ab.mstart, P, V, ab.scalars + 2); note_launches(1);
+}
+
+void agg_classify(const int32_t *size, int32_t V, AggBuffers &ab, const int32_t *P,
+                  const int32_t *offsets, cudaStream_t s) {
+    AggOffsets o;
+    for (int c = 0; c < NAC; ++c) o.off[c] = offsets[c];
+    cudaMemsetAsync(ab.cursor, 0, sizeof(int32_t) * NAC, s);
+    agg_class_scatter_kernel<<<grid_for(V), 256, 0, s>>>(size, ab.mstart, P, V, o, ab.cursor, ab.clist); note_launches(1);
+}
+
+template <typename WT>
+void agg_permute(int cls, const GraphView<WT> &g, const AggBuffers &ab, const int32_t *mslot,
+                 const int32_t *P, const int32_t *list, int32_t n, int32_t *vkey, u64 *vw,
+                 int sms, cudaStream_t s) {
+    if (n <= 0) return;
+    switch (cls) {
+    case CLS_B0: permute_group_kernel<4, WT><<<nblocks(n, 64), 256, 0, s>>>(g, ab.lab, mslot, P, list, n, vkey, vw); note_launches(1); break;
+    case CLS_B1: permute_group_kernel<8, WT><<<nblocks(n, 32), 256, 0, s>>>(g, ab.lab, mslot, P, list, n, vkey, vw); note_launches(1); break;
+    case CLS_B2: permute_group_kernel<16, WT><<<nblocks(n, 16), 256, 0, s>>>(g, ab.lab, mslot, P, list, n, vkey, vw); note_launches(1); break;
+    case CLS_B3:
+    case CLS_B4: permute_group_kernel<32, WT><<<nblocks(n, 8), 256, 0, s>>>(g, ab.lab, mslot, P, list, n, vkey, vw); note_launches(1); break;
+    case CLS_B5: permute_cta_kernel<128, WT><<<(unsigned)imin64(n, sms * 16), 128, 0, s>>>(g, ab.lab, mslot, P, list, n, vkey, vw); note_launches(1); break;
+    case CLS_H1: permute_cta_kernel<256, WT><<<(unsigned)imin64(n, sms * 8), 256, 0, s>>>(g, ab.lab, mslot, P, list, n, vkey, vw); note_launches(1); break;
+    default: permute_cta_kernel<512, WT><<<(unsigned)imin64(n, sms * 4), 512, 0, s>>>(g, ab.lab, mslot, P, list, n, vkey, vw); note_launches(1); break;
+    }
+}
+template void agg_permute<float>(int, const GraphView<float> &, const AggBuffers &, const int32_t *,
+                                 const int32_t *, const int32_t *, int32_t, int32_t *, u64 *, int,
+                                 cudaStream_t);
+template void agg_permute<u64>(int, const GraphView<u64> &, const AggBuffers &, const int32_t *,
+                               const int32_t *, const int32_t *, int32_t, int32_t *, u64 *, int,
+                               cudaStream_t);
+
+void agg_new_vertices(const int32_t *size, const u64 *S, int32_t V, const AggBuffers &ab,
+                      const int32_t *P, u64 *knew, cudaStream_t s) {
+    new_vertex_kernel<<<grid_for(V), 256, 0, s>>>(size, ab.flag, ab.mstart, P, S, V, knew,
+                                                   ab.newdeg, ab.epos_new); note_launches(1);
+}
+
+void agg_merge_class(int acls, const AggBuffers &ab, const int32_t *P, const int32_t *list,
+                     int32_t n, int32_t *vkey, u64 *vw, int *err, int sms, cudaStream_t s) {
+    if (n <= 0) return;
+    switch (acls) {
+    case AC1:
+        merge_group_kernel<8, 64><<<nblocks(n, 32), 256, 0, s>>>(list, n, ab.mstart, P, ab.flag, vkey,
+                                                                  vw, ab.newdeg, ab.epos_new, err); note_launches(1);
+        break;
+    case AC2:
+        merge_group_kernel<32, 256><<<nblocks(n, 8), 256, 0, s>>>(list, n, ab.mstart, P, ab.flag, vkey,
+                                                                   vw, ab.newdeg, ab.epos_new, err); note_launches(1);
+        break;
+    case AC3:
+        merge_cta_kernel<A3_T, A3_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a3), A3_T,
+                                         A3_CAP * 12, s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw,
+                                                           ab.newdeg, ab.epos_new, err); note_launches(1);
+        break;
+    case AC4:
+        merge_cta_kernel<A4_T, A4_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a4), A4_T,
+                                         A4_CAP * 12, s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw,
+                                                           ab.newdeg, ab.epos_new, err); note_launches(1);
+        break;
+    default: break;
+    }
+}
+
+void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *P, int32_t *vkey,
+                      u64 *vw, int *err, cudaStream_t s) {
+    if (hg.nhubs <= 0) return;
+    zero_rowcnt_kernel<<<grid_for(hg.nhubs), 256, 0, s>>>(hg, ab.flag, ab.cursor); note_launches(1);
+    mergeg_insert_kernel<<<hg.n_echunks, 256, 0, s>>>(hg, ab.mstart, P, vkey, vw, err); note_launches(1);
+    mergeg_emit_kernel<<<hg.n_schunks, 256, 0, s>>>(hg, ab.mstart, P, ab.flag, vkey, vw, ab.cursor); note_launches(1);
+    mergeg_finish_kernel<<<grid_for(hg.nhubs), 256, 0, s>>>(hg, ab.mstart, P, ab.flag, ab.cursor,
+                                                            ab.newdeg, ab.epos_new); note_launches(1);
+}
+
+void agg_compact(const int32_t *rowptr_new, int32_t Vn, int64_t En, const AggBuffers &ab,
+                 const int32_t *vkey, const u64 *vw, int32_t *col_out, u64 *w_out, cudaStream_t s) {
+    if (En <= 0) return;
+    const int64_t threads = (En + 7) / 8;
+    compact_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(rowptr_new, Vn, En, ab.epos_new,
+                                                                     vkey, vw, col_out, w_out); note_launches(1);
+}
+
+}  // namespace lv

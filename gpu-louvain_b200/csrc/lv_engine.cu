@@ -1,0 +1,977 @@
+// lv_engine.cu -- the engine handle, the level loop and the C ABI.
+//
+// Host orchestration of one Louvain run on one GPU (replaces main()'s level
+// loop, gpulouvain.cu:30-37, optimiseModularity,
+// modularity_optimisation.cu:284-363, and aggregateCommunities,
+// community_aggregation.cu:248-347).  All state lives in device memory; the
+// host reads back one small totals record per sweep (the sweep's modularity
+// parts, its move count and the device error word) and a few counts per
+// level.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/louvain_b200.h"
+#include "lv_internal.h"
+
+namespace lv {
+void init_agg_attributes();
+void agg_prepare(const int32_t *rowptr, const int32_t *comm, const int32_t *size, int32_t V,
+                 AggBuffers &ab, int32_t *mslot, int32_t *degm, int32_t *P, cudaStream_t s);
+void agg_classify(const int32_t *size, int32_t V, AggBuffers &ab, const int32_t *P,
+                  const int32_t *offsets, cudaStream_t s);
+template <typename WT>
+void agg_permute(int cls, const GraphView<WT> &g, const AggBuffers &ab, const int32_t *mslot,
+                 const int32_t *P, const int32_t *list, int32_t n, int32_t *vkey, u64 *vw, int sms,
+                 cudaStream_t s);
+void agg_new_vertices(const int32_t *size, const u64 *S, int32_t V, const AggBuffers &ab,
+                      const int32_t *P, u64 *knew, cudaStream_t s);
+void agg_merge_class(int acls, const AggBuffers &ab, const int32_t *P, const int32_t *list,
+                     int32_t n, int32_t *vkey, u64 *vw, int *err, int sms, cudaStream_t s);
+void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *P, int32_t *vkey,
+                      u64 *vw, int *err, cudaStream_t s);
+void agg_compact(const int32_t *rowptr_new, int32_t Vn, int64_t En, const AggBuffers &ab,
+                 const int32_t *vkey, const u64 *vw, int32_t *col_out, u64 *w_out, cudaStream_t s);
+void launch_gather_degrees(const int32_t *rowptr, const int32_t *list, int32_t n, int32_t *out,
+                           cudaStream_t s);
+void launch_gather_cdeg(const int32_t *mstart, const int32_t *P, const int32_t *list, int32_t n,
+                        int32_t *out, cudaStream_t s);
+}  // namespace lv
+
+using namespace lv;
+
+namespace {
+
+constexpr int NAC = 5;   // aggregation merge classes (lv_agg.cu)
+// cls_scratch layout: class counts, class cursors, then V0 int32 of scratch.
+constexpr int SCRATCH_OFF = CLASS_COUNT_WORDS + NCLS + 8;
+
+struct Totals {
+    u64 e_own;
+    u64 s2[2];   // hi, lo
+    u64 moves;
+    int err;
+    int pad;
+};
+
+struct Pending {
+    int kind;   // 0..NCLS-1 class, 100 move phase, 101 modularity, 102 aggregate, 103 setup
+    cudaEvent_t a, b;
+    double bytes;
+    int64_t verts, edges;
+};
+
+struct HubLayout {
+    HubGlobal view;
+    void *dev = nullptr;   // packed index arrays
+    size_t dev_bytes = 0;
+    std::vector<int32_t> ids;
+};
+
+}  // namespace
+
+struct lv_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    lv_opts opts{};
+    std::string err;
+    DeviceInfo di;
+
+    int32_t V0 = 0;
+    int64_t E0 = 0;
+    bool owns_input = false;
+    int32_t *in_rowptr = nullptr, *in_col = nullptr;
+    float *in_w = nullptr;
+    int scale = 0;
+    double scale_d = 1.0;
+    u64 T = 0;
+    int exact = 1;
+
+    int level = 0;
+    int32_t V = 0;
+    int64_t E = 0;
+    int32_t *cur_rowptr = nullptr, *cur_col = nullptr;
+    u64 *cur_w = nullptr;   // nullptr at level 0 (float input weights)
+
+    int32_t *lvl_rowptr[2] = {nullptr, nullptr};
+    int32_t *lvl_col[2] = {nullptr, nullptr};
+    u64 *lvl_w[2] = {nullptr, nullptr};
+    int cur_buf = -1;
+
+    int32_t *comm = nullptr, *newc = nullptr, *size = nullptr, *orig2comm = nullptr;
+    u64 *k = nullptr, *S = nullptr;
+    int32_t *list = nullptr;
+    int32_t *cls_scratch = nullptr;   // class counts, cursors, then V0 entries of scratch
+    int32_t cls_off[NCLS + 1] = {0};
+    int64_t cls_edges[NCLS] = {0};
+
+    HubLayout hub_move, hub_agg;
+    int32_t *tbl_keys = nullptr;
+    u64 *tbl_vals = nullptr;
+    size_t tbl_slots = 0;
+
+    bool agg_ready = false;
+    AggBuffers ab{};
+    int32_t *mslot = nullptr, *degm = nullptr, *P = nullptr;
+    int32_t *vkey = nullptr;
+    u64 *vw = nullptr;
+
+    Totals *tot_d = nullptr;
+    Totals *tot_h = nullptr;
+    int32_t *small_h = nullptr;   // pinned scratch for counts
+
+    lv_stats st{};
+    lv_class_stats cst{};
+    long long launch_base = 0;
+    std::vector<cudaEvent_t> ev_free;
+    std::vector<Pending> pend;
+};
+
+namespace {
+
+int fail(lv_handle *h, int code, const std::string &msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+#define LV_CUDA(h, call)                                                                   \
+    do {                                                                                   \
+        cudaError_t e__ = (call);                                                          \
+        if (e__ != cudaSuccess)                                                            \
+            return fail((h), e__ == cudaErrorMemoryAllocation ? LV_ERR_NOMEM : LV_ERR_CUDA, \
+                        std::string(#call) + ": " + cudaGetErrorString(e__));             \
+    } while (0)
+
+#define LV_TRY(expr)            \
+    do {                        \
+        int rc__ = (expr);      \
+        if (rc__) return rc__;  \
+    } while (0)
+
+template <typename T>
+int dalloc(lv_handle *h, T **p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(h, LV_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    return LV_OK;
+}
+
+template <typename T>
+void dfree(T *&p) {
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+cudaEvent_t ev_get(lv_handle *h) {
+    if (!h->ev_free.empty()) {
+        cudaEvent_t e = h->ev_free.back();
+        h->ev_free.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Begin / end a timed region on the handle's stream.
+struct Timer {
+    lv_handle *h;
+    int kind;
+    cudaEvent_t a = nullptr;
+    double bytes = 0;
+    int64_t verts = 0, edges = 0;
+    Timer(lv_handle *hh, int k) : h(hh), kind(k) {
+        a = ev_get(h);
+        cudaEventRecord(a, h->stream);
+    }
+    void stop() {
+        cudaEvent_t b = ev_get(h);
+        cudaEventRecord(b, h->stream);
+        h->pend.push_back(Pending{kind, a, b, bytes, verts, edges});
+    }
+};
+
+void resolve_events(lv_handle *h) {
+    for (const Pending &p : h->pend) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        if (p.kind < NCLS) {
+            h->cst.launches[p.kind] += 1;
+            h->cst.ms[p.kind] += ms;
+            h->cst.bytes[p.kind] += p.bytes;
+            h->cst.vertices[p.kind] += p.verts;
+            h->cst.edges[p.kind] += p.edges;
+        } else if (p.kind == 100) {
+            h->st.move_ms += ms;
+        } else if (p.kind == 101) {
+            h->st.modularity_ms += ms;
+        } else if (p.kind == 102) {
+            h->st.aggregate_ms += ms;
+        } else if (p.kind == 103) {
+            h->st.setup_ms += ms;
+        }
+        h->ev_free.push_back(p.a);
+        h->ev_free.push_back(p.b);
+    }
+    h->pend.clear();
+}
+
+int sync(lv_handle *h) {
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return fail(h, LV_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(h, LV_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    resolve_events(h);
+    return LV_OK;
+}
+
+int check_device_error(lv_handle *h, int errword) {
+    if (errword == 0) return LV_OK;
+    std::string m = "device check failed:";
+    if (errword & DEVERR_HASH_FULL) m += " hash table full";
+    if (errword & DEVERR_BAD_STATE) m += " invalid community id";
+    return fail(h, LV_ERR_DEVICE, m);
+}
+
+template <typename WT>
+GraphView<WT> view_of(lv_handle *h);
+template <>
+GraphView<float> view_of<float>(lv_handle *h) {
+    return GraphView<float>{h->cur_rowptr, h->cur_col, h->in_w, h->scale_d};
+}
+template <>
+GraphView<u64> view_of<u64>(lv_handle *h) {
+    return GraphView<u64>{h->cur_rowptr, h->cur_col, h->cur_w, h->scale_d};
+}
+
+StateView state_of(lv_handle *h) {
+    return StateView{h->comm, h->newc, h->size, h->k, h->S, h->T, &h->tot_d->err};
+}
+
+// ---------------------------------------------------------------------------
+// global hash-table layouts (hub vertices in the move phase, very large
+// communities in aggregation)
+// ---------------------------------------------------------------------------
+int ensure_tables(lv_handle *h, size_t slots) {
+    if (slots <= h->tbl_slots) return LV_OK;
+    size_t want = slots + slots / 4;
+    dfree(h->tbl_keys);
+    dfree(h->tbl_vals);
+    h->tbl_slots = 0;
+    LV_TRY(dalloc(h, &h->tbl_keys, want));
+    LV_TRY(dalloc(h, &h->tbl_vals, want));
+    LV_CUDA(h, cudaMemsetAsync(h->tbl_keys, 0xFF, want * sizeof(int32_t), h->stream));
+    LV_CUDA(h, cudaMemsetAsync(h->tbl_vals, 0, want * sizeof(u64), h->stream));
+    h->tbl_slots = want;
+    return LV_OK;
+}
+
+// ids: hub vertices / communities; deg: their degree bound; cap_limit caps
+// the distinct-key count (newV for aggregation, unlimited for moves).
+int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
+                 const std::vector<int32_t> &deg, int64_t cap_limit) {
+    const int32_t n = (int32_t)ids.size();
+    std::vector<int64_t> off(n);
+    std::vector<int32_t> lg(n), ech_hub, ech_e0, sch_hub, sch_s0, hub_s0(n + 1);
+    int64_t total = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        int64_t distinct = deg[i];
+        if (cap_limit > 0 && distinct > cap_limit) distinct = cap_limit;
+        int l = ceil_log2_i(2 * distinct);
+        if (l < 3) l = 3;
+        lg[i] = l;
+        off[i] = total;
+        total += int64_t(1) << l;
+        for (int32_t e0 = 0; e0 < deg[i]; e0 += HG_EDGE_CHUNK) {
+            ech_hub.push_back(i);
+            ech_e0.push_back(e0);
+        }
+        hub_s0[i] = (int32_t)sch_hub.size();
+        for (int64_t s0 = 0; s0 < (int64_t(1) << l); s0 += HG_SLOT_CHUNK) {
+            sch_hub.push_back(i);
+            sch_s0.push_back((int32_t)s0);
+        }
+    }
+    hub_s0[n] = (int32_t)sch_hub.size();
+    LV_TRY(ensure_tables(h, (size_t)total));
+    const size_t ne = ech_hub.size(), ns = sch_hub.size();
+    // packed: ids | lg | ech_hub | ech_e0 | sch_hub | sch_s0 | hub_s0 | res_c | (8-aligned) off | res_g | res_e
+    size_t i32_count = (size_t)n + n + ne + ne + ns + ns + (n + 1) + ns;
+    size_t i32_bytes = ((i32_count * 4 + 15) / 16) * 16;
+    size_t bytes = i32_bytes + (size_t)n * 8 + ns * 16 + ns * 8 + 64;
+    if (bytes > L.dev_bytes) {
+        if (L.dev) cudaFree(L.dev);
+        L.dev = nullptr;
+        L.dev_bytes = 0;
+        if (cudaMalloc(&L.dev, bytes) != cudaSuccess) return fail(h, LV_ERR_NOMEM, "layout alloc");
+        L.dev_bytes = bytes;
+    }
+    std::vector<unsigned char> host(bytes, 0);
+    int32_t *p32 = (int32_t *)host.data();
+    size_t at = 0;
+    auto put = [&](const int32_t *src, size_t cnt) {
+        size_t start = at;
+        if (cnt) std::memcpy(p32 + at, src, cnt * 4);
+        at += cnt;
+        return start;
+    };
+    size_t o_ids = put(ids.data(), n), o_lg = put(lg.data(), n);
+    size_t o_eh = put(ech_hub.data(), ne), o_e0 = put(ech_e0.data(), ne);
+    size_t o_sh = put(sch_hub.data(), ns), o_s0 = put(sch_s0.data(), ns);
+    size_t o_hs = put(hub_s0.data(), n + 1);
+    size_t o_rc = at;
+    at += ns;
+    unsigned char *base8 = host.data() + i32_bytes;
+    if (n) std::memcpy(base8, off.data(), (size_t)n * 8);
+    LV_CUDA(h, cudaMemcpyAsync(L.dev, host.data(), bytes, cudaMemcpyHostToDevice, h->stream));
+    // the host vector must outlive the async copy
+    LV_CUDA(h, cudaStreamSynchronize(h->stream));
+    int32_t *d32 = (int32_t *)L.dev;
+    unsigned char *d8 = (unsigned char *)L.dev + i32_bytes;
+    HubGlobal &v = L.view;
+    v.nhubs = n;
+    v.n_echunks = (int32_t)ne;
+    v.n_schunks = (int32_t)ns;
+    v.hubs = d32 + o_ids;
+    v.tbl_lg = d32 + o_lg;
+    v.echunk_hub = d32 + o_eh;
+    v.echunk_e0 = d32 + o_e0;
+    v.schunk_hub = d32 + o_sh;
+    v.schunk_s0 = d32 + o_s0;
+    v.hub_schunk0 = d32 + o_hs;
+    v.res_c = d32 + o_rc;
+    v.tbl_off = (const int64_t *)d8;
+    v.res_g = (u64 *)(d8 + (size_t)n * 8);
+    v.res_e = (u64 *)(d8 + (size_t)n * 8 + ns * 16);
+    v.keys = h->tbl_keys;
+    v.vals = h->tbl_vals;
+    L.ids = ids;
+    return LV_OK;
+}
+
+// ---------------------------------------------------------------------------
+// level set-up: degree classes, k_i (level 0), singleton state, hub layout
+// ---------------------------------------------------------------------------
+template <typename WT>
+int compute_k(lv_handle *h) {
+    GraphView<WT> g = view_of<WT>(h);
+    LV_CUDA(h, cudaMemsetAsync(h->k, 0, sizeof(u64) * (size_t)h->V, h->stream));
+    for (int c = 0; c < NCLS; ++c)
+        launch_row_reduce<WT>(c, 0, g, h->comm, h->k, nullptr, h->list + h->cls_off[c],
+                              h->cls_off[c + 1] - h->cls_off[c], h->di, h->stream);
+    return LV_OK;
+}
+
+int level_setup(lv_handle *h) {
+    Timer t(h, 103);
+    int32_t *counts = h->cls_scratch, *cursors = h->cls_scratch + CLASS_COUNT_WORDS;
+    launch_class_count(h->cur_rowptr, h->V, counts, h->stream);
+    LV_CUDA(h, cudaMemcpyAsync(h->small_h, counts, sizeof(int32_t) * CLASS_COUNT_WORDS,
+                               cudaMemcpyDeviceToHost, h->stream));
+    LV_TRY(sync(h));
+    h->cls_off[0] = 0;
+    const u64 *esum = reinterpret_cast<const u64 *>(h->small_h + NCLS + (NCLS & 1));
+    for (int c = 0; c < NCLS; ++c) {
+        h->cls_off[c + 1] = h->cls_off[c] + h->small_h[c];
+        h->cls_edges[c] = (int64_t)esum[c];
+    }
+    launch_class_scatter(h->cur_rowptr, h->V, h->cls_off, cursors, h->list, h->stream);
+    if (h->level == 0) {
+        LV_TRY(compute_k<float>(h));
+    }
+    launch_level_init(h->comm, h->newc, h->size, h->k, h->S, h->V, h->stream);
+    // global tables for the hubs of class HG
+    const int32_t nh = h->cls_off[CLS_HG + 1] - h->cls_off[CLS_HG];
+    std::vector<int32_t> ids(nh), deg(nh);
+    if (nh > 0) {
+        int32_t *dd = h->cls_scratch + SCRATCH_OFF;   // room reserved at create: V0 entries
+        launch_gather_degrees(h->cur_rowptr, h->list + h->cls_off[CLS_HG], nh, dd, h->stream);
+        LV_CUDA(h, cudaMemcpyAsync(ids.data(), h->list + h->cls_off[CLS_HG], sizeof(int32_t) * nh,
+                                   cudaMemcpyDeviceToHost, h->stream));
+        LV_CUDA(h, cudaMemcpyAsync(deg.data(), dd, sizeof(int32_t) * nh, cudaMemcpyDeviceToHost,
+                                   h->stream));
+        LV_TRY(sync(h));
+    }
+    LV_TRY(build_layout(h, h->hub_move, ids, deg, 0));
+    t.stop();
+    return LV_OK;
+}
+
+// ---------------------------------------------------------------------------
+// sweep and modularity
+// ---------------------------------------------------------------------------
+template <typename WT>
+void enqueue_sweep(lv_handle *h) {
+    GraphView<WT> g = view_of<WT>(h);
+    StateView st = state_of(h);
+    const double wbytes = sizeof(WT) == 4 ? 4.0 : 8.0;
+    Timer tm(h, 100);
+    int64_t sweep_edges = 0, sweep_verts = 0;
+    for (int b = 0; b < NBUCKETS; ++b) {
+        const int c0 = b, c1 = (b < 6) ? b + 1 : NCLS;
+        const int32_t lo = h->cls_off[c0], hi = h->cls_off[c1];
+        if (hi == lo) continue;
+        for (int c = c0; c < c1; ++c) {
+            const int32_t n = h->cls_off[c + 1] - h->cls_off[c];
+            if (n == 0) continue;
+            if (h->opts.profile) {
+                Timer tc(h, c);
+                tc.verts = n;
+                tc.edges = h->cls_edges[c];
+                tc.bytes = (8.0 + wbytes) * (double)h->cls_edges[c] + 20.0 * (double)n;
+                launch_move_class<WT>(c, g, st, h->list + h->cls_off[c], n, h->hub_move.view, h->di,
+                                      h->stream);
+                tc.stop();
+            } else {
+                launch_move_class<WT>(c, g, st, h->list + h->cls_off[c], n, h->hub_move.view, h->di,
+                                      h->stream);
+            }
+        }
+        launch_commit(st, h->list + lo, hi - lo, &h->tot_d->moves, h->stream);
+        sweep_verts += hi - lo;
+    }
+    sweep_edges = h->E;
+    tm.bytes = (8.0 + wbytes) * (double)sweep_edges + 20.0 * (double)sweep_verts;
+    tm.stop();
+    h->st.move_bytes += tm.bytes;
+}
+
+template <typename WT>
+void enqueue_modularity(lv_handle *h) {
+    GraphView<WT> g = view_of<WT>(h);
+    Timer tm(h, 101);
+    for (int c = 0; c < NCLS; ++c)
+        launch_row_reduce<WT>(c, 1, g, h->comm, nullptr, &h->tot_d->e_own, h->list + h->cls_off[c],
+                              h->cls_off[c + 1] - h->cls_off[c], h->di, h->stream);
+    launch_s2(h->S, h->V, h->tot_d->s2, h->stream);
+    tm.stop();
+}
+
+double q_from_totals(u64 T, const Totals &t) {
+    // Same FP64 formula as the oracle: e_own/T - sum(S^2)/T^2, i.e.
+    // toOwn/(2M) - sum(S^2)/(4M^2) of calculateModularity.
+    const u128 s2 = ((u128)t.s2[0] << 64) | (u128)t.s2[1];
+    const double td = (double)T;
+    const double a = (double)t.e_own / td;
+    const double b = (double)s2 / (td * td);
+    return a - b;
+}
+
+int reset_totals(lv_handle *h) {
+    LV_CUDA(h, cudaMemsetAsync(h->tot_d, 0, offsetof(Totals, err), h->stream));
+    return LV_OK;
+}
+
+int read_totals(lv_handle *h) {
+    LV_CUDA(h, cudaMemcpyAsync(h->tot_h, h->tot_d, sizeof(Totals), cudaMemcpyDeviceToHost, h->stream));
+    LV_TRY(sync(h));
+    return check_device_error(h, h->tot_h->err);
+}
+
+int modularity(lv_handle *h, double *q) {
+    LV_TRY(reset_totals(h));
+    if (h->cur_w) enqueue_modularity<u64>(h); else enqueue_modularity<float>(h);
+    LV_TRY(read_totals(h));
+    *q = q_from_totals(h->T, *h->tot_h);
+    return LV_OK;
+}
+
+// One sweep followed by the modularity of the resulting state.
+int sweep_and_q(lv_handle *h, int64_t *moves, double *q) {
+    LV_TRY(reset_totals(h));
+    if (h->cur_w) {
+        enqueue_sweep<u64>(h);
+        enqueue_modularity<u64>(h);
+    } else {
+        enqueue_sweep<float>(h);
+        enqueue_modularity<float>(h);
+    }
+    LV_TRY(read_totals(h));
+    *moves = (int64_t)h->tot_h->moves;
+    if (q) *q = q_from_totals(h->T, *h->tot_h);
+    h->st.sweeps += 1;
+    h->st.edge_sweeps += h->E;
+    h->st.moves += *moves;
+    return LV_OK;
+}
+
+int optimise_level(lv_handle *h, float min_gain, int32_t *changed) {
+    double q_before = 0, q_after = 0;
+    LV_TRY(modularity(h, &q_before));
+    double gain = (double)min_gain;
+    int ch = 0, sweeps = 0;
+    while (gain >= (double)min_gain) {
+        if (h->opts.max_sweeps > 0 && sweeps >= h->opts.max_sweeps) break;
+        int64_t moves = 0;
+        LV_TRY(sweep_and_q(h, &moves, &q_after));
+        sweeps++;
+        gain = q_after - q_before;
+        if (gain > 0) ch = 1;
+        q_before = q_after;
+        if (moves == 0) break;
+    }
+    launch_compose_map(h->orig2comm, h->comm, h->V0, h->stream);
+    h->st.levels += 1;
+    h->st.final_vertices = h->V;
+    if (changed) *changed = ch;
+    return sync(h);
+}
+
+// ---------------------------------------------------------------------------
+// aggregation
+// ---------------------------------------------------------------------------
+int ensure_agg(lv_handle *h) {
+    if (h->agg_ready) return LV_OK;
+    const size_t V = (size_t)h->V0, E = (size_t)(h->E0 > 0 ? h->E0 : 1);
+    AggBuffers &a = h->ab;
+    LV_TRY(dalloc(h, &a.flag, V + 1));
+    LV_TRY(dalloc(h, &a.cdeg, V + 1));
+    LV_TRY(dalloc(h, &a.mstart, V + 1));
+    LV_TRY(dalloc(h, &a.cursor, V + 16));
+    LV_TRY(dalloc(h, &a.members, V + 1));
+    LV_TRY(dalloc(h, &a.lab, V + 1));
+    LV_TRY(dalloc(h, &a.clist, V + 1));
+    LV_TRY(dalloc(h, &a.newdeg, V + 1));
+    LV_TRY(dalloc(h, &a.epos_new, V + 1));
+    LV_TRY(dalloc(h, &a.scan_tmp, (size_t)scan_tmp_elems((int64_t)V + 1) + 16));
+    LV_TRY(dalloc(h, &a.scalars, 64));
+    LV_TRY(dalloc(h, &h->mslot, V + 1));
+    LV_TRY(dalloc(h, &h->degm, V + 1));
+    LV_TRY(dalloc(h, &h->P, V + 1));
+    LV_TRY(dalloc(h, &h->vkey, E));
+    LV_TRY(dalloc(h, &h->vw, E));
+    for (int b = 0; b < 2; ++b) {
+        LV_TRY(dalloc(h, &h->lvl_rowptr[b], V + 1));
+        LV_TRY(dalloc(h, &h->lvl_col[b], E));
+        LV_TRY(dalloc(h, &h->lvl_w[b], E));
+    }
+    h->agg_ready = true;
+    return LV_OK;
+}
+
+template <typename WT>
+int aggregate_t(lv_handle *h) {
+    Timer tm(h, 102);
+    AggBuffers &ab = h->ab;
+    const int32_t V = h->V;
+    agg_prepare(h->cur_rowptr, h->comm, h->size, V, ab, h->mslot, h->degm, h->P, h->stream);
+    LV_CUDA(h, cudaMemcpyAsync(h->small_h, ab.scalars, sizeof(int32_t) * (2 + NAC),
+                               cudaMemcpyDeviceToHost, h->stream));
+    LV_TRY(sync(h));
+    const int32_t newV = h->small_h[0];
+    int32_t aoff[NAC + 1];
+    aoff[0] = 0;
+    for (int c = 0; c < NAC; ++c) aoff[c + 1] = aoff[c] + h->small_h[2 + c];
+    agg_classify(h->size, V, ab, h->P, aoff, h->stream);
+    const int32_t nbig = aoff[NAC] - aoff[NAC - 1];
+    std::vector<int32_t> ids(nbig), deg(nbig);
+    if (nbig > 0) {
+        launch_gather_cdeg(ab.mstart, h->P, ab.clist + aoff[NAC - 1], nbig, ab.cdeg, h->stream);
+        LV_CUDA(h, cudaMemcpyAsync(ids.data(), ab.clist + aoff[NAC - 1], sizeof(int32_t) * nbig,
+                                   cudaMemcpyDeviceToHost, h->stream));
+        LV_CUDA(h, cudaMemcpyAsync(deg.data(), ab.cdeg, sizeof(int32_t) * nbig,
+                                   cudaMemcpyDeviceToHost, h->stream));
+        LV_TRY(sync(h));
+    }
+    LV_TRY(build_layout(h, h->hub_agg, ids, deg, newV));
+    GraphView<WT> g = view_of<WT>(h);
+    for (int c = 0; c < NCLS; ++c)
+        agg_permute<WT>(c, g, ab, h->mslot, h->P, h->list + h->cls_off[c],
+                        h->cls_off[c + 1] - h->cls_off[c], h->vkey, h->vw, h->di.sms, h->stream);
+    agg_new_vertices(h->size, h->S, V, ab, h->P, h->k, h->stream);
+    for (int c = 0; c < NAC - 1; ++c)
+        agg_merge_class(c, ab, h->P, ab.clist + aoff[c], aoff[c + 1] - aoff[c], h->vkey, h->vw,
+                        &h->tot_d->err, h->di.sms, h->stream);
+    agg_merge_global(h->hub_agg.view, ab, h->P, h->vkey, h->vw, &h->tot_d->err, h->stream);
+    const int nb = (h->cur_buf == 0) ? 1 : 0;
+    int32_t *rp = h->lvl_rowptr[nb];
+    scan_exclusive_i32(ab.newdeg, rp, newV, rp + newV, ab.scan_tmp, h->stream);
+    LV_CUDA(h, cudaMemcpyAsync(h->small_h, rp + newV, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                               h->stream));
+    LV_CUDA(h, cudaMemcpyAsync(h->tot_h, h->tot_d, sizeof(Totals), cudaMemcpyDeviceToHost, h->stream));
+    LV_TRY(sync(h));
+    LV_TRY(check_device_error(h, h->tot_h->err));
+    const int64_t newE = h->small_h[0];
+    agg_compact(rp, newV, newE, ab, h->vkey, h->vw, h->lvl_col[nb], h->lvl_w[nb], h->stream);
+    launch_compose_map(h->orig2comm, ab.flag, h->V0, h->stream);
+    tm.stop();
+    h->cur_buf = nb;
+    h->cur_rowptr = rp;
+    h->cur_col = h->lvl_col[nb];
+    h->cur_w = h->lvl_w[nb];
+    h->V = newV;
+    h->E = newE;
+    h->level += 1;
+    return level_setup(h);
+}
+
+int aggregate(lv_handle *h) {
+    LV_TRY(ensure_agg(h));
+    return h->cur_w ? aggregate_t<u64>(h) : aggregate_t<float>(h);
+}
+
+// ---------------------------------------------------------------------------
+// creation
+// ---------------------------------------------------------------------------
+int to_level0(lv_handle *h) {
+    h->level = 0;
+    h->V = h->V0;
+    h->E = h->E0;
+    h->cur_rowptr = h->in_rowptr;
+    h->cur_col = h->in_col;
+    h->cur_w = nullptr;
+    h->cur_buf = -1;
+    launch_iota_i32(h->orig2comm, h->V0, h->stream);
+    return level_setup(h);
+}
+
+int finish_create(lv_handle *h) {
+    const size_t V = (size_t)h->V0;
+    LV_TRY(dalloc(h, &h->comm, V + 1));
+    LV_TRY(dalloc(h, &h->newc, V + 1));
+    LV_TRY(dalloc(h, &h->size, V + 1));
+    LV_TRY(dalloc(h, &h->orig2comm, V + 1));
+    LV_TRY(dalloc(h, &h->k, V + 1));
+    LV_TRY(dalloc(h, &h->S, V + 1));
+    LV_TRY(dalloc(h, &h->list, V + 1));
+    LV_TRY(dalloc(h, &h->cls_scratch, V + SCRATCH_OFF + 16));
+    LV_TRY(dalloc(h, &h->tot_d, 1));
+    LV_CUDA(h, cudaMemsetAsync(h->tot_d, 0, sizeof(Totals), h->stream));
+    LV_CUDA(h, cudaMallocHost((void **)&h->tot_h, sizeof(Totals)));
+    LV_CUDA(h, cudaMallocHost((void **)&h->small_h, sizeof(int32_t) * 128));
+    // CSR validation
+    launch_validate_csr(h->in_rowptr, h->in_col, h->V0, h->E0, &h->tot_d->err, h->stream);
+    LV_CUDA(h, cudaMemcpyAsync(h->tot_h, h->tot_d, sizeof(Totals), cudaMemcpyDeviceToHost, h->stream));
+    LV_TRY(sync(h));
+    if (h->tot_h->err) return fail(h, LV_ERR_INVALID, "malformed CSR (offsets or column ids)");
+    // fixed-point scale (same rule as the oracle's orc_choose_scale)
+    int32_t *ws = h->cls_scratch;
+    launch_weight_scan(h->in_w, h->E0, ws, h->stream);
+    LV_CUDA(h, cudaMemcpyAsync(h->small_h, ws, sizeof(int32_t) * 3, cudaMemcpyDeviceToHost, h->stream));
+    LV_TRY(sync(h));
+    if (h->small_h[2]) return fail(h, LV_ERR_WEIGHT, "negative, NaN or infinite edge weight");
+    const int need = h->small_h[0];
+    const int top = h->small_h[1] ? h->small_h[1] - 1024 : 0;
+    const int cap = 61 - top - ceil_log2_i(h->E0 > 0 ? h->E0 : 1);
+    const int s = need < cap ? need : cap;
+    if (s < 0) return fail(h, LV_ERR_TOO_LARGE, "total edge weight exceeds the fixed-point range");
+    h->scale = s;
+    h->exact = (s == need);
+    h->scale_d = std::ldexp(1.0, s);
+    u64 *tw = (u64 *)(h->tot_d);   // reuse e_own slot
+    launch_total_weight(h->in_w, h->E0, h->scale_d, tw, h->stream);
+    LV_CUDA(h, cudaMemcpyAsync(h->tot_h, h->tot_d, sizeof(Totals), cudaMemcpyDeviceToHost, h->stream));
+    LV_TRY(sync(h));
+    h->T = h->tot_h->e_own;
+    LV_CUDA(h, cudaMemsetAsync(h->tot_d, 0, sizeof(Totals), h->stream));
+    return to_level0(h);
+}
+
+int begin_create(const lv_opts *opts, int32_t V, int64_t E, lv_handle **out, lv_handle **hp) {
+    if (!out) return LV_ERR_INVALID;
+    *out = nullptr;
+    if (V < 0 || E < 0) return LV_ERR_INVALID;
+    if (E > 0x7fffffffLL || V >= 0x7fffffff) return LV_ERR_TOO_LARGE;
+    lv_handle *h = new lv_handle();
+    lv_default_opts(&h->opts);
+    if (opts) {
+        size_t n = opts->struct_size && opts->struct_size < sizeof(lv_opts) ? opts->struct_size : sizeof(lv_opts);
+        std::memcpy(&h->opts, opts, n);
+        h->opts.struct_size = sizeof(lv_opts);
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        delete h;
+        return LV_ERR_NO_DEVICE;
+    }
+    if (h->opts.device < 0 || h->opts.device >= ndev) {
+        delete h;
+        return LV_ERR_INVALID;
+    }
+    h->device = h->opts.device;
+    cudaSetDevice(h->device);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return LV_ERR_CUDA;
+    }
+    static bool attrs_done[64] = {false};
+    init_kernel_attributes(h->di);
+    if (h->device < 64 && !attrs_done[h->device]) {
+        init_agg_attributes();
+        attrs_done[h->device] = true;
+    }
+    h->V0 = V;
+    h->E0 = E;
+    h->launch_base = launches_total();
+    *hp = h;
+    return LV_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+void lv_default_opts(lv_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->struct_size = sizeof(lv_opts);
+    o->device = 0;
+    o->max_sweeps = 0;
+    o->profile = 0;
+}
+
+const char *lv_status_string(int s) {
+    switch (s) {
+    case LV_OK: return "ok";
+    case LV_ERR_INVALID: return "invalid argument or malformed CSR";
+    case LV_ERR_WEIGHT: return "negative, NaN or infinite weight";
+    case LV_ERR_TOO_LARGE: return "graph too large for int32 ids or the fixed-point grid";
+    case LV_ERR_NOMEM: return "out of memory";
+    case LV_ERR_CUDA: return "CUDA error";
+    case LV_ERR_DEVICE: return "device-side check failed";
+    case LV_ERR_IO: return "I/O or parse error";
+    case LV_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+    }
+}
+
+const char *lv_version(void) { return "louvain_b200 0.1 (sm_100a)"; }
+
+int lv_destroy(lv_handle *h) {
+    if (!h) return LV_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->owns_input) {
+        dfree(h->in_rowptr);
+        dfree(h->in_col);
+        dfree(h->in_w);
+    }
+    dfree(h->comm); dfree(h->newc); dfree(h->size); dfree(h->orig2comm);
+    dfree(h->k); dfree(h->S); dfree(h->list); dfree(h->cls_scratch);
+    dfree(h->tbl_keys); dfree(h->tbl_vals);
+    if (h->hub_move.dev) cudaFree(h->hub_move.dev);
+    if (h->hub_agg.dev) cudaFree(h->hub_agg.dev);
+    AggBuffers &a = h->ab;
+    dfree(a.flag); dfree(a.cdeg); dfree(a.mstart); dfree(a.cursor); dfree(a.members);
+    dfree(a.lab); dfree(a.clist); dfree(a.newdeg); dfree(a.epos_new); dfree(a.scan_tmp);
+    dfree(a.scalars);
+    dfree(h->mslot); dfree(h->degm); dfree(h->P); dfree(h->vkey); dfree(h->vw);
+    for (int b = 0; b < 2; ++b) { dfree(h->lvl_rowptr[b]); dfree(h->lvl_col[b]); dfree(h->lvl_w[b]); }
+    dfree(h->tot_d);
+    if (h->tot_h) cudaFreeHost(h->tot_h);
+    if (h->small_h) cudaFreeHost(h->small_h);
+    for (const Pending &p : h->pend) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+    for (cudaEvent_t e : h->ev_free) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return LV_OK;
+}
+
+int lv_create(const int32_t *rowptr, const int32_t *col, const float *w, int32_t V, int64_t E,
+              const lv_opts *opts, lv_handle **out) {
+    if (!rowptr || (E > 0 && (!col || !w))) return LV_ERR_INVALID;
+    lv_handle *h = nullptr;
+    int rc = begin_create(opts, V, E, out, &h);
+    if (rc) return rc;
+    h->owns_input = true;
+    rc = dalloc(h, &h->in_rowptr, (size_t)V + 1);
+    if (!rc) rc = dalloc(h, &h->in_col, (size_t)E);
+    if (!rc) rc = dalloc(h, &h->in_w, (size_t)E);
+    if (!rc && cudaMemcpyAsync(h->in_rowptr, rowptr, sizeof(int32_t) * ((size_t)V + 1),
+                               cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
+        rc = LV_ERR_CUDA;
+    if (!rc && E > 0 &&
+        cudaMemcpyAsync(h->in_col, col, sizeof(int32_t) * (size_t)E, cudaMemcpyHostToDevice,
+                        h->stream) != cudaSuccess)
+        rc = LV_ERR_CUDA;
+    if (!rc && E > 0 &&
+        cudaMemcpyAsync(h->in_w, w, sizeof(float) * (size_t)E, cudaMemcpyHostToDevice,
+                        h->stream) != cudaSuccess)
+        rc = LV_ERR_CUDA;
+    if (!rc) rc = finish_create(h);
+    if (rc) {
+        lv_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return LV_OK;
+}
+
+int lv_create_device(const int32_t *d_rowptr, const int32_t *d_col, const float *d_w, int32_t V,
+                     int64_t E, const lv_opts *opts, lv_handle **out) {
+    if (!d_rowptr || (E > 0 && (!d_col || !d_w))) return LV_ERR_INVALID;
+    lv_handle *h = nullptr;
+    int rc = begin_create(opts, V, E, out, &h);
+    if (rc) return rc;
+    h->owns_input = false;
+    h->in_rowptr = const_cast<int32_t *>(d_rowptr);
+    h->in_col = const_cast<int32_t *>(d_col);
+    h->in_w = const_cast<float *>(d_w);
+    rc = finish_create(h);
+    if (rc) {
+        lv_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return LV_OK;
+}
+
+const char *lv_last_error(const lv_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+int lv_reset(lv_handle *h) {
+    if (!h) return LV_ERR_INVALID;
+    cudaSetDevice(h->device);
+    return to_level0(h);
+}
+
+int lv_optimise_level(lv_handle *h, float min_gain, int32_t *changed) {
+    if (!h) return LV_ERR_INVALID;
+    cudaSetDevice(h->device);
+    return optimise_level(h, min_gain, changed);
+}
+
+int lv_aggregate(lv_handle *h) {
+    if (!h) return LV_ERR_INVALID;
+    cudaSetDevice(h->device);
+    return aggregate(h);
+}
+
+int lv_modularity(lv_handle *h, double *q) {
+    if (!h || !q) return LV_ERR_INVALID;
+    cudaSetDevice(h->device);
+    return modularity(h, q);
+}
+
+int lv_sweep(lv_handle *h, int64_t *moves) {
+    if (!h) return LV_ERR_INVALID;
+    cudaSetDevice(h->device);
+    int64_t m = 0;
+    LV_TRY(sweep_and_q(h, &m, nullptr));
+    if (moves) *moves = m;
+    return LV_OK;
+}
+
+int lv_run(lv_handle *h, float min_gain, double *q) {
+    if (!h) return LV_ERR_INVALID;
+    cudaSetDevice(h->device);
+    for (;;) {
+        int32_t changed = 0;
+        LV_TRY(optimise_level(h, min_gain, &changed));
+        if (!changed) break;
+        LV_TRY(aggregate(h));
+    }
+    double qq = 0;
+    LV_TRY(modularity(h, &qq));
+    if (q) *q = qq;
+    return LV_OK;
+}
+
+int lv_get_original_to_community(lv_handle *h, int32_t *out, int32_t *num_communities) {
+    if (!h) return LV_ERR_INVALID;
+    cudaSetDevice(h->device);
+    if (out && h->V0 > 0)
+        LV_CUDA(h, cudaMemcpyAsync(out, h->orig2comm, sizeof(int32_t) * (size_t)h->V0,
+                                   cudaMemcpyDeviceToHost, h->stream));
+    LV_TRY(sync(h));
+    if (num_communities) *num_communities = h->V;
+    return LV_OK;
+}
+
+int lv_get_communities(lv_handle *h, int32_t *out) {
+    if (!h || !out) return LV_ERR_INVALID;
+    cudaSetDevice(h->device);
+    if (h->V > 0)
+        LV_CUDA(h, cudaMemcpyAsync(out, h->comm, sizeof(int32_t) * (size_t)h->V,
+                                   cudaMemcpyDeviceToHost, h->stream));
+    return sync(h);
+}
+
+int lv_set_communities(lv_handle *h, const int32_t *comm) {
+    if (!h || !comm) return LV_ERR_INVALID;
+    cudaSetDevice(h->device);
+    if (h->V == 0) return LV_OK;
+    int32_t *tmp = h->cls_scratch + SCRATCH_OFF;   // V0 entries of scratch
+    LV_CUDA(h, cudaMemcpyAsync(tmp, comm, sizeof(int32_t) * (size_t)h->V, cudaMemcpyHostToDevice,
+                               h->stream));
+    LV_CUDA(h, cudaMemsetAsync(&h->tot_d->err, 0, sizeof(int), h->stream));
+    launch_set_communities(tmp, h->comm, h->newc, h->size, h->k, h->S, h->V, &h->tot_d->err, h->stream);
+    LV_TRY(read_totals(h));
+    return LV_OK;
+}
+
+int lv_get_level_info(lv_handle *h, int32_t *V, int64_t *E, int32_t *level) {
+    if (!h) return LV_ERR_INVALID;
+    if (V) *V = h->V;
+    if (E) *E = h->E;
+    if (level) *level = h->level;
+    return LV_OK;
+}
+
+int lv_get_csr(lv_handle *h, int32_t *rowptr, int32_t *col, int64_t *wfix) {
+    if (!h) return LV_ERR_INVALID;
+    cudaSetDevice(h->device);
+    if (rowptr)
+        LV_CUDA(h, cudaMemcpyAsync(rowptr, h->cur_rowptr, sizeof(int32_t) * ((size_t)h->V + 1),
+                                   cudaMemcpyDeviceToHost, h->stream));
+    if (col && h->E > 0)
+        LV_CUDA(h, cudaMemcpyAsync(col, h->cur_col, sizeof(int32_t) * (size_t)h->E,
+                                   cudaMemcpyDeviceToHost, h->stream));
+    if (wfix && h->E > 0) {
+        int64_t *tmp = nullptr;
+        LV_TRY(dalloc(h, &tmp, (size_t)h->E));
+        if (h->cur_w)
+            launch_weights_to_fixed<u64>(h->cur_w, h->E, h->scale_d, tmp, h->stream);
+        else
+            launch_weights_to_fixed<float>(h->in_w, h->E, h->scale_d, tmp, h->stream);
+        cudaError_t e = cudaMemcpyAsync(wfix, tmp, sizeof(int64_t) * (size_t)h->E,
+                                        cudaMemcpyDeviceToHost, h->stream);
+        cudaStreamSynchronize(h->stream);
+        cudaFree(tmp);
+        if (e != cudaSuccess) return fail(h, LV_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return sync(h);
+}
+
+int lv_get_scale(lv_handle *h, int32_t *scale, uint64_t *total_weight, int32_t *exact) {
+    if (!h) return LV_ERR_INVALID;
+    if (scale) *scale = h->scale;
+    if (total_weight) *total_weight = h->T;
+    if (exact) *exact = h->exact;
+    return LV_OK;
+}
+
+int lv_get_stats(lv_handle *h, lv_stats *s) {
+    if (!h || !s) return LV_ERR_INVALID;
+    LV_TRY(sync(h));
+    *s = h->st;
+    s->kernel_launches = launches_total() - h->launch_base;
+    return LV_OK;
+}
+
+int lv_get_class_stats(lv_handle *h, lv_class_stats *s) {
+    if (!h || !s) return LV_ERR_INVALID;
+    LV_TRY(sync(h));
+    *s = h->cst;
+    return LV_OK;
+}
+
+int lv_clear_stats(lv_handle *h) {
+    if (!h) return LV_ERR_INVALID;
+    LV_TRY(sync(h));
+    std::memset(&h->st, 0, sizeof(h->st));
+    std::memset(&h->cst, 0, sizeof(h->cst));
+    h->launch_base = launches_total();
+    return LV_OK;
+}
+
+}  // extern "C"

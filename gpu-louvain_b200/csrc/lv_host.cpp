@@ -1,0 +1,415 @@
+// lv_host.cpp -- host-side I/O and seeded graph generators (no GPU needed).
+//
+//   lv_read_mtx           readInputData (utils.cu:9-62): symmetric Matrix Market
+//                         -> CSR in file order, parsed from an mmap'd buffer.
+//   lv_write_mtx          symmetric Matrix Market writer (i > j, 1-based).
+//   lv_print_communities  printOriginalToCommunity (modularity_optimisation.cu:403-418).
+//   lv_gen_rmat / lv_gen_planted   seeded synthetic inputs (counter-based RNG,
+//                         identical on the host, the device and in numpy).
+#include <fcntl.h>
+#include <omp.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/louvain_b200.h"
+#include "lv_rng.h"
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Matrix Market reader
+// ---------------------------------------------------------------------------
+struct Mapped {
+    const char *p = nullptr;
+    size_t n = 0;
+    int fd = -1;
+    ~Mapped() {
+        if (p) munmap((void *)p, n);
+        if (fd >= 0) close(fd);
+    }
+};
+
+inline const char *skip_ws(const char *p, const char *end) {
+    while (p < end && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n')) ++p;
+    return p;
+}
+
+inline bool parse_i64(const char *&p, const char *end, long long *out) {
+    p = skip_ws(p, end);
+    bool neg = false;
+    if (p < end && (*p == '-' || *p == '+')) { neg = *p == '-'; ++p; }
+    if (p >= end || *p < '0' || *p > '9') return false;
+    long long v = 0;
+    while (p < end && *p >= '0' && *p <= '9') { v = v * 10 + (*p - '0'); ++p; }
+    *out = neg ? -v : v;
+    return true;
+}
+
+// Decimal -> float with the rounding of strtof (the reference reads with
+// `file >> w` into a float).  The token is copied to a NUL-terminated buffer.
+inline bool parse_f32(const char *&p, const char *end, float *out) {
+    p = skip_ws(p, end);
+    const char *q = p;
+    while (q < end && !(*q == ' ' || *q == '\t' || *q == '\r' || *q == '\n')) ++q;
+    size_t len = (size_t)(q - p);
+    if (len == 0 || len > 120) return false;
+    char buf[128];
+    std::memcpy(buf, p, len);
+    buf[len] = 0;
+    char *e = nullptr;
+    errno = 0;
+    float v = std::strtof(buf, &e);
+    if (e == buf) return false;
+    *out = v;
+    p = q;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+void lv_free_host(void *p) { std::free(p); }
+
+int lv_read_mtx(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr_out,
+                int32_t **col_out, float **w_out, float *m_ref) {
+    if (!path || !Vout || !Eout || !rowptr_out || !col_out || !w_out) return LV_ERR_INVALID;
+    Mapped m;
+    m.fd = open(path, O_RDONLY);
+    if (m.fd < 0) return LV_ERR_IO;
+    struct stat sb;
+    if (fstat(m.fd, &sb) != 0) return LV_ERR_IO;
+    m.n = (size_t)sb.st_size;
+    if (m.n == 0) return LV_ERR_IO;
+    void *mp = mmap(nullptr, m.n, PROT_READ, MAP_PRIVATE, m.fd, 0);
+    if (mp == MAP_FAILED) return LV_ERR_IO;
+    m.p = (const char *)mp;
+    const char *p = m.p, *end = m.p + m.n;
+    bool pattern = false;
+    // header: '%' lines are comments (utils.cu:14-16); blank lines skipped
+    for (;;) {
+        if (p >= end) return LV_ERR_IO;
+        const char *eol = (const char *)std::memchr(p, '\n', (size_t)(end - p));
+        if (!eol) eol = end;
+        if (*p == '%') {
+            if ((size_t)(eol - p) >= 14 && std::strncmp(p, "%%MatrixMarket", 14) == 0) {
+                std::string line(p, eol);
+                if (line.find("pattern") != std::string::npos) pattern = true;
+            }
+            p = eol < end ? eol + 1 : end;
+            continue;
+        }
+        const char *q = skip_ws(p, eol);
+        if (q == eol) {   // blank line
+            p = eol < end ? eol + 1 : end;
+            continue;
+        }
+        break;
+    }
+    long long rows = 0, cols = 0, nnz = 0;
+    // size line "rows cols nnz"; the vertex count is the second number (utils.cu:18)
+    if (!parse_i64(p, end, &rows) || !parse_i64(p, end, &cols) || !parse_i64(p, end, &nnz))
+        return LV_ERR_IO;
+    if (cols < 0 || nnz < 0) return LV_ERR_IO;
+    if (cols > 0x7ffffffeLL) return LV_ERR_TOO_LARGE;
+    const int32_t V = (int32_t)cols;
+    std::vector<int32_t> ea((size_t)nnz), eb((size_t)nnz);
+    std::vector<float> ew((size_t)nnz);
+    for (long long i = 0; i < nnz; ++i) {
+        long long a, b;
+        float wv = 1.0f;
+        if (!parse_i64(p, end, &a) || !parse_i64(p, end, &b)) return LV_ERR_IO;
+        if (!pattern && !parse_f32(p, end, &wv)) return LV_ERR_IO;
+        a -= 1;
+        b -= 1;
+        if (a < 0 || b < 0 || a >= V || b >= V) return LV_ERR_INVALID;
+        ea[(size_t)i] = (int32_t)a;
+        eb[(size_t)i] = (int32_t)b;
+        ew[(size_t)i] = wv;
+    }
+    // degrees: v1 gets (v2,w); v2 gets (v1,w) unless self-loop (utils.cu:32-46)
+    std::vector<int64_t> deg((size_t)V + 1, 0);
+    int64_t E = 0;
+    float M = 0;
+    for (long long i = 0; i < nnz; ++i) {
+        const int32_t a = ea[(size_t)i], b = eb[(size_t)i];
+        deg[(size_t)a]++;
+        E++;
+        if (a != b) {
+            deg[(size_t)b]++;
+            E++;
+            M += ew[(size_t)i];
+        }
+        M += ew[(size_t)i];
+    }
+    M /= 2;
+    if (E > 0x7fffffffLL) return LV_ERR_TOO_LARGE;
+    int32_t *rp = (int32_t *)std::malloc(sizeof(int32_t) * ((size_t)V + 1));
+    int32_t *cl = (int32_t *)std::malloc(sizeof(int32_t) * (size_t)(E > 0 ? E : 1));
+    float *wt = (float *)std::malloc(sizeof(float) * (size_t)(E > 0 ? E : 1));
+    if (!rp || !cl || !wt) {
+        std::free(rp); std::free(cl); std::free(wt);
+        return LV_ERR_NOMEM;
+    }
+    int64_t acc = 0;
+    for (int32_t v = 0; v < V; ++v) {
+        rp[v] = (int32_t)acc;
+        acc += deg[(size_t)v];
+    }
+    rp[V] = (int32_t)acc;
+    std::vector<int64_t> cur((size_t)V);
+    for (int32_t v = 0; v < V; ++v) cur[(size_t)v] = rp[v];
+    // rows keep file order (utils.cu:50-59)
+    for (long long i = 0; i < nnz; ++i) {
+        const int32_t a = ea[(size_t)i], b = eb[(size_t)i];
+        const float wv = ew[(size_t)i];
+        int64_t pa = cur[(size_t)a]++;
+        cl[pa] = b;
+        wt[pa] = wv;
+        if (a != b) {
+            int64_t pb = cur[(size_t)b]++;
+            cl[pb] = a;
+            wt[pb] = wv;
+        }
+    }
+    *Vout = V;
+    *Eout = E;
+    *rowptr_out = rp;
+    *col_out = cl;
+    *w_out = wt;
+    if (m_ref) *m_ref = M;
+    return LV_OK;
+}
+
+int lv_write_mtx(const char *path, int32_t V, int64_t n_edges, const int32_t *u, const int32_t *v,
+                 const float *w) {
+    if (!path || V < 0 || n_edges < 0 || (n_edges > 0 && (!u || !v))) return LV_ERR_INVALID;
+    FILE *f = std::fopen(path, "w");
+    if (!f) return LV_ERR_IO;
+    std::vector<char> buf(1 << 22);
+    std::setvbuf(f, buf.data(), _IOFBF, buf.size());
+    std::fprintf(f, "%%%%MatrixMarket matrix coordinate real symmetric\n");
+    std::fprintf(f, "%d %d %lld\n", V, V, (long long)n_edges);
+    for (int64_t i = 0; i < n_edges; ++i) {
+        int32_t a = u[i], b = v[i];
+        if (a < b) std::swap(a, b);
+        std::fprintf(f, "%d %d %.9g\n", a + 1, b + 1, w ? (double)w[i] : 1.0);
+    }
+    int rc = std::fclose(f);
+    return rc == 0 ? LV_OK : LV_ERR_IO;
+}
+
+int lv_print_communities(const char *path, const int32_t *orig2comm, int32_t V0,
+                         int32_t num_communities) {
+    if (V0 < 0 || num_communities < 0 || (V0 > 0 && !orig2comm)) return LV_ERR_INVALID;
+    std::vector<int64_t> start((size_t)num_communities + 1, 0);
+    for (int32_t v = 0; v < V0; ++v) {
+        const int32_t c = orig2comm[v];
+        if (c < 0 || c >= num_communities) return LV_ERR_INVALID;
+        start[(size_t)c + 1]++;
+    }
+    for (int32_t c = 0; c < num_communities; ++c) start[(size_t)c + 1] += start[(size_t)c];
+    std::vector<int32_t> mem((size_t)V0);
+    {
+        std::vector<int64_t> pos(start.begin(), start.end() - 1);
+        for (int32_t v = 0; v < V0; ++v) mem[(size_t)pos[(size_t)orig2comm[v]]++] = v;
+    }
+    FILE *f = path ? std::fopen(path, "w") : stdout;
+    if (!f) return LV_ERR_IO;
+    std::vector<char> out;
+    out.reserve(1 << 22);
+    char tmp[32];
+    auto flush = [&]() {
+        if (!out.empty()) std::fwrite(out.data(), 1, out.size(), f);
+        out.clear();
+    };
+    auto put_int = [&](int64_t x) {
+        int n = std::snprintf(tmp, sizeof(tmp), "%lld", (long long)x);
+        out.insert(out.end(), tmp, tmp + n);
+    };
+    put_int(num_communities);
+    out.push_back('\n');
+    for (int32_t c = 0; c < num_communities; ++c) {
+        put_int((int64_t)c + 1);
+        for (int64_t i = start[(size_t)c]; i < start[(size_t)c + 1]; ++i) {
+            out.push_back(' ');
+            put_int((int64_t)mem[(size_t)i] + 1);
+        }
+        out.push_back('\n');
+        if (out.size() > (1 << 21)) flush();
+    }
+    flush();
+    std::fflush(f);
+    if (path) std::fclose(f);
+    return LV_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// generators
+// ---------------------------------------------------------------------------
+namespace {
+
+// Parallel LSD radix sort of 64-bit keys whose significant bits are < nbits.
+void radix_sort_u64(std::vector<uint64_t> &a, int nbits) {
+    const size_t n = a.size();
+    if (n < 2) return;
+    std::vector<uint64_t> b(n);
+    const int nt = omp_get_max_threads();
+    std::vector<size_t> hist((size_t)nt * 256);
+    for (int shift = 0; shift < nbits; shift += 8) {
+        std::fill(hist.begin(), hist.end(), 0);
+#pragma omp parallel num_threads(nt)
+        {
+            const int t = omp_get_thread_num();
+            const size_t lo = n * t / nt, hi = n * (t + 1) / nt;
+            size_t *h = hist.data() + (size_t)t * 256;
+            for (size_t i = lo; i < hi; ++i) h[(a[i] >> shift) & 255]++;
+        }
+        size_t run = 0;
+        for (int d = 0; d < 256; ++d)
+            for (int t = 0; t < nt; ++t) {
+                size_t c = hist[(size_t)t * 256 + d];
+                hist[(size_t)t * 256 + d] = run;
+                run += c;
+            }
+#pragma omp parallel num_threads(nt)
+        {
+            const int t = omp_get_thread_num();
+            const size_t lo = n * t / nt, hi = n * (t + 1) / nt;
+            size_t *h = hist.data() + (size_t)t * 256;
+            for (size_t i = lo; i < hi; ++i) b[h[(a[i] >> shift) & 255]++] = a[i];
+        }
+        a.swap(b);
+    }
+}
+
+// keys = (lo << sh) | hi with lo < hi, sorted and unique -> symmetric CSR
+// with ascending rows.
+int keys_to_csr(const std::vector<uint64_t> &keys, int sh, int32_t V, int32_t weight_mode,
+                uint64_t seed, int64_t *Eout, int32_t **rowptr, int32_t **col, float **w) {
+    const uint64_t mask = (sh >= 64) ? ~0ull : ((1ull << sh) - 1);
+    const int64_t nk = (int64_t)keys.size();
+    const int64_t E = 2 * nk;
+    if (E > 0x7fffffffLL) return LV_ERR_TOO_LARGE;
+    std::vector<int64_t> dlo((size_t)V + 1, 0), dhi((size_t)V + 1, 0);
+    for (int64_t i = 0; i < nk; ++i) {
+        const int32_t a = (int32_t)(keys[(size_t)i] >> sh), b = (int32_t)(keys[(size_t)i] & mask);
+        dhi[(size_t)a]++;   // a's larger neighbours
+        dlo[(size_t)b]++;   // b's smaller neighbours
+    }
+    int32_t *rp = (int32_t *)std::malloc(sizeof(int32_t) * ((size_t)V + 1));
+    int32_t *cl = (int32_t *)std::malloc(sizeof(int32_t) * (size_t)(E > 0 ? E : 1));
+    float *wt = (float *)std::malloc(sizeof(float) * (size_t)(E > 0 ? E : 1));
+    if (!rp || !cl || !wt) {
+        std::free(rp); std::free(cl); std::free(wt);
+        return LV_ERR_NOMEM;
+    }
+    int64_t acc = 0;
+    std::vector<int64_t> clo((size_t)V), chi((size_t)V);
+    for (int32_t v = 0; v < V; ++v) {
+        rp[v] = (int32_t)acc;
+        clo[(size_t)v] = acc;
+        chi[(size_t)v] = acc + dlo[(size_t)v];
+        acc += dlo[(size_t)v] + dhi[(size_t)v];
+    }
+    rp[V] = (int32_t)acc;
+    const uint64_t wkey = lvrng::stream_key(seed, lvrng::WEIGHT_STREAM);
+    for (int64_t i = 0; i < nk; ++i) {
+        const int32_t a = (int32_t)(keys[(size_t)i] >> sh), b = (int32_t)(keys[(size_t)i] & mask);
+        const float wv = weight_mode == 1 ? lvrng::edge_weight(wkey, (uint32_t)a, (uint32_t)b) : 1.0f;
+        const int64_t pa = chi[(size_t)a]++, pb = clo[(size_t)b]++;
+        cl[pa] = b;
+        wt[pa] = wv;
+        cl[pb] = a;
+        wt[pb] = wv;
+    }
+    *Eout = E;
+    *rowptr = rp;
+    *col = cl;
+    *w = wt;
+    return LV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lv_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed, double a, double b, double c,
+                int32_t weight_mode, int32_t *Vout, int64_t *Eout, int32_t **rowptr, int32_t **col,
+                float **w) {
+    if (scale < 1 || scale > 30 || edge_factor < 1 || !Vout || !Eout || !rowptr || !col || !w)
+        return LV_ERR_INVALID;
+    const int64_t n = (int64_t)edge_factor << scale;
+    const lvrng::RmatParams rp = lvrng::rmat_params(scale, a, b, c, seed);
+    std::vector<uint64_t> keys((size_t)n);
+    int64_t kept = 0;
+    const int nt = omp_get_max_threads();
+    std::vector<int64_t> cnt((size_t)nt + 1, 0);
+#pragma omp parallel num_threads(nt)
+    {
+        const int t = omp_get_thread_num();
+        const int64_t lo = n * t / nt, hi = n * (t + 1) / nt;
+        int64_t k = lo;
+        for (int64_t i = lo; i < hi; ++i) {
+            uint32_t u, v;
+            lvrng::rmat_edge(rp, (uint64_t)i, &u, &v);
+            if (u == v) continue;
+            const uint32_t x = u < v ? u : v, y = u < v ? v : u;
+            keys[(size_t)k++] = ((uint64_t)x << scale) | y;
+        }
+        cnt[(size_t)t + 1] = k - lo;
+    }
+    // compact the per-thread runs
+    {
+        int64_t dst = 0;
+        for (int t = 0; t < nt; ++t) {
+            const int64_t lo = n * t / nt;
+            if (dst != lo) std::memmove(&keys[(size_t)dst], &keys[(size_t)lo], sizeof(uint64_t) * (size_t)cnt[(size_t)t + 1]);
+            dst += cnt[(size_t)t + 1];
+        }
+        kept = dst;
+    }
+    keys.resize((size_t)kept);
+    radix_sort_u64(keys, 2 * scale);
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    const int32_t V = (int32_t)(1u << scale);
+    int rc = keys_to_csr(keys, scale, V, weight_mode, seed, Eout, rowptr, col, w);
+    if (rc == LV_OK) *Vout = V;
+    return rc;
+}
+
+int lv_gen_planted(int32_t V, int32_t blocks, double d_in, double d_out, uint64_t seed,
+                   int32_t weight_mode, int64_t *Eout, int32_t **rowptr, int32_t **col, float **w) {
+    if (V < 1 || blocks < 1 || blocks > V || d_in < 0 || d_out < 0 || !Eout || !rowptr || !col || !w)
+        return LV_ERR_INVALID;
+    const int64_t m_in = (int64_t)std::llround((double)V * d_in / 2.0);
+    const int64_t m_out = (int64_t)std::llround((double)V * d_out / 2.0);
+    std::vector<uint64_t> keys;
+    keys.reserve((size_t)(m_in + m_out));
+    const uint64_t k1 = lvrng::stream_key(seed, 1), k2 = lvrng::stream_key(seed, 2);
+    for (int64_t i = 0; i < m_in + m_out; ++i) {
+        uint32_t u, v;
+        bool ok = i < m_in ? lvrng::planted_intra(k1, (uint64_t)i, V, blocks, &u, &v)
+                           : lvrng::planted_inter(k2, (uint64_t)(i - m_in), V, blocks, &u, &v);
+        if (!ok || u == v) continue;
+        const uint32_t x = u < v ? u : v, y = u < v ? v : u;
+        keys.push_back(((uint64_t)x << 32) | y);
+    }
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    return keys_to_csr(keys, 32, V, weight_mode, seed, Eout, rowptr, col, w);
+}
+
+}  // extern "C"

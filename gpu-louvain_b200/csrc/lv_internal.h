@@ -1,0 +1,105 @@
+// lv_internal.h -- launchers shared between the engine's translation units.
+#pragma once
+#include "lv_common.cuh"
+
+namespace lv {
+
+// Layout of the global-memory hash tables of class CLS_HG (degree > 4096)
+// for the current level.  Hubs are split into edge chunks (insert kernel)
+// and slot chunks (evaluate kernel) so that one hub spreads over many CTAs.
+constexpr int HG_EDGE_CHUNK = 4096;
+constexpr int HG_SLOT_CHUNK = 4096;
+
+struct HubGlobal {
+    int32_t nhubs = 0;
+    int32_t n_echunks = 0;
+    int32_t n_schunks = 0;
+    const int32_t *hubs = nullptr;        // [nhubs] vertex ids
+    const int64_t *tbl_off = nullptr;     // [nhubs] first slot of each hub's table
+    const int32_t *tbl_lg = nullptr;      // [nhubs] log2 capacity
+    const int32_t *echunk_hub = nullptr;  // [n_echunks]
+    const int32_t *echunk_e0 = nullptr;   // [n_echunks] edge offset within the row
+    const int32_t *schunk_hub = nullptr;  // [n_schunks]
+    const int32_t *schunk_s0 = nullptr;   // [n_schunks] first slot
+    const int32_t *hub_schunk0 = nullptr; // [nhubs + 1]
+    int32_t *keys = nullptr;              // table keys (-1 = empty)
+    u64 *vals = nullptr;                  // table sums
+    u64 *res_g = nullptr;                 // [2 * n_schunks] best gain (lo, hi)
+    int32_t *res_c = nullptr;             // [n_schunks] best community
+    u64 *res_e = nullptr;                 // [n_schunks] e_own contribution
+};
+
+// Count of engine kernel launches (all handles, all devices of the process).
+void note_launches(int n);
+long long launches_total();
+
+// Launch geometry helpers (filled once per device).
+struct DeviceInfo {
+    int sms = 148;
+    int occ_b5 = 8, occ_h1 = 4, occ_h2 = 2;   // resident CTAs per SM
+};
+void init_kernel_attributes(DeviceInfo &di);
+
+// ---- move phase (lv_move.cu) ----
+template <typename WT>
+void launch_move_class(int cls, const GraphView<WT> &g, const StateView &st, const int32_t *list,
+                       int32_t n, const HubGlobal &hg, const DeviceInfo &di, cudaStream_t s);
+void launch_commit(const StateView &st, const int32_t *list, int32_t n, u64 *moves,
+                   cudaStream_t s);
+
+// k_i = row sums (mode 0) or e_own total (mode 1) over the vertices of one class.
+template <typename WT>
+void launch_row_reduce(int cls, int mode, const GraphView<WT> &g, const int32_t *comm, u64 *k,
+                       u64 *total, const int32_t *list, int32_t n, const DeviceInfo &di,
+                       cudaStream_t s);
+void launch_s2(const u64 *S, int32_t V, u64 *total_hi_lo, cudaStream_t s);
+
+// ---- primitives (lv_prims.cu) ----
+// Exclusive scan of n int32 values (out may alias in); writes the total to
+// *total_dev.  tmp must hold scan_tmp_elems(n) int32.
+int64_t scan_tmp_elems(int64_t n);
+void scan_exclusive_i32(const int32_t *in, int32_t *out, int64_t n, int32_t *total_dev,
+                        int32_t *tmp, cudaStream_t s);
+// Degree classification of vertices: counts[NCLS] then scatter into list.
+// The count buffer holds CLASS_COUNT_WORDS int32: NCLS vertex counts, then
+// (8-byte aligned) NCLS uint64 edge totals.
+constexpr int CLASS_COUNT_WORDS = NCLS + (NCLS & 1) + 2 * NCLS;
+void launch_class_count(const int32_t *rowptr, int32_t V, int32_t *counts, cudaStream_t s);
+void launch_class_scatter(const int32_t *rowptr, int32_t V, const int32_t *offsets,
+                          int32_t *cursors, int32_t *list, cudaStream_t s);
+void launch_fill_i32(int32_t *p, int64_t n, int32_t v, cudaStream_t s);
+void launch_iota_i32(int32_t *p, int64_t n, cudaStream_t s);
+void launch_level_init(int32_t *comm, int32_t *newc, int32_t *size, const u64 *k, u64 *S,
+                       int32_t V, cudaStream_t s);
+void launch_set_communities(const int32_t *comm_in, int32_t *comm, int32_t *newc, int32_t *size,
+                            const u64 *k, u64 *S, int32_t V, int *err, cudaStream_t s);
+void launch_compose_map(int32_t *orig2comm, const int32_t *map, int32_t V0, cudaStream_t s);
+template <typename WT>
+void launch_weights_to_fixed(const WT *w, int64_t E, double scale, int64_t *out, cudaStream_t s);
+
+// Fixed-point scale analysis of float weights: out[0] = max fractional bits,
+// out[1] = max floor(log2 w) + 1024 (0 if no positive weight), out[2] = error flags.
+void launch_weight_scan(const float *w, int64_t E, int32_t *out, cudaStream_t s);
+void launch_total_weight(const float *w, int64_t E, double scale, u64 *total, cudaStream_t s);
+// CSR validation: error bit 1 bad offsets, 2 bad column.
+void launch_validate_csr(const int32_t *rowptr, const int32_t *col, int32_t V, int64_t E,
+                         int *err, cudaStream_t s);
+
+// ---- aggregation (lv_agg.cu) ----
+struct AggBuffers {
+    int32_t *flag;      // [V]   nonempty flag, then new id (exclusive scan)
+    int32_t *cdeg;      // [V]   community degree bound, then merged row start (scan)
+    int32_t *mstart;    // [V+1] member start per old community (scan of size)
+    int32_t *cursor;    // [V]   member cursor / row counter
+    int32_t *members;   // [V]   vertices grouped by community
+    int32_t *lab;       // [V]   new id of each vertex's community
+    int32_t *clist;     // [V]   nonempty communities grouped by merge class
+    int32_t *newdeg;    // [V]   distinct neighbours per new vertex
+    int32_t *epos_new;  // [V]   merged-row start per new vertex
+    int32_t *scan_tmp;
+    int32_t *scalars;   // [16]  device scalars (totals, counts)
+    int32_t *scol;      // [E]   merged rows (uncompacted)
+    u64 *sw;            // [E]
+};
+
+}  // namespace lv

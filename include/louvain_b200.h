@@ -1,0 +1,173 @@
+/*
+ * louvain_b200.h -- C ABI of the B200 Louvain engine (liblouvain_b200.so).
+ *
+ * Drop-in boundary for the level loop of olearczuk/gpu-louvain.  The
+ * reference has no library API: its boundary is the `gpulouvain` CLI and the
+ * three C++ functions that the CLI calls over `device_structures`.  Each entry
+ * point below names the reference interface it replaces (file:line in the
+ * reference tree).  All functions return an lv_status (0 = LV_OK) instead of
+ * calling exit() (the reference's HANDLE_ERROR, utils.cuh:92-98); the text of
+ * the last error of a handle is available from lv_last_error().
+ *
+ * Arithmetic: weights are mapped onto an integer grid of 2^-scale (exact for
+ * float32 weights whose binary expansions fit, see lv_get_scale); all sums
+ * are exact and gains are compared exactly, so results do not depend on the
+ * order of parallel additions and are bit-identical run to run.
+ *
+ * Threading: a handle owns one CUDA stream and its device memory; calls on
+ * one handle must not overlap.  Different handles are independent.
+ */
+#ifndef LOUVAIN_B200_H
+#define LOUVAIN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum lv_status {
+    LV_OK = 0,
+    LV_ERR_INVALID = 1,    /* bad argument or malformed CSR                 */
+    LV_ERR_WEIGHT = 2,     /* negative, NaN or infinite edge weight         */
+    LV_ERR_TOO_LARGE = 3,  /* beyond int32 ids/offsets or the fixed grid    */
+    LV_ERR_NOMEM = 4,      /* device or host allocation failed              */
+    LV_ERR_CUDA = 5,       /* CUDA runtime error                            */
+    LV_ERR_DEVICE = 6,     /* a device-side check failed (see lv_last_error) */
+    LV_ERR_IO = 7,         /* file could not be read or parsed              */
+    LV_ERR_NO_DEVICE = 8   /* no usable CUDA device                         */
+} lv_status;
+
+typedef struct lv_handle lv_handle;
+
+typedef struct lv_opts {
+    uint32_t struct_size;  /* sizeof(lv_opts), for forward compatibility   */
+    int32_t device;        /* CUDA device ordinal (default 0)              */
+    int32_t max_sweeps;    /* per-level sweep cap, 0 = unlimited (default) */
+    int32_t profile;       /* 1: time every kernel class with CUDA events  */
+    int32_t reserved[12];
+} lv_opts;
+
+/* Per-run counters; times in milliseconds (device time, CUDA events). */
+typedef struct lv_stats {
+    int32_t levels;            /* levels run by lv_run / lv_optimise_level   */
+    int32_t final_vertices;    /* vertices of the last level                 */
+    int64_t sweeps;            /* sweeps over all levels                     */
+    int64_t edge_sweeps;       /* sum over sweeps of that level's CSR size   */
+    int64_t moves;             /* committed vertex moves                     */
+    double move_ms;            /* move kernels + commits                     */
+    double modularity_ms;      /* modularity reductions                      */
+    double aggregate_ms;       /* aggregation                                */
+    double setup_ms;           /* level set-up (k_i, classes, hub tables)    */
+    double move_bytes;         /* algorithmic bytes of the move sweeps       */
+    int64_t kernel_launches;   /* engine kernels launched since the handle's
+                                  creation or last lv_clear_stats (counted
+                                  process-wide)                              */
+} lv_stats;
+
+/* Per work-class kernel timing (filled when opts.profile = 1). */
+#define LV_NUM_CLASSES 9
+typedef struct lv_class_stats {
+    int64_t launches[LV_NUM_CLASSES];
+    int64_t vertices[LV_NUM_CLASSES];
+    int64_t edges[LV_NUM_CLASSES];
+    double ms[LV_NUM_CLASSES];
+    double bytes[LV_NUM_CLASSES];   /* algorithmic bytes: 8+w per edge, 20 per vertex */
+} lv_class_stats;
+
+void lv_default_opts(lv_opts *opts);
+const char *lv_status_string(int status);
+const char *lv_version(void);
+
+/* Create an engine from a HOST CSR (symmetric, as produced by the MTX reader).
+ * Replaces copyStructures (utils.cu:64-106) + initM
+ * (modularity_optimisation.cu:420-422): device allocation, host->device copy
+ * and M.  rowptr has V+1 entries, col/w have E entries, E < 2^31. */
+int lv_create(const int32_t *rowptr, const int32_t *col, const float *w, int32_t V, int64_t E,
+              const lv_opts *opts, lv_handle **out);
+/* Same, for a CSR already resident in device memory.  The arrays are
+ * borrowed (not copied) and must stay valid and unchanged until
+ * lv_destroy. */
+int lv_create_device(const int32_t *d_rowptr, const int32_t *d_col, const float *d_w, int32_t V,
+                     int64_t E, const lv_opts *opts, lv_handle **out);
+/* Return to level 0 with singleton communities (no reallocation). */
+int lv_reset(lv_handle *h);
+int lv_destroy(lv_handle *h);
+const char *lv_last_error(const lv_handle *h);
+
+/* optimiseModularity (modularity_optimisation.cuh:28): sweeps of the current
+ * level until a sweep gains less than min_gain; *changed = 1 when any sweep
+ * gained (> 0), which is when the reference aggregates. */
+int lv_optimise_level(lv_handle *h, float min_gain, int32_t *changed);
+/* aggregateCommunities (community_aggregation.cuh:11): contract communities
+ * into the next level's vertices. */
+int lv_aggregate(lv_handle *h);
+/* calculateModularity (modularity_optimisation.cuh:30) of the current state,
+ * computed exactly and returned in FP64. */
+int lv_modularity(lv_handle *h, double *q);
+/* The level loop + final modularity of main() (gpulouvain.cu:30-37). */
+int lv_run(lv_handle *h, float min_gain, double *q);
+
+/* One sweep (the 7 degree-bucket sub-rounds) at the current level. */
+int lv_sweep(lv_handle *h, int64_t *moves);
+
+/* Original vertex -> final community (the data printed by
+ * printOriginalToCommunity, modularity_optimisation.cu:403-418); out has
+ * V0 entries; *num_communities = vertex count of the current level. */
+int lv_get_original_to_community(lv_handle *h, int32_t *out, int32_t *num_communities);
+/* Current level: vertex -> community (out has V entries). */
+int lv_get_communities(lv_handle *h, int32_t *out);
+/* Test hook: set the current level's communities (Sigma_tot and sizes are
+ * recomputed), e.g. to drive lv_aggregate from a given community vector. */
+int lv_set_communities(lv_handle *h, const int32_t *comm);
+int lv_get_level_info(lv_handle *h, int32_t *V, int64_t *E, int32_t *level);
+/* Test hook: current level CSR; weights as fixed-point integers
+ * (value = wfix / 2^scale).  Any pointer may be NULL. */
+int lv_get_csr(lv_handle *h, int32_t *rowptr, int32_t *col, int64_t *wfix);
+int lv_get_scale(lv_handle *h, int32_t *scale, uint64_t *total_weight, int32_t *exact);
+int lv_get_stats(lv_handle *h, lv_stats *stats);
+int lv_get_class_stats(lv_handle *h, lv_class_stats *stats);
+int lv_clear_stats(lv_handle *h);
+
+/* ---- host-side I/O (no GPU needed) ---- */
+
+/* readInputData (utils.cu:9-62): symmetric Matrix Market -> CSR in file
+ * order (both directions for off-diagonal entries, self-loops once).
+ * Arrays are malloc'd; release with lv_free_host.  m_ref receives M as the
+ * reference accumulates it (FP32, sequential). */
+int lv_read_mtx(const char *path, int32_t *V, int64_t *E, int32_t **rowptr, int32_t **col,
+                float **w, float *m_ref);
+/* Write an undirected edge list as symmetric Matrix Market (i > j, 1-based). */
+int lv_write_mtx(const char *path, int32_t V, int64_t n_edges, const int32_t *u, const int32_t *v,
+                 const float *w);
+void lv_free_host(void *p);
+
+/* Print the verbose map exactly as printOriginalToCommunity
+ * (modularity_optimisation.cu:403-418): first line = num_communities, then
+ * one line per community c: "c+1 m1+1 m2+1 ...".  path NULL = stdout. */
+int lv_print_communities(const char *path, const int32_t *orig2comm, int32_t V0,
+                         int32_t num_communities);
+
+/* ---- seeded synthetic graphs (host, OpenMP) ----
+ * Output CSR rows are sorted by neighbour id; arrays malloc'd.
+ * R-MAT: ef * 2^scale draws with quadrant probabilities a, b, c,
+ * self-loops and duplicates removed, symmetrised; weight_mode 0 = unit,
+ * 1 = uniform [0.5, 1.5) on the 2^-24 grid. */
+int lv_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed, double a, double b, double c,
+                int32_t weight_mode, int32_t *V, int64_t *E, int32_t **rowptr, int32_t **col,
+                float **w);
+/* Planted partition: V vertices in `blocks` equal blocks, round(V*d_in/2)
+ * intra-block and round(V*d_out/2) inter-block uniform draws. */
+int lv_gen_planted(int32_t V, int32_t blocks, double d_in, double d_out, uint64_t seed,
+                   int32_t weight_mode, int64_t *E, int32_t **rowptr, int32_t **col, float **w);
+/* R-MAT drawn on the device into device buffers allocated by the library
+ * (free with lv_free_device); same graph as lv_gen_rmat. */
+int lv_gen_rmat_device(int32_t scale, int32_t edge_factor, uint64_t seed, double a, double b,
+                       double c, int32_t weight_mode, int32_t device, int32_t *V, int64_t *E,
+                       int32_t **d_rowptr, int32_t **d_col, float **d_w);
+void lv_free_device(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,86 @@
+"""Host-side parts of the engine library (no GPU): the MTX reader against
+the oracle's restatement of readInputData, writers, the verbose printer and
+the generators against their numpy restatement."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+
+def test_generators_match_numpy(lvb, gnp):
+    for sc, seed in ((6, 1), (10, 2), (13, 7)):
+        a = gnp.rmat(sc, seed=seed)
+        b = lvb.gen_rmat(sc, seed=seed)
+        for x, y in zip(a, (b.rowptr, b.col, b.w)):
+            assert np.array_equal(x, y)
+    a = gnp.planted(3000, 20, 12.0, 3.0, 4, "uniform")
+    b = lvb.gen_planted(3000, 20, 12.0, 3.0, 4, "uniform")
+    for x, y in zip(a, (b.rowptr, b.col, b.w)):
+        assert np.array_equal(x, y)
+
+
+def test_rmat_weights_on_grid(lvb):
+    g = lvb.gen_rmat(10)
+    w = g.w.astype(np.float64)
+    assert w.min() >= 0.5 and w.max() < 1.5
+    assert np.all(w * 2 ** 24 == np.round(w * 2 ** 24))
+
+
+@pytest.mark.parametrize("kind", ["planted", "rmat"])
+def test_mtx_roundtrip_and_reader_parity(lvb, orc, tmp_path, kind):
+    g = lvb.gen_planted(500, 8, 10.0, 2.0, 1, "uniform") if kind == "planted" else lvb.gen_rmat(9)
+    p = str(tmp_path / "g.mtx")
+    lvb.write_mtx(p, g)
+    r = lvb.read_mtx(p)
+    rp, cl, w, m = orc.read_mtx(p)
+    assert np.array_equal(r.rowptr, rp) and np.array_equal(r.col, cl) and np.array_equal(r.w, w)
+    assert r.m_ref == m
+    # same graph as the generator's (row order differs: file order)
+    for v in range(g.V):
+        a = sorted(zip(g.col[g.rowptr[v]:g.rowptr[v + 1]], g.w[g.rowptr[v]:g.rowptr[v + 1]]))
+        b = sorted(zip(r.col[r.rowptr[v]:r.rowptr[v + 1]], r.w[r.rowptr[v]:r.rowptr[v + 1]]))
+        assert a == b
+
+
+def test_reader_edge_cases(lvb, orc, tmp_path):
+    p = tmp_path / "e.mtx"
+    p.write_text("%%MatrixMarket matrix coordinate real symmetric\n%c\n\n3 3 3\n1 1 4\n3 1 1e-3\n2 3 7\n")
+    r = lvb.read_mtx(str(p))
+    rp, cl, w, m = orc.read_mtx(str(p))
+    assert np.array_equal(r.rowptr, rp) and np.array_equal(r.col, cl) and np.array_equal(r.w, w)
+    assert list(r.rowptr) == [0, 2, 3, 5]
+    p2 = tmp_path / "pat.mtx"
+    p2.write_text("%%MatrixMarket matrix coordinate pattern symmetric\n3 3 2\n2 1\n3 2\n")
+    r2 = lvb.read_mtx(str(p2))
+    assert list(r2.w) == [1.0] * 4
+    p3 = tmp_path / "bad.mtx"
+    p3.write_text("%%MatrixMarket matrix coordinate real symmetric\n3 3 2\n2 1 1\n")
+    with pytest.raises(lvb.LouvainError):
+        lvb.read_mtx(str(p3))
+    p4 = tmp_path / "range.mtx"
+    p4.write_text("%%MatrixMarket matrix coordinate real symmetric\n3 3 1\n4 1 1\n")
+    with pytest.raises(lvb.LouvainError):
+        lvb.read_mtx(str(p4))
+    with pytest.raises(lvb.LouvainError):
+        lvb.read_mtx(str(tmp_path / "missing.mtx"))
+    p5 = tmp_path / "empty.mtx"
+    p5.write_text("%%MatrixMarket matrix coordinate real symmetric\n0 0 0\n")
+    r5 = lvb.read_mtx(str(p5))
+    assert r5.V == 0 and r5.E == 0
+
+
+def test_print_communities_format(lvb, tmp_path):
+    # printOriginalToCommunity: V_final, then "c+1 members+1..." for every
+    # community id (empty ones included), members in increasing id
+    p = str(tmp_path / "map.txt")
+    lvb.print_communities(np.array([2, 0, 2, 0, 2], np.int32), 4, p)
+    assert open(p).read() == "4\n1 2 4\n2\n3 1 3 5\n4\n"
+
+
+def test_cli_usage(lvb):
+    r = subprocess.run([lvb.CLI_PATH], capture_output=True, text=True)
+    assert r.returncode == 1
+    assert r.stdout == "Usage: ./gpulouvain -f mtx-matrix-file -g min-gain [-v]\n"
+    r = subprocess.run([lvb.CLI_PATH, "-f", "x.mtx"], capture_output=True, text=True)
+    assert r.returncode == 1
