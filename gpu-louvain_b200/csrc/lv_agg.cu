@@ -43,15 +43,29 @@ __global__ void label_kernel(const int32_t *__restrict__ comm, const int32_t *__
         lab[v] = newid[comm[v]];
 }
 
+// Vertices grouped by community: one warp-aggregated cursor increment per
+// distinct community in the warp (a giant community would otherwise
+// serialise on its cursor).
 __global__ void members_kernel(const int32_t *__restrict__ comm, const int32_t *__restrict__ mstart,
-                               const int32_t *__restrict__ rowptr, int32_t V, int32_t *cursor,
+                               const int32_t *__restrict__ rowptr, const int32_t *__restrict__ rowend,
+                               int32_t V, int32_t *cursor,
                                int32_t *members, int32_t *mslot, int32_t *degm) {
-    for (int32_t v = blockIdx.x * 256 + threadIdx.x; v < V; v += gridDim.x * 256) {
-        const int32_t c = comm[v];
-        const int32_t m = mstart[c] + atomicAdd(cursor + c, 1);
-        members[m] = v;
-        mslot[v] = m;
-        degm[m] = rowptr[v + 1] - rowptr[v];
+    const int lane = threadIdx.x & 31;
+    for (int32_t base = blockIdx.x * 256; base < V; base += gridDim.x * 256) {
+        const int32_t v = base + threadIdx.x;
+        const bool valid = v < V;
+        const int32_t c = valid ? comm[v] : -1;
+        const unsigned peers = __match_any_sync(FULL, c);
+        const int leader = __ffs(peers) - 1;
+        int32_t pos = 0;
+        if (lane == leader && valid) pos = atomicAdd(cursor + c, __popc(peers));
+        pos = __shfl_sync(FULL, pos, leader);
+        if (valid) {
+            const int32_t m = mstart[c] + pos + __popc(peers & ((1u << lane) - 1u));
+            members[m] = v;
+            mslot[v] = m;
+            degm[m] = rowend[v] - rowptr[v];
+        }
     }
 }
 
@@ -67,7 +81,7 @@ __global__ void __launch_bounds__(256) permute_group_kernel(GraphView<WT> g,
     const int32_t idx = blockIdx.x * (256 / G) + grp;
     if (idx >= n) return;
     const int32_t v = list[idx];
-    const int32_t r0 = g.rowptr[v], r1 = g.rowptr[v + 1];
+    const int32_t r0 = g.rowptr[v], r1 = g.rowend[v];
     const int32_t dst = P[mslot[v]] - r0;
     for (int32_t e = r0 + lane; e < r1; e += G) {
         vkey[dst + e] = lab[__ldg(g.col + e)];
@@ -84,7 +98,7 @@ __global__ void __launch_bounds__(T) permute_cta_kernel(GraphView<WT> g,
                                                         int32_t n, int32_t *vkey, u64 *vw) {
     for (int32_t idx = blockIdx.x; idx < n; idx += gridDim.x) {
         const int32_t v = list[idx];
-        const int32_t r0 = g.rowptr[v], r1 = g.rowptr[v + 1];
+        const int32_t r0 = g.rowptr[v], r1 = g.rowend[v];
         const int32_t dst = P[mslot[v]] - r0;
         for (int32_t e = r0 + threadIdx.x; e < r1; e += T) {
             vkey[dst + e] = lab[__ldg(g.col + e)];
@@ -184,6 +198,14 @@ __global__ void __launch_bounds__(256) merge_group_kernel(const int32_t *__restr
         c = clist[idx];
         a = P[mstart[c]];
         b = P[mstart[c + 1]];
+    }
+    if (G == 32) {
+        for (int32_t base = a; base < b; base += 32) {
+            const int32_t i = base + lane;
+            const bool valid = i < b;
+            warp_insert(keys, vals, LG, valid, valid ? vkey[i] : 0, valid ? vw[i] : 0, err);
+        }
+    } else {
         for (int32_t i = a + lane; i < b; i += G) table_insert(keys, vals, LG, vkey[i], vw[i], err);
     }
     __syncwarp();
@@ -230,7 +252,11 @@ __global__ void __launch_bounds__(T) merge_cta_kernel(const int32_t *__restrict_
         int lg = ceil_log2_i(2 * (int64_t)(b - a));
         lg = lg < 3 ? 3 : lg;
         const int cap = 1 << lg;
-        for (int32_t i = a + threadIdx.x; i < b; i += T) table_insert(keys, vals, lg, vkey[i], vw[i], err);
+        for (int32_t base = a; base < b; base += T) {
+            const int32_t i = base + threadIdx.x;
+            const bool valid = i < b;
+            warp_insert(keys, vals, lg, valid, valid ? vkey[i] : 0, valid ? vw[i] : 0, err);
+        }
         __syncthreads();
         for (int s = threadIdx.x; s < cap; s += T) {
             const int32_t key = keys[s];
@@ -253,21 +279,38 @@ __global__ void __launch_bounds__(T) merge_cta_kernel(const int32_t *__restrict_
     }
 }
 
-// Global-table merge for communities whose degree bound exceeds 4096.
-__global__ void __launch_bounds__(256) mergeg_insert_kernel(HubGlobal hg,
-                                                            const int32_t *__restrict__ mstart,
-                                                            const int32_t *__restrict__ P,
-                                                            const int32_t *__restrict__ vkey,
-                                                            const u64 *__restrict__ vw, int *err) {
+// Global-table merge for communities whose degree bound exceeds 4096: one CTA
+// per chunk of HG_EDGE_CHUNK entries, reduced first in a chunk-local shared
+// table (intra-community entries all carry the community's own key), then
+// added once per distinct key to the community's global table.
+__global__ void __launch_bounds__(HG_INSERT_THREADS) mergeg_insert_kernel(
+    HubGlobal hg, const int32_t *__restrict__ mstart, const int32_t *__restrict__ P,
+    const int32_t *__restrict__ vkey, const u64 *__restrict__ vw, int *err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int LCAP = 2 * HG_EDGE_CHUNK;
+    constexpr int LLG = ilog2_c(LCAP);
+    u64 *lvals = reinterpret_cast<u64 *>(smem_raw);
+    int32_t *lkeys = reinterpret_cast<int32_t *>(lvals + LCAP);
+    for (int s = threadIdx.x; s < LCAP; s += HG_INSERT_THREADS) { lkeys[s] = -1; lvals[s] = 0; }
+    __syncthreads();
     const int32_t h = hg.echunk_hub[blockIdx.x];
     const int32_t c = hg.hubs[h];
     const int32_t b = P[mstart[c + 1]];
     const int32_t i0 = P[mstart[c]] + hg.echunk_e0[blockIdx.x];
     const int32_t i1 = min(i0 + HG_EDGE_CHUNK, b);
+    for (int32_t base = i0; base < i1; base += HG_INSERT_THREADS) {
+        const int32_t i = base + threadIdx.x;
+        const bool valid = i < i1;
+        warp_insert(lkeys, lvals, LLG, valid, valid ? vkey[i] : 0, valid ? vw[i] : 0, err);
+    }
+    __syncthreads();
     int32_t *keys = hg.keys + hg.tbl_off[h];
     u64 *vals = hg.vals + hg.tbl_off[h];
     const int lg = hg.tbl_lg[h];
-    for (int32_t i = i0 + threadIdx.x; i < i1; i += 256) table_insert(keys, vals, lg, vkey[i], vw[i], err);
+    for (int s = threadIdx.x; s < LCAP; s += HG_INSERT_THREADS) {
+        const int32_t k = lkeys[s];
+        if (k >= 0) table_insert(keys, vals, lg, k, lvals[s], err);
+    }
 }
 
 __global__ void __launch_bounds__(256) mergeg_emit_kernel(HubGlobal hg,
@@ -314,30 +357,15 @@ __global__ void zero_rowcnt_kernel(HubGlobal hg, const int32_t *__restrict__ new
         rowcnt[newid[hg.hubs[h]]] = 0;
 }
 
-// Compaction: each thread copies 8 consecutive output entries; the row of
-// the first is found by binary search over the new offsets.
-__global__ void __launch_bounds__(256) compact_kernel(const int32_t *__restrict__ rowptr_new,
-                                                      int32_t Vn, int64_t En,
-                                                      const int32_t *__restrict__ epos_new,
-                                                      const int32_t *__restrict__ vkey,
-                                                      const u64 *__restrict__ vw, int32_t *col_out,
-                                                      u64 *w_out) {
-    const int64_t t = (int64_t)blockIdx.x * 256 + threadIdx.x;
-    int64_t i = t * 8;
-    if (i >= En) return;
-    // largest r with rowptr_new[r] <= i
-    int32_t lo = 0, hi = Vn;
-    while (hi - lo > 1) {
-        const int32_t mid = (lo + hi) >> 1;
-        if ((int64_t)rowptr_new[mid] <= i) lo = mid; else hi = mid;
-    }
-    int32_t r = lo;
-    const int64_t iend = min(i + 8, En);
-    for (; i < iend; ++i) {
-        while ((int64_t)rowptr_new[r + 1] <= i) ++r;
-        const int64_t src = (int64_t)epos_new[r] + (i - rowptr_new[r]);
-        col_out[i] = vkey[src];
-        w_out[i] = vw[src];
+// Rows of the next level stay where the merge wrote them: row c' spans
+// [epos_new[c'], epos_new[c'] + newdeg[c']).
+__global__ void row_bounds_kernel(const int32_t *__restrict__ epos_new,
+                                  const int32_t *__restrict__ newdeg, int32_t Vn, int32_t *start,
+                                  int32_t *end) {
+    for (int32_t c = blockIdx.x * 256 + threadIdx.x; c < Vn; c += gridDim.x * 256) {
+        const int32_t a = epos_new[c];
+        start[c] = a;
+        end[c] = a + newdeg[c];
     }
 }
 
@@ -352,6 +380,7 @@ void init_agg_attributes() {
                          A3_CAP * 12);
     cudaFuncSetAttribute(merge_cta_kernel<A4_T, A4_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          A4_CAP * 12);
+    cudaFuncSetAttribute(mergeg_insert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HG_INSERT_SMEM);
     int o3 = 0, o4 = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, merge_cta_kernel<A3_T, A3_CAP>, A3_T, A3_CAP * 12);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o4, merge_cta_kernel<A4_T, A4_CAP>, A4_T, A4_CAP * 12);
@@ -363,15 +392,16 @@ void init_agg_attributes() {
 //   flag -> newid (scan, total in scalars[0]), lab, mstart (scan of size),
 //   members / mslot / degm, P (scan of degm, total in scalars[1]),
 //   class counts in scalars[2..2+NAC).
-void agg_prepare(const int32_t *rowptr, const int32_t *comm, const int32_t *size, int32_t V,
-                 AggBuffers &ab, int32_t *mslot, int32_t *degm, int32_t *P, cudaStream_t s) {
+void agg_prepare(const int32_t *rowptr, const int32_t *rowend, const int32_t *comm,
+                 const int32_t *size, int32_t V, AggBuffers &ab, int32_t *mslot, int32_t *degm,
+                 int32_t *P, cudaStream_t s) {
     flag_kernel<<<grid_for(V), 256, 0, s>>>(size, V, ab.flag); note_launches(1);
     scan_exclusive_i32(ab.flag, ab.flag, V, ab.scalars + 0, ab.scan_tmp, s);
     label_kernel<<<grid_for(V), 256, 0, s>>>(comm, ab.flag, V, ab.lab); note_launches(1);
     scan_exclusive_i32(size, ab.mstart, V, ab.mstart + V, ab.scan_tmp, s);
     cudaMemsetAsync(ab.cursor, 0, sizeof(int32_t) * (size_t)V, s);
-    members_kernel<<<grid_for(V), 256, 0, s>>>(comm, ab.mstart, rowptr, V, ab.cursor, ab.members,
-                                                mslot, degm); note_launches(1);
+    members_kernel<<<grid_for(V), 256, 0, s>>>(comm, ab.mstart, rowptr, rowend, V, ab.cursor,
+                                                ab.members, mslot, degm); note_launches(1);
     scan_exclusive_i32(degm, P, V, P + V, ab.scan_tmp, s);
     cudaMemsetAsync(ab.scalars + 2, 0, sizeof(int32_t) * NAC, s);
     agg_class_count_kernel<<<grid_for(V), 256, 0, s>>>(size, ab.mstart, P, V, ab.scalars + 2); note_launches(1);
@@ -444,18 +474,15 @@ void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *
                       u64 *vw, int *err, cudaStream_t s) {
     if (hg.nhubs <= 0) return;
     zero_rowcnt_kernel<<<grid_for(hg.nhubs), 256, 0, s>>>(hg, ab.flag, ab.cursor); note_launches(1);
-    mergeg_insert_kernel<<<hg.n_echunks, 256, 0, s>>>(hg, ab.mstart, P, vkey, vw, err); note_launches(1);
+    mergeg_insert_kernel<<<hg.n_echunks, HG_INSERT_THREADS, HG_INSERT_SMEM, s>>>(hg, ab.mstart, P, vkey, vw, err); note_launches(1);
     mergeg_emit_kernel<<<hg.n_schunks, 256, 0, s>>>(hg, ab.mstart, P, ab.flag, vkey, vw, ab.cursor); note_launches(1);
     mergeg_finish_kernel<<<grid_for(hg.nhubs), 256, 0, s>>>(hg, ab.mstart, P, ab.flag, ab.cursor,
                                                             ab.newdeg, ab.epos_new); note_launches(1);
 }
 
-void agg_compact(const int32_t *rowptr_new, int32_t Vn, int64_t En, const AggBuffers &ab,
-                 const int32_t *vkey, const u64 *vw, int32_t *col_out, u64 *w_out, cudaStream_t s) {
-    if (En <= 0) return;
-    const int64_t threads = (En + 7) / 8;
-    compact_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(rowptr_new, Vn, En, ab.epos_new,
-                                                                     vkey, vw, col_out, w_out); note_launches(1);
+void agg_row_bounds(const AggBuffers &ab, int32_t Vn, int32_t *start, int32_t *end, cudaStream_t s) {
+    if (Vn <= 0) return;
+    row_bounds_kernel<<<grid_for(Vn), 256, 0, s>>>(ab.epos_new, ab.newdeg, Vn, start, end); note_launches(1);
 }
 
 }  // namespace lv

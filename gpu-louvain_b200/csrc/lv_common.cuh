@@ -62,6 +62,8 @@ enum DevErr { DEVERR_HASH_FULL = 1, DEVERR_BAD_STATE = 2 };
 
 __host__ __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
 
+__host__ __device__ constexpr int ilog2_c(int x) { return x <= 1 ? 0 : 1 + ilog2_c(x >> 1); }
+
 __host__ __device__ __forceinline__ int ceil_log2_i(int64_t x) {
     int r = 0;
     while ((int64_t(1) << r) < x) r++;
@@ -82,9 +84,13 @@ __device__ __forceinline__ u64 wfix(const float *w, int64_t e, double scale) {
 }
 __device__ __forceinline__ u64 wfix(const u64 *w, int64_t e, double) { return __ldg(w + e); }
 
+// A level's graph: row v is col/w[rowptr[v] .. rowend[v]).  Level 0 is a
+// plain CSR (rowend = rowptr + 1); aggregated levels keep each merged row
+// where the merge wrote it, so rows need not be contiguous.
 template <typename WT>
 struct GraphView {
     const int32_t *rowptr;
+    const int32_t *rowend;
     const int32_t *col;
     const WT *w;
     double scale;   // 2^scale (used for float weights only)
@@ -121,6 +127,32 @@ __device__ __forceinline__ void table_insert(int32_t *keys, u64 *vals, int lg, i
     atomicOr(err, DEVERR_HASH_FULL);
 }
 
+// Exact sum of a uint64 over the lanes in `mask` (redux.sync adds 32-bit
+// values): the value is split into 22/22/20-bit slices whose 32-lane sums
+// cannot overflow 32 bits.  Lanes of different masks may call it together.
+__device__ __forceinline__ u64 redux_add_u64(unsigned mask, u64 x) {
+    const unsigned p0 = (unsigned)(x & 0x3FFFFFull);
+    const unsigned p1 = (unsigned)((x >> 22) & 0x3FFFFFull);
+    const unsigned p2 = (unsigned)(x >> 44);
+    const u64 s0 = __reduce_add_sync(mask, p0);
+    const u64 s1 = __reduce_add_sync(mask, p1);
+    const u64 s2 = __reduce_add_sync(mask, p2);
+    return s0 + (s1 << 22) + (s2 << 44);
+}
+
+// Warp-aggregated insert: every lane of the warp calls it (uniformly);
+// valid lanes holding the same key first combine their weights, and one
+// lane per distinct key inserts.  A key shared by many neighbours (the common
+// case once communities form) then costs one atomic per warp instead of 32.
+__device__ __forceinline__ void warp_insert(int32_t *keys, u64 *vals, int lg, bool valid,
+                                            int32_t key, u64 w, int *err) {
+    const unsigned act = __ballot_sync(FULL, valid);
+    if (!valid) return;
+    const unsigned peers = __match_any_sync(act, key);
+    const u64 sum = redux_add_u64(peers, w);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) table_insert(keys, vals, lg, key, sum, err);
+}
+
 // Candidate ordering of computeMove: larger gain wins, equal gains go to the
 // lower community id (modularity_optimisation.cu:157,169,182).
 __device__ __forceinline__ bool better(i128 g1, int32_t c1, i128 g2, int32_t c2) {
@@ -138,23 +170,48 @@ struct MoveCtx {
     u64 sown;
 };
 
+// Running best of one thread (or group): gain, community, and the summed
+// weight e_best to that community (used for the exact modularity update);
+// e_own is the weight to the vertex's own community.
+struct Best {
+    i128 g;
+    int32_t c;
+    u64 eb;
+    u64 eo;
+};
+
+__device__ __forceinline__ Best best_init(int32_t own) {
+    Best b;
+    b.g = 0;
+    b.c = own;
+    b.eb = 0;
+    b.eo = 0;
+    return b;
+}
+
 __device__ __forceinline__ void eval_candidate(int32_t c, u64 ec, const MoveCtx &m, u64 T,
                                                const u64 *__restrict__ S,
-                                               const int32_t *__restrict__ size, i128 &best_g,
-                                               int32_t &best_c, u64 &e_own) {
-    if (c == m.own) { e_own = ec; return; }
+                                               const int32_t *__restrict__ size, Best &b) {
+    if (c == m.own) { b.eo = ec; return; }
     if (m.own_single && c > m.own && size[c] == 1) return;
     const i64 d = (i64)m.sown - (i64)m.kv - (i64)S[c];
     const i128 g = (i128)((u128)T * (u128)ec) + (i128)(i64)m.kv * (i128)d;
-    if (better(g, c, best_g, best_c)) { best_g = g; best_c = c; }
+    if (better(g, c, b.g, b.c)) { b.g = g; b.c = c; b.eb = ec; }
 }
 
 // Move rule (modularity_optimisation.cu:192): move iff g_best - e_own/M > 0,
-// i.e. G_best - T * e_own > 0.
-__device__ __forceinline__ int32_t move_decision(i128 best_g, int32_t best_c, u64 e_own, u64 T,
-                                                 int32_t own) {
-    const i128 stay = (i128)((u128)T * (u128)e_own);
-    return (best_g - stay > 0) ? best_c : own;
+// i.e. G_best - T * e_own > 0.  *delta receives the mover's contribution to
+// sum_i e_{i->C(i)} when none of its neighbours moves in the same sub-round,
+// 2 (e_best - e_own) as a wrapping uint64 (corrected for co-moving neighbours
+// by the correction kernel).
+__device__ __forceinline__ int32_t move_decision(const Best &b, u64 T, int32_t own, u64 *delta) {
+    const i128 stay = (i128)((u128)T * (u128)b.eo);
+    if (b.g - stay > 0) {
+        *delta = 2 * (b.eb - b.eo);
+        return b.c;
+    }
+    *delta = 0;
+    return own;
 }
 
 __device__ __forceinline__ i128 shfl_xor_i128(i128 x, int m, int width) {
@@ -165,14 +222,15 @@ __device__ __forceinline__ i128 shfl_xor_i128(i128 x, int m, int width) {
 }
 
 // Butterfly reduction inside aligned groups of `width` lanes; every lane of
-// the group ends with the group's best (g, c) and summed e_own.
-__device__ __forceinline__ void group_reduce_best(i128 &g, int32_t &c, u64 &e, int width) {
+// the group ends with the group's best (g, c, e_best) and summed e_own.
+__device__ __forceinline__ void group_reduce_best(Best &b, int width) {
     for (int off = width >> 1; off > 0; off >>= 1) {
-        i128 og = shfl_xor_i128(g, off, width);
-        int32_t oc = __shfl_xor_sync(FULL, c, off, width);
-        u64 oe = __shfl_xor_sync(FULL, e, off, width);
-        if (better(og, oc, g, c)) { g = og; c = oc; }
-        e += oe;
+        const i128 og = shfl_xor_i128(b.g, off, width);
+        const int32_t oc = __shfl_xor_sync(FULL, b.c, off, width);
+        const u64 ob = __shfl_xor_sync(FULL, b.eb, off, width);
+        const u64 oe = __shfl_xor_sync(FULL, b.eo, off, width);
+        if (better(og, oc, b.g, b.c)) { b.g = og; b.c = oc; b.eb = ob; }
+        b.eo += oe;
     }
 }
 

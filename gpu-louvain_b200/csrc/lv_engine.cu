@@ -18,8 +18,9 @@
 
 namespace lv {
 void init_agg_attributes();
-void agg_prepare(const int32_t *rowptr, const int32_t *comm, const int32_t *size, int32_t V,
-                 AggBuffers &ab, int32_t *mslot, int32_t *degm, int32_t *P, cudaStream_t s);
+void agg_prepare(const int32_t *rowptr, const int32_t *rowend, const int32_t *comm,
+                 const int32_t *size, int32_t V, AggBuffers &ab, int32_t *mslot, int32_t *degm,
+                 int32_t *P, cudaStream_t s);
 void agg_classify(const int32_t *size, int32_t V, AggBuffers &ab, const int32_t *P,
                   const int32_t *offsets, cudaStream_t s);
 template <typename WT>
@@ -32,10 +33,9 @@ void agg_merge_class(int acls, const AggBuffers &ab, const int32_t *P, const int
                      int32_t n, int32_t *vkey, u64 *vw, int *err, int sms, cudaStream_t s);
 void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *P, int32_t *vkey,
                       u64 *vw, int *err, cudaStream_t s);
-void agg_compact(const int32_t *rowptr_new, int32_t Vn, int64_t En, const AggBuffers &ab,
-                 const int32_t *vkey, const u64 *vw, int32_t *col_out, u64 *w_out, cudaStream_t s);
-void launch_gather_degrees(const int32_t *rowptr, const int32_t *list, int32_t n, int32_t *out,
-                           cudaStream_t s);
+void agg_row_bounds(const AggBuffers &ab, int32_t Vn, int32_t *start, int32_t *end, cudaStream_t s);
+void launch_gather_degrees(const int32_t *rowptr, const int32_t *rowend, const int32_t *list,
+                           int32_t n, int32_t *out, cudaStream_t s);
 void launch_gather_cdeg(const int32_t *mstart, const int32_t *P, const int32_t *list, int32_t n,
                         int32_t *out, cudaStream_t s);
 }  // namespace lv
@@ -49,9 +49,10 @@ constexpr int NAC = 5;   // aggregation merge classes (lv_agg.cu)
 constexpr int SCRATCH_OFF = CLASS_COUNT_WORDS + NCLS + 8;
 
 struct Totals {
-    u64 e_own;
-    u64 s2[2];   // hi, lo
+    u64 e_own;   // full pass: sum_i e_{i->C(i)}
+    u64 s2[2];   // hi, lo of sum_C Sigma_tot^2
     u64 moves;
+    u64 dE;      // exact change of e_own over the sweep (wrapping)
     int err;
     int pad;
 };
@@ -92,10 +93,13 @@ struct lv_handle {
     int level = 0;
     int32_t V = 0;
     int64_t E = 0;
-    int32_t *cur_rowptr = nullptr, *cur_col = nullptr;
+    // current level: row v = cur_col/cur_w[cur_rowptr[v] .. cur_rowend[v])
+    int32_t *cur_rowptr = nullptr, *cur_rowend = nullptr, *cur_col = nullptr;
     u64 *cur_w = nullptr;   // nullptr at level 0 (float input weights)
 
-    int32_t *lvl_rowptr[2] = {nullptr, nullptr};
+    // aggregated levels, ping-pong: rows stay where the merge wrote them
+    int32_t *lvl_start[2] = {nullptr, nullptr};
+    int32_t *lvl_end[2] = {nullptr, nullptr};
     int32_t *lvl_col[2] = {nullptr, nullptr};
     u64 *lvl_w[2] = {nullptr, nullptr};
     int cur_buf = -1;
@@ -115,8 +119,6 @@ struct lv_handle {
     bool agg_ready = false;
     AggBuffers ab{};
     int32_t *mslot = nullptr, *degm = nullptr, *P = nullptr;
-    int32_t *vkey = nullptr;
-    u64 *vw = nullptr;
 
     Totals *tot_d = nullptr;
     Totals *tot_h = nullptr;
@@ -125,6 +127,9 @@ struct lv_handle {
     lv_stats st{};
     lv_class_stats cst{};
     long long launch_base = 0;
+    // sum_i e_{i->C(i)} of the current state, maintained exactly across sweeps
+    u64 e_own_cur = 0;
+    bool e_own_valid = false;
     std::vector<cudaEvent_t> ev_free;
     std::vector<Pending> pend;
 };
@@ -243,11 +248,11 @@ template <typename WT>
 GraphView<WT> view_of(lv_handle *h);
 template <>
 GraphView<float> view_of<float>(lv_handle *h) {
-    return GraphView<float>{h->cur_rowptr, h->cur_col, h->in_w, h->scale_d};
+    return GraphView<float>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->in_w, h->scale_d};
 }
 template <>
 GraphView<u64> view_of<u64>(lv_handle *h) {
-    return GraphView<u64>{h->cur_rowptr, h->cur_col, h->cur_w, h->scale_d};
+    return GraphView<u64>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->cur_w, h->scale_d};
 }
 
 StateView state_of(lv_handle *h) {
@@ -301,10 +306,10 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
     hub_s0[n] = (int32_t)sch_hub.size();
     LV_TRY(ensure_tables(h, (size_t)total));
     const size_t ne = ech_hub.size(), ns = sch_hub.size();
-    // packed: ids | lg | ech_hub | ech_e0 | sch_hub | sch_s0 | hub_s0 | res_c | (8-aligned) off | res_g | res_e
+    // packed: ids | lg | ech_hub | ech_e0 | sch_hub | sch_s0 | hub_s0 | res_c | (8-aligned) off | res_g | res_e | res_b
     size_t i32_count = (size_t)n + n + ne + ne + ns + ns + (n + 1) + ns;
     size_t i32_bytes = ((i32_count * 4 + 15) / 16) * 16;
-    size_t bytes = i32_bytes + (size_t)n * 8 + ns * 16 + ns * 8 + 64;
+    size_t bytes = i32_bytes + (size_t)n * 8 + ns * 16 + ns * 8 + ns * 8 + 64;
     if (bytes > L.dev_bytes) {
         if (L.dev) cudaFree(L.dev);
         L.dev = nullptr;
@@ -349,6 +354,7 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
     v.tbl_off = (const int64_t *)d8;
     v.res_g = (u64 *)(d8 + (size_t)n * 8);
     v.res_e = (u64 *)(d8 + (size_t)n * 8 + ns * 16);
+    v.res_b = (u64 *)(d8 + (size_t)n * 8 + ns * 24);
     v.keys = h->tbl_keys;
     v.vals = h->tbl_vals;
     L.ids = ids;
@@ -371,7 +377,7 @@ int compute_k(lv_handle *h) {
 int level_setup(lv_handle *h) {
     Timer t(h, 103);
     int32_t *counts = h->cls_scratch, *cursors = h->cls_scratch + CLASS_COUNT_WORDS;
-    launch_class_count(h->cur_rowptr, h->V, counts, h->stream);
+    launch_class_count(h->cur_rowptr, h->cur_rowend, h->V, counts, h->stream);
     LV_CUDA(h, cudaMemcpyAsync(h->small_h, counts, sizeof(int32_t) * CLASS_COUNT_WORDS,
                                cudaMemcpyDeviceToHost, h->stream));
     LV_TRY(sync(h));
@@ -381,7 +387,7 @@ int level_setup(lv_handle *h) {
         h->cls_off[c + 1] = h->cls_off[c] + h->small_h[c];
         h->cls_edges[c] = (int64_t)esum[c];
     }
-    launch_class_scatter(h->cur_rowptr, h->V, h->cls_off, cursors, h->list, h->stream);
+    launch_class_scatter(h->cur_rowptr, h->cur_rowend, h->V, h->cls_off, cursors, h->list, h->stream);
     if (h->level == 0) {
         LV_TRY(compute_k<float>(h));
     }
@@ -391,7 +397,8 @@ int level_setup(lv_handle *h) {
     std::vector<int32_t> ids(nh), deg(nh);
     if (nh > 0) {
         int32_t *dd = h->cls_scratch + SCRATCH_OFF;   // room reserved at create: V0 entries
-        launch_gather_degrees(h->cur_rowptr, h->list + h->cls_off[CLS_HG], nh, dd, h->stream);
+        launch_gather_degrees(h->cur_rowptr, h->cur_rowend, h->list + h->cls_off[CLS_HG], nh, dd,
+                              h->stream);
         LV_CUDA(h, cudaMemcpyAsync(ids.data(), h->list + h->cls_off[CLS_HG], sizeof(int32_t) * nh,
                                    cudaMemcpyDeviceToHost, h->stream));
         LV_CUDA(h, cudaMemcpyAsync(deg.data(), dd, sizeof(int32_t) * nh, cudaMemcpyDeviceToHost,
@@ -411,8 +418,9 @@ void enqueue_sweep(lv_handle *h) {
     GraphView<WT> g = view_of<WT>(h);
     StateView st = state_of(h);
     const double wbytes = sizeof(WT) == 4 ? 4.0 : 8.0;
+    u64 *dE = &h->tot_d->dE;
     Timer tm(h, 100);
-    int64_t sweep_edges = 0, sweep_verts = 0;
+    int64_t sweep_verts = 0;
     for (int b = 0; b < NBUCKETS; ++b) {
         const int c0 = b, c1 = (b < 6) ? b + 1 : NCLS;
         const int32_t lo = h->cls_off[c0], hi = h->cls_off[c1];
@@ -426,18 +434,21 @@ void enqueue_sweep(lv_handle *h) {
                 tc.edges = h->cls_edges[c];
                 tc.bytes = (8.0 + wbytes) * (double)h->cls_edges[c] + 20.0 * (double)n;
                 launch_move_class<WT>(c, g, st, h->list + h->cls_off[c], n, h->hub_move.view, h->di,
-                                      h->stream);
+                                      dE, h->stream);
                 tc.stop();
             } else {
                 launch_move_class<WT>(c, g, st, h->list + h->cls_off[c], n, h->hub_move.view, h->di,
-                                      h->stream);
+                                      dE, h->stream);
             }
         }
+        // exact modularity bookkeeping for neighbours that moved together
+        for (int c = c0; c < c1; ++c)
+            launch_correction<WT>(c, g, st, h->list + h->cls_off[c], h->cls_off[c + 1] - h->cls_off[c],
+                                  h->di, dE, h->stream);
         launch_commit(st, h->list + lo, hi - lo, &h->tot_d->moves, h->stream);
         sweep_verts += hi - lo;
     }
-    sweep_edges = h->E;
-    tm.bytes = (8.0 + wbytes) * (double)sweep_edges + 20.0 * (double)sweep_verts;
+    tm.bytes = (8.0 + wbytes) * (double)h->E + 20.0 * (double)sweep_verts;
     tm.stop();
     h->st.move_bytes += tm.bytes;
 }
@@ -478,23 +489,41 @@ int modularity(lv_handle *h, double *q) {
     LV_TRY(reset_totals(h));
     if (h->cur_w) enqueue_modularity<u64>(h); else enqueue_modularity<float>(h);
     LV_TRY(read_totals(h));
+    h->e_own_cur = h->tot_h->e_own;
+    h->e_own_valid = true;
     *q = q_from_totals(h->T, *h->tot_h);
     return LV_OK;
 }
 
-// One sweep followed by the modularity of the resulting state.
+// One sweep followed by the modularity of the resulting state.  The edge
+// pass of calculateModularity is replaced by the exact update of
+// sum_i e_{i->C(i)} accumulated by the move and correction kernels; only the
+// sum of Sigma_tot^2 is recomputed (a pass over V).
 int sweep_and_q(lv_handle *h, int64_t *moves, double *q) {
+    if (!h->e_own_valid) {
+        double q0;
+        LV_TRY(modularity(h, &q0));
+    }
     LV_TRY(reset_totals(h));
-    if (h->cur_w) {
-        enqueue_sweep<u64>(h);
-        enqueue_modularity<u64>(h);
-    } else {
-        enqueue_sweep<float>(h);
-        enqueue_modularity<float>(h);
+    if (h->cur_w) enqueue_sweep<u64>(h); else enqueue_sweep<float>(h);
+    {
+        Timer tm(h, 101);
+        launch_s2(h->S, h->V, h->tot_d->s2, h->stream);
+        tm.stop();
     }
     LV_TRY(read_totals(h));
-    *moves = (int64_t)h->tot_h->moves;
-    if (q) *q = q_from_totals(h->T, *h->tot_h);
+    h->e_own_cur += h->tot_h->dE;
+    Totals t = *h->tot_h;
+    t.e_own = h->e_own_cur;
+    *moves = (int64_t)t.moves;
+    const double q_inc = q_from_totals(h->T, t);
+    if (h->opts.verify) {
+        double q_full = 0;
+        LV_TRY(modularity(h, &q_full));
+        if (h->e_own_cur != t.e_own || q_full != q_inc)
+            return fail(h, LV_ERR_DEVICE, "incremental modularity differs from the full pass");
+    }
+    if (q) *q = q_inc;
     h->st.sweeps += 1;
     h->st.edge_sweeps += h->E;
     h->st.moves += *moves;
@@ -544,10 +573,9 @@ int ensure_agg(lv_handle *h) {
     LV_TRY(dalloc(h, &h->mslot, V + 1));
     LV_TRY(dalloc(h, &h->degm, V + 1));
     LV_TRY(dalloc(h, &h->P, V + 1));
-    LV_TRY(dalloc(h, &h->vkey, E));
-    LV_TRY(dalloc(h, &h->vw, E));
     for (int b = 0; b < 2; ++b) {
-        LV_TRY(dalloc(h, &h->lvl_rowptr[b], V + 1));
+        LV_TRY(dalloc(h, &h->lvl_start[b], V + 1));
+        LV_TRY(dalloc(h, &h->lvl_end[b], V + 1));
         LV_TRY(dalloc(h, &h->lvl_col[b], E));
         LV_TRY(dalloc(h, &h->lvl_w[b], E));
     }
@@ -560,7 +588,12 @@ int aggregate_t(lv_handle *h) {
     Timer tm(h, 102);
     AggBuffers &ab = h->ab;
     const int32_t V = h->V;
-    agg_prepare(h->cur_rowptr, h->comm, h->size, V, ab, h->mslot, h->degm, h->P, h->stream);
+    // the next level's rows are built in the other ping-pong buffer
+    const int nb = (h->cur_buf == 0) ? 1 : 0;
+    int32_t *vkey = h->lvl_col[nb];
+    u64 *vw = h->lvl_w[nb];
+    agg_prepare(h->cur_rowptr, h->cur_rowend, h->comm, h->size, V, ab, h->mslot, h->degm, h->P,
+                h->stream);
     LV_CUDA(h, cudaMemcpyAsync(h->small_h, ab.scalars, sizeof(int32_t) * (2 + NAC),
                                cudaMemcpyDeviceToHost, h->stream));
     LV_TRY(sync(h));
@@ -583,31 +616,32 @@ int aggregate_t(lv_handle *h) {
     GraphView<WT> g = view_of<WT>(h);
     for (int c = 0; c < NCLS; ++c)
         agg_permute<WT>(c, g, ab, h->mslot, h->P, h->list + h->cls_off[c],
-                        h->cls_off[c + 1] - h->cls_off[c], h->vkey, h->vw, h->di.sms, h->stream);
+                        h->cls_off[c + 1] - h->cls_off[c], vkey, vw, h->di.sms, h->stream);
     agg_new_vertices(h->size, h->S, V, ab, h->P, h->k, h->stream);
     for (int c = 0; c < NAC - 1; ++c)
-        agg_merge_class(c, ab, h->P, ab.clist + aoff[c], aoff[c + 1] - aoff[c], h->vkey, h->vw,
+        agg_merge_class(c, ab, h->P, ab.clist + aoff[c], aoff[c + 1] - aoff[c], vkey, vw,
                         &h->tot_d->err, h->di.sms, h->stream);
-    agg_merge_global(h->hub_agg.view, ab, h->P, h->vkey, h->vw, &h->tot_d->err, h->stream);
-    const int nb = (h->cur_buf == 0) ? 1 : 0;
-    int32_t *rp = h->lvl_rowptr[nb];
-    scan_exclusive_i32(ab.newdeg, rp, newV, rp + newV, ab.scan_tmp, h->stream);
-    LV_CUDA(h, cudaMemcpyAsync(h->small_h, rp + newV, sizeof(int32_t), cudaMemcpyDeviceToHost,
+    agg_merge_global(h->hub_agg.view, ab, h->P, vkey, vw, &h->tot_d->err, h->stream);
+    agg_row_bounds(ab, newV, h->lvl_start[nb], h->lvl_end[nb], h->stream);
+    // E' = number of stored entries (P is free again after the merges)
+    scan_exclusive_i32(ab.newdeg, h->P, newV, h->P + newV, ab.scan_tmp, h->stream);
+    LV_CUDA(h, cudaMemcpyAsync(h->small_h, h->P + newV, sizeof(int32_t), cudaMemcpyDeviceToHost,
                                h->stream));
+    launch_compose_map(h->orig2comm, ab.flag, h->V0, h->stream);
     LV_CUDA(h, cudaMemcpyAsync(h->tot_h, h->tot_d, sizeof(Totals), cudaMemcpyDeviceToHost, h->stream));
+    tm.stop();
     LV_TRY(sync(h));
     LV_TRY(check_device_error(h, h->tot_h->err));
     const int64_t newE = h->small_h[0];
-    agg_compact(rp, newV, newE, ab, h->vkey, h->vw, h->lvl_col[nb], h->lvl_w[nb], h->stream);
-    launch_compose_map(h->orig2comm, ab.flag, h->V0, h->stream);
-    tm.stop();
     h->cur_buf = nb;
-    h->cur_rowptr = rp;
+    h->cur_rowptr = h->lvl_start[nb];
+    h->cur_rowend = h->lvl_end[nb];
     h->cur_col = h->lvl_col[nb];
     h->cur_w = h->lvl_w[nb];
     h->V = newV;
     h->E = newE;
     h->level += 1;
+    h->e_own_valid = false;
     return level_setup(h);
 }
 
@@ -624,9 +658,11 @@ int to_level0(lv_handle *h) {
     h->V = h->V0;
     h->E = h->E0;
     h->cur_rowptr = h->in_rowptr;
+    h->cur_rowend = h->in_rowptr + 1;
     h->cur_col = h->in_col;
     h->cur_w = nullptr;
     h->cur_buf = -1;
+    h->e_own_valid = false;
     launch_iota_i32(h->orig2comm, h->V0, h->stream);
     return level_setup(h);
 }
@@ -765,8 +801,10 @@ int lv_destroy(lv_handle *h) {
     dfree(a.flag); dfree(a.cdeg); dfree(a.mstart); dfree(a.cursor); dfree(a.members);
     dfree(a.lab); dfree(a.clist); dfree(a.newdeg); dfree(a.epos_new); dfree(a.scan_tmp);
     dfree(a.scalars);
-    dfree(h->mslot); dfree(h->degm); dfree(h->P); dfree(h->vkey); dfree(h->vw);
-    for (int b = 0; b < 2; ++b) { dfree(h->lvl_rowptr[b]); dfree(h->lvl_col[b]); dfree(h->lvl_w[b]); }
+    dfree(h->mslot); dfree(h->degm); dfree(h->P);
+    for (int b = 0; b < 2; ++b) {
+        dfree(h->lvl_start[b]); dfree(h->lvl_end[b]); dfree(h->lvl_col[b]); dfree(h->lvl_w[b]);
+    }
     dfree(h->tot_d);
     if (h->tot_h) cudaFreeHost(h->tot_h);
     if (h->small_h) cudaFreeHost(h->small_h);
@@ -905,6 +943,7 @@ int lv_set_communities(lv_handle *h, const int32_t *comm) {
                                h->stream));
     LV_CUDA(h, cudaMemsetAsync(&h->tot_d->err, 0, sizeof(int), h->stream));
     launch_set_communities(tmp, h->comm, h->newc, h->size, h->k, h->S, h->V, &h->tot_d->err, h->stream);
+    h->e_own_valid = false;
     LV_TRY(read_totals(h));
     return LV_OK;
 }
@@ -920,26 +959,56 @@ int lv_get_level_info(lv_handle *h, int32_t *V, int64_t *E, int32_t *level) {
 int lv_get_csr(lv_handle *h, int32_t *rowptr, int32_t *col, int64_t *wfix) {
     if (!h) return LV_ERR_INVALID;
     cudaSetDevice(h->device);
-    if (rowptr)
-        LV_CUDA(h, cudaMemcpyAsync(rowptr, h->cur_rowptr, sizeof(int32_t) * ((size_t)h->V + 1),
-                                   cudaMemcpyDeviceToHost, h->stream));
-    if (col && h->E > 0)
-        LV_CUDA(h, cudaMemcpyAsync(col, h->cur_col, sizeof(int32_t) * (size_t)h->E,
-                                   cudaMemcpyDeviceToHost, h->stream));
-    if (wfix && h->E > 0) {
-        int64_t *tmp = nullptr;
-        LV_TRY(dalloc(h, &tmp, (size_t)h->E));
-        if (h->cur_w)
-            launch_weights_to_fixed<u64>(h->cur_w, h->E, h->scale_d, tmp, h->stream);
-        else
+    if (h->level == 0) {
+        if (rowptr)
+            LV_CUDA(h, cudaMemcpyAsync(rowptr, h->cur_rowptr, sizeof(int32_t) * ((size_t)h->V + 1),
+                                       cudaMemcpyDeviceToHost, h->stream));
+        if (col && h->E > 0)
+            LV_CUDA(h, cudaMemcpyAsync(col, h->cur_col, sizeof(int32_t) * (size_t)h->E,
+                                       cudaMemcpyDeviceToHost, h->stream));
+        if (wfix && h->E > 0) {
+            int64_t *tmp = nullptr;
+            LV_TRY(dalloc(h, &tmp, (size_t)h->E));
             launch_weights_to_fixed<float>(h->in_w, h->E, h->scale_d, tmp, h->stream);
-        cudaError_t e = cudaMemcpyAsync(wfix, tmp, sizeof(int64_t) * (size_t)h->E,
-                                        cudaMemcpyDeviceToHost, h->stream);
-        cudaStreamSynchronize(h->stream);
-        cudaFree(tmp);
-        if (e != cudaSuccess) return fail(h, LV_ERR_CUDA, cudaGetErrorString(e));
+            cudaError_t e = cudaMemcpyAsync(wfix, tmp, sizeof(int64_t) * (size_t)h->E,
+                                            cudaMemcpyDeviceToHost, h->stream);
+            cudaStreamSynchronize(h->stream);
+            cudaFree(tmp);
+            if (e != cudaSuccess) return fail(h, LV_ERR_CUDA, cudaGetErrorString(e));
+        }
+        return sync(h);
     }
-    return sync(h);
+    // aggregated level: gather the (possibly non-contiguous) rows on the host
+    const size_t V = (size_t)h->V;
+    std::vector<int32_t> st(V + 1), en(V + 1);
+    if (V) {
+        LV_CUDA(h, cudaMemcpyAsync(st.data(), h->cur_rowptr, sizeof(int32_t) * V, cudaMemcpyDeviceToHost,
+                                   h->stream));
+        LV_CUDA(h, cudaMemcpyAsync(en.data(), h->cur_rowend, sizeof(int32_t) * V, cudaMemcpyDeviceToHost,
+                                   h->stream));
+    }
+    LV_TRY(sync(h));
+    int32_t span = 0;
+    for (size_t v = 0; v < V; ++v) span = en[v] > span ? en[v] : span;
+    std::vector<int32_t> c((size_t)span);
+    std::vector<u64> w((size_t)span);
+    if (span) {
+        LV_CUDA(h, cudaMemcpyAsync(c.data(), h->cur_col, sizeof(int32_t) * (size_t)span,
+                                   cudaMemcpyDeviceToHost, h->stream));
+        LV_CUDA(h, cudaMemcpyAsync(w.data(), h->cur_w, sizeof(u64) * (size_t)span, cudaMemcpyDeviceToHost,
+                                   h->stream));
+    }
+    LV_TRY(sync(h));
+    int64_t at = 0;
+    for (size_t v = 0; v < V; ++v) {
+        if (rowptr) rowptr[v] = (int32_t)at;
+        for (int32_t e = st[v]; e < en[v]; ++e, ++at) {
+            if (col) col[at] = c[(size_t)e];
+            if (wfix) wfix[at] = (int64_t)w[(size_t)e];
+        }
+    }
+    if (rowptr) rowptr[V] = (int32_t)at;
+    return LV_OK;
 }
 
 int lv_get_scale(lv_handle *h, int32_t *scale, uint64_t *total_weight, int32_t *exact) {

@@ -9,6 +9,8 @@ namespace lv {
 // and slot chunks (evaluate kernel) so that one hub spreads over many CTAs.
 constexpr int HG_EDGE_CHUNK = 4096;
 constexpr int HG_SLOT_CHUNK = 4096;
+constexpr int HG_INSERT_THREADS = 512;
+constexpr int HG_INSERT_SMEM = 2 * HG_EDGE_CHUNK * 12;   // chunk-local table
 
 struct HubGlobal {
     int32_t nhubs = 0;
@@ -27,6 +29,7 @@ struct HubGlobal {
     u64 *res_g = nullptr;                 // [2 * n_schunks] best gain (lo, hi)
     int32_t *res_c = nullptr;             // [n_schunks] best community
     u64 *res_e = nullptr;                 // [n_schunks] e_own contribution
+    u64 *res_b = nullptr;                 // [n_schunks] weight to the best community
 };
 
 // Count of engine kernel launches (all handles, all devices of the process).
@@ -41,9 +44,15 @@ struct DeviceInfo {
 void init_kernel_attributes(DeviceInfo &di);
 
 // ---- move phase (lv_move.cu) ----
+// dE accumulates (wrapping uint64) each mover's 2 (e_best - e_own).
 template <typename WT>
 void launch_move_class(int cls, const GraphView<WT> &g, const StateView &st, const int32_t *list,
-                       int32_t n, const HubGlobal &hg, const DeviceInfo &di, cudaStream_t s);
+                       int32_t n, const HubGlobal &hg, const DeviceInfo &di, u64 *dE,
+                       cudaStream_t s);
+// Exact correction of dE for neighbours that moved in the same sub-round.
+template <typename WT>
+void launch_correction(int cls, const GraphView<WT> &g, const StateView &st, const int32_t *list,
+                       int32_t n, const DeviceInfo &di, u64 *dE, cudaStream_t s);
 void launch_commit(const StateView &st, const int32_t *list, int32_t n, u64 *moves,
                    cudaStream_t s);
 
@@ -64,9 +73,10 @@ void scan_exclusive_i32(const int32_t *in, int32_t *out, int64_t n, int32_t *tot
 // The count buffer holds CLASS_COUNT_WORDS int32: NCLS vertex counts, then
 // (8-byte aligned) NCLS uint64 edge totals.
 constexpr int CLASS_COUNT_WORDS = NCLS + (NCLS & 1) + 2 * NCLS;
-void launch_class_count(const int32_t *rowptr, int32_t V, int32_t *counts, cudaStream_t s);
-void launch_class_scatter(const int32_t *rowptr, int32_t V, const int32_t *offsets,
-                          int32_t *cursors, int32_t *list, cudaStream_t s);
+void launch_class_count(const int32_t *rowptr, const int32_t *rowend, int32_t V, int32_t *counts,
+                        cudaStream_t s);
+void launch_class_scatter(const int32_t *rowptr, const int32_t *rowend, int32_t V,
+                          const int32_t *offsets, int32_t *cursors, int32_t *list, cudaStream_t s);
 void launch_fill_i32(int32_t *p, int64_t n, int32_t v, cudaStream_t s);
 void launch_iota_i32(int32_t *p, int64_t n, cudaStream_t s);
 void launch_level_init(int32_t *comm, int32_t *newc, int32_t *size, const u64 *k, u64 *S,
@@ -98,8 +108,6 @@ struct AggBuffers {
     int32_t *epos_new;  // [V]   merged-row start per new vertex
     int32_t *scan_tmp;
     int32_t *scalars;   // [16]  device scalars (totals, counts)
-    int32_t *scol;      // [E]   merged rows (uncompacted)
-    u64 *sw;            // [E]
 };
 
 }  // namespace lv

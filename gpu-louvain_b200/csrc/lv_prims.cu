@@ -99,13 +99,14 @@ __global__ void __launch_bounds__(SCAN_THREADS) scan_apply_kernel(const int32_t 
 // counts[0..NCLS) = vertices per class; counts[NCLS..) reinterpreted as
 // uint64 edge totals per class.
 __global__ void __launch_bounds__(256) class_count_kernel(const int32_t *__restrict__ rowptr,
+                                                          const int32_t *__restrict__ rowend,
                                                           int32_t V, int32_t *counts) {
     __shared__ int32_t c[NCLS];
     __shared__ u64 es[NCLS];
     if (threadIdx.x < NCLS) { c[threadIdx.x] = 0; es[threadIdx.x] = 0; }
     __syncthreads();
     for (int32_t v = blockIdx.x * 256 + threadIdx.x; v < V; v += gridDim.x * 256) {
-        const int32_t d = rowptr[v + 1] - rowptr[v];
+        const int32_t d = rowend[v] - rowptr[v];
         const int cls = degree_class(d);
         if (cls >= 0) {
             atomicAdd(c + cls, 1);
@@ -125,12 +126,13 @@ struct ClassOffsets {
 };
 
 __global__ void __launch_bounds__(256) class_scatter_kernel(const int32_t *__restrict__ rowptr,
+                                                            const int32_t *__restrict__ rowend,
                                                             int32_t V, ClassOffsets offs,
                                                             int32_t *cursors, int32_t *list) {
     const int lane = threadIdx.x & 31;
     for (int32_t base = blockIdx.x * 256; base < V; base += gridDim.x * 256) {
         const int32_t v = base + threadIdx.x;
-        const int cls = v < V ? degree_class(rowptr[v + 1] - rowptr[v]) : -1;
+        const int cls = v < V ? degree_class(rowend[v] - rowptr[v]) : -1;
         const unsigned peers = __match_any_sync(FULL, cls);
         const int leader = __ffs(peers) - 1;
         int32_t pos = 0;
@@ -285,19 +287,20 @@ void scan_exclusive_i32(const int32_t *in, int32_t *out, int64_t n, int32_t *tot
     scan_apply_kernel<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, tmp); note_launches(1);
 }
 
-void launch_class_count(const int32_t *rowptr, int32_t V, int32_t *counts, cudaStream_t s) {
+void launch_class_count(const int32_t *rowptr, const int32_t *rowend, int32_t V, int32_t *counts,
+                        cudaStream_t s) {
     cudaMemsetAsync(counts, 0, sizeof(int32_t) * CLASS_COUNT_WORDS, s);
     if (V <= 0) return;
-    class_count_kernel<<<grid_for(V), 256, 0, s>>>(rowptr, V, counts); note_launches(1);
+    class_count_kernel<<<grid_for(V), 256, 0, s>>>(rowptr, rowend, V, counts); note_launches(1);
 }
 
-void launch_class_scatter(const int32_t *rowptr, int32_t V, const int32_t *offsets,
-                          int32_t *cursors, int32_t *list, cudaStream_t s) {
+void launch_class_scatter(const int32_t *rowptr, const int32_t *rowend, int32_t V,
+                          const int32_t *offsets, int32_t *cursors, int32_t *list, cudaStream_t s) {
     cudaMemsetAsync(cursors, 0, sizeof(int32_t) * NCLS, s);
     if (V <= 0) return;
     ClassOffsets o;
     for (int c = 0; c < NCLS; ++c) o.off[c] = offsets[c];
-    class_scatter_kernel<<<grid_for(V), 256, 0, s>>>(rowptr, V, o, cursors, list); note_launches(1);
+    class_scatter_kernel<<<grid_for(V), 256, 0, s>>>(rowptr, rowend, V, o, cursors, list); note_launches(1);
 }
 
 void launch_fill_i32(int32_t *p, int64_t n, int32_t v, cudaStream_t s) {
@@ -358,10 +361,11 @@ void launch_validate_csr(const int32_t *rowptr, const int32_t *col, int32_t V, i
 namespace lv {
 namespace {
 __global__ void gather_degrees_kernel(const int32_t *__restrict__ rowptr,
+                                      const int32_t *__restrict__ rowend,
                                       const int32_t *__restrict__ list, int32_t n, int32_t *out) {
     for (int32_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
         const int32_t v = list[i];
-        out[i] = rowptr[v + 1] - rowptr[v];
+        out[i] = rowend[v] - rowptr[v];
     }
 }
 __global__ void gather_cdeg_kernel(const int32_t *__restrict__ mstart, const int32_t *__restrict__ P,
@@ -373,10 +377,10 @@ __global__ void gather_cdeg_kernel(const int32_t *__restrict__ mstart, const int
 }
 }  // namespace
 
-void launch_gather_degrees(const int32_t *rowptr, const int32_t *list, int32_t n, int32_t *out,
-                           cudaStream_t s) {
+void launch_gather_degrees(const int32_t *rowptr, const int32_t *rowend, const int32_t *list,
+                           int32_t n, int32_t *out, cudaStream_t s) {
     if (n <= 0) return;
-    gather_degrees_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rowptr, list, n, out); note_launches(1);
+    gather_degrees_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rowptr, rowend, list, n, out); note_launches(1);
 }
 
 void launch_gather_cdeg(const int32_t *mstart, const int32_t *P, const int32_t *list, int32_t n,

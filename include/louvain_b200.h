@@ -45,7 +45,9 @@ typedef struct lv_opts {
     int32_t device;        /* CUDA device ordinal (default 0)              */
     int32_t max_sweeps;    /* per-level sweep cap, 0 = unlimited (default) */
     int32_t profile;       /* 1: time every kernel class with CUDA events  */
-    int32_t reserved[12];
+    int32_t verify;        /* 1: after every sweep, check the incrementally
+                              maintained modularity against a full pass    */
+    int32_t reserved[11];
 } lv_opts;
 
 /* Per-run counters; times in milliseconds (device time, CUDA events). */

@@ -4,9 +4,16 @@ Runs where oracle/_ref/gpulouvain_ref and oracle/_ref/ref_harness were built
 (`make -C oracle ref`, compiled from the reference sources) and a GPU is
 present.  For each small graph it records:
   <name>.mtx            the input (symmetric Matrix Market)
-  <name>.sweeps.bin     the reference's community vector after each of the
-                        first N sweeps (optimiseModularity called with a gain
-                        threshold that admits exactly one sweep per call)
+  <name>.sweeps_stock.bin  the community vector after each of the first N
+                        sweeps of the stock reference (optimiseModularity
+                        called with a gain threshold that admits exactly one
+                        sweep per call).  On B200 these show (almost) no moves:
+                        computeMove's final store races between lane 0 (the
+                        move) and the other lanes (the old community),
+                        modularity_optimisation.cu:192-196.
+  <name>.sweeps1.bin    the same sweeps with the reference's own move kernels
+                        launched at one thread per vertex (no racing lanes),
+                        orchestrated like optimiseModularity
   <name>.agg_in.bin     a community vector (the oracle's level-0 result)
   <name>.agg_out.bin    the reference's aggregateCommunities of that vector
   <name>.cli.txt        stdout of `gpulouvain -f <name>.mtx -g <gain> -v`
@@ -54,6 +61,8 @@ def quarter_weights(rowptr, col, seed):
 
 def cases():
     out = []
+    rp, cl, w = graphs_np.rmat(12, seed=2, weights="unit")
+    out.append(("rmat12_unit", rp, cl, w, 1e-6))
     rp, cl, w = graphs_np.planted(10000, 64, 16.0, 2.0, 0)
     out.append(("planted10k_s0", rp, cl, w, 0.01))
     rp, cl, w = graphs_np.planted(2000, 16, 12.0, 2.0, 1)
@@ -74,7 +83,9 @@ def main():
         write_mtx(mtx, rp, cl, w)
         # the reference reads the file back: use its CSR (file order) everywhere
         frp, fcl, fw, _ = oracle.read_mtx(mtx)
-        subprocess.run([HARNESS, "sweeps", mtx, str(NSWEEPS), os.path.join(out_dir, name + ".sweeps.bin")],
+        subprocess.run([HARNESS, "sweeps", mtx, str(NSWEEPS),
+                        os.path.join(out_dir, name + ".sweeps_stock.bin")], check=True)
+        subprocess.run([HARNESS, "sweeps1", mtx, str(NSWEEPS), os.path.join(out_dir, name + ".sweeps1.bin")],
                        check=True)
         o = oracle.Oracle(frp, fcl, fw)
         o.optimise_modularity(gain)
@@ -85,7 +96,8 @@ def main():
                            text=True)
         with open(os.path.join(out_dir, name + ".cli.txt"), "w") as f:
             f.write(r.stdout)
-        index.append({"name": name, "mtx": name + ".mtx", "sweeps": name + ".sweeps.bin",
+        index.append({"name": name, "mtx": name + ".mtx", "sweeps": name + ".sweeps1.bin",
+                      "sweeps_stock": name + ".sweeps_stock.bin",
                       "agg_in": name + ".agg_in.bin", "agg_out": name + ".agg_out.bin",
                       "cli": name + ".cli.txt", "min_gain": gain})
     with open(os.path.join(out_dir, "index.json"), "w") as f:

@@ -75,7 +75,7 @@ def canon(rp, cl, wf):
 def test_sweeps_match_oracle(lvb, orc, graphs, name):
     rp, cl, w, _ = graphs[name]
     g = lvb.Graph(rp, cl, w)
-    e = lvb.Louvain(g)
+    e = lvb.Louvain(g, verify=True)
     o = orc.Oracle(rp, cl, w)
     assert e.scale()[:2] == o.scale()
     assert e.calculate_modularity() == o.modularity()
@@ -93,7 +93,7 @@ def test_sweeps_match_oracle(lvb, orc, graphs, name):
 @pytest.mark.parametrize("name", NAMES)
 def test_levels_and_aggregation_match_oracle(lvb, orc, graphs, name):
     rp, cl, w, gain = graphs[name]
-    e = lvb.Louvain(lvb.Graph(rp, cl, w))
+    e = lvb.Louvain(lvb.Graph(rp, cl, w), verify=True)
     o = orc.Oracle(rp, cl, w)
     for level in range(12):
         c1 = e.optimise_modularity(gain)
