@@ -230,7 +230,8 @@ def run_ours(args, ranks: Ranks):
     dg = lvb.gen_rmat_device(scale, EDGE_FACTOR, SEED, device=dev)
     V, E = dg.V, dg.E
     # --- value: resident inputs ---
-    eng = lvb.Louvain(device_csr=(dg.rowptr, dg.col, dg.w, V, E), device=dev, profile=True)
+    eng = lvb.Louvain(device_csr=(dg.rowptr, dg.col, dg.w, V, E), device=dev, profile=True,
+                      trace=args.trace)
     for _ in range(args.warmup):
         eng.reset()
         eng.run(MIN_GAIN)
@@ -384,6 +385,7 @@ def main():
     ap.add_argument("--scale", type=int, default=24)
     ap.add_argument("--cpu-sweeps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--trace", action="store_true", help="per-level / per-sweep lines on stderr")
     args = ap.parse_args()
     if args.impl == "reference":
         ranks = Ranks(backend="gloo")

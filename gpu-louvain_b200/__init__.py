@@ -55,7 +55,8 @@ class LouvainError(RuntimeError):
 
 class _Opts(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("device", C.c_int32), ("max_sweeps", C.c_int32),
-                ("profile", C.c_int32), ("verify", C.c_int32), ("reserved", C.c_int32 * 11)]
+                ("profile", C.c_int32), ("verify", C.c_int32), ("trace", C.c_int32),
+                ("reserved", C.c_int32 * 10)]
 
 
 class _Stats(C.Structure):
@@ -282,7 +283,8 @@ class Louvain:
     """One engine handle: a graph resident on one GPU plus its Louvain state."""
 
     def __init__(self, graph: Graph | None = None, *, device: int = 0, max_sweeps: int = 0,
-                 profile: bool = False, verify: bool = False, device_csr: tuple | None = None):
+                 profile: bool = False, verify: bool = False, trace: bool = False,
+                 device_csr: tuple | None = None):
         L = lib()
         opts = _Opts()
         L.lv_default_opts(C.byref(opts))
@@ -290,6 +292,7 @@ class Louvain:
         opts.max_sweeps = max_sweeps
         opts.profile = 1 if profile else 0
         opts.verify = 1 if verify else 0
+        opts.trace = 1 if trace else 0
         h = C.c_void_p()
         if device_csr is not None:
             rp, cl, w, V, E = device_csr

@@ -199,15 +199,18 @@ __global__ void __launch_bounds__(256) merge_group_kernel(const int32_t *__restr
         a = P[mstart[c]];
         b = P[mstart[c + 1]];
     }
-    if (G == 32) {
-        for (int32_t base = a; base < b; base += 32) {
-            const int32_t i = base + lane;
-            const bool valid = i < b;
-            warp_insert(keys, vals, LG, valid, valid ? vkey[i] : 0, valid ? vw[i] : 0, err);
-        }
-    } else {
-        for (int32_t i = a + lane; i < b; i += G) table_insert(keys, vals, LG, vkey[i], vw[i], err);
+    // entries keyed by the community's own new id (its intra-community
+    // weight, usually the bulk) are summed in registers
+    const int32_t self = active ? newid[c] : -1;
+    u64 w_self = 0;
+    for (int32_t i = a + lane; i < b; i += G) {
+        const int32_t k = vkey[i];
+        if (k == self) w_self += vw[i];
+        else table_insert(keys, vals, LG, k, vw[i], err);
     }
+    for (int off = G >> 1; off > 0; off >>= 1) w_self += __shfl_xor_sync(FULL, w_self, off, G);
+    __syncwarp();
+    if (active && lane == 0 && w_self) table_insert(keys, vals, LG, self, w_self, err);
     __syncwarp();
     // write the distinct entries back at the start of the range, in slot order
     const int wl = threadIdx.x & 31;
@@ -252,11 +255,15 @@ __global__ void __launch_bounds__(T) merge_cta_kernel(const int32_t *__restrict_
         int lg = ceil_log2_i(2 * (int64_t)(b - a));
         lg = lg < 3 ? 3 : lg;
         const int cap = 1 << lg;
-        for (int32_t base = a; base < b; base += T) {
-            const int32_t i = base + threadIdx.x;
-            const bool valid = i < b;
-            warp_insert(keys, vals, lg, valid, valid ? vkey[i] : 0, valid ? vw[i] : 0, err);
+        const int32_t self = newid[c];
+        u64 w_self = 0;
+        for (int32_t i = a + threadIdx.x; i < b; i += T) {
+            const int32_t k = vkey[i];
+            if (k == self) w_self += vw[i];
+            else table_insert(keys, vals, lg, k, vw[i], err);
         }
+        w_self = warp_sum_u64(w_self);
+        if ((threadIdx.x & 31) == 0 && w_self) table_insert(keys, vals, lg, self, w_self, err);
         __syncthreads();
         for (int s = threadIdx.x; s < cap; s += T) {
             const int32_t key = keys[s];
@@ -285,7 +292,8 @@ __global__ void __launch_bounds__(T) merge_cta_kernel(const int32_t *__restrict_
 // added once per distinct key to the community's global table.
 __global__ void __launch_bounds__(HG_INSERT_THREADS) mergeg_insert_kernel(
     HubGlobal hg, const int32_t *__restrict__ mstart, const int32_t *__restrict__ P,
-    const int32_t *__restrict__ vkey, const u64 *__restrict__ vw, int *err) {
+    const int32_t *__restrict__ newid, const int32_t *__restrict__ vkey,
+    const u64 *__restrict__ vw, int *err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int LCAP = 2 * HG_EDGE_CHUNK;
     constexpr int LLG = ilog2_c(LCAP);
@@ -298,64 +306,62 @@ __global__ void __launch_bounds__(HG_INSERT_THREADS) mergeg_insert_kernel(
     const int32_t b = P[mstart[c + 1]];
     const int32_t i0 = P[mstart[c]] + hg.echunk_e0[blockIdx.x];
     const int32_t i1 = min(i0 + HG_EDGE_CHUNK, b);
-    for (int32_t base = i0; base < i1; base += HG_INSERT_THREADS) {
-        const int32_t i = base + threadIdx.x;
-        const bool valid = i < i1;
-        warp_insert(lkeys, lvals, LLG, valid, valid ? vkey[i] : 0, valid ? vw[i] : 0, err);
+    const int32_t self = newid[c];
+    u64 w_self = 0;
+    for (int32_t i = i0 + threadIdx.x; i < i1; i += HG_INSERT_THREADS) {
+        const int32_t k = vkey[i];
+        if (k == self) w_self += vw[i];
+        else table_insert(lkeys, lvals, LLG, k, vw[i], err);
     }
+    w_self = warp_sum_u64(w_self);
+    if ((threadIdx.x & 31) == 0 && w_self) table_insert(lkeys, lvals, LLG, self, w_self, err);
     __syncthreads();
     int32_t *keys = hg.keys + hg.tbl_off[h];
     u64 *vals = hg.vals + hg.tbl_off[h];
+    int32_t *occ = hg.occ + hg.occ_off[h];
     const int lg = hg.tbl_lg[h];
     for (int s = threadIdx.x; s < LCAP; s += HG_INSERT_THREADS) {
         const int32_t k = lkeys[s];
-        if (k >= 0) table_insert(keys, vals, lg, k, lvals[s], err);
+        const int32_t claimed = k >= 0 ? table_insert_claim(keys, vals, lg, k, lvals[s], err) : -1;
+        warp_append(claimed, occ, hg.nocc + h);
     }
 }
 
+// Entry i of a community's occupied list becomes entry i of its merged row.
 __global__ void __launch_bounds__(256) mergeg_emit_kernel(HubGlobal hg,
                                                           const int32_t *__restrict__ mstart,
                                                           const int32_t *__restrict__ P,
-                                                          const int32_t *__restrict__ newid,
-                                                          int32_t *vkey, u64 *vw, int32_t *rowcnt) {
+                                                          int32_t *vkey, u64 *vw) {
     const int32_t bidx = blockIdx.x;
     const int32_t h = hg.schunk_hub[bidx];
     const int32_t c = hg.hubs[h];
     const int32_t a = P[mstart[c]];
-    const int32_t nid = newid[c];
     int32_t *keys = hg.keys + hg.tbl_off[h];
     u64 *vals = hg.vals + hg.tbl_off[h];
-    const int32_t cap = 1 << hg.tbl_lg[h];
+    const int32_t *occ = hg.occ + hg.occ_off[h];
     const int32_t s0 = hg.schunk_s0[bidx];
-    const int32_t s1 = min(s0 + HG_SLOT_CHUNK, cap);
-    for (int32_t s = s0 + threadIdx.x; s < s1; s += 256) {
-        const int32_t key = keys[s];
-        if (key >= 0) {
-            const int32_t pos = a + atomicAdd(rowcnt + nid, 1);
-            vkey[pos] = key;
-            vw[pos] = vals[s];
-            keys[s] = -1;
-            vals[s] = 0;
-        }
+    const int32_t n = min(hg.nocc[h] - s0, HG_SLOT_CHUNK);
+    for (int32_t i = threadIdx.x; i < n; i += 256) {
+        const int32_t sl = occ[s0 + i];
+        vkey[a + s0 + i] = keys[sl];
+        vw[a + s0 + i] = vals[sl];
+        keys[sl] = -1;
+        vals[sl] = 0;
     }
 }
 
 __global__ void mergeg_finish_kernel(HubGlobal hg, const int32_t *__restrict__ mstart,
                                      const int32_t *__restrict__ P, const int32_t *__restrict__ newid,
-                                     const int32_t *__restrict__ rowcnt, int32_t *newdeg,
-                                     int32_t *epos_new) {
+                                     int32_t *newdeg, int32_t *epos_new) {
     for (int32_t h = blockIdx.x * 256 + threadIdx.x; h < hg.nhubs; h += gridDim.x * 256) {
         const int32_t c = hg.hubs[h];
         const int32_t nid = newid[c];
-        newdeg[nid] = rowcnt[nid];
+        newdeg[nid] = hg.nocc[h];
         epos_new[nid] = P[mstart[c]];
+        hg.nocc[h] = 0;
     }
 }
 
-__global__ void zero_rowcnt_kernel(HubGlobal hg, const int32_t *__restrict__ newid, int32_t *rowcnt) {
-    for (int32_t h = blockIdx.x * 256 + threadIdx.x; h < hg.nhubs; h += gridDim.x * 256)
-        rowcnt[newid[hg.hubs[h]]] = 0;
-}
 
 // Rows of the next level stay where the merge wrote them: row c' spans
 // [epos_new[c'], epos_new[c'] + newdeg[c']).
@@ -473,11 +479,9 @@ void agg_merge_class(int acls, const AggBuffers &ab, const int32_t *P, const int
 void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *P, int32_t *vkey,
                       u64 *vw, int *err, cudaStream_t s) {
     if (hg.nhubs <= 0) return;
-    zero_rowcnt_kernel<<<grid_for(hg.nhubs), 256, 0, s>>>(hg, ab.flag, ab.cursor); note_launches(1);
-    mergeg_insert_kernel<<<hg.n_echunks, HG_INSERT_THREADS, HG_INSERT_SMEM, s>>>(hg, ab.mstart, P, vkey, vw, err); note_launches(1);
-    mergeg_emit_kernel<<<hg.n_schunks, 256, 0, s>>>(hg, ab.mstart, P, ab.flag, vkey, vw, ab.cursor); note_launches(1);
-    mergeg_finish_kernel<<<grid_for(hg.nhubs), 256, 0, s>>>(hg, ab.mstart, P, ab.flag, ab.cursor,
-                                                            ab.newdeg, ab.epos_new); note_launches(1);
+    mergeg_insert_kernel<<<hg.n_echunks, HG_INSERT_THREADS, HG_INSERT_SMEM, s>>>(hg, ab.mstart, P, ab.flag, vkey, vw, err); note_launches(1);
+    mergeg_emit_kernel<<<hg.n_schunks, 256, 0, s>>>(hg, ab.mstart, P, vkey, vw); note_launches(1);
+    mergeg_finish_kernel<<<grid_for(hg.nhubs), 256, 0, s>>>(hg, ab.mstart, P, ab.flag, ab.newdeg, ab.epos_new); note_launches(1);
 }
 
 void agg_row_bounds(const AggBuffers &ab, int32_t Vn, int32_t *start, int32_t *end, cudaStream_t s) {

@@ -127,76 +127,255 @@ __device__ __forceinline__ void table_insert(int32_t *keys, u64 *vals, int lg, i
     atomicOr(err, DEVERR_HASH_FULL);
 }
 
-// Exact sum of a uint64 over the lanes in `mask` (redux.sync adds 32-bit
-// values): the value is split into 22/22/20-bit slices whose 32-lane sums
-// cannot overflow 32 bits.  Lanes of different masks may call it together.
-__device__ __forceinline__ u64 redux_add_u64(unsigned mask, u64 x) {
-    const unsigned p0 = (unsigned)(x & 0x3FFFFFull);
-    const unsigned p1 = (unsigned)((x >> 22) & 0x3FFFFFull);
-    const unsigned p2 = (unsigned)(x >> 44);
-    const u64 s0 = __reduce_add_sync(mask, p0);
-    const u64 s1 = __reduce_add_sync(mask, p1);
-    const u64 s2 = __reduce_add_sync(mask, p2);
-    return s0 + (s1 << 22) + (s2 << 44);
+// table_insert that returns the slot it newly claimed for `key` (-1 when the
+// key was already present or the table is full).
+__device__ __forceinline__ int32_t table_insert_claim(int32_t *keys, u64 *vals, int lg, int32_t key,
+                                                      u64 w, int *err) {
+    const uint32_t mask = (1u << lg) - 1u;
+    uint32_t s = hash_slot(key, lg);
+    for (uint32_t p = 0; p <= mask; ++p) {
+        int32_t k = ((volatile int32_t *)keys)[s];
+        if (k == key) { atomicAdd(vals + s, w); return -1; }
+        if (k < 0) {
+            int32_t prev = atomicCAS(keys + s, -1, key);
+            if (prev < 0) { atomicAdd(vals + s, w); return (int32_t)s; }
+            if (prev == key) { atomicAdd(vals + s, w); return -1; }
+        }
+        s = (s + 1u) & mask;
+    }
+    atomicOr(err, DEVERR_HASH_FULL);
+    return -1;
 }
 
-// Warp-aggregated insert: every lane of the warp calls it (uniformly);
-// valid lanes holding the same key first combine their weights, and one
-// lane per distinct key inserts.  A key shared by many neighbours (the common
-// case once communities form) then costs one atomic per warp instead of 32.
-__device__ __forceinline__ void warp_insert(int32_t *keys, u64 *vals, int lg, bool valid,
-                                            int32_t key, u64 w, int *err) {
-    const unsigned act = __ballot_sync(FULL, valid);
-    if (!valid) return;
-    const unsigned peers = __match_any_sync(act, key);
-    const u64 sum = redux_add_u64(peers, w);
-    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) table_insert(keys, vals, lg, key, sum, err);
+// Append the slots claimed by this warp's lanes (claimed >= 0) to occ[],
+// reserving space with one atomic per warp.  All 32 lanes must call it.
+__device__ __forceinline__ void warp_append(int32_t claimed, int32_t *occ, int32_t *nocc) {
+    const unsigned bal = __ballot_sync(FULL, claimed >= 0);
+    if (!bal) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(bal) - 1;
+    int32_t base = 0;
+    if (lane == leader) base = atomicAdd(nocc, __popc(bal));
+    base = __shfl_sync(FULL, base, leader);
+    if (claimed >= 0) occ[base + __popc(bal & ((1u << lane) - 1u))] = claimed;
 }
 
-// Candidate ordering of computeMove: larger gain wins, equal gains go to the
-// lower community id (modularity_optimisation.cu:157,169,182).
-__device__ __forceinline__ bool better(i128 g1, int32_t c1, i128 g2, int32_t c2) {
-    return g1 > g2 || (g1 == g2 && c1 < c2);
+// table_insert that also appends every newly claimed slot to occ[] (count in
+// *nocc), so that evaluation and clearing visit only occupied slots.
+__device__ __forceinline__ void table_insert_occ(int32_t *keys, u64 *vals, int lg, int32_t key,
+                                                 u64 w, int *err, int32_t *occ, int32_t *nocc) {
+    const uint32_t mask = (1u << lg) - 1u;
+    uint32_t s = hash_slot(key, lg);
+    for (uint32_t p = 0; p <= mask; ++p) {
+        int32_t k = ((volatile int32_t *)keys)[s];
+        if (k == key) { atomicAdd(vals + s, w); return; }
+        if (k < 0) {
+            int32_t prev = atomicCAS(keys + s, -1, key);
+            if (prev < 0) {
+                atomicAdd(vals + s, w);
+                occ[atomicAdd(nocc, 1)] = (int32_t)s;
+                return;
+            }
+            if (prev == key) { atomicAdd(vals + s, w); return; }
+        }
+        s = (s + 1u) & mask;
+    }
+    atomicOr(err, DEVERR_HASH_FULL);
 }
 
-// Evaluate one neighbour community C of vertex v (e_C = summed weight to C,
-// self-loops excluded).  The community of v itself only contributes e_own.
-// Singleton guard (modularity_optimisation.cu:154-155): a singleton may not
-// move into a larger-id singleton.
+// Insert the row col/w[r0..r1) of vertex v, lanes lane, lane+stride, ...,
+// into a table, U edges per lane at a time so that U column loads and then U
+// community gathers are in flight together.  Self-loops are skipped; the
+// weight to the own community is summed into *e_own instead of the table.
+// OCC: record newly claimed slots in occ[] / *nocc.
+template <int U, bool OCC, typename WT>
+__device__ __forceinline__ void insert_row(const GraphView<WT> &g, const int32_t *__restrict__ comm,
+                                           int32_t v, int32_t own, int32_t r0, int32_t r1, int lane,
+                                           int stride, int32_t *keys, u64 *vals, int lg, int *err,
+                                           int32_t *occ, int32_t *nocc, u64 &e_own) {
+    for (int32_t base = r0 + lane; base < r1; base += U * stride) {
+        int32_t jj[U];
+        u64 ww[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int32_t e = base + u * stride;
+            jj[u] = -1;
+            ww[u] = 0;
+            if (e < r1) {
+                jj[u] = __ldg(g.col + e);
+                ww[u] = wfix(g.w, e, g.scale);
+            }
+        }
+        int32_t cc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(comm + jj[u]) : -1;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (cc[u] < 0) continue;
+            if (cc[u] == own) {
+                e_own += ww[u];
+            } else if (OCC) {
+                table_insert_occ(keys, vals, lg, cc[u], ww[u], err, occ, nocc);
+            } else {
+                table_insert(keys, vals, lg, cc[u], ww[u], err);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Gain comparison.
+//
+// For vertex v (own community o, weight k, S_o = Sigma_tot[o]) and candidate
+// community C with weight e_C from v and Sigma_tot S_C, the reference's gain
+// (modularity_optimisation.cu:96-102) scaled by T^2/2 is the integer
+//     G(C) = T e_C + k (S_o - k - S_C)                 (|G| < 2^126)
+// "Stay" is the initial best with G = 0 (:137-138).  Candidates are compared
+// with an FP64 estimate g~ whose error is bounded by
+//     |g~ - G| <= 2^-50 (T e_C + k |S_o - k - S_C|)
+// (each operand is one rounding away from its integer, the products and the
+// sum add three more, each <= 2^-53 relative); when the two intervals
+// overlap the exact 128-bit values decide, ties going to the lower id
+// (:157,169,182).  The result is the exact argmax.
+// ---------------------------------------------------------------------------
 struct MoveCtx {
     int32_t own;
     bool own_single;
+    u64 T;
     u64 kv;
     u64 sown;
+    double Td;
+    double kvd;
 };
 
-// Running best of one thread (or group): gain, community, and the summed
-// weight e_best to that community (used for the exact modularity update);
-// e_own is the weight to the vertex's own community.
+__device__ __forceinline__ MoveCtx move_ctx(int32_t own, bool own_single, u64 T, u64 kv, u64 sown) {
+    MoveCtx m;
+    m.own = own;
+    m.own_single = own_single;
+    m.T = T;
+    m.kv = kv;
+    m.sown = sown;
+    m.Td = (double)T;
+    m.kvd = (double)kv;
+    return m;
+}
+
+// Exact G for (e, S); the stay candidate (c == own) has G = 0.
+__device__ __forceinline__ i128 exact_gain(const MoveCtx &m, u64 e, u64 S) {
+    const u128 te = ((u128)__umul64hi(m.T, e) << 64) | (u128)(m.T * e);
+    const i64 d = (i64)m.sown - (i64)m.kv - (i64)S;
+    const u64 ad = d < 0 ? (u64)0 - (u64)d : (u64)d;
+    const u128 kd = ((u128)__umul64hi(m.kv, ad) << 64) | (u128)(m.kv * ad);
+    return d < 0 ? (i128)te - (i128)kd : (i128)te + (i128)kd;
+}
+
+// Running best of one thread (or group): FP64 estimate gd of G, community c,
+// weight e and Sigma_tot S of c (to recompute G exactly), and e_own, the
+// summed weight to the own community.
 struct Best {
-    i128 g;
+    double gd;
+    u64 e;
+    u64 S;
     int32_t c;
-    u64 eb;
     u64 eo;
 };
 
 __device__ __forceinline__ Best best_init(int32_t own) {
     Best b;
-    b.g = 0;
+    b.gd = 0.0;
+    b.e = 0;
+    b.S = 0;
     b.c = own;
-    b.eb = 0;
     b.eo = 0;
     return b;
 }
 
-__device__ __forceinline__ void eval_candidate(int32_t c, u64 ec, const MoveCtx &m, u64 T,
+__device__ __forceinline__ double gain_err(const MoveCtx &m, const Best &b) {
+    if (b.c == m.own) return 0.0;
+    const double dd = (double)((i64)m.sown - (i64)m.kv - (i64)b.S);
+    return (m.Td * (double)b.e + m.kvd * fabs(dd)) * 0x1p-50;
+}
+
+// true iff candidate a is strictly better than b (exact order).
+__device__ __forceinline__ bool better(const MoveCtx &m, const Best &a, const Best &b) {
+    const double ea = gain_err(m, a), eb = gain_err(m, b);
+    if (a.gd - ea > b.gd + eb) return true;
+    if (b.gd - eb > a.gd + ea) return false;
+    const i128 ga = a.c == m.own ? (i128)0 : exact_gain(m, a.e, a.S);
+    const i128 gb = b.c == m.own ? (i128)0 : exact_gain(m, b.e, b.S);
+    return ga > gb || (ga == gb && a.c < b.c);
+}
+
+// Evaluate one neighbour community c (self-loops excluded) whose Sigma_tot
+// Sc and (when the singleton guard needs it) size szc were already loaded.
+// Singleton guard (modularity_optimisation.cu:154-155): a singleton may not
+// move into a larger-id singleton.
+__device__ __forceinline__ bool guard_needs_size(const MoveCtx &m, int32_t c) {
+    return m.own_single && c > m.own;
+}
+
+__device__ __forceinline__ void eval_loaded(int32_t c, u64 ec, u64 Sc, int32_t szc, const MoveCtx &m,
+                                            Best &b) {
+    if (c == m.own) { b.eo += ec; return; }
+    if (guard_needs_size(m, c) && szc == 1) return;
+    Best x;
+    x.S = Sc;
+    x.e = ec;
+    x.c = c;
+    x.eo = 0;
+    const double dd = (double)((i64)m.sown - (i64)m.kv - (i64)Sc);
+    x.gd = fma(m.Td, (double)ec, m.kvd * dd);
+    if (better(m, x, b)) { b.gd = x.gd; b.e = x.e; b.S = x.S; b.c = x.c; }
+}
+
+__device__ __forceinline__ void eval_candidate(int32_t c, u64 ec, const MoveCtx &m,
                                                const u64 *__restrict__ S,
                                                const int32_t *__restrict__ size, Best &b) {
-    if (c == m.own) { b.eo = ec; return; }
-    if (m.own_single && c > m.own && size[c] == 1) return;
-    const i64 d = (i64)m.sown - (i64)m.kv - (i64)S[c];
-    const i128 g = (i128)((u128)T * (u128)ec) + (i128)(i64)m.kv * (i128)d;
-    if (better(g, c, b.g, b.c)) { b.g = g; b.c = c; b.eb = ec; }
+    if (c == m.own) { b.eo += ec; return; }
+    eval_loaded(c, ec, __ldg(S + c), guard_needs_size(m, c) ? __ldg(size + c) : 0, m, b);
+}
+
+// Evaluate U table entries per lane at a time: first U keys/sums, then their
+// U Sigma_tot (and guard size) gathers, then the comparisons.  Entries come
+// from slot indices (OCC: occ[i], else i itself, i < n); each visited slot is
+// cleared when CLEAR is set.
+template <int U, bool OCC, bool CLEAR>
+__device__ __forceinline__ void eval_slots(int32_t *keys, u64 *vals, const int32_t *occ, int32_t n,
+                                           int lane, int stride, const MoveCtx &m,
+                                           const u64 *__restrict__ S,
+                                           const int32_t *__restrict__ size, Best &b) {
+    for (int32_t i0 = lane; i0 < n; i0 += U * stride) {
+        int32_t cc[U];
+        u64 ee[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int32_t i = i0 + u * stride;
+            cc[u] = -1;
+            ee[u] = 0;
+            if (i < n) {
+                const int32_t sl = OCC ? occ[i] : i;
+                cc[u] = keys[sl];
+                if (cc[u] >= 0) {
+                    ee[u] = vals[sl];
+                    if (CLEAR) {
+                        keys[sl] = -1;
+                        vals[sl] = 0;
+                    }
+                }
+            }
+        }
+        u64 SS[U];
+        int32_t zz[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const bool cand = cc[u] >= 0 && cc[u] != m.own;
+            SS[u] = cand ? __ldg(S + cc[u]) : 0;
+            zz[u] = (cand && guard_needs_size(m, cc[u])) ? __ldg(size + cc[u]) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (cc[u] >= 0) eval_loaded(cc[u], ee[u], SS[u], zz[u], m, b);
+    }
 }
 
 // Move rule (modularity_optimisation.cu:192): move iff g_best - e_own/M > 0,
@@ -204,32 +383,29 @@ __device__ __forceinline__ void eval_candidate(int32_t c, u64 ec, const MoveCtx 
 // sum_i e_{i->C(i)} when none of its neighbours moves in the same sub-round,
 // 2 (e_best - e_own) as a wrapping uint64 (corrected for co-moving neighbours
 // by the correction kernel).
-__device__ __forceinline__ int32_t move_decision(const Best &b, u64 T, int32_t own, u64 *delta) {
-    const i128 stay = (i128)((u128)T * (u128)b.eo);
-    if (b.g - stay > 0) {
-        *delta = 2 * (b.eb - b.eo);
+__device__ __forceinline__ int32_t move_decision(const MoveCtx &m, const Best &b, u64 *delta) {
+    *delta = 0;
+    if (b.c == m.own) return m.own;
+    const i128 g = exact_gain(m, b.e, b.S);
+    const i128 stay = (i128)(((u128)__umul64hi(m.T, b.eo) << 64) | (u128)(m.T * b.eo));
+    if (g - stay > 0) {
+        *delta = 2 * (b.e - b.eo);
         return b.c;
     }
-    *delta = 0;
-    return own;
-}
-
-__device__ __forceinline__ i128 shfl_xor_i128(i128 x, int m, int width) {
-    u64 lo = (u64)x, hi = (u64)((u128)x >> 64);
-    lo = __shfl_xor_sync(FULL, lo, m, width);
-    hi = __shfl_xor_sync(FULL, hi, m, width);
-    return (i128)(((u128)hi << 64) | (u128)lo);
+    return m.own;
 }
 
 // Butterfly reduction inside aligned groups of `width` lanes; every lane of
-// the group ends with the group's best (g, c, e_best) and summed e_own.
-__device__ __forceinline__ void group_reduce_best(Best &b, int width) {
+// the group ends with the group's best and the summed e_own.
+__device__ __forceinline__ void group_reduce_best(const MoveCtx &m, Best &b, int width) {
     for (int off = width >> 1; off > 0; off >>= 1) {
-        const i128 og = shfl_xor_i128(b.g, off, width);
-        const int32_t oc = __shfl_xor_sync(FULL, b.c, off, width);
-        const u64 ob = __shfl_xor_sync(FULL, b.eb, off, width);
+        Best o;
+        o.gd = __shfl_xor_sync(FULL, b.gd, off, width);
+        o.e = __shfl_xor_sync(FULL, b.e, off, width);
+        o.S = __shfl_xor_sync(FULL, b.S, off, width);
+        o.c = __shfl_xor_sync(FULL, b.c, off, width);
         const u64 oe = __shfl_xor_sync(FULL, b.eo, off, width);
-        if (better(og, oc, b.g, b.c)) { b.g = og; b.c = oc; b.eb = ob; }
+        if (better(m, o, b)) { b.gd = o.gd; b.e = o.e; b.S = o.S; b.c = o.c; }
         b.eo += oe;
     }
 }

@@ -115,6 +115,10 @@ struct lv_handle {
     int32_t *tbl_keys = nullptr;
     u64 *tbl_vals = nullptr;
     size_t tbl_slots = 0;
+    int32_t *occ_buf = nullptr;    // occupied-slot lists of the global tables
+    size_t occ_cap = 0;
+    int32_t *nocc_buf = nullptr;   // per-hub list lengths, zero between uses
+    size_t nocc_cap = 0;
 
     bool agg_ready = false;
     AggBuffers ab{};
@@ -277,12 +281,32 @@ int ensure_tables(lv_handle *h, size_t slots) {
     return LV_OK;
 }
 
+int ensure_occ(lv_handle *h, size_t entries, size_t hubs) {
+    if (entries > h->occ_cap) {
+        dfree(h->occ_buf);
+        h->occ_cap = 0;
+        size_t want = entries + entries / 4 + 1;
+        LV_TRY(dalloc(h, &h->occ_buf, want));
+        h->occ_cap = want;
+    }
+    if (hubs > h->nocc_cap) {
+        dfree(h->nocc_buf);
+        h->nocc_cap = 0;
+        size_t want = hubs + hubs / 4 + 1;
+        LV_TRY(dalloc(h, &h->nocc_buf, want));
+        LV_CUDA(h, cudaMemsetAsync(h->nocc_buf, 0, want * sizeof(int32_t), h->stream));
+        h->nocc_cap = want;
+    }
+    return LV_OK;
+}
+
 // ids: hub vertices / communities; deg: their degree bound; cap_limit caps
 // the distinct-key count (newV for aggregation, unlimited for moves).
 int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
                  const std::vector<int32_t> &deg, int64_t cap_limit) {
     const int32_t n = (int32_t)ids.size();
-    std::vector<int64_t> off(n);
+    std::vector<int64_t> off(n), occ_off(n);
+    int64_t occ_total = 0;
     std::vector<int32_t> lg(n), ech_hub, ech_e0, sch_hub, sch_s0, hub_s0(n + 1);
     int64_t total = 0;
     for (int32_t i = 0; i < n; ++i) {
@@ -297,19 +321,29 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
             ech_hub.push_back(i);
             ech_e0.push_back(e0);
         }
+        // a hub of degree d has at most min(d, cap) occupied slots: its
+        // occupied list has room for d entries, evaluated in slot chunks
         hub_s0[i] = (int32_t)sch_hub.size();
-        for (int64_t s0 = 0; s0 < (int64_t(1) << l); s0 += HG_SLOT_CHUNK) {
+        occ_off[i] = occ_total;
+        occ_total += deg[i];
+        for (int64_t s0 = 0; s0 < (int64_t)deg[i]; s0 += HG_SLOT_CHUNK) {
             sch_hub.push_back(i);
             sch_s0.push_back((int32_t)s0);
+        }
+        if (deg[i] == 0) {
+            sch_hub.push_back(i);
+            sch_s0.push_back(0);
         }
     }
     hub_s0[n] = (int32_t)sch_hub.size();
     LV_TRY(ensure_tables(h, (size_t)total));
+    LV_TRY(ensure_occ(h, (size_t)occ_total, (size_t)n));
     const size_t ne = ech_hub.size(), ns = sch_hub.size();
-    // packed: ids | lg | ech_hub | ech_e0 | sch_hub | sch_s0 | hub_s0 | res_c | (8-aligned) off | res_g | res_e | res_b
+    // packed: ids | lg | ech_hub | ech_e0 | sch_hub | sch_s0 | hub_s0 | res_c | (8-aligned) off |
+    // res_g | res_e | res_b | occ_off
     size_t i32_count = (size_t)n + n + ne + ne + ns + ns + (n + 1) + ns;
     size_t i32_bytes = ((i32_count * 4 + 15) / 16) * 16;
-    size_t bytes = i32_bytes + (size_t)n * 8 + ns * 16 + ns * 8 + ns * 8 + 64;
+    size_t bytes = i32_bytes + (size_t)n * 8 + ns * 16 + ns * 8 + ns * 8 + (size_t)n * 8 + 64;
     if (bytes > L.dev_bytes) {
         if (L.dev) cudaFree(L.dev);
         L.dev = nullptr;
@@ -334,6 +368,7 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
     at += ns;
     unsigned char *base8 = host.data() + i32_bytes;
     if (n) std::memcpy(base8, off.data(), (size_t)n * 8);
+    if (n) std::memcpy(base8 + (size_t)n * 8 + ns * 32, occ_off.data(), (size_t)n * 8);
     LV_CUDA(h, cudaMemcpyAsync(L.dev, host.data(), bytes, cudaMemcpyHostToDevice, h->stream));
     // the host vector must outlive the async copy
     LV_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -355,6 +390,9 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
     v.res_g = (u64 *)(d8 + (size_t)n * 8);
     v.res_e = (u64 *)(d8 + (size_t)n * 8 + ns * 16);
     v.res_b = (u64 *)(d8 + (size_t)n * 8 + ns * 24);
+    v.occ_off = (const int64_t *)(d8 + (size_t)n * 8 + ns * 32);
+    v.occ = h->occ_buf;
+    v.nocc = h->nocc_buf;
     v.keys = h->tbl_keys;
     v.vals = h->tbl_vals;
     L.ids = ids;
@@ -407,6 +445,13 @@ int level_setup(lv_handle *h) {
     }
     LV_TRY(build_layout(h, h->hub_move, ids, deg, 0));
     t.stop();
+    if (h->opts.trace) {
+        std::fprintf(stderr, "[lv] level %d: V=%d E=%lld hub_table_slots=%zu classes:", h->level, h->V,
+                     (long long)h->E, h->tbl_slots);
+        for (int c = 0; c < NCLS; ++c)
+            std::fprintf(stderr, " %d/%lld", h->cls_off[c + 1] - h->cls_off[c], (long long)h->cls_edges[c]);
+        std::fprintf(stderr, "\n");
+    }
     return LV_OK;
 }
 
@@ -524,6 +569,16 @@ int sweep_and_q(lv_handle *h, int64_t *moves, double *q) {
             return fail(h, LV_ERR_DEVICE, "incremental modularity differs from the full pass");
     }
     if (q) *q = q_inc;
+    if (h->opts.trace) {
+        // per-class device time of this sweep (profile mode) and move phase
+        std::fprintf(stderr, "[lv]   sweep: moves=%lld q=%.9f move_ms_total=%.3f", (long long)t.moves,
+                     q_inc, h->st.move_ms);
+        if (h->opts.profile) {
+            std::fprintf(stderr, " class_ms_total:");
+            for (int c = 0; c < NCLS; ++c) std::fprintf(stderr, " %.2f", h->cst.ms[c]);
+        }
+        std::fprintf(stderr, "\n");
+    }
     h->st.sweeps += 1;
     h->st.edge_sweeps += h->E;
     h->st.moves += *moves;
@@ -631,6 +686,9 @@ int aggregate_t(lv_handle *h) {
     LV_CUDA(h, cudaMemcpyAsync(h->tot_h, h->tot_d, sizeof(Totals), cudaMemcpyDeviceToHost, h->stream));
     tm.stop();
     LV_TRY(sync(h));
+    if (h->opts.trace)
+        std::fprintf(stderr, "[lv] aggregate: newV=%d big_communities=%d agg_ms_total=%.3f\n", newV, nbig,
+                     h->st.aggregate_ms);
     LV_TRY(check_device_error(h, h->tot_h->err));
     const int64_t newE = h->small_h[0];
     h->cur_buf = nb;
@@ -794,7 +852,7 @@ int lv_destroy(lv_handle *h) {
     }
     dfree(h->comm); dfree(h->newc); dfree(h->size); dfree(h->orig2comm);
     dfree(h->k); dfree(h->S); dfree(h->list); dfree(h->cls_scratch);
-    dfree(h->tbl_keys); dfree(h->tbl_vals);
+    dfree(h->tbl_keys); dfree(h->tbl_vals); dfree(h->occ_buf); dfree(h->nocc_buf);
     if (h->hub_move.dev) cudaFree(h->hub_move.dev);
     if (h->hub_agg.dev) cudaFree(h->hub_agg.dev);
     AggBuffers &a = h->ab;

@@ -6,7 +6,8 @@ namespace lv {
 
 // Layout of the global-memory hash tables of class CLS_HG (degree > 4096)
 // for the current level.  Hubs are split into edge chunks (insert kernel)
-// and slot chunks (evaluate kernel) so that one hub spreads over many CTAs.
+// and chunks of their occupied-slot list (evaluate kernel) so that one hub
+// spreads over many CTAs; a hub of degree d has at most d occupied slots.
 constexpr int HG_EDGE_CHUNK = 4096;
 constexpr int HG_SLOT_CHUNK = 4096;
 constexpr int HG_INSERT_THREADS = 512;
@@ -30,6 +31,9 @@ struct HubGlobal {
     int32_t *res_c = nullptr;             // [n_schunks] best community
     u64 *res_e = nullptr;                 // [n_schunks] e_own contribution
     u64 *res_b = nullptr;                 // [n_schunks] weight to the best community
+    const int64_t *occ_off = nullptr;     // [nhubs] first entry of each hub's occupied list
+    int32_t *occ = nullptr;               // occupied slots, listed per hub
+    int32_t *nocc = nullptr;              // [nhubs] occupied-list lengths (kept zero between uses)
 };
 
 // Count of engine kernel launches (all handles, all devices of the process).

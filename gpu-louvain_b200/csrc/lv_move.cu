@@ -57,82 +57,53 @@ __global__ void __launch_bounds__(256) move_group_kernel(GraphView<WT> g, StateV
     __syncwarp();
     const bool active = idx < n;
     int32_t v = 0, own = 0;
-    if (G == 32) {
-        // one warp per vertex: uniform trip count, warp-aggregated inserts
-        int32_t r0 = 0, r1 = 0;
-        if (active) {
-            v = list[idx];
-            own = st.comm[v];
-            r0 = g.rowptr[v];
-            r1 = g.rowend[v];
-        }
-        for (int32_t base = r0; base < r1; base += 32) {
-            const int32_t e = base + lane;
-            bool valid = e < r1;
-            int32_t c = 0;
-            u64 w = 0;
-            if (valid) {
-                const int32_t j = __ldg(g.col + e);
-                valid = j != v;
-                if (valid) { c = st.comm[j]; w = wfix(g.w, e, g.scale); }
-            }
-            warp_insert(keys, vals, LG, valid, c, w, st.err);
-        }
-    } else if (active) {
+    u64 e_own = 0;   // weight to the own community: kept out of the table
+    if (active) {
         v = list[idx];
-        own = st.comm[v];
-        const int32_t r0 = g.rowptr[v], r1 = g.rowend[v];
-        for (int32_t e = r0 + lane; e < r1; e += G) {
-            const int32_t j = __ldg(g.col + e);
-            if (j != v) table_insert(keys, vals, LG, st.comm[j], wfix(g.w, e, g.scale), st.err);
-        }
+        own = __ldg(st.comm + v);
+        insert_row<(CAP > 32 ? 4 : 2), false>(g, st.comm, v, own, g.rowptr[v], g.rowend[v], lane, G,
+                                               keys, vals, LG, st.err, nullptr, nullptr, e_own);
     }
     __syncwarp();
+    const MoveCtx m = move_ctx(own, active ? __ldg(st.size + own) == 1 : false, st.T,
+                               active ? __ldg(st.k + v) : 0, active ? __ldg(st.S + own) : 0);
     Best b = best_init(own);
-    if (active) {
-        MoveCtx m;
-        m.own = own;
-        m.own_single = st.size[own] == 1;
-        m.kv = st.k[v];
-        m.sown = st.S[own];
-#pragma unroll
-        for (int s = lane; s < CAP; s += G) {
-            const int32_t c = keys[s];
-            if (c >= 0) eval_candidate(c, vals[s], m, st.T, st.S, st.size, b);
-        }
-    }
-    group_reduce_best(b, G);
+    b.eo = e_own;
+    if (active) eval_slots<(CAP / G > 1 ? 2 : 1), false, false>(keys, vals, nullptr, CAP, lane, G, m, st.S, st.size, b);
+    group_reduce_best(m, b, G);
     u64 delta = 0;
-    if (active && lane == 0) st.newc[v] = move_decision(b, st.T, own, &delta);
+    if (active && lane == 0) st.newc[v] = move_decision(m, b, &delta);
     block_add_total<256>(delta, dE);
 }
 
 // CTA-wide reduction of a Best; the result is valid in thread 0.
 template <int THREADS>
-__device__ __forceinline__ void cta_reduce_best(Best &b, int32_t fill_c) {
+__device__ __forceinline__ void cta_reduce_best(const MoveCtx &m, Best &b) {
     constexpr int NW = THREADS / 32;
-    __shared__ u64 rg_lo[NW], rg_hi[NW], reb[NW], reo[NW];
+    __shared__ double rgd[NW];
+    __shared__ u64 re[NW], rS[NW], reo[NW];
     __shared__ int32_t rc[NW];
-    group_reduce_best(b, 32);
+    group_reduce_best(m, b, 32);
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     if (l == 0) {
-        rg_lo[w] = (u64)b.g;
-        rg_hi[w] = (u64)((u128)b.g >> 64);
+        rgd[w] = b.gd;
+        re[w] = b.e;
+        rS[w] = b.S;
         rc[w] = b.c;
-        reb[w] = b.eb;
         reo[w] = b.eo;
     }
     __syncthreads();
     if (w == 0) {
         if (l < NW) {
-            b.g = (i128)(((u128)rg_hi[l] << 64) | (u128)rg_lo[l]);
+            b.gd = rgd[l];
+            b.e = re[l];
+            b.S = rS[l];
             b.c = rc[l];
-            b.eb = reb[l];
             b.eo = reo[l];
         } else {
-            b = best_init(fill_c);
+            b = best_init(m.own);
         }
-        group_reduce_best(b, 32);
+        group_reduce_best(m, b, 32);
     }
 }
 
@@ -146,48 +117,32 @@ __global__ void __launch_bounds__(THREADS) move_cta_kernel(GraphView<WT> g, Stat
     extern __shared__ __align__(16) unsigned char smem_raw[];
     u64 *vals = reinterpret_cast<u64 *>(smem_raw);
     int32_t *keys = reinterpret_cast<int32_t *>(vals + CAPMAX);
+    int32_t *occ = keys + CAPMAX;   // occupied slots (at most CAPMAX / 2)
+    __shared__ int32_t nocc;
     for (int s = threadIdx.x; s < CAPMAX; s += THREADS) { keys[s] = -1; vals[s] = 0; }
+    if (threadIdx.x == 0) nocc = 0;
     __syncthreads();
     u64 delta_sum = 0;
     for (int32_t idx = blockIdx.x; idx < n; idx += gridDim.x) {
         const int32_t v = list[idx];
-        const int32_t own = st.comm[v];
+        const int32_t own = __ldg(st.comm + v);
         const int32_t r0 = g.rowptr[v], r1 = g.rowend[v];
         int lg = ceil_log2_i(2 * (int64_t)(r1 - r0));
         lg = lg < 3 ? 3 : lg;
-        const int cap = 1 << lg;
-        for (int32_t base = r0; base < r1; base += THREADS) {
-            const int32_t e = base + threadIdx.x;
-            bool valid = e < r1;
-            int32_t c = 0;
-            u64 w = 0;
-            if (valid) {
-                const int32_t j = __ldg(g.col + e);
-                valid = j != v;
-                if (valid) { c = st.comm[j]; w = wfix(g.w, e, g.scale); }
-            }
-            warp_insert(keys, vals, lg, valid, c, w, st.err);
-        }
+        u64 e_own = 0;
+        insert_row<4, true>(g, st.comm, v, own, r0, r1, threadIdx.x, THREADS, keys, vals, lg, st.err,
+                            occ, &nocc, e_own);
         __syncthreads();
-        MoveCtx m;
-        m.own = own;
-        m.own_single = st.size[own] == 1;
-        m.kv = st.k[v];
-        m.sown = st.S[own];
+        const MoveCtx m = move_ctx(own, __ldg(st.size + own) == 1, st.T, __ldg(st.k + v), __ldg(st.S + own));
         Best b = best_init(own);
-        for (int s = threadIdx.x; s < cap; s += THREADS) {
-            const int32_t c = keys[s];
-            if (c >= 0) {
-                eval_candidate(c, vals[s], m, st.T, st.S, st.size, b);
-                keys[s] = -1;
-                vals[s] = 0;
-            }
-        }
-        cta_reduce_best<THREADS>(b, own);
+        b.eo = e_own;
+        eval_slots<4, true, true>(keys, vals, occ, nocc, threadIdx.x, THREADS, m, st.S, st.size, b);
+        cta_reduce_best<THREADS>(m, b);
         if (threadIdx.x == 0) {
             u64 delta = 0;
-            st.newc[v] = move_decision(b, st.T, own, &delta);
+            st.newc[v] = move_decision(m, b, &delta);
             delta_sum += delta;
+            nocc = 0;
         }
         __syncthreads();
     }
@@ -215,25 +170,22 @@ __global__ void __launch_bounds__(HG_INSERT_THREADS) hubg_insert_kernel(GraphVie
     const int32_t r1 = g.rowend[v];
     const int32_t e0 = g.rowptr[v] + hg.echunk_e0[blockIdx.x];
     const int32_t e1 = min(e0 + HG_EDGE_CHUNK, r1);
-    for (int32_t base = e0; base < e1; base += HG_INSERT_THREADS) {
-        const int32_t e = base + threadIdx.x;
-        bool valid = e < e1;
-        int32_t c = 0;
-        u64 w = 0;
-        if (valid) {
-            const int32_t j = __ldg(g.col + e);
-            valid = j != v;
-            if (valid) { c = st.comm[j]; w = wfix(g.w, e, g.scale); }
-        }
-        warp_insert(lkeys, lvals, LLG, valid, c, w, st.err);
-    }
+    const int32_t own = __ldg(st.comm + v);
+    u64 e_own = 0;
+    insert_row<4, false>(g, st.comm, v, own, e0, e1, threadIdx.x, HG_INSERT_THREADS, lkeys, lvals, LLG,
+                         st.err, nullptr, nullptr, e_own);
+    // the chunk's weight to the own community enters the table once
+    e_own = warp_sum_u64(e_own);
+    if ((threadIdx.x & 31) == 0 && e_own) table_insert(lkeys, lvals, LLG, own, e_own, st.err);
     __syncthreads();
     int32_t *keys = hg.keys + hg.tbl_off[h];
     u64 *vals = hg.vals + hg.tbl_off[h];
+    int32_t *occ = hg.occ + hg.occ_off[h];
     const int lg = hg.tbl_lg[h];
     for (int s = threadIdx.x; s < LCAP; s += HG_INSERT_THREADS) {
         const int32_t c = lkeys[s];
-        if (c >= 0) table_insert(keys, vals, lg, c, lvals[s], st.err);
+        const int32_t claimed = c >= 0 ? table_insert_claim(keys, vals, lg, c, lvals[s], st.err) : -1;
+        warp_append(claimed, occ, hg.nocc + h);
     }
 }
 
@@ -242,32 +194,21 @@ __global__ void __launch_bounds__(256) hubg_eval_kernel(StateView st, HubGlobal 
     const int32_t h = hg.schunk_hub[bi];
     const int32_t v = hg.hubs[h];
     const int32_t own = st.comm[v];
-    MoveCtx m;
-    m.own = own;
-    m.own_single = st.size[own] == 1;
-    m.kv = st.k[v];
-    m.sown = st.S[own];
+    const MoveCtx m = move_ctx(own, st.size[own] == 1, st.T, st.k[v], st.S[own]);
     int32_t *keys = hg.keys + hg.tbl_off[h];
     u64 *vals = hg.vals + hg.tbl_off[h];
-    const int32_t cap = 1 << hg.tbl_lg[h];
     const int32_t s0 = hg.schunk_s0[bi];
-    const int32_t s1 = min(s0 + HG_SLOT_CHUNK, cap);
+    const int32_t n = min(hg.nocc[h] - s0, HG_SLOT_CHUNK);
     Best b = best_init(own);
-    for (int32_t s = s0 + threadIdx.x; s < s1; s += 256) {
-        const int32_t c = keys[s];
-        if (c >= 0) {
-            eval_candidate(c, vals[s], m, st.T, st.S, st.size, b);
-            keys[s] = -1;
-            vals[s] = 0;
-        }
-    }
-    cta_reduce_best<256>(b, own);
+    eval_slots<4, true, true>(keys, vals, hg.occ + hg.occ_off[h] + s0, n, threadIdx.x, 256, m, st.S,
+                              st.size, b);
+    cta_reduce_best<256>(m, b);
     if (threadIdx.x == 0) {
-        hg.res_g[2 * bi] = (u64)b.g;
-        hg.res_g[2 * bi + 1] = (u64)((u128)b.g >> 64);
+        hg.res_g[2 * bi] = (u64)__double_as_longlong(b.gd);
+        hg.res_g[2 * bi + 1] = b.S;
         hg.res_c[bi] = b.c;
         hg.res_e[bi] = b.eo;
-        hg.res_b[bi] = b.eb;
+        hg.res_b[bi] = b.e;
     }
 }
 
@@ -280,18 +221,27 @@ __global__ void __launch_bounds__(256) hubg_final_kernel(StateView st, HubGlobal
         v = hg.hubs[h];
         own = st.comm[v];
     }
+    const MoveCtx m = move_ctx(own, active ? st.size[own] == 1 : false, st.T, active ? st.k[v] : 0,
+                               active ? st.S[own] : 0);
     Best b = best_init(own);
     if (active) {
         for (int32_t bi = hg.hub_schunk0[h] + lane; bi < hg.hub_schunk0[h + 1]; bi += 32) {
-            const i128 og = (i128)(((u128)hg.res_g[2 * bi + 1] << 64) | (u128)hg.res_g[2 * bi]);
-            const int32_t oc = hg.res_c[bi];
-            if (better(og, oc, b.g, b.c)) { b.g = og; b.c = oc; b.eb = hg.res_b[bi]; }
+            Best o;
+            o.gd = __longlong_as_double((long long)hg.res_g[2 * bi]);
+            o.S = hg.res_g[2 * bi + 1];
+            o.c = hg.res_c[bi];
+            o.e = hg.res_b[bi];
+            o.eo = 0;
+            if (better(m, o, b)) { b.gd = o.gd; b.e = o.e; b.S = o.S; b.c = o.c; }
             b.eo += hg.res_e[bi];
         }
     }
-    group_reduce_best(b, 32);
+    group_reduce_best(m, b, 32);
     u64 delta = 0;
-    if (active && lane == 0) st.newc[v] = move_decision(b, st.T, own, &delta);
+    if (active && lane == 0) {
+        st.newc[v] = move_decision(m, b, &delta);
+        hg.nocc[h] = 0;   // the table and its list are clean again
+    }
     block_add_total<256>(delta, dE);
 }
 
@@ -358,42 +308,24 @@ __global__ void __launch_bounds__(T) corr_cta_kernel(GraphView<WT> g, const int3
 // ------------------------------------------------------------------------
 // commit of one sub-round (updateVertexCommunity + Sigma_tot update)
 // ------------------------------------------------------------------------
-// Size and Sigma_tot updates are aggregated per warp by destination (and by
-// source) community, so many vertices joining one community in a sub-round
-// cost one atomic per warp.
 __global__ void __launch_bounds__(256) commit_kernel(StateView st, const int32_t *__restrict__ list,
                                                      int32_t n, u64 *moves) {
     const int32_t i = blockIdx.x * 256 + threadIdx.x;
-    const int lane = threadIdx.x & 31;
-    bool mv = false;
-    int32_t v = 0, nc = 0, oc = 0;
-    u64 kv = 0;
+    u64 mv = 0;
     if (i < n) {
-        v = list[i];
-        nc = st.newc[v];
-        oc = st.comm[v];
-        mv = nc != oc;
-        if (mv) {
+        const int32_t v = list[i];
+        const int32_t nc = st.newc[v], oc = st.comm[v];
+        if (nc != oc) {
+            mv = 1;
             st.comm[v] = nc;
-            kv = st.k[v];
+            atomicAdd(st.size + nc, 1);
+            atomicSub(st.size + oc, 1);
+            const u64 kv = st.k[v];
+            atomicAdd(st.S + nc, kv);
+            atomicAdd(st.S + oc, (u64)0 - kv);
         }
     }
-    const unsigned act = __ballot_sync(FULL, mv);
-    if (mv) {
-        unsigned peers = __match_any_sync(act, nc);
-        u64 sum = redux_add_u64(peers, kv);
-        if (lane == __ffs(peers) - 1) {
-            atomicAdd(st.size + nc, __popc(peers));
-            atomicAdd(st.S + nc, sum);
-        }
-        peers = __match_any_sync(act, oc);
-        sum = redux_add_u64(peers, kv);
-        if (lane == __ffs(peers) - 1) {
-            atomicSub(st.size + oc, __popc(peers));
-            atomicAdd(st.S + oc, (u64)0 - sum);
-        }
-    }
-    block_add_total<256>(mv ? 1ull : 0ull, moves);
+    block_add_total<256>(mv, moves);
 }
 
 // ------------------------------------------------------------------------
@@ -494,7 +426,9 @@ inline unsigned nblocks(int64_t items, int per_block) {
 
 }  // namespace
 
-// Dynamic shared memory of the CTA kernels: CAPMAX * (8 + 4) bytes.
+// Dynamic shared memory of the CTA kernels: CAPMAX * (8 + 4) bytes of table
+// plus CAPMAX / 2 occupied-slot indices.
+constexpr int CTA_SLOT_BYTES = 14;
 constexpr int B5_THREADS = 128, B5_CAP = 1024;
 constexpr int H1_THREADS = 256, H1_CAP = 2048;
 constexpr int H2_THREADS = 512, H2_CAP = 8192;
@@ -504,15 +438,15 @@ static void set_attrs_for(DeviceInfo &di) {
     auto k5 = move_cta_kernel<B5_THREADS, B5_CAP, WT>;
     auto k6 = move_cta_kernel<H1_THREADS, H1_CAP, WT>;
     auto k7 = move_cta_kernel<H2_THREADS, H2_CAP, WT>;
-    cudaFuncSetAttribute(k5, cudaFuncAttributeMaxDynamicSharedMemorySize, B5_CAP * 12);
-    cudaFuncSetAttribute(k6, cudaFuncAttributeMaxDynamicSharedMemorySize, H1_CAP * 12);
-    cudaFuncSetAttribute(k7, cudaFuncAttributeMaxDynamicSharedMemorySize, H2_CAP * 12);
+    cudaFuncSetAttribute(k5, cudaFuncAttributeMaxDynamicSharedMemorySize, B5_CAP * CTA_SLOT_BYTES);
+    cudaFuncSetAttribute(k6, cudaFuncAttributeMaxDynamicSharedMemorySize, H1_CAP * CTA_SLOT_BYTES);
+    cudaFuncSetAttribute(k7, cudaFuncAttributeMaxDynamicSharedMemorySize, H2_CAP * CTA_SLOT_BYTES);
     cudaFuncSetAttribute(hubg_insert_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          HG_INSERT_SMEM);
     int o5 = 0, o6 = 0, o7 = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o5, k5, B5_THREADS, B5_CAP * 12);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o6, k6, H1_THREADS, H1_CAP * 12);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o7, k7, H2_THREADS, H2_CAP * 12);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o5, k5, B5_THREADS, B5_CAP * CTA_SLOT_BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o6, k6, H1_THREADS, H1_CAP * CTA_SLOT_BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o7, k7, H2_THREADS, H2_CAP * CTA_SLOT_BYTES);
     di.occ_b5 = o5 > 0 ? o5 : 1;
     di.occ_h1 = o6 > 0 ? o6 : 1;
     di.occ_h2 = o7 > 0 ? o7 : 1;
@@ -539,17 +473,17 @@ void launch_move_class(int cls, const GraphView<WT> &g, const StateView &st, con
     case CLS_B4: move_group_kernel<32, 256, WT><<<nblocks(n, 8), 256, 0, s>>>(g, st, list, n, dE); note_launches(1); break;
     case CLS_B5: {
         unsigned grid = (unsigned)imin64(n, (int64_t)di.sms * di.occ_b5);
-        move_cta_kernel<B5_THREADS, B5_CAP, WT><<<grid, B5_THREADS, B5_CAP * 12, s>>>(g, st, list, n, dE); note_launches(1);
+        move_cta_kernel<B5_THREADS, B5_CAP, WT><<<grid, B5_THREADS, B5_CAP * CTA_SLOT_BYTES, s>>>(g, st, list, n, dE); note_launches(1);
         break;
     }
     case CLS_H1: {
         unsigned grid = (unsigned)imin64(n, (int64_t)di.sms * di.occ_h1);
-        move_cta_kernel<H1_THREADS, H1_CAP, WT><<<grid, H1_THREADS, H1_CAP * 12, s>>>(g, st, list, n, dE); note_launches(1);
+        move_cta_kernel<H1_THREADS, H1_CAP, WT><<<grid, H1_THREADS, H1_CAP * CTA_SLOT_BYTES, s>>>(g, st, list, n, dE); note_launches(1);
         break;
     }
     case CLS_H2: {
         unsigned grid = (unsigned)imin64(n, (int64_t)di.sms * di.occ_h2);
-        move_cta_kernel<H2_THREADS, H2_CAP, WT><<<grid, H2_THREADS, H2_CAP * 12, s>>>(g, st, list, n, dE); note_launches(1);
+        move_cta_kernel<H2_THREADS, H2_CAP, WT><<<grid, H2_THREADS, H2_CAP * CTA_SLOT_BYTES, s>>>(g, st, list, n, dE); note_launches(1);
         break;
     }
     case CLS_HG: {

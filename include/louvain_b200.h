@@ -47,7 +47,9 @@ typedef struct lv_opts {
     int32_t profile;       /* 1: time every kernel class with CUDA events  */
     int32_t verify;        /* 1: after every sweep, check the incrementally
                               maintained modularity against a full pass    */
-    int32_t reserved[11];
+    int32_t trace;         /* 1: per-level and per-sweep lines on stderr
+                              (class sizes, moves, modularity, device ms)  */
+    int32_t reserved[10];
 } lv_opts;
 
 /* Per-run counters; times in milliseconds (device time, CUDA events). */
