@@ -41,8 +41,9 @@ SEED = 1
 EDGE_FACTOR = 16
 MIN_GAIN = 1e-6
 FALLBACK_HBM_GBS = 6650.0
+# move-phase profile slots: the update buckets (degree ranges) 0..6
 CLASS_NAMES = ["b0_deg4", "b1_deg8", "b2_deg16", "b3_deg32", "b4_deg84", "b5_deg319",
-               "h1_deg1024", "h2_deg4096", "hg_global"]
+               "b6_deg8192", "b6_giants", "unused8"]
 
 
 def load_pkg():

@@ -29,7 +29,8 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "liblouvain_b200.so")
+# LV_LIB may point at another build of the same library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("LV_LIB") or os.path.join(_HERE, "lib", "liblouvain_b200.so")
 CLI_PATH = os.path.join(_HERE, "bin", "gpulouvain")
 
 LV_OK = 0
@@ -43,8 +44,9 @@ LV_ERR_IO = 7
 LV_ERR_NO_DEVICE = 8
 
 NUM_CLASSES = 9
+# move-phase profile slots: the update buckets (degree ranges) 0..6
 CLASS_NAMES = ["b0_deg4", "b1_deg8", "b2_deg16", "b3_deg32", "b4_deg84", "b5_deg319",
-               "h1_deg1024", "h2_deg4096", "hg_global"]
+               "b6_deg8192", "b6_giants", "unused8"]
 
 
 class LouvainError(RuntimeError):

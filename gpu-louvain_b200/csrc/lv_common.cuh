@@ -12,6 +12,19 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// Tuning knobs (compile-time): edges per lane in flight in the insert loops
+// of the group (LV_U_GROUP) and CTA (LV_U_CTA) kernels, and table entries per
+// lane in flight in the evaluation loops (LV_U_EVAL).
+#ifndef LV_U_GROUP
+#define LV_U_GROUP 2
+#endif
+#ifndef LV_U_CTA
+#define LV_U_CTA 4
+#endif
+#ifndef LV_U_EVAL
+#define LV_U_EVAL 4
+#endif
+
 namespace lv {
 
 typedef unsigned long long u64;
@@ -29,18 +42,18 @@ constexpr int NBUCKETS = 7;
 // buckets 0..5; bucket 6 (degree > 319) is split by degree into three
 // classes that differ only in where their hash table lives.
 enum WorkClass {
-    CLS_B0 = 0,   // (0,4]      4 lanes / vertex, shared table of 8
-    CLS_B1,       // (4,8]      8 lanes, table 16
-    CLS_B2,       // (8,16]     16 lanes, table 32
-    CLS_B3,       // (16,32]    32 lanes, table 64
-    CLS_B4,       // (32,84]    32 lanes, table 256
-    CLS_B5,       // (84,319]   CTA of 128, table <= 1024
-    CLS_H1,       // (319,1024] CTA of 256, table <= 2048
-    CLS_H2,       // (1024,4096] CTA of 512, table <= 8192
-    CLS_HG,       // > 4096     multi-CTA, table in global memory
+    CLS_B0 = 0,   // (0,4]       4 lanes / vertex, shared table of 8
+    CLS_B1,       // (4,8]       8 lanes, table 16
+    CLS_B2,       // (8,16]      16 lanes, table 32
+    CLS_B3,       // (16,32]     32 lanes, table 64
+    CLS_B4,       // (32,84]     warp table (bucket 4)
+    CLS_B5,       // (84,319]    warp table (bucket 5)
+    CLS_H1,       // (319,1024]  warp table, CTA fallback (bucket 6)
+    CLS_H2,       // (1024,8192] warp table, CTA fallback (bucket 6)
+    CLS_HG,       // > 8192      edge chunks staged and merged (bucket 6)
     NCLS
 };
-constexpr int CLASS_MAX_DEG[NCLS] = {4, 8, 16, 32, 84, 319, 1024, 4096, 0x7fffffff};
+constexpr int HG_MIN_DEG = 8192;   // giants: degree above this
 // class -> update bucket
 __host__ __device__ constexpr int class_bucket(int c) { return c < CLS_H1 ? c : 6; }
 
@@ -53,12 +66,12 @@ __host__ __device__ __forceinline__ int degree_class(int32_t d) {
     if (d <= 84) return CLS_B4;
     if (d <= 319) return CLS_B5;
     if (d <= 1024) return CLS_H1;
-    if (d <= 4096) return CLS_H2;
+    if (d <= HG_MIN_DEG) return CLS_H2;
     return CLS_HG;
 }
 
 // Device error bits (OR-ed into a device word, read back once per sweep).
-enum DevErr { DEVERR_HASH_FULL = 1, DEVERR_BAD_STATE = 2 };
+enum DevErr { DEVERR_HASH_FULL = 1, DEVERR_BAD_STATE = 2, DEVERR_FALLBACK_FULL = 4 };
 
 __host__ __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
 

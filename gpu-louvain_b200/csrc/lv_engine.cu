@@ -119,10 +119,16 @@ struct lv_handle {
     size_t occ_cap = 0;
     int32_t *nocc_buf = nullptr;   // per-hub list lengths, zero between uses
     size_t nocc_cap = 0;
+    int32_t *stage_key = nullptr;  // staging area of the hub path (entries = occ_cap)
+    u64 *stage_val = nullptr;
+    u64 *eown_buf = nullptr;       // per hub, zero between uses (nocc_cap entries)
+    int32_t *ovf_buf = nullptr;    // overflow list (nocc_cap entries) then its count
 
     bool agg_ready = false;
     AggBuffers ab{};
     int32_t *mslot = nullptr, *degm = nullptr, *P = nullptr;
+
+    Fallback fb;
 
     Totals *tot_d = nullptr;
     Totals *tot_h = nullptr;
@@ -245,6 +251,7 @@ int check_device_error(lv_handle *h, int errword) {
     std::string m = "device check failed:";
     if (errword & DEVERR_HASH_FULL) m += " hash table full";
     if (errword & DEVERR_BAD_STATE) m += " invalid community id";
+    if (errword & DEVERR_FALLBACK_FULL) m += " fallback list full";
     return fail(h, LV_ERR_DEVICE, m);
 }
 
@@ -284,17 +291,27 @@ int ensure_tables(lv_handle *h, size_t slots) {
 int ensure_occ(lv_handle *h, size_t entries, size_t hubs) {
     if (entries > h->occ_cap) {
         dfree(h->occ_buf);
+        dfree(h->stage_key);
+        dfree(h->stage_val);
         h->occ_cap = 0;
         size_t want = entries + entries / 4 + 1;
         LV_TRY(dalloc(h, &h->occ_buf, want));
+        LV_TRY(dalloc(h, &h->stage_key, want));
+        LV_TRY(dalloc(h, &h->stage_val, want));
         h->occ_cap = want;
     }
     if (hubs > h->nocc_cap) {
         dfree(h->nocc_buf);
+        dfree(h->eown_buf);
+        dfree(h->ovf_buf);
         h->nocc_cap = 0;
         size_t want = hubs + hubs / 4 + 1;
         LV_TRY(dalloc(h, &h->nocc_buf, want));
+        LV_TRY(dalloc(h, &h->eown_buf, want));
+        LV_TRY(dalloc(h, &h->ovf_buf, want + 1));   // overflow list + its count
         LV_CUDA(h, cudaMemsetAsync(h->nocc_buf, 0, want * sizeof(int32_t), h->stream));
+        LV_CUDA(h, cudaMemsetAsync(h->eown_buf, 0, want * sizeof(u64), h->stream));
+        LV_CUDA(h, cudaMemsetAsync(h->ovf_buf, 0, (want + 1) * sizeof(int32_t), h->stream));
         h->nocc_cap = want;
     }
     return LV_OK;
@@ -303,7 +320,8 @@ int ensure_occ(lv_handle *h, size_t entries, size_t hubs) {
 // ids: hub vertices / communities; deg: their degree bound; cap_limit caps
 // the distinct-key count (newV for aggregation, unlimited for moves).
 int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
-                 const std::vector<int32_t> &deg, int64_t cap_limit) {
+                 const std::vector<int32_t> &deg, int64_t cap_limit, bool occ_lists, int echunk,
+                 bool tables) {
     const int32_t n = (int32_t)ids.size();
     std::vector<int64_t> off(n), occ_off(n);
     int64_t occ_total = 0;
@@ -317,26 +335,27 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
         lg[i] = l;
         off[i] = total;
         total += int64_t(1) << l;
-        for (int32_t e0 = 0; e0 < deg[i]; e0 += HG_EDGE_CHUNK) {
+        for (int32_t e0 = 0; e0 < deg[i]; e0 += echunk) {
             ech_hub.push_back(i);
             ech_e0.push_back(e0);
         }
-        // a hub of degree d has at most min(d, cap) occupied slots: its
-        // occupied list has room for d entries, evaluated in slot chunks
+        // evaluation chunks: over the occupied list (room for deg entries)
+        // when occ_lists is set, else over the contiguous table
         hub_s0[i] = (int32_t)sch_hub.size();
         occ_off[i] = occ_total;
         occ_total += deg[i];
-        for (int64_t s0 = 0; s0 < (int64_t)deg[i]; s0 += HG_SLOT_CHUNK) {
+        const int64_t span = occ_lists ? (int64_t)deg[i] : (int64_t(1) << l);
+        for (int64_t s0 = 0; s0 < span; s0 += HG_SLOT_CHUNK) {
             sch_hub.push_back(i);
             sch_s0.push_back((int32_t)s0);
         }
-        if (deg[i] == 0) {
+        if (span == 0) {
             sch_hub.push_back(i);
             sch_s0.push_back(0);
         }
     }
     hub_s0[n] = (int32_t)sch_hub.size();
-    LV_TRY(ensure_tables(h, (size_t)total));
+    if (tables) LV_TRY(ensure_tables(h, (size_t)total));
     LV_TRY(ensure_occ(h, (size_t)occ_total, (size_t)n));
     const size_t ne = ech_hub.size(), ns = sch_hub.size();
     // packed: ids | lg | ech_hub | ech_e0 | sch_hub | sch_s0 | hub_s0 | res_c | (8-aligned) off |
@@ -393,6 +412,11 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
     v.occ_off = (const int64_t *)(d8 + (size_t)n * 8 + ns * 32);
     v.occ = h->occ_buf;
     v.nocc = h->nocc_buf;
+    v.stage_key = h->stage_key;
+    v.stage_val = h->stage_val;
+    v.eown = h->eown_buf;
+    v.ovf_list = h->ovf_buf;
+    v.ovf_count = h->ovf_buf + h->nocc_cap;
     v.keys = h->tbl_keys;
     v.vals = h->tbl_vals;
     L.ids = ids;
@@ -430,7 +454,7 @@ int level_setup(lv_handle *h) {
         LV_TRY(compute_k<float>(h));
     }
     launch_level_init(h->comm, h->newc, h->size, h->k, h->S, h->V, h->stream);
-    // global tables for the hubs of class HG
+    // giants (degree > HG_MIN_DEG): staging areas and global tables
     const int32_t nh = h->cls_off[CLS_HG + 1] - h->cls_off[CLS_HG];
     std::vector<int32_t> ids(nh), deg(nh);
     if (nh > 0) {
@@ -443,11 +467,10 @@ int level_setup(lv_handle *h) {
                                    h->stream));
         LV_TRY(sync(h));
     }
-    LV_TRY(build_layout(h, h->hub_move, ids, deg, 0));
+    LV_TRY(build_layout(h, h->hub_move, ids, deg, 0, false, STAGE_CHUNK, false));
     t.stop();
     if (h->opts.trace) {
-        std::fprintf(stderr, "[lv] level %d: V=%d E=%lld hub_table_slots=%zu classes:", h->level, h->V,
-                     (long long)h->E, h->tbl_slots);
+        std::fprintf(stderr, "[lv] level %d: V=%d E=%lld classes:", h->level, h->V, (long long)h->E);
         for (int c = 0; c < NCLS; ++c)
             std::fprintf(stderr, " %d/%lld", h->cls_off[c + 1] - h->cls_off[c], (long long)h->cls_edges[c]);
         std::fprintf(stderr, "\n");
@@ -458,6 +481,8 @@ int level_setup(lv_handle *h) {
 // ---------------------------------------------------------------------------
 // sweep and modularity
 // ---------------------------------------------------------------------------
+// Profile slots of the move phase: 0..3 the group kernels of buckets 0..3,
+// 4, 5, 6 the warp + fallback kernels of buckets 4, 5 and 6.
 template <typename WT>
 void enqueue_sweep(lv_handle *h) {
     GraphView<WT> g = view_of<WT>(h);
@@ -470,20 +495,37 @@ void enqueue_sweep(lv_handle *h) {
         const int c0 = b, c1 = (b < 6) ? b + 1 : NCLS;
         const int32_t lo = h->cls_off[c0], hi = h->cls_off[c1];
         if (hi == lo) continue;
-        for (int c = c0; c < c1; ++c) {
-            const int32_t n = h->cls_off[c + 1] - h->cls_off[c];
-            if (n == 0) continue;
+        const int32_t hg0 = (b == 6) ? h->cls_off[CLS_HG] : hi;   // bucket 6: giants after
+        int64_t edges = 0;
+        for (int c = c0; c < c1; ++c)
+            if (c != CLS_HG) edges += h->cls_edges[c];
+        Timer *tc = nullptr;
+        if (h->opts.profile) {
+            tc = new Timer(h, b);
+            tc->verts = hg0 - lo;
+            tc->edges = edges;
+            tc->bytes = (8.0 + wbytes) * (double)edges + 20.0 * (double)(hg0 - lo);
+        }
+        if (b < 4)
+            launch_move_class<WT>(b, g, st, h->list + lo, hi - lo, h->di, dE, h->stream);
+        else if (hg0 > lo)
+            launch_move_wide<WT>(g, st, h->list + lo, hg0 - lo, h->fb, h->di, dE, h->stream);
+        if (tc) {
+            tc->stop();
+            delete tc;
+            tc = nullptr;
+        }
+        if (hi > hg0) {
             if (h->opts.profile) {
-                Timer tc(h, c);
-                tc.verts = n;
-                tc.edges = h->cls_edges[c];
-                tc.bytes = (8.0 + wbytes) * (double)h->cls_edges[c] + 20.0 * (double)n;
-                launch_move_class<WT>(c, g, st, h->list + h->cls_off[c], n, h->hub_move.view, h->di,
-                                      dE, h->stream);
-                tc.stop();
-            } else {
-                launch_move_class<WT>(c, g, st, h->list + h->cls_off[c], n, h->hub_move.view, h->di,
-                                      dE, h->stream);
+                tc = new Timer(h, 7);
+                tc->verts = hi - hg0;
+                tc->edges = h->cls_edges[CLS_HG];
+                tc->bytes = (8.0 + wbytes) * (double)tc->edges + 20.0 * (double)tc->verts;
+            }
+            launch_move_giants<WT>(g, st, h->hub_move.view, h->fb, h->di, dE, h->stream);
+            if (tc) {
+                tc->stop();
+                delete tc;
             }
         }
         // exact modularity bookkeeping for neighbours that moved together
@@ -667,7 +709,7 @@ int aggregate_t(lv_handle *h) {
                                    cudaMemcpyDeviceToHost, h->stream));
         LV_TRY(sync(h));
     }
-    LV_TRY(build_layout(h, h->hub_agg, ids, deg, newV));
+    LV_TRY(build_layout(h, h->hub_agg, ids, deg, newV, true, HG_EDGE_CHUNK, true));
     GraphView<WT> g = view_of<WT>(h);
     for (int c = 0; c < NCLS; ++c)
         agg_permute<WT>(c, g, ab, h->mslot, h->P, h->list + h->cls_off[c],
@@ -735,6 +777,27 @@ int finish_create(lv_handle *h) {
     LV_TRY(dalloc(h, &h->S, V + 1));
     LV_TRY(dalloc(h, &h->list, V + 1));
     LV_TRY(dalloc(h, &h->cls_scratch, V + SCRATCH_OFF + 16));
+    {
+        // fallback work list of the move phase: at most one item per FB_KEYS
+        // edges of each vertex
+        Fallback &f = h->fb;
+        const size_t cap = V + (size_t)(h->E0 / FB_KEYS) + 64;
+        LV_TRY(dalloc(h, &f.count, 2));
+        f.next = f.count + 1;
+        f.cap = (int32_t)cap;
+        LV_TRY(dalloc(h, &f.v, cap));
+        LV_TRY(dalloc(h, &f.p, cap));
+        LV_TRY(dalloc(h, &f.P, cap));
+        LV_TRY(dalloc(h, &f.first, cap));
+        LV_TRY(dalloc(h, &f.src, cap));
+        LV_TRY(dalloc(h, &f.done, cap));
+        LV_TRY(dalloc(h, &f.gd, cap));
+        LV_TRY(dalloc(h, &f.e, cap));
+        LV_TRY(dalloc(h, &f.S, cap));
+        LV_TRY(dalloc(h, &f.eo, cap));
+        LV_TRY(dalloc(h, &f.c, cap));
+        LV_CUDA(h, cudaMemsetAsync(f.done, 0, cap * sizeof(int32_t), h->stream));
+    }
     LV_TRY(dalloc(h, &h->tot_d, 1));
     LV_CUDA(h, cudaMemsetAsync(h->tot_d, 0, sizeof(Totals), h->stream));
     LV_CUDA(h, cudaMallocHost((void **)&h->tot_h, sizeof(Totals)));
@@ -850,9 +913,15 @@ int lv_destroy(lv_handle *h) {
         dfree(h->in_col);
         dfree(h->in_w);
     }
+    {
+        Fallback &f = h->fb;
+        dfree(f.count); dfree(f.v); dfree(f.p); dfree(f.P); dfree(f.first); dfree(f.done); dfree(f.src);
+        dfree(f.gd); dfree(f.e); dfree(f.S); dfree(f.eo); dfree(f.c);
+    }
     dfree(h->comm); dfree(h->newc); dfree(h->size); dfree(h->orig2comm);
     dfree(h->k); dfree(h->S); dfree(h->list); dfree(h->cls_scratch);
     dfree(h->tbl_keys); dfree(h->tbl_vals); dfree(h->occ_buf); dfree(h->nocc_buf);
+    dfree(h->stage_key); dfree(h->stage_val); dfree(h->eown_buf); dfree(h->ovf_buf);
     if (h->hub_move.dev) cudaFree(h->hub_move.dev);
     if (h->hub_agg.dev) cudaFree(h->hub_agg.dev);
     AggBuffers &a = h->ab;

@@ -8,10 +8,18 @@ namespace lv {
 // for the current level.  Hubs are split into edge chunks (insert kernel)
 // and chunks of their occupied-slot list (evaluate kernel) so that one hub
 // spreads over many CTAs; a hub of degree d has at most d occupied slots.
-constexpr int HG_EDGE_CHUNK = 4096;
-constexpr int HG_SLOT_CHUNK = 4096;
+constexpr int HG_EDGE_CHUNK = 4096;   // aggregation: entries per insert CTA
+constexpr int HG_SLOT_CHUNK = 4096;   // table slots per evaluation CTA
 constexpr int HG_INSERT_THREADS = 512;
 constexpr int HG_INSERT_SMEM = 2 * HG_EDGE_CHUNK * 12;   // chunk-local table
+// move phase, giant vertices: chunks of STAGE_CHUNK edges reduced by
+// STAGE_THREADS-thread CTAs in a 2*STAGE_CHUNK-slot table
+constexpr int STAGE_CHUNK = 2048;
+constexpr int STAGE_THREADS = 256;
+constexpr int STAGE_SMEM = 2 * STAGE_CHUNK * 14;
+constexpr int HG_MERGE_THREADS = 1024;
+constexpr int HG_MERGE_CAP = 16384;                      // shared slots of the per-hub merge
+constexpr int HG_MERGE_SMEM = HG_MERGE_CAP * 14;
 
 struct HubGlobal {
     int32_t nhubs = 0;
@@ -31,28 +39,68 @@ struct HubGlobal {
     int32_t *res_c = nullptr;             // [n_schunks] best community
     u64 *res_e = nullptr;                 // [n_schunks] e_own contribution
     u64 *res_b = nullptr;                 // [n_schunks] weight to the best community
-    const int64_t *occ_off = nullptr;     // [nhubs] first entry of each hub's occupied list
+    const int64_t *occ_off = nullptr;     // [nhubs] first entry of each hub's list / staging area
     int32_t *occ = nullptr;               // occupied slots, listed per hub
-    int32_t *nocc = nullptr;              // [nhubs] occupied-list lengths (kept zero between uses)
+    int32_t *nocc = nullptr;              // [nhubs] list / staging lengths (kept zero between uses)
+    // staged two-level reduction of the move phase (room for deg entries per hub)
+    int32_t *stage_key = nullptr;
+    u64 *stage_val = nullptr;
+    u64 *eown = nullptr;                  // [nhubs] weight to the own community (zero between uses)
+    int32_t *ovf_list = nullptr;          // hubs whose staged pairs overflow shared memory
+    int32_t *ovf_count = nullptr;         // length of ovf_list (reset by the host per use)
 };
 
 // Count of engine kernel launches (all handles, all devices of the process).
 void note_launches(int n);
 long long launches_total();
 
+// Move phase for degree > 32: warp tables of WARP_CAP slots (a vertex with
+// more than WARP_LIMIT distinct neighbour communities falls back), fallback
+// CTAs of FB_THREADS threads with FB_CAP-slot tables, one item per FB_KEYS
+// edges of the vertex.
+constexpr int WARP_CAP = 512;
+constexpr int WARP_LIMIT = 352;
+constexpr int FB_THREADS = 1024;
+constexpr int FB_CAP = 16384;
+constexpr int FB_KEYS = 6144;
+constexpr int FB_SMEM = FB_CAP * 14;   // table + occupied list
+constexpr int WARP_SMEM = 8 * WARP_CAP * 12;   // 8 warp tables per CTA
+
+// Fallback work list (device memory; count and next are adjacent).
+struct Fallback {
+    int32_t *count = nullptr;   // items queued by the warp kernel
+    int32_t *next = nullptr;    // next item to take (= count + 1)
+    int32_t cap = 0;
+    int32_t *v = nullptr, *p = nullptr, *P = nullptr, *first = nullptr;
+    int32_t *src = nullptr;     // -1: the vertex's row; h >= 0: staged pairs of giant h
+    int32_t *done = nullptr;    // per first item, zero between uses
+    double *gd = nullptr;
+    u64 *e = nullptr, *S = nullptr, *eo = nullptr;
+    int32_t *c = nullptr;
+};
+
 // Launch geometry helpers (filled once per device).
 struct DeviceInfo {
     int sms = 148;
-    int occ_b5 = 8, occ_h1 = 4, occ_h2 = 2;   // resident CTAs per SM
+    int occ_warp = 4;   // resident CTAs per SM of the warp kernel
 };
 void init_kernel_attributes(DeviceInfo &di);
 
 // ---- move phase (lv_move.cu) ----
 // dE accumulates (wrapping uint64) each mover's 2 (e_best - e_own).
+// Classes B0..B3 (degree <= 32): group kernels.
 template <typename WT>
 void launch_move_class(int cls, const GraphView<WT> &g, const StateView &st, const int32_t *list,
-                       int32_t n, const HubGlobal &hg, const DeviceInfo &di, u64 *dE,
-                       cudaStream_t s);
+                       int32_t n, const DeviceInfo &di, u64 *dE, cudaStream_t s);
+// 32 < degree <= 8192 (the vertices of one update bucket): warp kernel +
+// fallback.  Degree > 8192: staged chunks + merge (hg describes the giants).
+template <typename WT>
+void launch_move_wide(const GraphView<WT> &g, const StateView &st, const int32_t *list, int32_t n,
+                      const Fallback &fb, const DeviceInfo &di, u64 *dE, cudaStream_t s,
+                      bool split = false);
+template <typename WT>
+void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGlobal &hg,
+                        const Fallback &fb, const DeviceInfo &di, u64 *dE, cudaStream_t s);
 // Exact correction of dE for neighbours that moved in the same sub-round.
 template <typename WT>
 void launch_correction(int cls, const GraphView<WT> &g, const StateView &st, const int32_t *list,

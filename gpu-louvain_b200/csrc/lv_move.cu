@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(256) move_group_kernel(GraphView<WT> g, StateV
     if (active) {
         v = list[idx];
         own = __ldg(st.comm + v);
-        insert_row<(CAP > 32 ? 4 : 2), false>(g, st.comm, v, own, g.rowptr[v], g.rowend[v], lane, G,
+        insert_row<(CAP > 32 ? LV_U_CTA : LV_U_GROUP), false>(g, st.comm, v, own, g.rowptr[v], g.rowend[v], lane, G,
                                                keys, vals, LG, st.err, nullptr, nullptr, e_own);
     }
     __syncwarp();
@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(256) move_group_kernel(GraphView<WT> g, StateV
                                active ? __ldg(st.k + v) : 0, active ? __ldg(st.S + own) : 0);
     Best b = best_init(own);
     b.eo = e_own;
-    if (active) eval_slots<(CAP / G > 1 ? 2 : 1), false, false>(keys, vals, nullptr, CAP, lane, G, m, st.S, st.size, b);
+    if (active) eval_slots<(CAP / G > 1 ? (LV_U_EVAL < 2 ? LV_U_EVAL : 2) : 1), false, false>(keys, vals, nullptr, CAP, lane, G, m, st.S, st.size, b);
     group_reduce_best(m, b, G);
     u64 delta = 0;
     if (active && lane == 0) st.newc[v] = move_decision(m, b, &delta);
@@ -108,141 +108,309 @@ __device__ __forceinline__ void cta_reduce_best(const MoveCtx &m, Best &b) {
 }
 
 // ------------------------------------------------------------------------
-// CTA-per-vertex move kernel (84 < degree <= 4096), persistent grid-stride
+// degree > 32: warp per vertex with an optimistic shared table, partitioned
+// fallback for vertices with many distinct neighbour communities
 // ------------------------------------------------------------------------
-template <int THREADS, int CAPMAX, typename WT>
-__global__ void __launch_bounds__(THREADS) move_cta_kernel(GraphView<WT> g, StateView st,
-                                                           const int32_t *__restrict__ list,
-                                                           int32_t n, u64 *dE) {
+// W. A warp per vertex inserts its row into a WARP_CAP-slot shared table and
+//    counts newly claimed slots with a ballot.  Once communities have formed
+//    a vertex has few distinct neighbour communities (a few percent of its
+//    degree on aggregated levels), so this decides almost every vertex.  A
+//    vertex whose count passes WARP_LIMIT stops, clears its table and is
+//    queued as P = ceil(degree / FB_KEYS) fallback items (v, p).
+// F. Persistent 1024-thread CTAs with FB_CAP-slot shared tables take items;
+//    item (v, p) streams v's row and keeps only the communities whose hash
+//    falls in partition p, evaluates them, and stores its partial best.  The
+//    CTA that finishes the last item of v combines the P partials (all the
+//    items of v are contiguous) and decides.  No global hash tables.
+__device__ __forceinline__ uint32_t part_of(int32_t c, int32_t P) {
+    const uint32_t hsh = (uint32_t)c * 0x85EBCA6Bu;
+    return (uint32_t)(((u64)(hsh ^ (hsh >> 15)) * (u64)P) >> 32);
+}
+
+template <typename WT>
+__global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateView st,
+                                                        const int32_t *__restrict__ list, int32_t n,
+                                                        Fallback fb, u64 *dE) {
+    constexpr int NW = 8;
+    constexpr int LG = ilog2_c(WARP_CAP);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    u64 *vals = reinterpret_cast<u64 *>(smem_raw);
-    int32_t *keys = reinterpret_cast<int32_t *>(vals + CAPMAX);
-    int32_t *occ = keys + CAPMAX;   // occupied slots (at most CAPMAX / 2)
-    __shared__ int32_t nocc;
-    for (int s = threadIdx.x; s < CAPMAX; s += THREADS) { keys[s] = -1; vals[s] = 0; }
-    if (threadIdx.x == 0) nocc = 0;
-    __syncthreads();
-    u64 delta_sum = 0;
-    for (int32_t idx = blockIdx.x; idx < n; idx += gridDim.x) {
+    u64 *svals = reinterpret_cast<u64 *>(smem_raw);
+    int32_t *skeys = reinterpret_cast<int32_t *>(svals + NW * WARP_CAP);
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int32_t *keys = skeys + wid * WARP_CAP;
+    u64 *vals = svals + wid * WARP_CAP;
+    for (int s = lane; s < WARP_CAP; s += 32) { keys[s] = -1; vals[s] = 0; }
+    __syncwarp();
+    u64 delta_acc = 0;
+    const int32_t nwarps = gridDim.x * NW;
+    for (int32_t idx = blockIdx.x * NW + wid; idx < n; idx += nwarps) {
         const int32_t v = list[idx];
         const int32_t own = __ldg(st.comm + v);
         const int32_t r0 = g.rowptr[v], r1 = g.rowend[v];
-        int lg = ceil_log2_i(2 * (int64_t)(r1 - r0));
-        lg = lg < 3 ? 3 : lg;
         u64 e_own = 0;
-        insert_row<4, true>(g, st.comm, v, own, r0, r1, threadIdx.x, THREADS, keys, vals, lg, st.err,
-                            occ, &nocc, e_own);
+        int32_t nclaim = 0;
+        bool overflow = false;
+        for (int32_t base = r0; base < r1; base += 32) {
+            const int32_t e = base + lane;
+            int32_t c = -1;
+            u64 w = 0;
+            if (e < r1) {
+                const int32_t j = __ldg(g.col + e);
+                if (j != v) {
+                    c = __ldg(st.comm + j);
+                    w = wfix(g.w, e, g.scale);
+                }
+            }
+            int32_t claimed = -1;
+            if (c >= 0) {
+                if (c == own) e_own += w;
+                else claimed = table_insert_claim(keys, vals, LG, c, w, st.err);
+            }
+            nclaim += __popc(__ballot_sync(FULL, claimed >= 0));
+            if (nclaim > WARP_LIMIT) { overflow = true; break; }
+        }
+        __syncwarp();
+        if (overflow) {
+            for (int s = lane; s < WARP_CAP; s += 32) {
+                if (keys[s] >= 0) { keys[s] = -1; vals[s] = 0; }
+            }
+            if (lane == 0) {
+                const int32_t P = (int32_t)((r1 - r0 + FB_KEYS - 1) / FB_KEYS);
+                const int32_t first = atomicAdd(fb.count, P);
+                if (first + P <= fb.cap) {
+                    for (int32_t q = 0; q < P; ++q) {
+                        fb.v[first + q] = v;
+                        fb.p[first + q] = q;
+                        fb.P[first + q] = P;
+                        fb.first[first + q] = first;
+                        fb.src[first + q] = -1;
+                    }
+                } else {
+                    atomicOr(st.err, DEVERR_FALLBACK_FULL);
+                }
+            }
+            __syncwarp();
+            continue;
+        }
+        const MoveCtx m = move_ctx(own, __ldg(st.size + own) == 1, st.T, __ldg(st.k + v), __ldg(st.S + own));
+        Best b = best_init(own);
+        b.eo = e_own;
+        eval_slots<1, false, true>(keys, vals, nullptr, WARP_CAP, lane, 32, m, st.S, st.size, b);
+        group_reduce_best(m, b, 32);
+        if (lane == 0) {
+            u64 delta = 0;
+            st.newc[v] = move_decision(m, b, &delta);
+            delta_acc += delta;
+        }
+        __syncwarp();
+    }
+    block_add_total<256>(delta_acc, dE);
+}
+
+template <typename WT>
+__global__ void __launch_bounds__(FB_THREADS) move_fallback_kernel(GraphView<WT> g, StateView st,
+                                                                   Fallback fb, HubGlobal hg, u64 *dE) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    u64 *vals = reinterpret_cast<u64 *>(smem_raw);
+    int32_t *keys = reinterpret_cast<int32_t *>(vals + FB_CAP);
+    int32_t *occ = keys + FB_CAP;
+    __shared__ int32_t nocc, item_sh, last_sh;
+    for (int s = threadIdx.x; s < FB_CAP; s += FB_THREADS) { keys[s] = -1; vals[s] = 0; }
+    if (threadIdx.x == 0) nocc = 0;
+    __syncthreads();
+    const int32_t count = *fb.count;
+    u64 delta_acc = 0;
+    for (;;) {
+        if (threadIdx.x == 0) item_sh = atomicAdd(fb.next, 1);
+        __syncthreads();
+        const int32_t item = item_sh;
+        if (item >= count || item >= fb.cap) break;
+        const int32_t v = fb.v[item], p = fb.p[item], P = fb.P[item], first = fb.first[item];
+        const int32_t src = fb.src[item];
+        const int32_t own = __ldg(st.comm + v);
+        u64 e_own = 0;
+        if (src < 0) {
+            // the vertex's row
+            const int32_t r0 = g.rowptr[v], r1 = g.rowend[v];
+            int lg = P > 1 ? ilog2_c(FB_CAP) : ceil_log2_i(2 * (int64_t)(r1 - r0));
+            lg = lg < 3 ? 3 : lg;
+            for (int32_t e = r0 + threadIdx.x; e < r1; e += FB_THREADS) {
+                const int32_t j = __ldg(g.col + e);
+                if (j == v) continue;
+                const int32_t c = __ldg(st.comm + j);
+                if (c == own) {
+                    if (p == 0) e_own += wfix(g.w, e, g.scale);
+                } else if (P == 1 || (int32_t)part_of(c, P) == p) {
+                    table_insert_occ(keys, vals, lg, c, wfix(g.w, e, g.scale), st.err, occ, &nocc);
+                }
+            }
+        } else {
+            // the staged (community, weight) pairs of giant src
+            const int32_t n = hg.nocc[src];
+            int lg = P > 1 ? ilog2_c(FB_CAP) : ceil_log2_i(2 * (int64_t)n);
+            lg = lg < 3 ? 3 : lg;
+            const int32_t *sk = hg.stage_key + hg.occ_off[src];
+            const u64 *sv = hg.stage_val + hg.occ_off[src];
+            for (int32_t i = threadIdx.x; i < n; i += FB_THREADS) {
+                const int32_t c = sk[i];
+                if (P == 1 || (int32_t)part_of(c, P) == p) table_insert_occ(keys, vals, lg, c, sv[i], st.err, occ, &nocc);
+            }
+            if (p == 0 && threadIdx.x == 0) e_own = hg.eown[src];
+        }
         __syncthreads();
         const MoveCtx m = move_ctx(own, __ldg(st.size + own) == 1, st.T, __ldg(st.k + v), __ldg(st.S + own));
         Best b = best_init(own);
         b.eo = e_own;
-        eval_slots<4, true, true>(keys, vals, occ, nocc, threadIdx.x, THREADS, m, st.S, st.size, b);
-        cta_reduce_best<THREADS>(m, b);
+        eval_slots<1, true, true>(keys, vals, occ, nocc, threadIdx.x, FB_THREADS, m, st.S, st.size, b);
+        cta_reduce_best<FB_THREADS>(m, b);
         if (threadIdx.x == 0) {
-            u64 delta = 0;
-            st.newc[v] = move_decision(m, b, &delta);
-            delta_sum += delta;
             nocc = 0;
+            bool decide = P == 1;
+            Best t = b;
+            if (P > 1) {
+                fb.gd[item] = b.gd;
+                fb.e[item] = b.e;
+                fb.S[item] = b.S;
+                fb.c[item] = b.c;
+                fb.eo[item] = b.eo;
+                __threadfence();
+                const int32_t done = atomicAdd(fb.done + first, 1);
+                decide = done == P - 1;
+                if (decide) {
+                    __threadfence();
+                    t = best_init(own);
+                    for (int32_t q = 0; q < P; ++q) {
+                        Best o;
+                        o.gd = __ldcg(fb.gd + first + q);
+                        o.e = __ldcg(fb.e + first + q);
+                        o.S = __ldcg(fb.S + first + q);
+                        o.c = __ldcg(fb.c + first + q);
+                        o.eo = 0;
+                        if (better(m, o, t)) { t.gd = o.gd; t.e = o.e; t.S = o.S; t.c = o.c; }
+                        t.eo += __ldcg(fb.eo + first + q);
+                    }
+                    fb.done[first] = 0;
+                }
+            }
+            if (decide) {
+                u64 delta = 0;
+                st.newc[v] = move_decision(m, t, &delta);
+                delta_acc += delta;
+                if (src >= 0) {
+                    hg.nocc[src] = 0;
+                    hg.eown[src] = 0;
+                }
+            }
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0 && delta_sum) atomicAdd(dE, delta_sum);
+    if (threadIdx.x == 0 && delta_acc) atomicAdd(dE, delta_acc);
 }
 
 // ------------------------------------------------------------------------
-// global-table hub path (degree > 4096)
+// giants (degree > 8192): staged two-level reduction
 // ------------------------------------------------------------------------
-// One CTA per chunk of HG_EDGE_CHUNK edges of one hub: the chunk is first
-// reduced in a shared table (2 * chunk slots), then each distinct key is
-// added once to the hub's global table.
+// G1. One CTA per chunk of STAGE_CHUNK edges of a giant reduces the chunk in
+//     shared memory and appends its distinct (community, weight) pairs to the
+//     giant's staging area (room for `degree` pairs); the weight to the
+//     giant's own community goes to eown[h].
+// G2. Persistent CTAs merge each giant's staged pairs in a shared table and
+//     decide its move; a giant with more staged pairs than the table holds
+//     is queued as key-space partitions of its staged pairs (fallback items
+//     with src = h), which the fallback kernel then decides.
 template <typename WT>
-__global__ void __launch_bounds__(HG_INSERT_THREADS) hubg_insert_kernel(GraphView<WT> g,
-                                                                        StateView st, HubGlobal hg) {
+__global__ void __launch_bounds__(STAGE_THREADS) giant_stage_kernel(GraphView<WT> g, StateView st,
+                                                                    HubGlobal hg) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int LCAP = 2 * HG_EDGE_CHUNK;
+    constexpr int LCAP = 2 * STAGE_CHUNK;
     constexpr int LLG = ilog2_c(LCAP);
     u64 *lvals = reinterpret_cast<u64 *>(smem_raw);
     int32_t *lkeys = reinterpret_cast<int32_t *>(lvals + LCAP);
-    for (int s = threadIdx.x; s < LCAP; s += HG_INSERT_THREADS) { lkeys[s] = -1; lvals[s] = 0; }
+    int32_t *locc = lkeys + LCAP;
+    __shared__ int32_t lnocc, base;
+    for (int s = threadIdx.x; s < LCAP; s += STAGE_THREADS) { lkeys[s] = -1; lvals[s] = 0; }
+    if (threadIdx.x == 0) lnocc = 0;
     __syncthreads();
     const int32_t h = hg.echunk_hub[blockIdx.x];
     const int32_t v = hg.hubs[h];
     const int32_t r1 = g.rowend[v];
     const int32_t e0 = g.rowptr[v] + hg.echunk_e0[blockIdx.x];
-    const int32_t e1 = min(e0 + HG_EDGE_CHUNK, r1);
+    const int32_t e1 = min(e0 + STAGE_CHUNK, r1);
     const int32_t own = __ldg(st.comm + v);
     u64 e_own = 0;
-    insert_row<4, false>(g, st.comm, v, own, e0, e1, threadIdx.x, HG_INSERT_THREADS, lkeys, lvals, LLG,
-                         st.err, nullptr, nullptr, e_own);
-    // the chunk's weight to the own community enters the table once
-    e_own = warp_sum_u64(e_own);
-    if ((threadIdx.x & 31) == 0 && e_own) table_insert(lkeys, lvals, LLG, own, e_own, st.err);
+    insert_row<1, true>(g, st.comm, v, own, e0, e1, threadIdx.x, STAGE_THREADS, lkeys, lvals, LLG, st.err,
+                        locc, &lnocc, e_own);
+    block_add_total<STAGE_THREADS>(e_own, hg.eown + h);   // contains the barrier
+    const int32_t n = lnocc;
+    if (threadIdx.x == 0) base = atomicAdd(hg.nocc + h, n);
     __syncthreads();
-    int32_t *keys = hg.keys + hg.tbl_off[h];
-    u64 *vals = hg.vals + hg.tbl_off[h];
-    int32_t *occ = hg.occ + hg.occ_off[h];
-    const int lg = hg.tbl_lg[h];
-    for (int s = threadIdx.x; s < LCAP; s += HG_INSERT_THREADS) {
-        const int32_t c = lkeys[s];
-        const int32_t claimed = c >= 0 ? table_insert_claim(keys, vals, lg, c, lvals[s], st.err) : -1;
-        warp_append(claimed, occ, hg.nocc + h);
+    int32_t *sk = hg.stage_key + hg.occ_off[h] + base;
+    u64 *sv = hg.stage_val + hg.occ_off[h] + base;
+    for (int32_t i = threadIdx.x; i < n; i += STAGE_THREADS) {
+        const int32_t sl = locc[i];
+        sk[i] = lkeys[sl];
+        sv[i] = lvals[sl];
     }
 }
 
-__global__ void __launch_bounds__(256) hubg_eval_kernel(StateView st, HubGlobal hg) {
-    const int32_t bi = blockIdx.x;
-    const int32_t h = hg.schunk_hub[bi];
-    const int32_t v = hg.hubs[h];
-    const int32_t own = st.comm[v];
-    const MoveCtx m = move_ctx(own, st.size[own] == 1, st.T, st.k[v], st.S[own]);
-    int32_t *keys = hg.keys + hg.tbl_off[h];
-    u64 *vals = hg.vals + hg.tbl_off[h];
-    const int32_t s0 = hg.schunk_s0[bi];
-    const int32_t n = min(hg.nocc[h] - s0, HG_SLOT_CHUNK);
-    Best b = best_init(own);
-    eval_slots<4, true, true>(keys, vals, hg.occ + hg.occ_off[h] + s0, n, threadIdx.x, 256, m, st.S,
-                              st.size, b);
-    cta_reduce_best<256>(m, b);
-    if (threadIdx.x == 0) {
-        hg.res_g[2 * bi] = (u64)__double_as_longlong(b.gd);
-        hg.res_g[2 * bi + 1] = b.S;
-        hg.res_c[bi] = b.c;
-        hg.res_e[bi] = b.eo;
-        hg.res_b[bi] = b.e;
-    }
-}
-
-__global__ void __launch_bounds__(256) hubg_final_kernel(StateView st, HubGlobal hg, u64 *dE) {
-    const int32_t h = (blockIdx.x * 256 + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    const bool active = h < hg.nhubs;
-    int32_t v = 0, own = 0;
-    if (active) {
-        v = hg.hubs[h];
-        own = st.comm[v];
-    }
-    const MoveCtx m = move_ctx(own, active ? st.size[own] == 1 : false, st.T, active ? st.k[v] : 0,
-                               active ? st.S[own] : 0);
-    Best b = best_init(own);
-    if (active) {
-        for (int32_t bi = hg.hub_schunk0[h] + lane; bi < hg.hub_schunk0[h + 1]; bi += 32) {
-            Best o;
-            o.gd = __longlong_as_double((long long)hg.res_g[2 * bi]);
-            o.S = hg.res_g[2 * bi + 1];
-            o.c = hg.res_c[bi];
-            o.e = hg.res_b[bi];
-            o.eo = 0;
-            if (better(m, o, b)) { b.gd = o.gd; b.e = o.e; b.S = o.S; b.c = o.c; }
-            b.eo += hg.res_e[bi];
+__global__ void __launch_bounds__(HG_MERGE_THREADS) giant_merge_kernel(StateView st, HubGlobal hg,
+                                                                       Fallback fb, u64 *dE) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    u64 *vals = reinterpret_cast<u64 *>(smem_raw);
+    int32_t *keys = reinterpret_cast<int32_t *>(vals + HG_MERGE_CAP);
+    int32_t *occ = keys + HG_MERGE_CAP;
+    __shared__ int32_t nocc;
+    for (int s = threadIdx.x; s < HG_MERGE_CAP; s += HG_MERGE_THREADS) { keys[s] = -1; vals[s] = 0; }
+    if (threadIdx.x == 0) nocc = 0;
+    __syncthreads();
+    u64 delta_sum = 0;
+    for (int32_t h = blockIdx.x; h < hg.nhubs; h += gridDim.x) {
+        const int32_t n = hg.nocc[h];
+        if (2 * (int64_t)n > HG_MERGE_CAP) {
+            // too many staged pairs for one shared table: queue key-space
+            // partitions of the staged pairs for the fallback kernel
+            if (threadIdx.x == 0) {
+                const int32_t P = (n + FB_KEYS - 1) / FB_KEYS;
+                const int32_t first = atomicAdd(fb.count, P);
+                if (first + P <= fb.cap) {
+                    for (int32_t q = 0; q < P; ++q) {
+                        fb.v[first + q] = hg.hubs[h];
+                        fb.p[first + q] = q;
+                        fb.P[first + q] = P;
+                        fb.first[first + q] = first;
+                        fb.src[first + q] = h;
+                    }
+                } else {
+                    atomicOr(st.err, DEVERR_FALLBACK_FULL);
+                }
+            }
+            continue;
         }
+        const int32_t v = hg.hubs[h];
+        const int32_t own = __ldg(st.comm + v);
+        int lg = ceil_log2_i(2 * (int64_t)n);
+        lg = lg < 3 ? 3 : lg;
+        const int32_t *sk = hg.stage_key + hg.occ_off[h];
+        const u64 *sv = hg.stage_val + hg.occ_off[h];
+        for (int32_t i = threadIdx.x; i < n; i += HG_MERGE_THREADS)
+            table_insert_occ(keys, vals, lg, sk[i], sv[i], st.err, occ, &nocc);
+        __syncthreads();
+        const MoveCtx m = move_ctx(own, __ldg(st.size + own) == 1, st.T, __ldg(st.k + v), __ldg(st.S + own));
+        Best b = best_init(own);
+        if (threadIdx.x == 0) b.eo = hg.eown[h];
+        eval_slots<1, true, true>(keys, vals, occ, nocc, threadIdx.x, HG_MERGE_THREADS, m, st.S, st.size, b);
+        cta_reduce_best<HG_MERGE_THREADS>(m, b);
+        if (threadIdx.x == 0) {
+            u64 delta = 0;
+            st.newc[v] = move_decision(m, b, &delta);
+            delta_sum += delta;
+            nocc = 0;
+            hg.nocc[h] = 0;
+            hg.eown[h] = 0;
+        }
+        __syncthreads();
     }
-    group_reduce_best(m, b, 32);
-    u64 delta = 0;
-    if (active && lane == 0) {
-        st.newc[v] = move_decision(m, b, &delta);
-        hg.nocc[h] = 0;   // the table and its list are clean again
-    }
-    block_add_total<256>(delta, dE);
+    if (threadIdx.x == 0 && delta_sum) atomicAdd(dE, delta_sum);
 }
 
 // ------------------------------------------------------------------------
@@ -426,30 +594,14 @@ inline unsigned nblocks(int64_t items, int per_block) {
 
 }  // namespace
 
-// Dynamic shared memory of the CTA kernels: CAPMAX * (8 + 4) bytes of table
-// plus CAPMAX / 2 occupied-slot indices.
-constexpr int CTA_SLOT_BYTES = 14;
-constexpr int B5_THREADS = 128, B5_CAP = 1024;
-constexpr int H1_THREADS = 256, H1_CAP = 2048;
-constexpr int H2_THREADS = 512, H2_CAP = 8192;
-
 template <typename WT>
 static void set_attrs_for(DeviceInfo &di) {
-    auto k5 = move_cta_kernel<B5_THREADS, B5_CAP, WT>;
-    auto k6 = move_cta_kernel<H1_THREADS, H1_CAP, WT>;
-    auto k7 = move_cta_kernel<H2_THREADS, H2_CAP, WT>;
-    cudaFuncSetAttribute(k5, cudaFuncAttributeMaxDynamicSharedMemorySize, B5_CAP * CTA_SLOT_BYTES);
-    cudaFuncSetAttribute(k6, cudaFuncAttributeMaxDynamicSharedMemorySize, H1_CAP * CTA_SLOT_BYTES);
-    cudaFuncSetAttribute(k7, cudaFuncAttributeMaxDynamicSharedMemorySize, H2_CAP * CTA_SLOT_BYTES);
-    cudaFuncSetAttribute(hubg_insert_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         HG_INSERT_SMEM);
-    int o5 = 0, o6 = 0, o7 = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o5, k5, B5_THREADS, B5_CAP * CTA_SLOT_BYTES);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o6, k6, H1_THREADS, H1_CAP * CTA_SLOT_BYTES);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o7, k7, H2_THREADS, H2_CAP * CTA_SLOT_BYTES);
-    di.occ_b5 = o5 > 0 ? o5 : 1;
-    di.occ_h1 = o6 > 0 ? o6 : 1;
-    di.occ_h2 = o7 > 0 ? o7 : 1;
+    cudaFuncSetAttribute(move_fallback_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM);
+    cudaFuncSetAttribute(giant_stage_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM);
+    cudaFuncSetAttribute(move_warp_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_SMEM);
+    int o = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_warp_kernel<WT>, 256, WARP_SMEM);
+    di.occ_warp = o > 0 ? o : 1;
 }
 
 void init_kernel_attributes(DeviceInfo &di) {
@@ -458,43 +610,40 @@ void init_kernel_attributes(DeviceInfo &di) {
     cudaDeviceGetAttribute(&di.sms, cudaDevAttrMultiProcessorCount, dev);
     set_attrs_for<u64>(di);
     set_attrs_for<float>(di);
+    cudaFuncSetAttribute(giant_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HG_MERGE_SMEM);
 }
 
 template <typename WT>
 void launch_move_class(int cls, const GraphView<WT> &g, const StateView &st, const int32_t *list,
-                       int32_t n, const HubGlobal &hg, const DeviceInfo &di, u64 *dE,
-                       cudaStream_t s) {
-    if (cls != CLS_HG && n <= 0) return;
+                       int32_t n, const DeviceInfo &di, u64 *dE, cudaStream_t s) {
+    if (n <= 0) return;
     switch (cls) {
     case CLS_B0: move_group_kernel<4, 8, WT><<<nblocks(n, 64), 256, 0, s>>>(g, st, list, n, dE); note_launches(1); break;
     case CLS_B1: move_group_kernel<8, 16, WT><<<nblocks(n, 32), 256, 0, s>>>(g, st, list, n, dE); note_launches(1); break;
     case CLS_B2: move_group_kernel<16, 32, WT><<<nblocks(n, 16), 256, 0, s>>>(g, st, list, n, dE); note_launches(1); break;
     case CLS_B3: move_group_kernel<32, 64, WT><<<nblocks(n, 8), 256, 0, s>>>(g, st, list, n, dE); note_launches(1); break;
-    case CLS_B4: move_group_kernel<32, 256, WT><<<nblocks(n, 8), 256, 0, s>>>(g, st, list, n, dE); note_launches(1); break;
-    case CLS_B5: {
-        unsigned grid = (unsigned)imin64(n, (int64_t)di.sms * di.occ_b5);
-        move_cta_kernel<B5_THREADS, B5_CAP, WT><<<grid, B5_THREADS, B5_CAP * CTA_SLOT_BYTES, s>>>(g, st, list, n, dE); note_launches(1);
-        break;
-    }
-    case CLS_H1: {
-        unsigned grid = (unsigned)imin64(n, (int64_t)di.sms * di.occ_h1);
-        move_cta_kernel<H1_THREADS, H1_CAP, WT><<<grid, H1_THREADS, H1_CAP * CTA_SLOT_BYTES, s>>>(g, st, list, n, dE); note_launches(1);
-        break;
-    }
-    case CLS_H2: {
-        unsigned grid = (unsigned)imin64(n, (int64_t)di.sms * di.occ_h2);
-        move_cta_kernel<H2_THREADS, H2_CAP, WT><<<grid, H2_THREADS, H2_CAP * CTA_SLOT_BYTES, s>>>(g, st, list, n, dE); note_launches(1);
-        break;
-    }
-    case CLS_HG: {
-        if (hg.nhubs <= 0) return;
-        hubg_insert_kernel<WT><<<hg.n_echunks, HG_INSERT_THREADS, HG_INSERT_SMEM, s>>>(g, st, hg); note_launches(1);
-        hubg_eval_kernel<<<hg.n_schunks, 256, 0, s>>>(st, hg); note_launches(1);
-        hubg_final_kernel<<<nblocks((int64_t)hg.nhubs * 32, 256), 256, 0, s>>>(st, hg, dE); note_launches(1);
-        break;
-    }
     default: break;
     }
+}
+
+template <typename WT>
+void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGlobal &hg,
+                        const Fallback &fb, const DeviceInfo &di, u64 *dE, cudaStream_t s) {
+    if (hg.nhubs <= 0) return;
+    cudaMemsetAsync(fb.count, 0, 2 * sizeof(int32_t), s);   // count, next
+    giant_stage_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg); note_launches(1);
+    giant_merge_kernel<<<(unsigned)imin64(hg.nhubs, di.sms), HG_MERGE_THREADS, HG_MERGE_SMEM, s>>>(st, hg, fb, dE); note_launches(1);
+    move_fallback_kernel<WT><<<di.sms, FB_THREADS, FB_SMEM, s>>>(g, st, fb, hg, dE); note_launches(1);
+}
+
+template <typename WT>
+void launch_move_wide(const GraphView<WT> &g, const StateView &st, const int32_t *list, int32_t n,
+                      const Fallback &fb, const DeviceInfo &di, u64 *dE, cudaStream_t s, bool) {
+    if (n <= 0) return;
+    cudaMemsetAsync(fb.count, 0, 2 * sizeof(int32_t), s);   // count, next
+    const unsigned grid = (unsigned)imin64((n + 7) / 8, (int64_t)di.sms * di.occ_warp);
+    move_warp_kernel<WT><<<grid, 256, WARP_SMEM, s>>>(g, st, list, n, fb, dE); note_launches(1);
+    move_fallback_kernel<WT><<<di.sms, FB_THREADS, FB_SMEM, s>>>(g, st, fb, HubGlobal(), dE); note_launches(1);
 }
 
 template <typename WT>
@@ -568,11 +717,22 @@ void launch_s2(const u64 *S, int32_t V, u64 *total_hi_lo, cudaStream_t s) {
 }
 
 template void launch_move_class<float>(int, const GraphView<float> &, const StateView &,
-                                       const int32_t *, int32_t, const HubGlobal &,
-                                       const DeviceInfo &, u64 *, cudaStream_t);
+                                       const int32_t *, int32_t, const DeviceInfo &, u64 *,
+                                       cudaStream_t);
 template void launch_move_class<u64>(int, const GraphView<u64> &, const StateView &,
-                                     const int32_t *, int32_t, const HubGlobal &,
-                                     const DeviceInfo &, u64 *, cudaStream_t);
+                                     const int32_t *, int32_t, const DeviceInfo &, u64 *,
+                                     cudaStream_t);
+template void launch_move_wide<float>(const GraphView<float> &, const StateView &, const int32_t *,
+                                      int32_t, const Fallback &, const DeviceInfo &, u64 *,
+                                      cudaStream_t, bool);
+template void launch_move_wide<u64>(const GraphView<u64> &, const StateView &, const int32_t *,
+                                    int32_t, const Fallback &, const DeviceInfo &, u64 *,
+                                    cudaStream_t, bool);
+template void launch_move_giants<float>(const GraphView<float> &, const StateView &,
+                                        const HubGlobal &, const Fallback &, const DeviceInfo &,
+                                        u64 *, cudaStream_t);
+template void launch_move_giants<u64>(const GraphView<u64> &, const StateView &, const HubGlobal &,
+                                      const Fallback &, const DeviceInfo &, u64 *, cudaStream_t);
 template void launch_correction<float>(int, const GraphView<float> &, const StateView &,
                                        const int32_t *, int32_t, const DeviceInfo &, u64 *,
                                        cudaStream_t);
