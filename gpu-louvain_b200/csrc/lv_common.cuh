@@ -196,6 +196,32 @@ __device__ __forceinline__ void table_insert_occ(int32_t *keys, u64 *vals, int l
     atomicOr(err, DEVERR_HASH_FULL);
 }
 
+// table_insert_occ for tables whose occupied list holds occ_cap slots: a
+// claim beyond that is reported as DEVERR_HASH_FULL and not listed.
+__device__ __forceinline__ void table_insert_occ_capped(int32_t *keys, u64 *vals, int lg, int32_t key,
+                                                        u64 w, int *err, int32_t *occ, int32_t *nocc,
+                                                        int32_t occ_cap) {
+    const uint32_t mask = (1u << lg) - 1u;
+    uint32_t s = hash_slot(key, lg);
+    for (uint32_t p = 0; p <= mask; ++p) {
+        int32_t k = ((volatile int32_t *)keys)[s];
+        if (k == key) { atomicAdd(vals + s, w); return; }
+        if (k < 0) {
+            int32_t prev = atomicCAS(keys + s, -1, key);
+            if (prev < 0) {
+                atomicAdd(vals + s, w);
+                const int32_t i = atomicAdd(nocc, 1);
+                if (i < occ_cap) occ[i] = (int32_t)s;
+                else atomicOr(err, DEVERR_HASH_FULL);
+                return;
+            }
+            if (prev == key) { atomicAdd(vals + s, w); return; }
+        }
+        s = (s + 1u) & mask;
+    }
+    atomicOr(err, DEVERR_HASH_FULL);
+}
+
 // Insert the row col/w[r0..r1) of vertex v, lanes lane, lane+stride, ...,
 // into a table, U edges per lane at a time so that U column loads and then U
 // community gathers are in flight together.  Self-loops are skipped; the

@@ -128,7 +128,7 @@ struct lv_handle {
     AggBuffers ab{};
     int32_t *mslot = nullptr, *degm = nullptr, *P = nullptr;
 
-    Fallback fb;
+    FallbackSet fb;
 
     Totals *tot_d = nullptr;
     Totals *tot_h = nullptr;
@@ -449,7 +449,8 @@ int level_setup(lv_handle *h) {
         h->cls_off[c + 1] = h->cls_off[c] + h->small_h[c];
         h->cls_edges[c] = (int64_t)esum[c];
     }
-    launch_class_scatter(h->cur_rowptr, h->cur_rowend, h->V, h->cls_off, cursors, h->list, h->stream);
+    launch_class_scatter(h->cur_rowptr, h->cur_rowend, h->V, h->cls_off, cursors, h->list, h->fb.hint,
+                         h->stream);
     if (h->level == 0) {
         LV_TRY(compute_k<float>(h));
     }
@@ -509,7 +510,8 @@ void enqueue_sweep(lv_handle *h) {
         if (b < 4)
             launch_move_class<WT>(b, g, st, h->list + lo, hi - lo, h->di, dE, h->stream);
         else if (hg0 > lo)
-            launch_move_wide<WT>(g, st, h->list + lo, hg0 - lo, h->fb, h->di, dE, h->stream);
+            launch_move_wide<WT>(g, st, h->list + lo, hg0 - lo, h->fb, h->di, dE, h->stream,
+                                 b == 6 ? HG_MIN_DEG : (b == 4 ? 84 : 319));
         if (tc) {
             tc->stop();
             delete tc;
@@ -778,25 +780,38 @@ int finish_create(lv_handle *h) {
     LV_TRY(dalloc(h, &h->list, V + 1));
     LV_TRY(dalloc(h, &h->cls_scratch, V + SCRATCH_OFF + 16));
     {
-        // fallback work list of the move phase: at most one item per FB_KEYS
-        // edges of each vertex
-        Fallback &f = h->fb;
-        const size_t cap = V + (size_t)(h->E0 / FB_KEYS) + 64;
-        LV_TRY(dalloc(h, &f.count, 2));
-        f.next = f.count + 1;
-        f.cap = (int32_t)cap;
-        LV_TRY(dalloc(h, &f.v, cap));
-        LV_TRY(dalloc(h, &f.p, cap));
-        LV_TRY(dalloc(h, &f.P, cap));
-        LV_TRY(dalloc(h, &f.first, cap));
-        LV_TRY(dalloc(h, &f.src, cap));
-        LV_TRY(dalloc(h, &f.done, cap));
-        LV_TRY(dalloc(h, &f.gd, cap));
-        LV_TRY(dalloc(h, &f.e, cap));
-        LV_TRY(dalloc(h, &f.S, cap));
-        LV_TRY(dalloc(h, &f.eo, cap));
-        LV_TRY(dalloc(h, &f.c, cap));
-        LV_CUDA(h, cudaMemsetAsync(f.done, 0, cap * sizeof(int32_t), h->stream));
+        // fallback work lists of the move phase.  Only vertices of degree
+        // > WARP_LIMIT are queued (at most E / WARP_LIMIT of them at any
+        // level); a large item covers FB_KEYS edges of a vertex of degree
+        // > FBM_MAXDEG, or as many staged pairs of a giant.
+        FallbackSet &fs = h->fb;
+        int32_t *counters = nullptr;
+        LV_TRY(dalloc(h, &counters, 6));
+        LV_TRY(dalloc(h, &fs.hint, V + 1));
+        LV_CUDA(h, cudaMemsetAsync(fs.hint, 0, V + 1, h->stream));
+        const size_t cap_row = (size_t)(h->E0 / WARP_LIMIT) + 64;
+        const size_t cap_large = (size_t)(2 * (h->E0 / FBM_MAXDEG + h->E0 / FB_KEYS)) + 64;
+        for (int q = 0; q < 3; ++q) {
+            Fallback &f = fs.q[q];
+            f.count = counters + 2 * q;
+            f.next = f.count + 1;
+            const size_t cap = q < 2 ? cap_row : cap_large;
+            f.cap = (int32_t)cap;
+            LV_TRY(dalloc(h, &f.v, cap));
+            if (q < 2) continue;
+            LV_TRY(dalloc(h, &f.p, cap));
+            LV_TRY(dalloc(h, &f.P, cap));
+            LV_TRY(dalloc(h, &f.first, cap));
+            LV_TRY(dalloc(h, &f.src, cap));
+            LV_TRY(dalloc(h, &f.done, cap));
+            LV_TRY(dalloc(h, &f.gd, cap));
+            LV_TRY(dalloc(h, &f.e, cap));
+            LV_TRY(dalloc(h, &f.S, cap));
+            LV_TRY(dalloc(h, &f.eo, cap));
+            LV_TRY(dalloc(h, &f.c, cap));
+            LV_TRY(dalloc(h, &f.cnt, cap));
+            LV_CUDA(h, cudaMemsetAsync(f.done, 0, cap * sizeof(int32_t), h->stream));
+        }
     }
     LV_TRY(dalloc(h, &h->tot_d, 1));
     LV_CUDA(h, cudaMemsetAsync(h->tot_d, 0, sizeof(Totals), h->stream));
@@ -914,9 +929,13 @@ int lv_destroy(lv_handle *h) {
         dfree(h->in_w);
     }
     {
-        Fallback &f = h->fb;
-        dfree(f.count); dfree(f.v); dfree(f.p); dfree(f.P); dfree(f.first); dfree(f.done); dfree(f.src);
-        dfree(f.gd); dfree(f.e); dfree(f.S); dfree(f.eo); dfree(f.c);
+        FallbackSet &fs = h->fb;
+        dfree(fs.q[0].count); dfree(fs.hint);
+        for (int q = 0; q < 3; ++q) {
+            Fallback &f = fs.q[q];
+            dfree(f.v); dfree(f.p); dfree(f.P); dfree(f.first); dfree(f.done); dfree(f.src);
+            dfree(f.gd); dfree(f.e); dfree(f.S); dfree(f.eo); dfree(f.c); dfree(f.cnt);
+        }
     }
     dfree(h->comm); dfree(h->newc); dfree(h->size); dfree(h->orig2comm);
     dfree(h->k); dfree(h->S); dfree(h->list); dfree(h->cls_scratch);

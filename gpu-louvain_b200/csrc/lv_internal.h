@@ -55,20 +55,22 @@ void note_launches(int n);
 long long launches_total();
 
 // Move phase for degree > 32: warp tables of WARP_CAP slots (a vertex with
-// more than WARP_LIMIT distinct neighbour communities falls back), fallback
-// CTAs of FB_THREADS threads with FB_CAP-slot tables, one item per FB_KEYS
-// edges of the vertex.
+// more than WARP_LIMIT distinct neighbour communities falls back).  Fallback
+// items go to one of three queues by degree: small (<= FBS_MAXDEG, CTAs of
+// 256 threads, 2048-slot tables), medium (<= FBM_MAXDEG, 512 / 8192) and
+// large (1024 / 16384, split into key-space partitions of FB_KEYS edges).
 constexpr int WARP_CAP = 512;
 constexpr int WARP_LIMIT = 352;
-constexpr int FB_THREADS = 1024;
-constexpr int FB_CAP = 16384;
+constexpr int FBS_THREADS = 256, FBS_CAP = 2048, FBS_MAXDEG = 1024;
+constexpr int FBM_THREADS = 512, FBM_CAP = 8192, FBM_MAXDEG = 4096;
+constexpr int FB_THREADS = 1024, FB_CAP = 16384;
 constexpr int FB_KEYS = 6144;
 constexpr int FB_SMEM = FB_CAP * 14;   // table + occupied list
 constexpr int WARP_SMEM = 8 * WARP_CAP * 12;   // 8 warp tables per CTA
 
-// Fallback work list (device memory; count and next are adjacent).
+// A fallback work list (device memory; count and next are adjacent).
 struct Fallback {
-    int32_t *count = nullptr;   // items queued by the warp kernel
+    int32_t *count = nullptr;   // items queued
     int32_t *next = nullptr;    // next item to take (= count + 1)
     int32_t cap = 0;
     int32_t *v = nullptr, *p = nullptr, *P = nullptr, *first = nullptr;
@@ -77,12 +79,24 @@ struct Fallback {
     double *gd = nullptr;
     u64 *e = nullptr, *S = nullptr, *eo = nullptr;
     int32_t *c = nullptr;
+    int32_t *cnt = nullptr;     // distinct communities seen by the item
+};
+
+// The three fallback queues and the per-vertex hint "had more than
+// WARP_LIMIT distinct neighbour communities at its last evaluation" (such a
+// vertex skips the warp attempt; the hint only routes work, results do not
+// depend on it).
+struct FallbackSet {
+    Fallback q[3];
+    uint8_t *hint = nullptr;
 };
 
 // Launch geometry helpers (filled once per device).
 struct DeviceInfo {
     int sms = 148;
     int occ_warp = 4;   // resident CTAs per SM of the warp kernel
+    int occ_fbs = 1;    // ... of the small and medium fallback kernels
+    int occ_fbm = 1;
 };
 void init_kernel_attributes(DeviceInfo &di);
 
@@ -96,11 +110,11 @@ void launch_move_class(int cls, const GraphView<WT> &g, const StateView &st, con
 // fallback.  Degree > 8192: staged chunks + merge (hg describes the giants).
 template <typename WT>
 void launch_move_wide(const GraphView<WT> &g, const StateView &st, const int32_t *list, int32_t n,
-                      const Fallback &fb, const DeviceInfo &di, u64 *dE, cudaStream_t s,
-                      bool split = false);
+                      const FallbackSet &fb, const DeviceInfo &di, u64 *dE, cudaStream_t s,
+                      int32_t max_degree);
 template <typename WT>
 void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGlobal &hg,
-                        const Fallback &fb, const DeviceInfo &di, u64 *dE, cudaStream_t s);
+                        const FallbackSet &fb, const DeviceInfo &di, u64 *dE, cudaStream_t s);
 // Exact correction of dE for neighbours that moved in the same sub-round.
 template <typename WT>
 void launch_correction(int cls, const GraphView<WT> &g, const StateView &st, const int32_t *list,
@@ -128,7 +142,8 @@ constexpr int CLASS_COUNT_WORDS = NCLS + (NCLS & 1) + 2 * NCLS;
 void launch_class_count(const int32_t *rowptr, const int32_t *rowend, int32_t V, int32_t *counts,
                         cudaStream_t s);
 void launch_class_scatter(const int32_t *rowptr, const int32_t *rowend, int32_t V,
-                          const int32_t *offsets, int32_t *cursors, int32_t *list, cudaStream_t s);
+                          const int32_t *offsets, int32_t *cursors, int32_t *list, uint8_t *hint,
+                          cudaStream_t s);
 void launch_fill_i32(int32_t *p, int64_t n, int32_t v, cudaStream_t s);
 void launch_iota_i32(int32_t *p, int64_t n, cudaStream_t s);
 void launch_level_init(int32_t *comm, int32_t *newc, int32_t *size, const u64 *k, u64 *S,

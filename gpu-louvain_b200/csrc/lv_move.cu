@@ -108,29 +108,61 @@ __device__ __forceinline__ void cta_reduce_best(const MoveCtx &m, Best &b) {
 }
 
 // ------------------------------------------------------------------------
-// degree > 32: warp per vertex with an optimistic shared table, partitioned
-// fallback for vertices with many distinct neighbour communities
+// degree > 32: warp per vertex with an optimistic shared table, fallback
+// CTAs for vertices with many distinct neighbour communities
 // ------------------------------------------------------------------------
-// W. A warp per vertex inserts its row into a WARP_CAP-slot shared table and
-//    counts newly claimed slots with a ballot.  Once communities have formed
-//    a vertex has few distinct neighbour communities (a few percent of its
-//    degree on aggregated levels), so this decides almost every vertex.  A
-//    vertex whose count passes WARP_LIMIT stops, clears its table and is
-//    queued as P = ceil(degree / FB_KEYS) fallback items (v, p).
-// F. Persistent 1024-thread CTAs with FB_CAP-slot shared tables take items;
-//    item (v, p) streams v's row and keeps only the communities whose hash
-//    falls in partition p, evaluates them, and stores its partial best.  The
-//    CTA that finishes the last item of v combines the P partials (all the
-//    items of v are contiguous) and decides.  No global hash tables.
+// W. A warp per vertex inserts its row into a shared table of
+//    min(WARP_CAP, 2^ceil(log2(2 degree))) slots and counts newly claimed
+//    slots with a ballot.  Once communities have formed a vertex has few
+//    distinct neighbour communities (a few percent of its degree on
+//    aggregated levels), so this decides almost every vertex.  A vertex whose
+//    count passes WARP_LIMIT, or whose hint says it did at its last
+//    evaluation, is queued for a fallback CTA instead: degree <= FBS_MAXDEG
+//    to the small queue, <= FBM_MAXDEG to the medium queue, else as
+//    P = ceil(degree / FB_KEYS) key-space partitions (v, p) to the large queue.
+// F. Persistent fallback CTAs take items from their queue.  Small and medium
+//    items are whole rows in a table of 2^ceil(log2(2 degree)) slots.  A large
+//    item (v, p) streams v's row (or the staged pairs of a giant), keeps the
+//    communities whose hash falls in partition p, evaluates them and stores
+//    its partial best; the CTA that finishes the last item of v combines the
+//    P partials (the items of v are contiguous) and decides.
+// Results do not depend on which path decides a vertex.
+constexpr int HINT_SET = (WARP_LIMIT * 3) / 4;   // hint = distinct count above this
+
 __device__ __forceinline__ uint32_t part_of(int32_t c, int32_t P) {
     const uint32_t hsh = (uint32_t)c * 0x85EBCA6Bu;
     return (uint32_t)(((u64)(hsh ^ (hsh >> 15)) * (u64)P) >> 32);
 }
 
+// Queue vertex v (degree d) for a fallback CTA.  One lane calls it.
+__device__ __forceinline__ void enqueue_fallback(const FallbackSet &fs, int32_t v, int32_t d, int *err) {
+    if (d <= FBM_MAXDEG) {
+        const Fallback &f = fs.q[d <= FBS_MAXDEG ? 0 : 1];
+        const int32_t i = atomicAdd(f.count, 1);
+        if (i < f.cap) f.v[i] = v;
+        else atomicOr(err, DEVERR_FALLBACK_FULL);
+        return;
+    }
+    const Fallback &f = fs.q[2];
+    const int32_t P = (d + FB_KEYS - 1) / FB_KEYS;
+    const int32_t first = atomicAdd(f.count, P);
+    if (first + P <= f.cap) {
+        for (int32_t q = 0; q < P; ++q) {
+            f.v[first + q] = v;
+            f.p[first + q] = q;
+            f.P[first + q] = P;
+            f.first[first + q] = first;
+            f.src[first + q] = -1;
+        }
+    } else {
+        atomicOr(err, DEVERR_FALLBACK_FULL);
+    }
+}
+
 template <typename WT>
 __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateView st,
                                                         const int32_t *__restrict__ list, int32_t n,
-                                                        Fallback fb, u64 *dE) {
+                                                        FallbackSet fs, u64 *dE) {
     constexpr int NW = 8;
     constexpr int LG = ilog2_c(WARP_CAP);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -145,49 +177,47 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
     const int32_t nwarps = gridDim.x * NW;
     for (int32_t idx = blockIdx.x * NW + wid; idx < n; idx += nwarps) {
         const int32_t v = list[idx];
-        const int32_t own = __ldg(st.comm + v);
         const int32_t r0 = g.rowptr[v], r1 = g.rowend[v];
+        const int32_t d = r1 - r0;
+        if (d > WARP_LIMIT && fs.hint[v]) {
+            if (lane == 0) enqueue_fallback(fs, v, d, st.err);
+            continue;
+        }
+        const int32_t own = __ldg(st.comm + v);
+        int lg = ceil_log2_i(2 * (int64_t)d);
+        lg = lg < 5 ? 5 : (lg > LG ? LG : lg);
         u64 e_own = 0;
         int32_t nclaim = 0;
         bool overflow = false;
+        // edge e = base + lane; the next chunk's column and weight are loaded
+        // before the current chunk's gather and insert
+        int32_t jn = -1;
+        u64 wn = 0;
+        if (r0 + lane < r1) { jn = __ldg(g.col + r0 + lane); wn = wfix(g.w, r0 + lane, g.scale); }
         for (int32_t base = r0; base < r1; base += 32) {
-            const int32_t e = base + lane;
-            int32_t c = -1;
-            u64 w = 0;
-            if (e < r1) {
-                const int32_t j = __ldg(g.col + e);
-                if (j != v) {
-                    c = __ldg(st.comm + j);
-                    w = wfix(g.w, e, g.scale);
-                }
-            }
+            const int32_t j = jn;
+            const u64 w = wn;
+            const int32_t en = base + 32 + lane;
+            jn = -1;
+            if (en < r1) { jn = __ldg(g.col + en); wn = wfix(g.w, en, g.scale); }
             int32_t claimed = -1;
-            if (c >= 0) {
+            if (j >= 0 && j != v) {
+                const int32_t c = __ldg(st.comm + j);
                 if (c == own) e_own += w;
-                else claimed = table_insert_claim(keys, vals, LG, c, w, st.err);
+                else claimed = table_insert_claim(keys, vals, lg, c, w, st.err);
             }
             nclaim += __popc(__ballot_sync(FULL, claimed >= 0));
             if (nclaim > WARP_LIMIT) { overflow = true; break; }
         }
         __syncwarp();
+        const int nslots = 1 << lg;
         if (overflow) {
-            for (int s = lane; s < WARP_CAP; s += 32) {
+            for (int s = lane; s < nslots; s += 32) {
                 if (keys[s] >= 0) { keys[s] = -1; vals[s] = 0; }
             }
             if (lane == 0) {
-                const int32_t P = (int32_t)((r1 - r0 + FB_KEYS - 1) / FB_KEYS);
-                const int32_t first = atomicAdd(fb.count, P);
-                if (first + P <= fb.cap) {
-                    for (int32_t q = 0; q < P; ++q) {
-                        fb.v[first + q] = v;
-                        fb.p[first + q] = q;
-                        fb.P[first + q] = P;
-                        fb.first[first + q] = first;
-                        fb.src[first + q] = -1;
-                    }
-                } else {
-                    atomicOr(st.err, DEVERR_FALLBACK_FULL);
-                }
+                fs.hint[v] = 1;
+                enqueue_fallback(fs, v, d, st.err);
             }
             __syncwarp();
             continue;
@@ -195,7 +225,7 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
         const MoveCtx m = move_ctx(own, __ldg(st.size + own) == 1, st.T, __ldg(st.k + v), __ldg(st.S + own));
         Best b = best_init(own);
         b.eo = e_own;
-        eval_slots<1, false, true>(keys, vals, nullptr, WARP_CAP, lane, 32, m, st.S, st.size, b);
+        eval_slots<1, false, true>(keys, vals, nullptr, nslots, lane, 32, m, st.S, st.size, b);
         group_reduce_best(m, b, 32);
         if (lane == 0) {
             u64 delta = 0;
@@ -204,68 +234,85 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
         }
         __syncwarp();
     }
-    block_add_total<256>(delta_acc, dE);
+    if (lane == 0 && delta_acc) atomicAdd(dE, delta_acc);
 }
 
-template <typename WT>
-__global__ void __launch_bounds__(FB_THREADS) move_fallback_kernel(GraphView<WT> g, StateView st,
-                                                                   Fallback fb, HubGlobal hg, u64 *dE) {
+// Fallback CTAs.  PART = false: items are whole rows of degree <= CAP / 2
+// (small and medium queues).  PART = true: key-space partitions of a row or
+// of a giant's staged pairs (large queue).  The occupied list holds CAP / 2
+// slots; a partition with more distinct communities than that reports
+// DEVERR_HASH_FULL.
+template <typename WT, int THREADS, int CAP, bool PART>
+__global__ void __launch_bounds__(THREADS) move_fallback_kernel(GraphView<WT> g, StateView st,
+                                                                Fallback fb, HubGlobal hg,
+                                                                uint8_t *hint, u64 *dE) {
+    constexpr int OCC_CAP = CAP / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     u64 *vals = reinterpret_cast<u64 *>(smem_raw);
-    int32_t *keys = reinterpret_cast<int32_t *>(vals + FB_CAP);
-    int32_t *occ = keys + FB_CAP;
-    __shared__ int32_t nocc, item_sh, last_sh;
-    for (int s = threadIdx.x; s < FB_CAP; s += FB_THREADS) { keys[s] = -1; vals[s] = 0; }
+    int32_t *keys = reinterpret_cast<int32_t *>(vals + CAP);
+    int32_t *occ = keys + CAP;
+    __shared__ int32_t nocc, item_sh;
+    for (int s = threadIdx.x; s < CAP; s += THREADS) { keys[s] = -1; vals[s] = 0; }
     if (threadIdx.x == 0) nocc = 0;
     __syncthreads();
-    const int32_t count = *fb.count;
+    const int32_t count = min(*fb.count, fb.cap);
     u64 delta_acc = 0;
     for (;;) {
         if (threadIdx.x == 0) item_sh = atomicAdd(fb.next, 1);
         __syncthreads();
         const int32_t item = item_sh;
-        if (item >= count || item >= fb.cap) break;
-        const int32_t v = fb.v[item], p = fb.p[item], P = fb.P[item], first = fb.first[item];
-        const int32_t src = fb.src[item];
+        if (item >= count) break;
+        const int32_t v = fb.v[item];
+        int32_t p = 0, P = 1, first = item, src = -1;
+        if (PART) { p = fb.p[item]; P = fb.P[item]; first = fb.first[item]; src = fb.src[item]; }
         const int32_t own = __ldg(st.comm + v);
         u64 e_own = 0;
         if (src < 0) {
             // the vertex's row
             const int32_t r0 = g.rowptr[v], r1 = g.rowend[v];
-            int lg = P > 1 ? ilog2_c(FB_CAP) : ceil_log2_i(2 * (int64_t)(r1 - r0));
+            int lg = P > 1 ? ilog2_c(CAP) : ceil_log2_i(2 * (int64_t)(r1 - r0));
             lg = lg < 3 ? 3 : lg;
-            for (int32_t e = r0 + threadIdx.x; e < r1; e += FB_THREADS) {
-                const int32_t j = __ldg(g.col + e);
-                if (j == v) continue;
-                const int32_t c = __ldg(st.comm + j);
-                if (c == own) {
-                    if (p == 0) e_own += wfix(g.w, e, g.scale);
-                } else if (P == 1 || (int32_t)part_of(c, P) == p) {
-                    table_insert_occ(keys, vals, lg, c, wfix(g.w, e, g.scale), st.err, occ, &nocc);
+            if (!PART) {
+                insert_row<1, true>(g, st.comm, v, own, r0, r1, threadIdx.x, THREADS, keys, vals, lg,
+                                    st.err, occ, &nocc, e_own);
+            } else {
+                for (int32_t e = r0 + threadIdx.x; e < r1; e += THREADS) {
+                    const int32_t j = __ldg(g.col + e);
+                    if (j == v) continue;
+                    const int32_t c = __ldg(st.comm + j);
+                    if (c == own) {
+                        if (p == 0) e_own += wfix(g.w, e, g.scale);
+                    } else if (P == 1 || (int32_t)part_of(c, P) == p) {
+                        table_insert_occ_capped(keys, vals, lg, c, wfix(g.w, e, g.scale), st.err, occ,
+                                                &nocc, OCC_CAP);
+                    }
                 }
             }
         } else {
             // the staged (community, weight) pairs of giant src
             const int32_t n = hg.nocc[src];
-            int lg = P > 1 ? ilog2_c(FB_CAP) : ceil_log2_i(2 * (int64_t)n);
+            int lg = P > 1 ? ilog2_c(CAP) : ceil_log2_i(2 * (int64_t)n);
             lg = lg < 3 ? 3 : lg;
             const int32_t *sk = hg.stage_key + hg.occ_off[src];
             const u64 *sv = hg.stage_val + hg.occ_off[src];
-            for (int32_t i = threadIdx.x; i < n; i += FB_THREADS) {
+            for (int32_t i = threadIdx.x; i < n; i += THREADS) {
                 const int32_t c = sk[i];
-                if (P == 1 || (int32_t)part_of(c, P) == p) table_insert_occ(keys, vals, lg, c, sv[i], st.err, occ, &nocc);
+                if (P == 1 || (int32_t)part_of(c, P) == p)
+                    table_insert_occ_capped(keys, vals, lg, c, sv[i], st.err, occ, &nocc, OCC_CAP);
             }
             if (p == 0 && threadIdx.x == 0) e_own = hg.eown[src];
         }
         __syncthreads();
+        const int32_t nd = min(nocc, OCC_CAP);
         const MoveCtx m = move_ctx(own, __ldg(st.size + own) == 1, st.T, __ldg(st.k + v), __ldg(st.S + own));
         Best b = best_init(own);
         b.eo = e_own;
-        eval_slots<1, true, true>(keys, vals, occ, nocc, threadIdx.x, FB_THREADS, m, st.S, st.size, b);
-        cta_reduce_best<FB_THREADS>(m, b);
+        eval_slots<1, true, true>(keys, vals, occ, nd, threadIdx.x, THREADS, m, st.S, st.size, b);
+        cta_reduce_best<THREADS>(m, b);
         if (threadIdx.x == 0) {
             nocc = 0;
             bool decide = P == 1;
+            int32_t distinct = nd;
             Best t = b;
             if (P > 1) {
                 fb.gd[item] = b.gd;
@@ -273,12 +320,14 @@ __global__ void __launch_bounds__(FB_THREADS) move_fallback_kernel(GraphView<WT>
                 fb.S[item] = b.S;
                 fb.c[item] = b.c;
                 fb.eo[item] = b.eo;
+                fb.cnt[item] = nd;
                 __threadfence();
                 const int32_t done = atomicAdd(fb.done + first, 1);
                 decide = done == P - 1;
                 if (decide) {
                     __threadfence();
                     t = best_init(own);
+                    distinct = 0;
                     for (int32_t q = 0; q < P; ++q) {
                         Best o;
                         o.gd = __ldcg(fb.gd + first + q);
@@ -288,6 +337,7 @@ __global__ void __launch_bounds__(FB_THREADS) move_fallback_kernel(GraphView<WT>
                         o.eo = 0;
                         if (better(m, o, t)) { t.gd = o.gd; t.e = o.e; t.S = o.S; t.c = o.c; }
                         t.eo += __ldcg(fb.eo + first + q);
+                        distinct += __ldcg(fb.cnt + first + q);
                     }
                     fb.done[first] = 0;
                 }
@@ -299,6 +349,8 @@ __global__ void __launch_bounds__(FB_THREADS) move_fallback_kernel(GraphView<WT>
                 if (src >= 0) {
                     hg.nocc[src] = 0;
                     hg.eown[src] = 0;
+                } else {
+                    hint[v] = distinct > HINT_SET ? 1 : 0;
                 }
             }
         }
@@ -355,6 +407,7 @@ __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_kernel(GraphView<WT
 
 __global__ void __launch_bounds__(HG_MERGE_THREADS) giant_merge_kernel(StateView st, HubGlobal hg,
                                                                        Fallback fb, u64 *dE) {
+    // fb: the large fallback queue
     extern __shared__ __align__(16) unsigned char smem_raw[];
     u64 *vals = reinterpret_cast<u64 *>(smem_raw);
     int32_t *keys = reinterpret_cast<int32_t *>(vals + HG_MERGE_CAP);
@@ -594,14 +647,29 @@ inline unsigned nblocks(int64_t items, int per_block) {
 
 }  // namespace
 
+constexpr int FBS_SMEM = FBS_CAP * 14, FBM_SMEM = FBM_CAP * 14;
+
 template <typename WT>
 static void set_attrs_for(DeviceInfo &di) {
-    cudaFuncSetAttribute(move_fallback_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM);
+    cudaFuncSetAttribute(move_fallback_kernel<WT, FBS_THREADS, FBS_CAP, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, FBS_SMEM);
+    cudaFuncSetAttribute(move_fallback_kernel<WT, FBM_THREADS, FBM_CAP, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, FBM_SMEM);
+    cudaFuncSetAttribute(move_fallback_kernel<WT, FB_THREADS, FB_CAP, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM);
     cudaFuncSetAttribute(giant_stage_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM);
     cudaFuncSetAttribute(move_warp_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_SMEM);
     int o = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_warp_kernel<WT>, 256, WARP_SMEM);
     di.occ_warp = o > 0 ? o : 1;
+    o = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_fallback_kernel<WT, FBS_THREADS, FBS_CAP, false>,
+                                                  FBS_THREADS, FBS_SMEM);
+    di.occ_fbs = o > 0 ? o : 1;
+    o = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_fallback_kernel<WT, FBM_THREADS, FBM_CAP, false>,
+                                                  FBM_THREADS, FBM_SMEM);
+    di.occ_fbm = o > 0 ? o : 1;
 }
 
 void init_kernel_attributes(DeviceInfo &di) {
@@ -627,23 +695,42 @@ void launch_move_class(int cls, const GraphView<WT> &g, const StateView &st, con
 }
 
 template <typename WT>
+static void launch_fallback_large(const GraphView<WT> &g, const StateView &st, const HubGlobal &hg,
+                                  const FallbackSet &fs, const DeviceInfo &di, u64 *dE, cudaStream_t s) {
+    move_fallback_kernel<WT, FB_THREADS, FB_CAP, true><<<di.sms, FB_THREADS, FB_SMEM, s>>>(
+        g, st, fs.q[2], hg, fs.hint, dE);
+    note_launches(1);
+}
+
+template <typename WT>
 void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGlobal &hg,
-                        const Fallback &fb, const DeviceInfo &di, u64 *dE, cudaStream_t s) {
+                        const FallbackSet &fs, const DeviceInfo &di, u64 *dE, cudaStream_t s) {
     if (hg.nhubs <= 0) return;
-    cudaMemsetAsync(fb.count, 0, 2 * sizeof(int32_t), s);   // count, next
+    cudaMemsetAsync(fs.q[2].count, 0, 2 * sizeof(int32_t), s);   // count, next
     giant_stage_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg); note_launches(1);
-    giant_merge_kernel<<<(unsigned)imin64(hg.nhubs, di.sms), HG_MERGE_THREADS, HG_MERGE_SMEM, s>>>(st, hg, fb, dE); note_launches(1);
-    move_fallback_kernel<WT><<<di.sms, FB_THREADS, FB_SMEM, s>>>(g, st, fb, hg, dE); note_launches(1);
+    giant_merge_kernel<<<(unsigned)imin64(hg.nhubs, di.sms), HG_MERGE_THREADS, HG_MERGE_SMEM, s>>>(
+        st, hg, fs.q[2], dE);
+    note_launches(1);
+    launch_fallback_large<WT>(g, st, hg, fs, di, dE, s);
 }
 
 template <typename WT>
 void launch_move_wide(const GraphView<WT> &g, const StateView &st, const int32_t *list, int32_t n,
-                      const Fallback &fb, const DeviceInfo &di, u64 *dE, cudaStream_t s, bool) {
+                      const FallbackSet &fs, const DeviceInfo &di, u64 *dE, cudaStream_t s,
+                      int32_t max_degree) {
     if (n <= 0) return;
-    cudaMemsetAsync(fb.count, 0, 2 * sizeof(int32_t), s);   // count, next
+    // the three queues' (count, next) pairs are contiguous
+    cudaMemsetAsync(fs.q[0].count, 0, 6 * sizeof(int32_t), s);
     const unsigned grid = (unsigned)imin64((n + 7) / 8, (int64_t)di.sms * di.occ_warp);
-    move_warp_kernel<WT><<<grid, 256, WARP_SMEM, s>>>(g, st, list, n, fb, dE); note_launches(1);
-    move_fallback_kernel<WT><<<di.sms, FB_THREADS, FB_SMEM, s>>>(g, st, fb, HubGlobal(), dE); note_launches(1);
+    move_warp_kernel<WT><<<grid, 256, WARP_SMEM, s>>>(g, st, list, n, fs, dE); note_launches(1);
+    if (max_degree <= WARP_LIMIT) return;   // no vertex can overflow its warp table
+    launch_fallback_large<WT>(g, st, HubGlobal(), fs, di, dE, s);
+    move_fallback_kernel<WT, FBM_THREADS, FBM_CAP, false><<<di.sms * di.occ_fbm, FBM_THREADS, FBM_SMEM, s>>>(
+        g, st, fs.q[1], HubGlobal(), fs.hint, dE);
+    note_launches(1);
+    move_fallback_kernel<WT, FBS_THREADS, FBS_CAP, false><<<di.sms * di.occ_fbs, FBS_THREADS, FBS_SMEM, s>>>(
+        g, st, fs.q[0], HubGlobal(), fs.hint, dE);
+    note_launches(1);
 }
 
 template <typename WT>
@@ -723,16 +810,16 @@ template void launch_move_class<u64>(int, const GraphView<u64> &, const StateVie
                                      const int32_t *, int32_t, const DeviceInfo &, u64 *,
                                      cudaStream_t);
 template void launch_move_wide<float>(const GraphView<float> &, const StateView &, const int32_t *,
-                                      int32_t, const Fallback &, const DeviceInfo &, u64 *,
-                                      cudaStream_t, bool);
+                                      int32_t, const FallbackSet &, const DeviceInfo &, u64 *,
+                                      cudaStream_t, int32_t);
 template void launch_move_wide<u64>(const GraphView<u64> &, const StateView &, const int32_t *,
-                                    int32_t, const Fallback &, const DeviceInfo &, u64 *,
-                                    cudaStream_t, bool);
+                                    int32_t, const FallbackSet &, const DeviceInfo &, u64 *,
+                                    cudaStream_t, int32_t);
 template void launch_move_giants<float>(const GraphView<float> &, const StateView &,
-                                        const HubGlobal &, const Fallback &, const DeviceInfo &,
+                                        const HubGlobal &, const FallbackSet &, const DeviceInfo &,
                                         u64 *, cudaStream_t);
 template void launch_move_giants<u64>(const GraphView<u64> &, const StateView &, const HubGlobal &,
-                                      const Fallback &, const DeviceInfo &, u64 *, cudaStream_t);
+                                      const FallbackSet &, const DeviceInfo &, u64 *, cudaStream_t);
 template void launch_correction<float>(int, const GraphView<float> &, const StateView &,
                                        const int32_t *, int32_t, const DeviceInfo &, u64 *,
                                        cudaStream_t);

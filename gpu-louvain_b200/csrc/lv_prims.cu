@@ -125,14 +125,20 @@ struct ClassOffsets {
     int32_t off[NCLS];
 };
 
+// Also sets the move phase's fallback hint: at the start of a level every
+// vertex is a singleton community, so a row with more than WARP_LIMIT
+// entries has (up to duplicates) more distinct neighbour communities.
 __global__ void __launch_bounds__(256) class_scatter_kernel(const int32_t *__restrict__ rowptr,
                                                             const int32_t *__restrict__ rowend,
                                                             int32_t V, ClassOffsets offs,
-                                                            int32_t *cursors, int32_t *list) {
+                                                            int32_t *cursors, int32_t *list,
+                                                            uint8_t *hint) {
     const int lane = threadIdx.x & 31;
     for (int32_t base = blockIdx.x * 256; base < V; base += gridDim.x * 256) {
         const int32_t v = base + threadIdx.x;
-        const int cls = v < V ? degree_class(rowend[v] - rowptr[v]) : -1;
+        const int32_t d = v < V ? rowend[v] - rowptr[v] : 0;
+        const int cls = v < V ? degree_class(d) : -1;
+        if (v < V) hint[v] = d > WARP_LIMIT ? 1 : 0;
         const unsigned peers = __match_any_sync(FULL, cls);
         const int leader = __ffs(peers) - 1;
         int32_t pos = 0;
@@ -295,12 +301,13 @@ void launch_class_count(const int32_t *rowptr, const int32_t *rowend, int32_t V,
 }
 
 void launch_class_scatter(const int32_t *rowptr, const int32_t *rowend, int32_t V,
-                          const int32_t *offsets, int32_t *cursors, int32_t *list, cudaStream_t s) {
+                          const int32_t *offsets, int32_t *cursors, int32_t *list, uint8_t *hint,
+                          cudaStream_t s) {
     cudaMemsetAsync(cursors, 0, sizeof(int32_t) * NCLS, s);
     if (V <= 0) return;
     ClassOffsets o;
     for (int c = 0; c < NCLS; ++c) o.off[c] = offsets[c];
-    class_scatter_kernel<<<grid_for(V), 256, 0, s>>>(rowptr, rowend, V, o, cursors, list); note_launches(1);
+    class_scatter_kernel<<<grid_for(V), 256, 0, s>>>(rowptr, rowend, V, o, cursors, list, hint); note_launches(1);
 }
 
 void launch_fill_i32(int32_t *p, int64_t n, int32_t v, cudaStream_t s) {
