@@ -13,8 +13,10 @@
 #include <stdint.h>
 
 // Tuning knobs (compile-time): edges per lane in flight in the insert loops
-// of the group (LV_U_GROUP) and CTA (LV_U_CTA) kernels, and table entries per
-// lane in flight in the evaluation loops (LV_U_EVAL).
+// of the group kernels (LV_U_GROUP), the warp kernel (LV_U_WARP), the small
+// and medium fallback CTAs (LV_U_FB) and the giant staging CTAs
+// (LV_U_STAGE), and table entries per lane in flight in the evaluation loops
+// of the group kernels (LV_U_EVAL).
 #ifndef LV_U_GROUP
 #define LV_U_GROUP 2
 #endif
@@ -23,6 +25,15 @@
 #endif
 #ifndef LV_U_EVAL
 #define LV_U_EVAL 4
+#endif
+#ifndef LV_U_WARP
+#define LV_U_WARP 4
+#endif
+#ifndef LV_U_FB
+#define LV_U_FB 4
+#endif
+#ifndef LV_U_STAGE
+#define LV_U_STAGE 8
 #endif
 
 namespace lv {

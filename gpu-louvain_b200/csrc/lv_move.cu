@@ -189,25 +189,34 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
         u64 e_own = 0;
         int32_t nclaim = 0;
         bool overflow = false;
-        // edge e = base + lane; the next chunk's column and weight are loaded
-        // before the current chunk's gather and insert
-        int32_t jn = -1;
-        u64 wn = 0;
-        if (r0 + lane < r1) { jn = __ldg(g.col + r0 + lane); wn = wfix(g.w, r0 + lane, g.scale); }
-        for (int32_t base = r0; base < r1; base += 32) {
-            const int32_t j = jn;
-            const u64 w = wn;
-            const int32_t en = base + 32 + lane;
-            jn = -1;
-            if (en < r1) { jn = __ldg(g.col + en); wn = wfix(g.w, en, g.scale); }
-            int32_t claimed = -1;
-            if (j >= 0 && j != v) {
-                const int32_t c = __ldg(st.comm + j);
-                if (c == own) e_own += w;
-                else claimed = table_insert_claim(keys, vals, lg, c, w, st.err);
+        // U chunks of 32 edges per step: U column and weight loads, then U
+        // community gathers, are in flight together.  The claim count is
+        // checked after every chunk, so at most WARP_LIMIT + 32 slots of
+        // the WARP_CAP-slot table are ever claimed.
+        constexpr int U = LV_U_WARP;
+        for (int32_t base = r0 + lane; base < r1 + lane && !overflow; base += 32 * U) {
+            int32_t jj[U];
+            u64 ww[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int32_t e = base + 32 * u;
+                jj[u] = -1;
+                ww[u] = 0;
+                if (e < r1) { jj[u] = __ldg(g.col + e); ww[u] = wfix(g.w, e, g.scale); }
             }
-            nclaim += __popc(__ballot_sync(FULL, claimed >= 0));
-            if (nclaim > WARP_LIMIT) { overflow = true; break; }
+            int32_t cc[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(st.comm + jj[u]) : -1;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                int32_t claimed = -1;
+                if (cc[u] >= 0) {
+                    if (cc[u] == own) e_own += ww[u];
+                    else claimed = table_insert_claim(keys, vals, lg, cc[u], ww[u], st.err);
+                }
+                nclaim += __popc(__ballot_sync(FULL, claimed >= 0));
+                if (nclaim > WARP_LIMIT) { overflow = true; break; }
+            }
         }
         __syncwarp();
         const int nslots = 1 << lg;
@@ -273,8 +282,8 @@ __global__ void __launch_bounds__(THREADS) move_fallback_kernel(GraphView<WT> g,
             int lg = P > 1 ? ilog2_c(CAP) : ceil_log2_i(2 * (int64_t)(r1 - r0));
             lg = lg < 3 ? 3 : lg;
             if (!PART) {
-                insert_row<1, true>(g, st.comm, v, own, r0, r1, threadIdx.x, THREADS, keys, vals, lg,
-                                    st.err, occ, &nocc, e_own);
+                insert_row<LV_U_FB, true>(g, st.comm, v, own, r0, r1, threadIdx.x, THREADS, keys, vals,
+                                          lg, st.err, occ, &nocc, e_own);
             } else {
                 for (int32_t e = r0 + threadIdx.x; e < r1; e += THREADS) {
                     const int32_t j = __ldg(g.col + e);
@@ -390,8 +399,8 @@ __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_kernel(GraphView<WT
     const int32_t e1 = min(e0 + STAGE_CHUNK, r1);
     const int32_t own = __ldg(st.comm + v);
     u64 e_own = 0;
-    insert_row<1, true>(g, st.comm, v, own, e0, e1, threadIdx.x, STAGE_THREADS, lkeys, lvals, LLG, st.err,
-                        locc, &lnocc, e_own);
+    insert_row<LV_U_STAGE, true>(g, st.comm, v, own, e0, e1, threadIdx.x, STAGE_THREADS, lkeys, lvals, LLG,
+                                 st.err, locc, &lnocc, e_own);
     block_add_total<STAGE_THREADS>(e_own, hg.eown + h);   // contains the barrier
     const int32_t n = lnocc;
     if (threadIdx.x == 0) base = atomicAdd(hg.nocc + h, n);

@@ -37,6 +37,30 @@ def hub_graph(seed=0):
     return rowptr, dst[o].astype(np.int32), ww[o].astype(np.float32)
 
 
+def megahub_graph(seed=5):
+    """Random background plus a hub adjacent to 1.6M vertices and a hub of
+    degree 300000: in the first sweep their staged pairs exceed one shared
+    table and are decided as hundreds of key-space partitions."""
+    rng = np.random.default_rng(seed)
+    V = 1_700_000
+    m = 1_000_000
+    u = rng.integers(0, V, m)
+    v = rng.integers(0, V, m)
+    for h, d in [(7, 1_600_000), (70001, 300_000)]:
+        nb = rng.choice(V, d, replace=False)
+        u = np.concatenate([u, np.full(d, h)])
+        v = np.concatenate([v, nb])
+    keep = u != v
+    a, b = np.minimum(u[keep], v[keep]), np.maximum(u[keep], v[keep])
+    key = np.unique(a.astype(np.int64) * V + b)
+    a, b = key // V, key % V
+    w = (rng.integers(1, 8, len(a)) * 0.25).astype(np.float32)
+    src = np.concatenate([a, b]); dst = np.concatenate([b, a]); ww = np.concatenate([w, w])
+    o = np.lexsort((dst, src))
+    rowptr = np.concatenate([[0], np.cumsum(np.bincount(src, minlength=V))]).astype(np.int32)
+    return rowptr, dst[o].astype(np.int32), ww[o].astype(np.float32)
+
+
 def cases(lvb):
     out = {}
     g = lvb.gen_planted(10000, 64, 16.0, 2.0, 0)
@@ -130,6 +154,25 @@ def test_full_run_matches_oracle(lvb, orc, graphs, name):
     e.reset()
     assert e.run(gain) == q1
     assert np.array_equal(e.original_to_community()[0], o2c1)
+
+
+def test_megahub_matches_oracle(lvb, orc):
+    rp, cl, w = megahub_graph()
+    e = lvb.Louvain(lvb.Graph(rp, cl, w), verify=True)
+    o = orc.Oracle(rp, cl, w)
+    for s in range(6):
+        m1, m2 = e.sweep(), o.sweep()
+        assert m1 == m2, f"sweep {s}: moves {m1} vs {m2}"
+        assert np.array_equal(e.communities(), o.communities()), f"sweep {s}"
+        assert e.calculate_modularity() == o.modularity()
+        if m1 == 0:
+            break
+    e.close()
+    e = lvb.Louvain(lvb.Graph(rp, cl, w))
+    q1 = e.run(1e-6)
+    q2, _ = o.__class__(rp, cl, w).run(1e-6)
+    assert q1 == q2
+    e.close()
 
 
 def test_aggregation_from_given_communities(lvb, orc, graphs):
