@@ -171,6 +171,32 @@ int lv_gen_rmat_device(int32_t scale, int32_t edge_factor, uint64_t seed, double
                        int32_t **d_rowptr, int32_t **d_col, float **d_w);
 void lv_free_device(void *p);
 
+/* ---- allocation-free modularity of a given partition ----
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they need the value: a process whose device memory is all
+ * owned by another allocator (a framework's caching allocator, or a pool
+ * sized to the whole GPU), or a latency-critical loop that cannot take the
+ * device-wide synchronisation of cudaMalloc / cudaFree.  Returns the same
+ * modularity as lv_create_device + lv_set_communities + lv_modularity for a
+ * level-0 device CSR (as lv_create_device takes it) and a device array
+ * d_comm of V community ids in [0, V).
+ *
+ * Working memory is a fixed array inside the library (about 8 MiB per
+ * device, held by every GPU that loads the library until exit), so V may be
+ * at most LV_NOALLOC_MAX_VERTICES; larger V returns LV_ERR_TOO_LARGE.  No
+ * device memory is allocated.  Runs on the calling thread's current device
+ * and on `stream` (a cudaStream_t; NULL = the default stream), and
+ * synchronises that stream before returning.  The first call on a device
+ * looks up the array's device address; make that first call before any
+ * stream capture on that device.  All calls on one device share the array:
+ * calls that overlap on the GPU (other threads or streams) race and must be
+ * serialised by the caller.  On failure a message is written to err (may be
+ * NULL) of err_len bytes. */
+#define LV_NOALLOC_MAX_VERTICES (1 << 20)
+int lv_modularity_noalloc(const int32_t *d_rowptr, const int32_t *d_col, const float *d_w, int32_t V,
+                          int64_t E, const int32_t *d_comm, void *stream, double *q, char *err,
+                          int32_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,62 @@
+"""lv_modularity_noalloc: the modularity of a given partition for callers that
+cannot allocate device memory (their device memory is owned by another
+allocator, or they cannot take the synchronisation of cudaMalloc/cudaFree).
+
+It is called through the C ABI and must return exactly what the handle-based
+entry points (lv_create_device + lv_set_communities + lv_modularity) return,
+on two calls in a row and after a call on a different partition (the
+library's scratch array keeps the previous call's contents)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc(lvb, d_rp, d_cl, d_w, V, E, d_comm):
+    q = C.c_double()
+    err = C.create_string_buffer(256)
+    rc = lvb.lib().lv_modularity_noalloc(C.c_void_p(d_rp), C.c_void_p(d_cl), C.c_void_p(d_w), V, E,
+                                         C.c_void_p(d_comm), None, C.byref(q), err, 256)
+    return rc, q.value, err.value.decode()
+
+
+def test_noalloc_modularity_matches_handle_path(lvb):
+    import torch
+    rng = np.random.default_rng(3)
+    graphs = [lvb.gen_planted(6000, 48, 16.0, 2.0, 5, "uniform"), lvb.gen_rmat(13, seed=9)]
+    for g in graphs:
+        rp, cl, w = g.rowptr, g.col, g.w
+        V, E = len(rp) - 1, len(cl)
+        d_rp = torch.from_numpy(np.ascontiguousarray(rp)).cuda()
+        d_cl = torch.from_numpy(np.ascontiguousarray(cl)).cuda()
+        d_w = torch.from_numpy(np.ascontiguousarray(w)).cuda()
+        dev_csr = (d_rp.data_ptr(), d_cl.data_ptr(), d_w.data_ptr(), V, E)
+        # partitions: the final communities of a full run, a random one and singletons
+        e = lvb.Louvain(device_csr=dev_csr)
+        e.run(1e-6)
+        found, _ = e.original_to_community()
+        e.close()
+        parts = [found.astype(np.int32), rng.integers(0, 50, V).astype(np.int32),
+                 np.arange(V, dtype=np.int32)]
+        ref = lvb.Louvain(device_csr=dev_csr)
+        for comm in parts:
+            ref.set_communities(comm)
+            q_ref = ref.calculate_modularity()
+            d_comm = torch.from_numpy(comm).cuda()
+            for _ in range(2):
+                rc, q, msg = _noalloc(lvb, *dev_csr, d_comm.data_ptr())
+                assert rc == lvb.LV_OK, msg
+                assert q == q_ref          # exact: same fixed-point sums and FP64 formula
+        ref.close()
+        torch.cuda.synchronize()
+
+
+def test_noalloc_rejects_too_many_vertices(lvb):
+    import torch
+    d = torch.zeros(16, dtype=torch.int32, device="cuda")
+    V = (1 << 20) + 1
+    rc, _, msg = _noalloc(lvb, d.data_ptr(), d.data_ptr(), d.data_ptr(), V, 0, d.data_ptr())
+    assert rc == lvb.LV_ERR_TOO_LARGE
+    assert "LV_NOALLOC_MAX_VERTICES" in msg
