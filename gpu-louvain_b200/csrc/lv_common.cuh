@@ -130,6 +130,24 @@ struct StateView {
     int *err;
 };
 
+// Exact 64-bit add to a table value.  In shared memory a 64-bit atomicAdd
+// is a compare-and-swap loop that spins when many lanes hit one slot, so it
+// is done as two native 32-bit atomic adds: the low word's returned old value
+// gives the carry into the high word.  The final hi:lo equals the 64-bit sum
+// whatever the order of the adds (read it only after they have all
+// completed).  Global tables use the native 64-bit atomic.
+__device__ __forceinline__ void table_add(u64 *p, u64 w) {
+    if (__isShared(p)) {
+        unsigned *q = reinterpret_cast<unsigned *>(p);
+        const unsigned lo = (unsigned)w, hi = (unsigned)(w >> 32);
+        const unsigned old = atomicAdd(q, lo);
+        const unsigned carry = (old + lo < old) ? 1u : 0u;
+        if (hi | carry) atomicAdd(q + 1, hi + carry);
+    } else {
+        atomicAdd(p, w);
+    }
+}
+
 // Insert (key, w) into an open-addressing table with linear probing; works
 // for shared and global tables (generic addressing).  A key once written
 // never changes, so a stale EMPTY read only costs a failed CAS.  The probe
@@ -141,10 +159,10 @@ __device__ __forceinline__ void table_insert(int32_t *keys, u64 *vals, int lg, i
     uint32_t s = hash_slot(key, lg);
     for (uint32_t p = 0; p <= mask; ++p) {
         int32_t k = ((volatile int32_t *)keys)[s];
-        if (k == key) { atomicAdd(vals + s, w); return; }
+        if (k == key) { table_add(vals + s, w); return; }
         if (k < 0) {
             int32_t prev = atomicCAS(keys + s, -1, key);
-            if (prev < 0 || prev == key) { atomicAdd(vals + s, w); return; }
+            if (prev < 0 || prev == key) { table_add(vals + s, w); return; }
         }
         s = (s + 1u) & mask;
     }
@@ -159,11 +177,11 @@ __device__ __forceinline__ int32_t table_insert_claim(int32_t *keys, u64 *vals, 
     uint32_t s = hash_slot(key, lg);
     for (uint32_t p = 0; p <= mask; ++p) {
         int32_t k = ((volatile int32_t *)keys)[s];
-        if (k == key) { atomicAdd(vals + s, w); return -1; }
+        if (k == key) { table_add(vals + s, w); return -1; }
         if (k < 0) {
             int32_t prev = atomicCAS(keys + s, -1, key);
-            if (prev < 0) { atomicAdd(vals + s, w); return (int32_t)s; }
-            if (prev == key) { atomicAdd(vals + s, w); return -1; }
+            if (prev < 0) { table_add(vals + s, w); return (int32_t)s; }
+            if (prev == key) { table_add(vals + s, w); return -1; }
         }
         s = (s + 1u) & mask;
     }
@@ -192,15 +210,15 @@ __device__ __forceinline__ void table_insert_occ(int32_t *keys, u64 *vals, int l
     uint32_t s = hash_slot(key, lg);
     for (uint32_t p = 0; p <= mask; ++p) {
         int32_t k = ((volatile int32_t *)keys)[s];
-        if (k == key) { atomicAdd(vals + s, w); return; }
+        if (k == key) { table_add(vals + s, w); return; }
         if (k < 0) {
             int32_t prev = atomicCAS(keys + s, -1, key);
             if (prev < 0) {
-                atomicAdd(vals + s, w);
+                table_add(vals + s, w);
                 occ[atomicAdd(nocc, 1)] = (int32_t)s;
                 return;
             }
-            if (prev == key) { atomicAdd(vals + s, w); return; }
+            if (prev == key) { table_add(vals + s, w); return; }
         }
         s = (s + 1u) & mask;
     }
@@ -216,17 +234,17 @@ __device__ __forceinline__ void table_insert_occ_capped(int32_t *keys, u64 *vals
     uint32_t s = hash_slot(key, lg);
     for (uint32_t p = 0; p <= mask; ++p) {
         int32_t k = ((volatile int32_t *)keys)[s];
-        if (k == key) { atomicAdd(vals + s, w); return; }
+        if (k == key) { table_add(vals + s, w); return; }
         if (k < 0) {
             int32_t prev = atomicCAS(keys + s, -1, key);
             if (prev < 0) {
-                atomicAdd(vals + s, w);
+                table_add(vals + s, w);
                 const int32_t i = atomicAdd(nocc, 1);
                 if (i < occ_cap) occ[i] = (int32_t)s;
                 else atomicOr(err, DEVERR_HASH_FULL);
                 return;
             }
-            if (prev == key) { atomicAdd(vals + s, w); return; }
+            if (prev == key) { table_add(vals + s, w); return; }
         }
         s = (s + 1u) & mask;
     }
