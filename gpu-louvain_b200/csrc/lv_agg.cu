@@ -206,11 +206,11 @@ __global__ void __launch_bounds__(256) merge_group_kernel(const int32_t *__restr
     for (int32_t i = a + lane; i < b; i += G) {
         const int32_t k = vkey[i];
         if (k == self) w_self += vw[i];
-        else table_insert(keys, vals, LG, k, vw[i], err);
+        else table_insert<1>(keys, vals, LG, k, vw[i], err);
     }
     for (int off = G >> 1; off > 0; off >>= 1) w_self += __shfl_xor_sync(FULL, w_self, off, G);
     __syncwarp();
-    if (active && lane == 0 && w_self) table_insert(keys, vals, LG, self, w_self, err);
+    if (active && lane == 0 && w_self) table_insert<1>(keys, vals, LG, self, w_self, err);
     __syncwarp();
     // write the distinct entries back at the start of the range, in slot order
     const int wl = threadIdx.x & 31;
@@ -260,10 +260,10 @@ __global__ void __launch_bounds__(T) merge_cta_kernel(const int32_t *__restrict_
         for (int32_t i = a + threadIdx.x; i < b; i += T) {
             const int32_t k = vkey[i];
             if (k == self) w_self += vw[i];
-            else table_insert(keys, vals, lg, k, vw[i], err);
+            else table_insert<1>(keys, vals, lg, k, vw[i], err);
         }
         w_self = warp_sum_u64(w_self);
-        if ((threadIdx.x & 31) == 0 && w_self) table_insert(keys, vals, lg, self, w_self, err);
+        if ((threadIdx.x & 31) == 0 && w_self) table_insert<1>(keys, vals, lg, self, w_self, err);
         __syncthreads();
         for (int s = threadIdx.x; s < cap; s += T) {
             const int32_t key = keys[s];
@@ -311,18 +311,22 @@ __global__ void __launch_bounds__(HG_INSERT_THREADS) mergeg_insert_kernel(
     for (int32_t i = i0 + threadIdx.x; i < i1; i += HG_INSERT_THREADS) {
         const int32_t k = vkey[i];
         if (k == self) w_self += vw[i];
-        else table_insert(lkeys, lvals, LLG, k, vw[i], err);
+        else table_insert<1>(lkeys, lvals, LLG, k, vw[i], err);
     }
     w_self = warp_sum_u64(w_self);
-    if ((threadIdx.x & 31) == 0 && w_self) table_insert(lkeys, lvals, LLG, self, w_self, err);
+    if ((threadIdx.x & 31) == 0 && w_self) table_insert<1>(lkeys, lvals, LLG, self, w_self, err);
     __syncthreads();
+    // the chunk table (aggregation hash) is drained in slot order into the
+    // community's global table (move-phase hash), so consecutive inserts land
+    // far apart; the merged row comes out in claim order, i.e. in the chunk
+    // table's slot order, which is independent of the move phase's hash
     int32_t *keys = hg.keys + hg.tbl_off[h];
     u64 *vals = hg.vals + hg.tbl_off[h];
     int32_t *occ = hg.occ + hg.occ_off[h];
     const int lg = hg.tbl_lg[h];
     for (int s = threadIdx.x; s < LCAP; s += HG_INSERT_THREADS) {
         const int32_t k = lkeys[s];
-        const int32_t claimed = k >= 0 ? table_insert_claim(keys, vals, lg, k, lvals[s], err) : -1;
+        const int32_t claimed = k >= 0 ? table_insert_claim<0>(keys, vals, lg, k, lvals[s], err) : -1;
         warp_append(claimed, occ, hg.nocc + h);
     }
 }

@@ -99,6 +99,25 @@ __device__ __forceinline__ uint32_t hash_slot(int32_t key, int lg) {
     return ((uint32_t)key * 0x9E3779B1u) >> (32 - lg);
 }
 
+// Hash of the aggregation's tables, independent of hash_slot.  Aggregation
+// writes each merged row in the slot order of its table, so with a shared
+// hash a chunk of such a row holds keys whose hash_slot top bits nearly
+// coincide and the move phase's chunk tables degenerate into one long probe
+// run.  Two multiply-xorshift rounds decorrelate the two orders.
+__device__ __forceinline__ uint32_t hash_slot_agg(int32_t key, int lg) {
+    uint32_t x = (uint32_t)key * 0x2C1B3C6Du;
+    x ^= x >> 15;
+    x *= 0x297A2D39u;
+    x ^= x >> 13;
+    return x >> (32 - lg);
+}
+
+// H = 0: move-phase tables; H = 1: aggregation tables.
+template <int H>
+__device__ __forceinline__ uint32_t table_hash(int32_t key, int lg) {
+    return H == 0 ? hash_slot(key, lg) : hash_slot_agg(key, lg);
+}
+
 // Weight access: level 0 reads float32 and maps it onto the fixed grid
 // (exact: w * 2^scale is a power-of-two scaling, then round-to-nearest-even,
 // the same rule as the host's llrint(ldexp(w, scale))); later levels read the
@@ -153,10 +172,11 @@ __device__ __forceinline__ void table_add(u64 *p, u64 w) {
 // never changes, so a stale EMPTY read only costs a failed CAS.  The probe
 // count is bounded by the capacity; a full table sets an error bit instead
 // of spinning.
+template <int H = 0>
 __device__ __forceinline__ void table_insert(int32_t *keys, u64 *vals, int lg, int32_t key,
                                              u64 w, int *err) {
     const uint32_t mask = (1u << lg) - 1u;
-    uint32_t s = hash_slot(key, lg);
+    uint32_t s = table_hash<H>(key, lg);
     for (uint32_t p = 0; p <= mask; ++p) {
         int32_t k = ((volatile int32_t *)keys)[s];
         if (k == key) { table_add(vals + s, w); return; }
@@ -171,10 +191,11 @@ __device__ __forceinline__ void table_insert(int32_t *keys, u64 *vals, int lg, i
 
 // table_insert that returns the slot it newly claimed for `key` (-1 when the
 // key was already present or the table is full).
+template <int H = 0>
 __device__ __forceinline__ int32_t table_insert_claim(int32_t *keys, u64 *vals, int lg, int32_t key,
                                                       u64 w, int *err) {
     const uint32_t mask = (1u << lg) - 1u;
-    uint32_t s = hash_slot(key, lg);
+    uint32_t s = table_hash<H>(key, lg);
     for (uint32_t p = 0; p <= mask; ++p) {
         int32_t k = ((volatile int32_t *)keys)[s];
         if (k == key) { table_add(vals + s, w); return -1; }
