@@ -783,22 +783,22 @@ int finish_create(lv_handle *h) {
         // fallback work lists of the move phase.  Only vertices of degree
         // > WARP_LIMIT are queued (at most E / WARP_LIMIT of them at any
         // level); a large item covers FB_KEYS edges of a vertex of degree
-        // > FBM_MAXDEG, or as many staged pairs of a giant.
+        // > FBQ_MAXDEG(NFBQ - 1), or as many staged pairs of a giant.
         FallbackSet &fs = h->fb;
         int32_t *counters = nullptr;
-        LV_TRY(dalloc(h, &counters, 6));
+        LV_TRY(dalloc(h, &counters, 2 * (NFBQ + 1)));
         LV_TRY(dalloc(h, &fs.hint, V + 1));
         LV_CUDA(h, cudaMemsetAsync(fs.hint, 0, V + 1, h->stream));
         const size_t cap_row = (size_t)(h->E0 / WARP_LIMIT) + 64;
-        const size_t cap_large = (size_t)(2 * (h->E0 / FBM_MAXDEG + h->E0 / FB_KEYS)) + 64;
-        for (int q = 0; q < 3; ++q) {
+        const size_t cap_large = (size_t)(2 * (h->E0 / FBQ_MAXDEG(NFBQ - 1) + h->E0 / FB_KEYS)) + 64;
+        for (int q = 0; q <= NFBQ; ++q) {
             Fallback &f = fs.q[q];
             f.count = counters + 2 * q;
             f.next = f.count + 1;
-            const size_t cap = q < 2 ? cap_row : cap_large;
+            const size_t cap = q < NFBQ ? cap_row : cap_large;
             f.cap = (int32_t)cap;
             LV_TRY(dalloc(h, &f.v, cap));
-            if (q < 2) continue;
+            if (q < NFBQ) continue;
             LV_TRY(dalloc(h, &f.p, cap));
             LV_TRY(dalloc(h, &f.P, cap));
             LV_TRY(dalloc(h, &f.first, cap));
@@ -931,7 +931,7 @@ int lv_destroy(lv_handle *h) {
     {
         FallbackSet &fs = h->fb;
         dfree(fs.q[0].count); dfree(fs.hint);
-        for (int q = 0; q < 3; ++q) {
+        for (int q = 0; q <= NFBQ; ++q) {
             Fallback &f = fs.q[q];
             dfree(f.v); dfree(f.p); dfree(f.P); dfree(f.first); dfree(f.done); dfree(f.src);
             dfree(f.gd); dfree(f.e); dfree(f.S); dfree(f.eo); dfree(f.c); dfree(f.cnt);

@@ -56,13 +56,15 @@ long long launches_total();
 
 // Move phase for degree > 32: warp tables of WARP_CAP slots (a vertex with
 // more than WARP_LIMIT distinct neighbour communities falls back).  Fallback
-// items go to one of three queues by degree: small (<= FBS_MAXDEG, CTAs of
-// 256 threads, 2048-slot tables), medium (<= FBM_MAXDEG, 512 / 8192) and
-// large (1024 / 16384, split into key-space partitions of FB_KEYS edges).
+// items go to one of NFBQ row queues by degree (bin b takes degrees up to
+// FBQ_MAXDEG(b), with CTAs of FBQ_THREADS(b) threads and shared tables of
+// 2 * FBQ_MAXDEG(b) slots), or to the large queue (FB_THREADS threads,
+// FB_CAP slots, key-space partitions of FB_KEYS edges).
 constexpr int WARP_CAP = 512;
 constexpr int WARP_LIMIT = 352;
-constexpr int FBS_THREADS = 256, FBS_CAP = 2048, FBS_MAXDEG = 1024;
-constexpr int FBM_THREADS = 512, FBM_CAP = 8192, FBM_MAXDEG = 4096;
+constexpr int NFBQ = 4;
+__host__ __device__ constexpr int FBQ_MAXDEG(int b) { return 512 << b; }                 // 512 .. 4096
+__host__ __device__ constexpr int FBQ_THREADS(int b) { return b == 0 ? 128 : (b == 3 ? 512 : 256); }
 constexpr int FB_THREADS = 1024, FB_CAP = 16384;
 constexpr int FB_KEYS = 6144;
 constexpr int FB_SMEM = FB_CAP * 14;   // table + occupied list
@@ -87,7 +89,7 @@ struct Fallback {
 // vertex skips the warp attempt; the hint only routes work, results do not
 // depend on it).
 struct FallbackSet {
-    Fallback q[3];
+    Fallback q[NFBQ + 1];   // row queues by degree, then the large queue
     uint8_t *hint = nullptr;
 };
 
@@ -95,8 +97,7 @@ struct FallbackSet {
 struct DeviceInfo {
     int sms = 148;
     int occ_warp = 4;   // resident CTAs per SM of the warp kernel
-    int occ_fbs = 1;    // ... of the small and medium fallback kernels
-    int occ_fbm = 1;
+    int occ_fbq[NFBQ] = {1, 1, 1, 1};   // ... of the row fallback kernels
 };
 void init_kernel_attributes(DeviceInfo &di);
 

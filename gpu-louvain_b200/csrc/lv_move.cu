@@ -117,8 +117,8 @@ __device__ __forceinline__ void cta_reduce_best(const MoveCtx &m, Best &b) {
 //    distinct neighbour communities (a few percent of its degree on
 //    aggregated levels), so this decides almost every vertex.  A vertex whose
 //    count passes WARP_LIMIT, or whose hint says it did at its last
-//    evaluation, is queued for a fallback CTA instead: degree <= FBS_MAXDEG
-//    to the small queue, <= FBM_MAXDEG to the medium queue, else as
+//    evaluation, is queued for a fallback CTA instead: to the first row
+//    queue b with degree <= FBQ_MAXDEG(b), else as
 //    P = ceil(degree / FB_KEYS) key-space partitions (v, p) to the large queue.
 // F. Persistent fallback CTAs take items from their queue.  Small and medium
 //    items are whole rows in a table of 2^ceil(log2(2 degree)) slots.  A large
@@ -136,14 +136,16 @@ __device__ __forceinline__ uint32_t part_of(int32_t c, int32_t P) {
 
 // Queue vertex v (degree d) for a fallback CTA.  One lane calls it.
 __device__ __forceinline__ void enqueue_fallback(const FallbackSet &fs, int32_t v, int32_t d, int *err) {
-    if (d <= FBM_MAXDEG) {
-        const Fallback &f = fs.q[d <= FBS_MAXDEG ? 0 : 1];
+    if (d <= FBQ_MAXDEG(NFBQ - 1)) {
+        int b = 0;
+        while (d > FBQ_MAXDEG(b)) ++b;
+        const Fallback &f = fs.q[b];
         const int32_t i = atomicAdd(f.count, 1);
         if (i < f.cap) f.v[i] = v;
         else atomicOr(err, DEVERR_FALLBACK_FULL);
         return;
     }
-    const Fallback &f = fs.q[2];
+    const Fallback &f = fs.q[NFBQ];
     const int32_t P = (d + FB_KEYS - 1) / FB_KEYS;
     const int32_t first = atomicAdd(f.count, P);
     if (first + P <= f.cap) {
@@ -656,14 +658,32 @@ inline unsigned nblocks(int64_t items, int per_block) {
 
 }  // namespace
 
-constexpr int FBS_SMEM = FBS_CAP * 14, FBM_SMEM = FBM_CAP * 14;
+__host__ __device__ constexpr int FBQ_SMEM(int b) { return 2 * FBQ_MAXDEG(b) * 14; }
+
+template <typename WT, int B>
+static void set_row_queue_attrs(DeviceInfo &di) {
+    constexpr int T = FBQ_THREADS(B), CAP = 2 * FBQ_MAXDEG(B), SM = FBQ_SMEM(B);
+    cudaFuncSetAttribute(move_fallback_kernel<WT, T, CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+    int o = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_fallback_kernel<WT, T, CAP, false>, T, SM);
+    di.occ_fbq[B] = o > 0 ? o : 1;
+}
+
+template <typename WT, int B>
+static void launch_row_queue(const GraphView<WT> &g, const StateView &st, const FallbackSet &fs,
+                             const DeviceInfo &di, u64 *dE, cudaStream_t s) {
+    constexpr int T = FBQ_THREADS(B), CAP = 2 * FBQ_MAXDEG(B), SM = FBQ_SMEM(B);
+    move_fallback_kernel<WT, T, CAP, false><<<di.sms * di.occ_fbq[B], T, SM, s>>>(g, st, fs.q[B], HubGlobal(),
+                                                                                fs.hint, dE);
+    note_launches(1);
+}
 
 template <typename WT>
 static void set_attrs_for(DeviceInfo &di) {
-    cudaFuncSetAttribute(move_fallback_kernel<WT, FBS_THREADS, FBS_CAP, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, FBS_SMEM);
-    cudaFuncSetAttribute(move_fallback_kernel<WT, FBM_THREADS, FBM_CAP, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, FBM_SMEM);
+    set_row_queue_attrs<WT, 0>(di);
+    set_row_queue_attrs<WT, 1>(di);
+    set_row_queue_attrs<WT, 2>(di);
+    set_row_queue_attrs<WT, 3>(di);
     cudaFuncSetAttribute(move_fallback_kernel<WT, FB_THREADS, FB_CAP, true>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM);
     cudaFuncSetAttribute(giant_stage_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM);
@@ -671,14 +691,6 @@ static void set_attrs_for(DeviceInfo &di) {
     int o = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_warp_kernel<WT>, 256, WARP_SMEM);
     di.occ_warp = o > 0 ? o : 1;
-    o = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_fallback_kernel<WT, FBS_THREADS, FBS_CAP, false>,
-                                                  FBS_THREADS, FBS_SMEM);
-    di.occ_fbs = o > 0 ? o : 1;
-    o = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_fallback_kernel<WT, FBM_THREADS, FBM_CAP, false>,
-                                                  FBM_THREADS, FBM_SMEM);
-    di.occ_fbm = o > 0 ? o : 1;
 }
 
 void init_kernel_attributes(DeviceInfo &di) {
@@ -707,7 +719,7 @@ template <typename WT>
 static void launch_fallback_large(const GraphView<WT> &g, const StateView &st, const HubGlobal &hg,
                                   const FallbackSet &fs, const DeviceInfo &di, u64 *dE, cudaStream_t s) {
     move_fallback_kernel<WT, FB_THREADS, FB_CAP, true><<<di.sms, FB_THREADS, FB_SMEM, s>>>(
-        g, st, fs.q[2], hg, fs.hint, dE);
+        g, st, fs.q[NFBQ], hg, fs.hint, dE);
     note_launches(1);
 }
 
@@ -715,10 +727,10 @@ template <typename WT>
 void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGlobal &hg,
                         const FallbackSet &fs, const DeviceInfo &di, u64 *dE, cudaStream_t s) {
     if (hg.nhubs <= 0) return;
-    cudaMemsetAsync(fs.q[2].count, 0, 2 * sizeof(int32_t), s);   // count, next
+    cudaMemsetAsync(fs.q[NFBQ].count, 0, 2 * sizeof(int32_t), s);   // count, next
     giant_stage_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg); note_launches(1);
     giant_merge_kernel<<<(unsigned)imin64(hg.nhubs, di.sms), HG_MERGE_THREADS, HG_MERGE_SMEM, s>>>(
-        st, hg, fs.q[2], dE);
+        st, hg, fs.q[NFBQ], dE);
     note_launches(1);
     launch_fallback_large<WT>(g, st, hg, fs, di, dE, s);
 }
@@ -728,18 +740,16 @@ void launch_move_wide(const GraphView<WT> &g, const StateView &st, const int32_t
                       const FallbackSet &fs, const DeviceInfo &di, u64 *dE, cudaStream_t s,
                       int32_t max_degree) {
     if (n <= 0) return;
-    // the three queues' (count, next) pairs are contiguous
-    cudaMemsetAsync(fs.q[0].count, 0, 6 * sizeof(int32_t), s);
+    // the queues' (count, next) pairs are contiguous
+    cudaMemsetAsync(fs.q[0].count, 0, 2 * (NFBQ + 1) * sizeof(int32_t), s);
     const unsigned grid = (unsigned)imin64((n + 7) / 8, (int64_t)di.sms * di.occ_warp);
     move_warp_kernel<WT><<<grid, 256, WARP_SMEM, s>>>(g, st, list, n, fs, dE); note_launches(1);
     if (max_degree <= WARP_LIMIT) return;   // no vertex can overflow its warp table
     launch_fallback_large<WT>(g, st, HubGlobal(), fs, di, dE, s);
-    move_fallback_kernel<WT, FBM_THREADS, FBM_CAP, false><<<di.sms * di.occ_fbm, FBM_THREADS, FBM_SMEM, s>>>(
-        g, st, fs.q[1], HubGlobal(), fs.hint, dE);
-    note_launches(1);
-    move_fallback_kernel<WT, FBS_THREADS, FBS_CAP, false><<<di.sms * di.occ_fbs, FBS_THREADS, FBS_SMEM, s>>>(
-        g, st, fs.q[0], HubGlobal(), fs.hint, dE);
-    note_launches(1);
+    launch_row_queue<WT, 3>(g, st, fs, di, dE, s);
+    launch_row_queue<WT, 2>(g, st, fs, di, dE, s);
+    launch_row_queue<WT, 1>(g, st, fs, di, dE, s);
+    launch_row_queue<WT, 0>(g, st, fs, di, dE, s);
 }
 
 template <typename WT>
