@@ -82,7 +82,7 @@ EXPORTED = [
     "lv_set_communities", "lv_get_level_info", "lv_get_csr", "lv_get_scale", "lv_get_stats",
     "lv_get_class_stats", "lv_clear_stats", "lv_read_mtx", "lv_write_mtx", "lv_free_host",
     "lv_print_communities", "lv_gen_rmat", "lv_gen_planted", "lv_gen_rmat_device",
-    "lv_free_device", "lv_modularity_noalloc",
+    "lv_free_device", "lv_modularity_noalloc", "lv_trim_device_memory",
 ]
 
 _lib = None
@@ -144,6 +144,7 @@ def lib() -> C.CDLL:
                                      C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                      C.POINTER(C.c_void_p)]
     L.lv_free_device.argtypes = [C.c_void_p]
+    L.lv_trim_device_memory.argtypes = [C.c_int32]
     L.lv_modularity_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64,
                                         C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_char_p,
                                         C.c_int32]

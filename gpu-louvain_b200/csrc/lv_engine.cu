@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -165,21 +166,58 @@ int fail(lv_handle *h, int code, const std::string &msg) {
         if (rc__) return rc__;  \
     } while (0)
 
+// Device memory of every handle comes from one stream-ordered pool per
+// device whose release threshold keeps freed memory mapped, so creating a
+// handle after another was destroyed reuses the mapping instead of paying
+// cudaMalloc/cudaFree for the ~20 GB working set of an R-MAT-24 run again.
+// lv_trim_device_memory returns the unused part to the system.
+constexpr int LV_MAX_DEVICES = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[LV_MAX_DEVICES] = {};
+
+cudaMemPool_t device_pool(int dev) {
+    if (dev < 0 || dev >= LV_MAX_DEVICES) return nullptr;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        g_pool[dev] = pool;
+    }
+    return g_pool[dev];
+}
+
 template <typename T>
 int dalloc(lv_handle *h, T **p, size_t n) {
     *p = nullptr;
     if (n == 0) n = 1;
-    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    cudaMemPool_t pool = device_pool(h->device);
+    cudaError_t e = pool ? cudaMallocFromPoolAsync((void **)p, n * sizeof(T), pool, h->stream)
+                         : cudaMalloc((void **)p, n * sizeof(T));
     if (e != cudaSuccess) {
+        cudaGetLastError();
         *p = nullptr;
-        return fail(h, LV_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        return fail(h, LV_ERR_NOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
     }
     return LV_OK;
 }
 
+// Stream-ordered free (after the handle's queued work); the memory returns
+// to the device pool.
 template <typename T>
-void dfree(T *&p) {
-    if (p) cudaFree((void *)p);
+void dfree(lv_handle *h, T *&p) {
+    if (p) {
+        if (device_pool(h->device)) cudaFreeAsync((void *)p, h->stream);
+        else cudaFree((void *)p);
+    }
     p = nullptr;
 }
 
@@ -277,8 +315,8 @@ StateView state_of(lv_handle *h) {
 int ensure_tables(lv_handle *h, size_t slots) {
     if (slots <= h->tbl_slots) return LV_OK;
     size_t want = slots + slots / 4;
-    dfree(h->tbl_keys);
-    dfree(h->tbl_vals);
+    dfree(h, h->tbl_keys);
+    dfree(h, h->tbl_vals);
     h->tbl_slots = 0;
     LV_TRY(dalloc(h, &h->tbl_keys, want));
     LV_TRY(dalloc(h, &h->tbl_vals, want));
@@ -290,9 +328,9 @@ int ensure_tables(lv_handle *h, size_t slots) {
 
 int ensure_occ(lv_handle *h, size_t entries, size_t hubs) {
     if (entries > h->occ_cap) {
-        dfree(h->occ_buf);
-        dfree(h->stage_key);
-        dfree(h->stage_val);
+        dfree(h, h->occ_buf);
+        dfree(h, h->stage_key);
+        dfree(h, h->stage_val);
         h->occ_cap = 0;
         size_t want = entries + entries / 4 + 1;
         LV_TRY(dalloc(h, &h->occ_buf, want));
@@ -301,9 +339,9 @@ int ensure_occ(lv_handle *h, size_t entries, size_t hubs) {
         h->occ_cap = want;
     }
     if (hubs > h->nocc_cap) {
-        dfree(h->nocc_buf);
-        dfree(h->eown_buf);
-        dfree(h->ovf_buf);
+        dfree(h, h->nocc_buf);
+        dfree(h, h->eown_buf);
+        dfree(h, h->ovf_buf);
         h->nocc_cap = 0;
         size_t want = hubs + hubs / 4 + 1;
         LV_TRY(dalloc(h, &h->nocc_buf, want));
@@ -364,10 +402,13 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
     size_t i32_bytes = ((i32_count * 4 + 15) / 16) * 16;
     size_t bytes = i32_bytes + (size_t)n * 8 + ns * 16 + ns * 8 + ns * 8 + (size_t)n * 8 + 64;
     if (bytes > L.dev_bytes) {
-        if (L.dev) cudaFree(L.dev);
+        unsigned char *old_dev = (unsigned char *)L.dev;
+        dfree(h, old_dev);
         L.dev = nullptr;
         L.dev_bytes = 0;
-        if (cudaMalloc(&L.dev, bytes) != cudaSuccess) return fail(h, LV_ERR_NOMEM, "layout alloc");
+        unsigned char *nd = nullptr;
+        LV_TRY(dalloc(h, &nd, bytes));
+        L.dev = nd;
         L.dev_bytes = bytes;
     }
     std::vector<unsigned char> host(bytes, 0);
@@ -917,6 +958,17 @@ const char *lv_status_string(int s) {
     }
 }
 
+int lv_trim_device_memory(int32_t device) {
+    if (device < 0 || device >= LV_MAX_DEVICES) return LV_ERR_INVALID;
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        pool = g_pool[device];
+    }
+    if (!pool) return LV_OK;
+    return cudaMemPoolTrimTo(pool, 0) == cudaSuccess ? LV_OK : LV_ERR_CUDA;
+}
+
 const char *lv_version(void) { return "louvain_b200 0.1 (sm_100a)"; }
 
 int lv_destroy(lv_handle *h) {
@@ -924,39 +976,45 @@ int lv_destroy(lv_handle *h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->owns_input) {
-        dfree(h->in_rowptr);
-        dfree(h->in_col);
-        dfree(h->in_w);
+        dfree(h, h->in_rowptr);
+        dfree(h, h->in_col);
+        dfree(h, h->in_w);
     }
     {
         FallbackSet &fs = h->fb;
-        dfree(fs.q[0].count); dfree(fs.hint);
+        dfree(h, fs.q[0].count); dfree(h, fs.hint);
         for (int q = 0; q <= NFBQ; ++q) {
             Fallback &f = fs.q[q];
-            dfree(f.v); dfree(f.p); dfree(f.P); dfree(f.first); dfree(f.done); dfree(f.src);
-            dfree(f.gd); dfree(f.e); dfree(f.S); dfree(f.eo); dfree(f.c); dfree(f.cnt);
+            dfree(h, f.v); dfree(h, f.p); dfree(h, f.P); dfree(h, f.first); dfree(h, f.done); dfree(h, f.src);
+            dfree(h, f.gd); dfree(h, f.e); dfree(h, f.S); dfree(h, f.eo); dfree(h, f.c); dfree(h, f.cnt);
         }
     }
-    dfree(h->comm); dfree(h->newc); dfree(h->size); dfree(h->orig2comm);
-    dfree(h->k); dfree(h->S); dfree(h->list); dfree(h->cls_scratch);
-    dfree(h->tbl_keys); dfree(h->tbl_vals); dfree(h->occ_buf); dfree(h->nocc_buf);
-    dfree(h->stage_key); dfree(h->stage_val); dfree(h->eown_buf); dfree(h->ovf_buf);
-    if (h->hub_move.dev) cudaFree(h->hub_move.dev);
-    if (h->hub_agg.dev) cudaFree(h->hub_agg.dev);
-    AggBuffers &a = h->ab;
-    dfree(a.flag); dfree(a.cdeg); dfree(a.mstart); dfree(a.cursor); dfree(a.members);
-    dfree(a.lab); dfree(a.clist); dfree(a.newdeg); dfree(a.epos_new); dfree(a.scan_tmp);
-    dfree(a.scalars);
-    dfree(h->mslot); dfree(h->degm); dfree(h->P);
-    for (int b = 0; b < 2; ++b) {
-        dfree(h->lvl_start[b]); dfree(h->lvl_end[b]); dfree(h->lvl_col[b]); dfree(h->lvl_w[b]);
+    dfree(h, h->comm); dfree(h, h->newc); dfree(h, h->size); dfree(h, h->orig2comm);
+    dfree(h, h->k); dfree(h, h->S); dfree(h, h->list); dfree(h, h->cls_scratch);
+    dfree(h, h->tbl_keys); dfree(h, h->tbl_vals); dfree(h, h->occ_buf); dfree(h, h->nocc_buf);
+    dfree(h, h->stage_key); dfree(h, h->stage_val); dfree(h, h->eown_buf); dfree(h, h->ovf_buf);
+    for (HubLayout *L : {&h->hub_move, &h->hub_agg}) {
+        unsigned char *d = (unsigned char *)L->dev;
+        dfree(h, d);
+        L->dev = nullptr;
     }
-    dfree(h->tot_d);
+    AggBuffers &a = h->ab;
+    dfree(h, a.flag); dfree(h, a.cdeg); dfree(h, a.mstart); dfree(h, a.cursor); dfree(h, a.members);
+    dfree(h, a.lab); dfree(h, a.clist); dfree(h, a.newdeg); dfree(h, a.epos_new); dfree(h, a.scan_tmp);
+    dfree(h, a.scalars);
+    dfree(h, h->mslot); dfree(h, h->degm); dfree(h, h->P);
+    for (int b = 0; b < 2; ++b) {
+        dfree(h, h->lvl_start[b]); dfree(h, h->lvl_end[b]); dfree(h, h->lvl_col[b]); dfree(h, h->lvl_w[b]);
+    }
+    dfree(h, h->tot_d);
     if (h->tot_h) cudaFreeHost(h->tot_h);
     if (h->small_h) cudaFreeHost(h->small_h);
     for (const Pending &p : h->pend) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     for (cudaEvent_t e : h->ev_free) cudaEventDestroy(e);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->stream) {
+        cudaStreamSynchronize(h->stream);   // the stream-ordered frees above
+        cudaStreamDestroy(h->stream);
+    }
     delete h;
     return LV_OK;
 }
@@ -1119,7 +1177,7 @@ int lv_get_csr(lv_handle *h, int32_t *rowptr, int32_t *col, int64_t *wfix) {
             cudaError_t e = cudaMemcpyAsync(wfix, tmp, sizeof(int64_t) * (size_t)h->E,
                                             cudaMemcpyDeviceToHost, h->stream);
             cudaStreamSynchronize(h->stream);
-            cudaFree(tmp);
+            dfree(h, tmp);
             if (e != cudaSuccess) return fail(h, LV_ERR_CUDA, cudaGetErrorString(e));
         }
         return sync(h);

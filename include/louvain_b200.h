@@ -96,7 +96,15 @@ int lv_create_device(const int32_t *d_rowptr, const int32_t *d_col, const float 
                      int64_t E, const lv_opts *opts, lv_handle **out);
 /* Return to level 0 with singleton communities (no reallocation). */
 int lv_reset(lv_handle *h);
+/* deleteStructures (utils.cu:108-141).  The handle's device memory goes back
+ * to the library's per-device memory pool, which keeps it mapped so that the
+ * next handle on that device reuses it instead of allocating again; call
+ * lv_trim_device_memory to return it to the system. */
 int lv_destroy(lv_handle *h);
+/* Release the device memory that destroyed handles left in the library's pool
+ * for `device` (memory of live handles is untouched).  No counterpart in the
+ * reference, which allocates and frees per call. */
+int lv_trim_device_memory(int32_t device);
 const char *lv_last_error(const lv_handle *h);
 
 /* optimiseModularity (modularity_optimisation.cuh:28): sweeps of the current

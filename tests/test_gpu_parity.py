@@ -175,6 +175,22 @@ def test_megahub_matches_oracle(lvb, orc):
     e.close()
 
 
+def test_handles_reuse_pooled_memory(lvb, orc, graphs):
+    """Handles created after others were destroyed (memory reused from the
+    library's device pool) and after the pool was trimmed give the same
+    results."""
+    rp, cl, w, gain = graphs["rmat14_unit"]
+    qs = []
+    for trim in (False, False, True, False):
+        e = lvb.Louvain(lvb.Graph(rp, cl, w))
+        qs.append((e.run(gain), e.original_to_community()[0].tobytes()))
+        e.close()
+        if trim:
+            assert lvb.lib().lv_trim_device_memory(0) == lvb.LV_OK
+    assert all(q == qs[0] for q in qs)
+    assert lvb.lib().lv_trim_device_memory(-1) == lvb.LV_ERR_INVALID
+
+
 def test_aggregation_from_given_communities(lvb, orc, graphs):
     rng = np.random.default_rng(7)
     for name in ("rmat12", "hubs", "planted10k_uniform"):
