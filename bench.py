@@ -287,14 +287,26 @@ def run_ours(args, ranks: Ranks):
     out_map = torch.empty(V, dtype=torch.int32, pin_memory=True).numpy()
     e2e_steps = max(1, args.steps)
 
+    parts = {"create": 0.0, "run": 0.0, "map": 0.0, "close": 0.0}
+
     def e2e_step():
+        t_a = time.perf_counter()
         with lvb.Louvain(host_graph, device=dev) as e:
+            t_b = time.perf_counter()
             e.run(MIN_GAIN)
+            t_c = time.perf_counter()
             m, nc = e.original_to_community()
             out_map[:] = m
-            return e.stats()["edge_sweeps"]
+            units = e.stats()["edge_sweeps"]
+            t_d = time.perf_counter()
+        t_e = time.perf_counter()
+        for k, dt in (("create", t_b - t_a), ("run", t_c - t_b), ("map", t_d - t_c), ("close", t_e - t_d)):
+            parts[k] += dt
+        return units
 
     e2e_step()   # warm-up (allocator, module load)
+    for k in parts:
+        parts[k] = 0.0
     ranks.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -328,7 +340,8 @@ def run_ours(args, ranks: Ranks):
         "modularity": qs[-1], "communities": ncomm, "levels": st["levels"] // args.steps,
         "sweeps": st["sweeps"] // args.steps, "edge_sweeps_per_run": st["edge_sweeps"] // args.steps,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * (V + 1) + 8 * E,
-                "d2h_bytes_per_step": 4 * V, "seconds_per_step": t_e2e / e2e_steps},
+                "d2h_bytes_per_step": 4 * V, "seconds_per_step": t_e2e / e2e_steps,
+                "ms_per_step_parts": {k: round(1e3 * v / e2e_steps, 1) for k, v in parts.items()}},
         "gpu_launches": st["kernel_launches"],
         "roofline": {"bound": "hbm", "kernel": CLASS_NAMES[dom], "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
