@@ -486,17 +486,39 @@ __device__ __forceinline__ int32_t move_decision(const MoveCtx &m, const Best &b
 
 // Butterfly reduction inside aligned groups of `width` lanes; every lane of
 // the group ends with the group's best and the summed e_own.
+// The exact gain of each lane's best lies in [gd - err, gd + err].  A lane
+// whose upper bound is below the group's largest lower bound cannot win; when
+// one lane per group is left (the usual case) it is the exact argmax and is
+// broadcast.  Otherwise (ties or near-ties in some group of the warp) the
+// butterfly of exact comparisons decides.
 __device__ __forceinline__ void group_reduce_best(const MoveCtx &m, Best &b, int width) {
+    const int lane = threadIdx.x & 31;
+    const unsigned gmask = width == 32 ? FULL : (((1u << width) - 1u) << (lane & ~(width - 1)));
+    const double eb = gain_err(m, b);
+    double lo = b.gd - eb;
+    u64 eo = b.eo;
     for (int off = width >> 1; off > 0; off >>= 1) {
-        Best o;
-        o.gd = __shfl_xor_sync(FULL, b.gd, off, width);
-        o.e = __shfl_xor_sync(FULL, b.e, off, width);
-        o.S = __shfl_xor_sync(FULL, b.S, off, width);
-        o.c = __shfl_xor_sync(FULL, b.c, off, width);
-        const u64 oe = __shfl_xor_sync(FULL, b.eo, off, width);
-        if (better(m, o, b)) { b.gd = o.gd; b.e = o.e; b.S = o.S; b.c = o.c; }
-        b.eo += oe;
+        lo = fmax(lo, __shfl_xor_sync(FULL, lo, off, width));
+        eo += __shfl_xor_sync(FULL, eo, off, width);
     }
+    const unsigned alive = __ballot_sync(FULL, b.gd + eb >= lo) & gmask;
+    if (!__any_sync(FULL, __popc(alive) != 1)) {
+        const int src = (__ffs(alive) - 1) & (width - 1);
+        b.gd = __shfl_sync(FULL, b.gd, src, width);
+        b.e = __shfl_sync(FULL, b.e, src, width);
+        b.S = __shfl_sync(FULL, b.S, src, width);
+        b.c = __shfl_sync(FULL, b.c, src, width);
+    } else {
+        for (int off = width >> 1; off > 0; off >>= 1) {
+            Best o;
+            o.gd = __shfl_xor_sync(FULL, b.gd, off, width);
+            o.e = __shfl_xor_sync(FULL, b.e, off, width);
+            o.S = __shfl_xor_sync(FULL, b.S, off, width);
+            o.c = __shfl_xor_sync(FULL, b.c, off, width);
+            if (better(m, o, b)) { b.gd = o.gd; b.e = o.e; b.S = o.S; b.c = o.c; }
+        }
+    }
+    b.eo = eo;
 }
 
 __device__ __forceinline__ u64 warp_sum_u64(u64 x) {
