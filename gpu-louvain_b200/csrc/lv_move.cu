@@ -177,15 +177,32 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
     __syncwarp();
     u64 delta_acc = 0;
     const int32_t nwarps = gridDim.x * NW;
-    for (int32_t idx = blockIdx.x * NW + wid; idx < n; idx += nwarps) {
-        const int32_t v = list[idx];
-        const int32_t r0 = g.rowptr[v], r1 = g.rowend[v];
+    // the next vertex's id, row bounds and community are loaded while the
+    // current one is processed (none of them changes during the sub-round)
+    int32_t idx = blockIdx.x * NW + wid;
+    int32_t nv = 0, nr0 = 0, nr1 = 0, nown = 0;
+    if (idx < n) {
+        nv = list[idx];
+        nr0 = g.rowptr[nv];
+        nr1 = g.rowend[nv];
+        nown = __ldg(st.comm + nv);
+    }
+    for (; idx < n; idx += nwarps) {
+        const int32_t v = nv, r0 = nr0, r1 = nr1, own = nown;
+        if (idx + nwarps < n) {
+            nv = list[idx + nwarps];
+            nr0 = g.rowptr[nv];
+            nr1 = g.rowend[nv];
+            nown = __ldg(st.comm + nv);
+        }
         const int32_t d = r1 - r0;
         if (d > WARP_LIMIT && fs.hint[v]) {
             if (lane == 0) enqueue_fallback(fs, v, d, st.err);
             continue;
         }
-        const int32_t own = __ldg(st.comm + v);
+        // the vertex's own terms, issued before the edge loop
+        const int32_t sz_own = __ldg(st.size + own);
+        const u64 k_v = __ldg(st.k + v), s_own = __ldg(st.S + own);
         int lg = ceil_log2_i(2 * (int64_t)d);
         lg = lg < 5 ? 5 : (lg > LG ? LG : lg);
         u64 e_own = 0;
@@ -233,7 +250,7 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
             __syncwarp();
             continue;
         }
-        const MoveCtx m = move_ctx(own, __ldg(st.size + own) == 1, st.T, __ldg(st.k + v), __ldg(st.S + own));
+        const MoveCtx m = move_ctx(own, sz_own == 1, st.T, k_v, s_own);
         Best b = best_init(own);
         b.eo = e_own;
         eval_slots<1, false, true>(keys, vals, nullptr, nslots, lane, 32, m, st.S, st.size, b);
