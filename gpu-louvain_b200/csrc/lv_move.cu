@@ -533,23 +533,48 @@ __global__ void __launch_bounds__(256) corr_group_kernel(GraphView<WT> g, const 
     block_add_total<256>(acc, dE);
 }
 
+// Rows of T threads each.  A pass checks CORR_BATCH vertices of the list at
+// once (one per lane of warp 0), gathers the ones that moved in shared
+// memory, and then scans only their rows, so a sub-round with few movers
+// costs one parallel check per CORR_BATCH vertices instead of a serial check
+// per vertex.
+constexpr int CORR_BATCH = 32;
+
 template <int T, typename WT>
 __global__ void __launch_bounds__(T) corr_cta_kernel(GraphView<WT> g, const int32_t *__restrict__ comm,
                                                      const int32_t *__restrict__ newc,
                                                      const int32_t *__restrict__ list, int32_t n,
                                                      u64 *dE) {
+    __shared__ int32_t movers[CORR_BATCH];
+    __shared__ int32_t nm;
     u64 acc = 0;
-    for (int32_t idx = blockIdx.x; idx < n; idx += gridDim.x) {
-        const int32_t u = list[idx];
-        const int32_t cu = comm[u], nu = newc[u];
-        if (cu == nu) continue;
-        const int32_t r0 = g.rowptr[u], r1 = g.rowend[u];
-        for (int32_t e = r0 + threadIdx.x; e < r1; e += T) {
-            const int32_t j = __ldg(g.col + e);
-            if (j == u) continue;
-            const int32_t cj = comm[j], nj = newc[j];
-            if (cj != nj) acc += pair_correction(cu, nu, cj, nj, wfix(g.w, e, g.scale));
+    for (int32_t base = blockIdx.x * CORR_BATCH; base < n; base += gridDim.x * CORR_BATCH) {
+        if (threadIdx.x < 32) {
+            const int32_t idx = base + threadIdx.x;
+            bool moved = false;
+            int32_t u = 0;
+            if (idx < n) {
+                u = list[idx];
+                moved = comm[u] != newc[u];
+            }
+            const unsigned bal = __ballot_sync(FULL, moved);
+            if (moved) movers[__popc(bal & ((1u << threadIdx.x) - 1u))] = u;
+            if (threadIdx.x == 0) nm = __popc(bal);
         }
+        __syncthreads();
+        const int32_t cnt = nm;
+        for (int32_t k = 0; k < cnt; ++k) {
+            const int32_t u = movers[k];
+            const int32_t cu = comm[u], nu = newc[u];
+            const int32_t r0 = g.rowptr[u], r1 = g.rowend[u];
+            for (int32_t e = r0 + threadIdx.x; e < r1; e += T) {
+                const int32_t j = __ldg(g.col + e);
+                if (j == u) continue;
+                const int32_t cj = comm[j], nj = newc[j];
+                if (cj != nj) acc += pair_correction(cu, nu, cj, nj, wfix(g.w, e, g.scale));
+            }
+        }
+        __syncthreads();   // movers / nm are rewritten by the next pass
     }
     block_add_total<T>(acc, dE);
 }
@@ -780,13 +805,13 @@ void launch_correction(int cls, const GraphView<WT> &g, const StateView &st, con
     case CLS_B3:
     case CLS_B4: corr_group_kernel<32, WT><<<nblocks(n, 8), 256, 0, s>>>(g, st.comm, st.newc, list, n, dE); break;
     case CLS_B5:
-        corr_cta_kernel<128, WT><<<(unsigned)imin64(n, (int64_t)di.sms * 16), 128, 0, s>>>(g, st.comm, st.newc, list, n, dE);
+        corr_cta_kernel<128, WT><<<(unsigned)imin64(nblocks(n, CORR_BATCH), (int64_t)di.sms * 16), 128, 0, s>>>(g, st.comm, st.newc, list, n, dE);
         break;
     case CLS_H1:
-        corr_cta_kernel<256, WT><<<(unsigned)imin64(n, (int64_t)di.sms * 8), 256, 0, s>>>(g, st.comm, st.newc, list, n, dE);
+        corr_cta_kernel<256, WT><<<(unsigned)imin64(nblocks(n, CORR_BATCH), (int64_t)di.sms * 8), 256, 0, s>>>(g, st.comm, st.newc, list, n, dE);
         break;
     default:
-        corr_cta_kernel<512, WT><<<(unsigned)imin64(n, (int64_t)di.sms * 4), 512, 0, s>>>(g, st.comm, st.newc, list, n, dE);
+        corr_cta_kernel<512, WT><<<(unsigned)imin64(nblocks(n, CORR_BATCH), (int64_t)di.sms * 4), 512, 0, s>>>(g, st.comm, st.newc, list, n, dE);
         break;
     }
     note_launches(1);
