@@ -175,6 +175,47 @@ def test_megahub_matches_oracle(lvb, orc):
     e.close()
 
 
+def test_giant_paths_match_oracle(lvb, orc):
+    """Giants (degree > 8192) whose neighbours fall into few communities
+    (staged pairs merged in one shared table) and into as many communities as
+    neighbours (staged pairs split into key-space partitions), with the
+    communities changed between sweeps."""
+    rng = np.random.default_rng(11)
+    V = 60000
+    u = rng.integers(0, V, 120000)
+    v = rng.integers(0, V, 120000)
+    for h, d in [(0, 30000), (1, 10000), (2, 25000)]:
+        nb = rng.choice(V, d, replace=False)
+        u = np.concatenate([u, np.full(d, h)])
+        v = np.concatenate([v, nb])
+    keep = u != v
+    a, b = np.minimum(u[keep], v[keep]), np.maximum(u[keep], v[keep])
+    key = np.unique(a.astype(np.int64) * V + b)
+    a, b = key // V, key % V
+    w = (rng.integers(1, 8, len(a)) * 0.25).astype(np.float32)
+    src = np.concatenate([a, b]); dst = np.concatenate([b, a]); ww = np.concatenate([w, w])
+    o_ = np.lexsort((dst, src))
+    rp = np.concatenate([[0], np.cumsum(np.bincount(src, minlength=V))]).astype(np.int32)
+    cl, w = dst[o_].astype(np.int32), ww[o_].astype(np.float32)
+    e = lvb.Louvain(lvb.Graph(rp, cl, w), verify=True)
+    o = orc.Oracle(rp, cl, w)
+
+    def sweeps(k, tag):
+        for s in range(k):
+            m1, m2 = e.sweep(), o.sweep()
+            assert m1 == m2, f"{tag} sweep {s}"
+            assert np.array_equal(e.communities(), o.communities()), f"{tag} sweep {s}"
+            assert e.calculate_modularity() == o.modularity()
+
+    blocks = (np.arange(V) // 1000).astype(np.int32)
+    e.set_communities(blocks); o.set_communities(blocks)
+    sweeps(3, "blocks")
+    single = np.arange(V, dtype=np.int32)
+    e.set_communities(single); o.set_communities(single)
+    sweeps(3, "singletons")
+    e.close()
+
+
 def test_handles_reuse_pooled_memory(lvb, orc, graphs):
     """Handles created after others were destroyed (memory reused from the
     library's device pool) and after the pool was trimmed give the same
