@@ -288,6 +288,7 @@ def run_ours(args, ranks: Ranks):
     e2e_steps = max(1, args.steps)
 
     parts = {"create": 0.0, "run": 0.0, "map": 0.0, "close": 0.0}
+    step_ms = []
 
     def e2e_step():
         t_a = time.perf_counter()
@@ -302,11 +303,13 @@ def run_ours(args, ranks: Ranks):
         t_e = time.perf_counter()
         for k, dt in (("create", t_b - t_a), ("run", t_c - t_b), ("map", t_d - t_c), ("close", t_e - t_d)):
             parts[k] += dt
+        step_ms.append(round(1e3 * (t_e - t_a), 1))
         return units
 
     e2e_step()   # warm-up (allocator, module load)
     for k in parts:
         parts[k] = 0.0
+    step_ms.clear()
     ranks.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -341,7 +344,8 @@ def run_ours(args, ranks: Ranks):
         "sweeps": st["sweeps"] // args.steps, "edge_sweeps_per_run": st["edge_sweeps"] // args.steps,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * (V + 1) + 8 * E,
                 "d2h_bytes_per_step": 4 * V, "seconds_per_step": t_e2e / e2e_steps,
-                "ms_per_step_parts": {k: round(1e3 * v / e2e_steps, 1) for k, v in parts.items()}},
+                "ms_per_step_parts": {k: round(1e3 * v / e2e_steps, 1) for k, v in parts.items()},
+                "step_ms": step_ms},
         "gpu_launches": st["kernel_launches"],
         "roofline": {"bound": "hbm", "kernel": CLASS_NAMES[dom], "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,

@@ -179,6 +179,10 @@ cudaMemPool_t device_pool(int dev) {
     if (dev < 0 || dev >= LV_MAX_DEVICES) return nullptr;
     std::lock_guard<std::mutex> lock(g_pool_mu);
     if (!g_pool[dev]) {
+        // an error left pending by an earlier asynchronous call would be
+        // reported by the calls below; set-up is retried by the next
+        // allocation if it fails
+        cudaGetLastError();
         cudaMemPoolProps props = {};
         props.allocType = cudaMemAllocationTypePinned;
         props.location.type = cudaMemLocationTypeDevice;
@@ -189,7 +193,11 @@ cudaMemPool_t device_pool(int dev) {
             return nullptr;
         }
         uint64_t keep = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+            cudaGetLastError();
+            cudaMemPoolDestroy(pool);
+            return nullptr;
+        }
         g_pool[dev] = pool;
     }
     return g_pool[dev];
@@ -812,6 +820,9 @@ int to_level0(lv_handle *h) {
 
 int finish_create(lv_handle *h) {
     const size_t V = (size_t)h->V0;
+    if (h->opts.trace)
+        std::fprintf(stderr, "[lv] device %d memory pool: %s\n", h->device,
+                     device_pool(h->device) ? "on" : "off (cudaMalloc per buffer)");
     LV_TRY(dalloc(h, &h->comm, V + 1));
     LV_TRY(dalloc(h, &h->newc, V + 1));
     LV_TRY(dalloc(h, &h->size, V + 1));
