@@ -8,7 +8,10 @@ namespace lv {
 // for the current level.  Hubs are split into edge chunks (insert kernel)
 // and chunks of their occupied-slot list (evaluate kernel) so that one hub
 // spreads over many CTAs; a hub of degree d has at most d occupied slots.
-constexpr int HG_EDGE_CHUNK = 4096;   // aggregation: entries per insert CTA
+#ifndef LV_HG_EDGE_CHUNK
+#define LV_HG_EDGE_CHUNK 2048
+#endif
+constexpr int HG_EDGE_CHUNK = LV_HG_EDGE_CHUNK;   // aggregation: entries per insert CTA
 constexpr int HG_SLOT_CHUNK = 4096;   // table slots per evaluation CTA
 constexpr int HG_INSERT_THREADS = 512;
 constexpr int HG_INSERT_SMEM = 2 * HG_EDGE_CHUNK * 12;   // chunk-local table
@@ -20,6 +23,12 @@ constexpr int STAGE_SMEM = 2 * STAGE_CHUNK * 14;
 constexpr int HG_MERGE_THREADS = 1024;
 constexpr int HG_MERGE_CAP = 16384;                      // shared slots of the per-hub merge
 constexpr int HG_MERGE_SMEM = HG_MERGE_CAP * 14;
+// giants with at most MERGE_S_CAP / 2 staged pairs are merged by smaller CTAs
+constexpr int MERGE_S_THREADS = 256, MERGE_S_CAP = 2048;
+#ifndef LV_MERGE_SMALL
+#define LV_MERGE_SMALL 1
+#endif
+
 
 struct HubGlobal {
     int32_t nhubs = 0;
@@ -98,6 +107,7 @@ struct DeviceInfo {
     int sms = 148;
     int occ_warp = 4;   // resident CTAs per SM of the warp kernel
     int occ_fbq[NFBQ] = {1, 1, 1, 1};   // ... of the row fallback kernels
+    int occ_merge_s = 1;                 // ... of the small giant-merge kernel
 };
 void init_kernel_attributes(DeviceInfo &di);
 

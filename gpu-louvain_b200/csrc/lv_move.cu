@@ -433,21 +433,25 @@ __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_kernel(GraphView<WT
     }
 }
 
-__global__ void __launch_bounds__(HG_MERGE_THREADS) giant_merge_kernel(StateView st, HubGlobal hg,
-                                                                       Fallback fb, u64 *dE) {
+// Two instances: CAP = HG_MERGE_CAP decides the giants with
+// n_min < n <= HG_MERGE_CAP / 2 staged pairs and queues the larger ones; a
+// smaller instance (more CTAs per SM) runs first and takes n <= CAP / 2.
+template <int THREADS, int CAP>
+__global__ void __launch_bounds__(THREADS) giant_merge_kernel(StateView st, HubGlobal hg, Fallback fb,
+                                                              u64 *dE, int32_t n_min) {
     // fb: the large fallback queue
     extern __shared__ __align__(16) unsigned char smem_raw[];
     u64 *vals = reinterpret_cast<u64 *>(smem_raw);
-    int32_t *keys = reinterpret_cast<int32_t *>(vals + HG_MERGE_CAP);
-    int32_t *occ = keys + HG_MERGE_CAP;
+    int32_t *keys = reinterpret_cast<int32_t *>(vals + CAP);
+    int32_t *occ = keys + CAP;
     __shared__ int32_t nocc;
-    for (int s = threadIdx.x; s < HG_MERGE_CAP; s += HG_MERGE_THREADS) { keys[s] = -1; vals[s] = 0; }
+    for (int s = threadIdx.x; s < CAP; s += THREADS) { keys[s] = -1; vals[s] = 0; }
     if (threadIdx.x == 0) nocc = 0;
     __syncthreads();
     u64 delta_sum = 0;
     for (int32_t h = blockIdx.x; h < hg.nhubs; h += gridDim.x) {
         const int32_t n = hg.nocc[h];
-        if (2 * (int64_t)n > HG_MERGE_CAP) {
+        if (2 * (int64_t)n > HG_MERGE_CAP && CAP == HG_MERGE_CAP) {
             // too many staged pairs for one shared table: queue key-space
             // partitions of the staged pairs for the fallback kernel
             if (threadIdx.x == 0) {
@@ -467,20 +471,21 @@ __global__ void __launch_bounds__(HG_MERGE_THREADS) giant_merge_kernel(StateView
             }
             continue;
         }
+        if (n <= n_min || 2 * (int64_t)n > CAP) continue;   // the other instance's range
         const int32_t v = hg.hubs[h];
         const int32_t own = __ldg(st.comm + v);
         int lg = ceil_log2_i(2 * (int64_t)n);
         lg = lg < 3 ? 3 : lg;
         const int32_t *sk = hg.stage_key + hg.occ_off[h];
         const u64 *sv = hg.stage_val + hg.occ_off[h];
-        for (int32_t i = threadIdx.x; i < n; i += HG_MERGE_THREADS)
+        for (int32_t i = threadIdx.x; i < n; i += THREADS)
             table_insert_occ(keys, vals, lg, sk[i], sv[i], st.err, occ, &nocc);
         __syncthreads();
         const MoveCtx m = move_ctx(own, __ldg(st.size + own) == 1, st.T, __ldg(st.k + v), __ldg(st.S + own));
         Best b = best_init(own);
         if (threadIdx.x == 0) b.eo = hg.eown[h];
-        eval_slots<1, true, true>(keys, vals, occ, nocc, threadIdx.x, HG_MERGE_THREADS, m, st.S, st.size, b);
-        cta_reduce_best<HG_MERGE_THREADS>(m, b);
+        eval_slots<1, true, true>(keys, vals, occ, nocc, threadIdx.x, THREADS, m, st.S, st.size, b);
+        cta_reduce_best<THREADS>(m, b);
         if (threadIdx.x == 0) {
             u64 delta = 0;
             st.newc[v] = move_decision(m, b, &delta);
@@ -741,7 +746,14 @@ void init_kernel_attributes(DeviceInfo &di) {
     cudaDeviceGetAttribute(&di.sms, cudaDevAttrMultiProcessorCount, dev);
     set_attrs_for<u64>(di);
     set_attrs_for<float>(di);
-    cudaFuncSetAttribute(giant_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HG_MERGE_SMEM);
+    cudaFuncSetAttribute(giant_merge_kernel<HG_MERGE_THREADS, HG_MERGE_CAP>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, HG_MERGE_SMEM);
+    cudaFuncSetAttribute(giant_merge_kernel<MERGE_S_THREADS, MERGE_S_CAP>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, MERGE_S_CAP * 14);
+    int o = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, giant_merge_kernel<MERGE_S_THREADS, MERGE_S_CAP>,
+                                                  MERGE_S_THREADS, MERGE_S_CAP * 14);
+    di.occ_merge_s = o > 0 ? o : 1;
 }
 
 template <typename WT>
@@ -771,8 +783,18 @@ void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGl
     if (hg.nhubs <= 0) return;
     cudaMemsetAsync(fs.q[NFBQ].count, 0, 2 * sizeof(int32_t), s);   // count, next
     giant_stage_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg); note_launches(1);
-    giant_merge_kernel<<<(unsigned)imin64(hg.nhubs, di.sms), HG_MERGE_THREADS, HG_MERGE_SMEM, s>>>(
-        st, hg, fs.q[NFBQ], dE);
+#if LV_MERGE_SMALL
+    giant_merge_kernel<MERGE_S_THREADS, MERGE_S_CAP>
+        <<<(unsigned)imin64(hg.nhubs, (int64_t)di.sms * di.occ_merge_s), MERGE_S_THREADS, MERGE_S_CAP * 14, s>>>(
+            st, hg, fs.q[NFBQ], dE, -1);
+    note_launches(1);
+    const int32_t big_min = MERGE_S_CAP / 2;
+#else
+    const int32_t big_min = -1;
+#endif
+    giant_merge_kernel<HG_MERGE_THREADS, HG_MERGE_CAP>
+        <<<(unsigned)imin64(hg.nhubs, di.sms), HG_MERGE_THREADS, HG_MERGE_SMEM, s>>>(st, hg, fs.q[NFBQ], dE,
+                                                                                   big_min);
     note_launches(1);
     launch_fallback_large<WT>(g, st, hg, fs, di, dE, s);
 }
