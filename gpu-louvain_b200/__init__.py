@@ -58,7 +58,7 @@ class LouvainError(RuntimeError):
 class _Opts(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("device", C.c_int32), ("max_sweeps", C.c_int32),
                 ("profile", C.c_int32), ("verify", C.c_int32), ("trace", C.c_int32),
-                ("reserved", C.c_int32 * 10)]
+                ("sweep_graph", C.c_int32), ("reserved", C.c_int32 * 9)]
 
 
 class _Stats(C.Structure):
@@ -290,7 +290,7 @@ class Louvain:
 
     def __init__(self, graph: Graph | None = None, *, device: int = 0, max_sweeps: int = 0,
                  profile: bool = False, verify: bool = False, trace: bool = False,
-                 device_csr: tuple | None = None):
+                 device_csr: tuple | None = None, sweep_graph: bool = True):
         L = lib()
         opts = _Opts()
         L.lv_default_opts(C.byref(opts))
@@ -299,6 +299,7 @@ class Louvain:
         opts.profile = 1 if profile else 0
         opts.verify = 1 if verify else 0
         opts.trace = 1 if trace else 0
+        opts.sweep_graph = 1 if sweep_graph else 0
         h = C.c_void_p()
         if device_csr is not None:
             rp, cl, w, V, E = device_csr

@@ -124,6 +124,8 @@ struct lv_handle {
     u64 *stage_val = nullptr;
     u64 *eown_buf = nullptr;       // per hub, zero between uses (nocc_cap entries)
     int32_t *ovf_buf = nullptr;    // overflow list (nocc_cap entries) then its count
+    bool capturing = false;        // a sweep is being captured into a graph (timers off)
+    void *loop_d = nullptr;        // device state of the graph sweep loop
 
     bool agg_ready = false;
     AggBuffers ab{};
@@ -248,10 +250,12 @@ struct Timer {
     double bytes = 0;
     int64_t verts = 0, edges = 0;
     Timer(lv_handle *hh, int k) : h(hh), kind(k) {
+        if (h->capturing) return;   // graph bodies hold no event nodes
         a = ev_get(h);
         cudaEventRecord(a, h->stream);
     }
     void stop() {
+        if (!a) return;
         cudaEvent_t b = ev_get(h);
         cudaEventRecord(b, h->stream);
         h->pend.push_back(Pending{kind, a, b, bytes, verts, edges});
@@ -678,9 +682,160 @@ int sweep_and_q(lv_handle *h, int64_t *moves, double *q) {
     return LV_OK;
 }
 
+// ---------------------------------------------------------------------------
+// device-side sweep control: a level's sweep loop as one CUDA graph
+// ---------------------------------------------------------------------------
+// The graph is a while-conditional node whose body is one sweep (totals reset,
+// the seven sub-rounds with corrections and commits, the sum of Sigma_tot^2)
+// followed by sweep_end_kernel, which updates sum_i e_{i->C(i)} by the sweep's
+// exact change, forms Q with the host's FP64 operations (each correctly
+// rounded, so the value is the same bit for bit), and sets the loop condition
+// exactly as the host loop decides: continue while the sweep gained at least
+// min_gain, moved something, the sweep cap is not reached and no device
+// check failed.
+struct LoopState {
+    double q_before;
+    double min_gain;
+    u64 e_own;          // sum_i e_{i->C(i)} of the current state
+    u64 T;
+    u64 moves_total;
+    double q_last;
+    int32_t max_sweeps;
+    int32_t sweeps;
+    int32_t changed;
+    int32_t pad;
+};
+
+// u128 -> double, round to nearest even (as the host's conversion): the top 64
+// significant bits with every lower bit folded into bit 0 round the same way
+// as the full value, then an exact power-of-two scale.
+__device__ double u128_to_double_rn(u64 hi, u64 lo) {
+    if (hi == 0) return __ull2double_rn(lo);
+    const int lz = __clzll((long long)hi);
+    const u64 top = lz ? ((hi << lz) | (lo >> (64 - lz))) : hi;
+    const u64 rest = lz ? (lo << lz) : lo;
+    return ldexp(__ull2double_rn(top | (rest != 0 ? 1ull : 0ull)), 64 - lz);
+}
+
+__global__ void sweep_end_kernel(cudaGraphConditionalHandle cond, const Totals *t, LoopState *ls) {
+    if (threadIdx.x != 0) return;
+    ls->e_own += t->dE;
+    const double td = __ull2double_rn(ls->T);
+    const double a = __ddiv_rn(__ull2double_rn(ls->e_own), td);
+    const double b = __ddiv_rn(u128_to_double_rn(t->s2[0], t->s2[1]), __dmul_rn(td, td));
+    const double q = __dsub_rn(a, b);
+    ls->sweeps += 1;
+    ls->moves_total += t->moves;
+    const double gain = __dsub_rn(q, ls->q_before);
+    if (gain > 0) ls->changed = 1;
+    ls->q_before = q;
+    ls->q_last = q;
+    const bool more = gain >= ls->min_gain && t->moves != 0 &&
+                      !(ls->max_sweeps > 0 && ls->sweeps >= ls->max_sweeps) && t->err == 0;
+    cudaGraphSetConditional(cond, more ? 1u : 0u);
+}
+
+// Returns LV_OK with *done = 1 when the loop ran as a graph; *done = 0 when
+// the graph could not be built (the caller then runs the host loop).
+int sweep_loop_graph(lv_handle *h, float min_gain, double q_start, int *ch, int *done) {
+    *done = 0;
+    if (!h->loop_d) {
+        LoopState *p = nullptr;
+        LV_TRY(dalloc(h, &p, 1));
+        h->loop_d = p;
+    }
+    LoopState *ld = (LoopState *)h->loop_d;
+    LoopState ls{};
+    ls.q_before = q_start;
+    ls.min_gain = (double)min_gain;
+    ls.e_own = h->e_own_cur;
+    ls.T = h->T;
+    ls.q_last = q_start;
+    ls.max_sweeps = h->opts.max_sweeps;
+    LV_CUDA(h, cudaMemcpyAsync(ld, &ls, sizeof(ls), cudaMemcpyHostToDevice, h->stream));
+    LV_TRY(sync(h));
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphConditionalHandle cond = 0;
+    cudaGraphNode_t node = nullptr;
+    bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess &&
+              cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    cudaGraphNodeParams np = {};
+    if (ok) {
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = cond;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        ok = cudaGraphAddNode(&node, graph, nullptr, 0, &np) == cudaSuccess;
+    }
+    const long long launches0 = launches_total();
+    const double bytes0 = h->st.move_bytes;
+    if (ok) {
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        ok = cudaStreamBeginCaptureToGraph(h->stream, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeRelaxed) == cudaSuccess;
+        if (ok) {
+            h->capturing = true;
+            cudaMemsetAsync(h->tot_d, 0, offsetof(Totals, err), h->stream);
+            if (h->cur_w) enqueue_sweep<u64>(h); else enqueue_sweep<float>(h);
+            launch_s2(h->S, h->V, h->tot_d->s2, h->stream);
+            sweep_end_kernel<<<1, 32, 0, h->stream>>>(cond, h->tot_d, ld);
+            note_launches(1);
+            h->capturing = false;
+            cudaGraph_t captured = nullptr;
+            ok = cudaStreamEndCapture(h->stream, &captured) == cudaSuccess;
+        }
+    }
+    if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    const long long per_sweep = launches_total() - launches0;
+    const double bytes_per_sweep = h->st.move_bytes - bytes0;
+    if (!ok) {
+        cudaGetLastError();
+        h->capturing = false;
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        note_launches((int)-per_sweep);   // nothing ran
+        h->st.move_bytes = bytes0;
+        return LV_OK;
+    }
+    {
+        Timer tm(h, 100);
+        LV_CUDA(h, cudaGraphLaunch(exec, h->stream));
+        tm.stop();
+    }
+    LV_CUDA(h, cudaMemcpyAsync(&ls, ld, sizeof(ls), cudaMemcpyDeviceToHost, h->stream));
+    LV_CUDA(h, cudaMemcpyAsync(h->tot_h, h->tot_d, sizeof(Totals), cudaMemcpyDeviceToHost, h->stream));
+    const int rc = sync(h);
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    LV_TRY(rc);
+    LV_TRY(check_device_error(h, h->tot_h->err));
+    // the captured sweep was counted once; it ran ls.sweeps times
+    note_launches((int)(per_sweep * (ls.sweeps - 1)));
+    h->st.move_bytes = bytes0 + bytes_per_sweep * ls.sweeps;
+    h->e_own_cur = ls.e_own;
+    h->st.sweeps += ls.sweeps;
+    h->st.edge_sweeps += h->E * (int64_t)ls.sweeps;
+    h->st.moves += (int64_t)ls.moves_total;
+    *ch = ls.changed;
+    *done = 1;
+    return LV_OK;
+}
+
 int optimise_level(lv_handle *h, float min_gain, int32_t *changed) {
     double q_before = 0, q_after = 0;
     LV_TRY(modularity(h, &q_before));
+    if (h->opts.sweep_graph && !h->opts.profile && !h->opts.verify && !h->opts.trace) {
+        int ch = 0, done = 0;
+        LV_TRY(sweep_loop_graph(h, min_gain, q_before, &ch, &done));
+        if (done) {
+            launch_compose_map(h->orig2comm, h->comm, h->V0, h->stream);
+            h->st.levels += 1;
+            h->st.final_vertices = h->V;
+            if (changed) *changed = ch;
+            return sync(h);
+        }
+    }
     double gain = (double)min_gain;
     int ch = 0, sweeps = 0;
     while (gain >= (double)min_gain) {
@@ -951,6 +1106,7 @@ void lv_default_opts(lv_opts *o) {
     o->struct_size = sizeof(lv_opts);
     o->device = 0;
     o->max_sweeps = 0;
+    o->sweep_graph = 1;
     o->profile = 0;
 }
 
@@ -1018,6 +1174,11 @@ int lv_destroy(lv_handle *h) {
         dfree(h, h->lvl_start[b]); dfree(h, h->lvl_end[b]); dfree(h, h->lvl_col[b]); dfree(h, h->lvl_w[b]);
     }
     dfree(h, h->tot_d);
+    {
+        LoopState *ld = (LoopState *)h->loop_d;
+        dfree(h, ld);
+        h->loop_d = nullptr;
+    }
     if (h->tot_h) cudaFreeHost(h->tot_h);
     if (h->small_h) cudaFreeHost(h->small_h);
     for (const Pending &p : h->pend) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }

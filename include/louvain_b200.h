@@ -49,7 +49,13 @@ typedef struct lv_opts {
                               maintained modularity against a full pass    */
     int32_t trace;         /* 1: per-level and per-sweep lines on stderr
                               (class sizes, moves, modularity, device ms)  */
-    int32_t reserved[10];
+    int32_t sweep_graph;   /* 1 (default): a level's sweep loop runs as one
+                              CUDA graph whose while-node condition is set
+                              on the device after each sweep (no host round
+                              trip per sweep); used when profile, verify and
+                              trace are 0.  0: one host round trip per sweep.
+                              Results are identical.                      */
+    int32_t reserved[9];
 } lv_opts;
 
 /* Per-run counters; times in milliseconds (device time, CUDA events). */

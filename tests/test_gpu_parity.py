@@ -216,6 +216,25 @@ def test_giant_paths_match_oracle(lvb, orc):
     e.close()
 
 
+@pytest.mark.parametrize("name", ["planted10k_uniform", "rmat15", "hubs"])
+def test_sweep_graph_matches_host_loop(lvb, orc, graphs, name):
+    """A level's sweep loop run as one CUDA graph (device-side continuation
+    test) gives the same sweeps, moves, levels, modularity and map as the
+    loop with one host round trip per sweep, and the same as the oracle."""
+    rp, cl, w, gain = graphs[name]
+    out = []
+    for graph_loop in (True, False):
+        e = lvb.Louvain(lvb.Graph(rp, cl, w), sweep_graph=graph_loop)
+        q = e.run(gain)
+        s = e.stats()
+        out.append((q, s["sweeps"], s["moves"], s["levels"], s["edge_sweeps"],
+                    e.original_to_community()[0].tobytes()))
+        e.close()
+    assert out[0] == out[1]
+    q2, st = orc.Oracle(rp, cl, w).run(gain)
+    assert out[0][0] == q2 and out[0][1] == st["sweeps"]
+
+
 def test_handles_reuse_pooled_memory(lvb, orc, graphs):
     """Handles created after others were destroyed (memory reused from the
     library's device pool) and after the pool was trimmed give the same
