@@ -75,7 +75,7 @@ constexpr int NFBQ = 4;
 __host__ __device__ constexpr int FBQ_MAXDEG(int b) { return 512 << b; }                 // 512 .. 4096
 __host__ __device__ constexpr int FBQ_THREADS(int b) { return b == 0 ? 128 : (b == 3 ? 512 : 256); }
 constexpr int FB_THREADS = 1024, FB_CAP = 16384;
-constexpr int FB_KEYS = 6144;
+constexpr int FB_KEYS = 7168;
 constexpr int FB_SMEM = FB_CAP * 14;   // table + occupied list
 constexpr int WARP_SMEM = 8 * WARP_CAP * 12;   // 8 warp tables per CTA
 
