@@ -378,6 +378,162 @@ def run_ours(args, ranks: Ranks):
     return line
 
 
+# ---------------------------------------------------------------------------
+# batched workload: thousands of independent planted-partition graphs
+# ---------------------------------------------------------------------------
+BATCH_SEED = 5
+BATCH_UNIT = "graphs/s"
+
+
+def batch_graph_params(i: int):
+    """Seeded parameters of graph i of the batched workload: V log-uniform in
+    [100, 50000], blocks uniform in [4, 256] (at most V), expected intra-block
+    degree uniform in [8, 24] and inter-block degree in [1, 4]."""
+    import numpy as np
+    r = np.random.default_rng([BATCH_SEED, i])
+    V = int(round(float(np.exp(r.uniform(np.log(100.0), np.log(50000.0))))))
+    blocks = min(int(r.integers(4, 257)), V)
+    return V, blocks, float(r.uniform(8.0, 24.0)), float(r.uniform(1.0, 4.0))
+
+
+def batch_graphs(lvb, indices):
+    out = []
+    for i in indices:
+        V, blocks, d_in, d_out = batch_graph_params(i)
+        out.append(lvb.gen_planted(V, blocks, d_in, d_out, seed=BATCH_SEED * 1000003 + i))
+    return out
+
+
+def batch_shard(lvb, n_graphs: int, ranks: Ranks):
+    """This rank's graph indices: largest expected entry counts first, each to
+    the least-loaded rank (lvb.assign_shards)."""
+    est = [p[0] * (p[2] + p[3]) for p in map(batch_graph_params, range(n_graphs))]
+    return lvb.assign_shards(est, ranks.world)[ranks.rank]
+
+
+def run_batch(args, ranks: Ranks):
+    import numpy as np
+    import torch
+    lvb = load_pkg()
+    dev = ranks.local
+    torch.cuda.set_device(dev)
+    mine = batch_shard(lvb, args.batch_graphs, ranks)
+    t_gen = time.perf_counter()
+    graphs = batch_graphs(lvb, mine)
+    t_gen = time.perf_counter() - t_gen
+    rp, cl, w, gptr = lvb.concat_graphs(graphs)
+    V, E, G = len(rp) - 1, len(cl), len(graphs)
+    h_rp = torch.from_numpy(rp).pin_memory().numpy()
+    h_cl = torch.from_numpy(cl).pin_memory().numpy()
+    h_w = torch.from_numpy(w).pin_memory().numpy()
+    # --- value: resident batch, one lv_batch_run per step ---
+    b = lvb.Batch(rowptr=h_rp, col=h_cl, w=h_w, graph_ptr=gptr, device=dev)
+    for _ in range(args.warmup):
+        b.run(MIN_GAIN)
+    sampler = ClockSampler(gpu_index_for(dev))
+    ranks.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    dev_ms, es_tot, vs_tot = 0.0, 0, 0
+    for _ in range(args.steps):
+        b.run(MIN_GAIN)
+        st = b.stats()
+        dev_ms += st["device_ms"]
+        es_tot += st["edge_sweeps"]
+        vs_tot += st["vertex_sweeps"]
+    torch.cuda.synchronize()
+    ranks.barrier()
+    clocks = sampler.stop()
+    res = b.results()
+    gst = b.graph_stats()
+    ctas = b.stats()["ctas"]
+    b.close()
+    assert (res["status"] == lvb.LV_OK).all()
+    units, secs, value = combine(ranks, float(G * args.steps), dev_ms / 1e3)
+    es_units, _, es_value = combine(ranks, float(es_tot), dev_ms / 1e3)
+    lat = gst["latency_ms"]
+    # roofline of the batch kernel: the sweep bytes 12 E + 20 V per sweep (the
+    # kernel also runs a modularity pass per sweep and the aggregation)
+    peak, peak_kind = measured_peak()
+    sweep_bytes = 12.0 * es_tot + 20.0 * vs_tot
+    achieved = sweep_bytes / (dev_ms * 1e-3) / 1e9 if dev_ms > 0 else 0.0
+    # --- e2e: host buffers through the C ABI, create + run + results + destroy ---
+    out_comm = torch.empty(V, dtype=torch.int32, pin_memory=True).numpy()
+
+    def e2e_step():
+        with lvb.Batch(rowptr=h_rp, col=h_cl, w=h_w, graph_ptr=gptr, device=dev) as bb:
+            bb.run(MIN_GAIN)
+            r = bb.results()
+            out_comm[:] = r["communities"]
+
+    e2e_step()
+    ranks.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    t_e2e = time.perf_counter() - t0
+    ranks.barrier()
+    _, _, e2e_value = combine(ranks, float(G * args.steps), t_e2e)
+    assert np.array_equal(out_comm, res["communities"]), "e2e partition differs from the resident run"
+    # --- sequential launches of the single-graph engine on a sample ---
+    n_seq = min(args.batch_seq_sample, G)
+    pick = sorted(set(int(x) for x in np.linspace(0, G - 1, n_seq))) if G else []
+    parts = [gptr[i:i + 2] for i in range(G)]
+    t0 = time.perf_counter()
+    for i in pick:
+        with lvb.Louvain(graphs[i], device=dev) as e:
+            q = e.run(MIN_GAIN)
+            m, _ = e.original_to_community()
+        assert q == res["modularity"][i] and np.array_equal(m, res["communities"][parts[i][0]:parts[i][1]])
+    t_seq = time.perf_counter() - t0
+    seq_lat = (t_seq / len(pick)) if pick else 0.0
+    # --- CPU baseline: the oracle on the same sample, rank 0 at N=1 ---
+    cpu = None
+    if ranks.world == 1 and ranks.rank == 0 and not args.no_cpu_baseline:
+        orc = load_oracle()
+        nt = host_threads()
+        t0 = time.perf_counter()
+        for i in pick:
+            o = orc.Oracle(graphs[i].rowptr, graphs[i].col, graphs[i].w, nt)
+            o.run(MIN_GAIN)
+            o.close()
+        dt = time.perf_counter() - t0
+        cpu = {"value": len(pick) / dt, "unit": BATCH_UNIT, "cores": nt, "kind": "port",
+               "sample": f"oracle (OpenMP, exact rule) full runs of {len(pick)} graphs spread over "
+                         f"the batch, {dt:.2f} s"}
+    return {
+        "metric": "batched Louvain graphs/s (planted-partition batch)", "value": value,
+        "unit": BATCH_UNIT, "n_gpus": ranks.world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded planted-partition graphs generated on the host)",
+        "config": {"workload": f"batch{args.batch_graphs}_planted", "graphs": args.batch_graphs,
+                   "graphs_this_rank": G, "V_total": V, "E_csr_total": E,
+                   "V": "log-uniform [100, 50000]", "blocks": "uniform [4, 256]",
+                   "d_in": "uniform [8, 24]", "d_out": "uniform [1, 4]", "weights": "unit",
+                   "min_gain": MIN_GAIN, "parallelism": f"shards{ranks.world}",
+                   "l2": "inputs larger than L2 (CSR %.2f GB vs 126 MB L2)" % ((8 * E + 4 * V) / 1e9),
+                   "ctas": ctas, "generation_s": round(t_gen, 1)},
+        "edge_sweeps_per_s": es_value, "edge_sweeps_per_run": es_tot // max(args.steps, 1),
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(lat.max()), "note": "device time from a graph's start to its end "
+                                                        "inside the persistent launch"},
+        "sequential": {"graphs_per_s": (1.0 / seq_lat) if seq_lat else None, "sample": len(pick),
+                       "mean_latency_ms": seq_lat * 1e3,
+                       "note": "lv_create + lv_run + map per graph (host buffers), graphs spread "
+                               "over the batch; results identical to the batch"},
+        "e2e": {"value": e2e_value, "unit": BATCH_UNIT, "h2d_bytes_per_step": 4 * (V + 1) + 8 * E,
+                "d2h_bytes_per_step": 4 * V + 16 * G, "seconds_per_step": t_e2e / args.steps},
+        "gpu_launches": 1,
+        "roofline": {"bound": "hbm", "kernel": "batch_kernel", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "bytes_per_launch": sweep_bytes / max(args.steps, 1), "traffic": None},
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+
+
 def run_reference(args, ranks: Ranks):
     """The reference arm: CPU restatement of the reference's rule, all host
     threads, rank 0 only."""
@@ -411,6 +567,47 @@ def run_reference(args, ranks: Ranks):
     }
 
 
+def run_reference_batch(args, ranks: Ranks):
+    """Reference arm of the batched workload: the CPU restatement of the rule
+    (the oracle, all host threads), rank 0 only, one step = full runs of a
+    bounded sample of graphs spread over the batch."""
+    if ranks.rank != 0:
+        return None
+    import numpy as np
+    lvb = load_pkg()
+    orc = load_oracle()
+    nt = host_threads()
+    n = min(args.batch_seq_sample, args.batch_graphs)
+    pick = sorted(set(int(x) for x in np.linspace(0, args.batch_graphs - 1, n)))
+    graphs = batch_graphs(lvb, pick)
+
+    def step():
+        for g in graphs:
+            o = orc.Oracle(g.rowptr, g.col, g.w, nt)
+            o.run(MIN_GAIN)
+            o.close()
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = len(graphs) * args.steps / dt
+    sample = (f"full runs of {len(graphs)} graphs spread over the batch by the CPU restatement of the "
+              f"reference rule, {nt} threads")
+    return {
+        "metric": "batched Louvain graphs/s (planted-partition batch)", "value": value,
+        "unit": BATCH_UNIT, "n_gpus": ranks.world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded planted-partition graphs)",
+        "config": {"workload": f"batch{args.batch_graphs}_planted", "graphs": args.batch_graphs,
+                   "min_gain": MIN_GAIN, "parallelism": "cpu"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": BATCH_UNIT, "cores": nt, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": BATCH_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -421,13 +618,19 @@ def main():
     ap.add_argument("--cpu-sweeps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--trace", action="store_true", help="per-level / per-sweep lines on stderr")
+    ap.add_argument("--workload", default="rmat", choices=["rmat", "batch"],
+                    help="rmat: one R-MAT graph per GPU (default); batch: thousands of planted-"
+                         "partition graphs per launch, sharded over the GPUs")
+    ap.add_argument("--batch-graphs", type=int, default=4096)
+    ap.add_argument("--batch-seq-sample", type=int, default=64,
+                    help="graphs run one by one through the single-graph engine for comparison")
     args = ap.parse_args()
     if args.impl == "reference":
         ranks = Ranks(backend="gloo")
-        line = run_reference(args, ranks)
+        line = run_reference_batch(args, ranks) if args.workload == "batch" else run_reference(args, ranks)
     else:
         ranks = Ranks()
-        line = run_ours(args, ranks)
+        line = run_batch(args, ranks) if args.workload == "batch" else run_ours(args, ranks)
     if ranks.rank == 0 and line is not None:
         print(json.dumps(line), flush=True)
     ranks.close()

@@ -83,6 +83,9 @@ EXPORTED = [
     "lv_get_class_stats", "lv_clear_stats", "lv_read_mtx", "lv_write_mtx", "lv_free_host",
     "lv_print_communities", "lv_gen_rmat", "lv_gen_planted", "lv_gen_rmat_device",
     "lv_free_device", "lv_modularity_noalloc", "lv_trim_device_memory",
+    "lv_batch_create", "lv_batch_create_device", "lv_batch_run", "lv_batch_get_results",
+    "lv_batch_get_graph_stats", "lv_batch_get_stats", "lv_batch_last_error", "lv_batch_destroy",
+    "lv_gen_lfr",
 ]
 
 _lib = None
@@ -144,10 +147,24 @@ def lib() -> C.CDLL:
                                      C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                      C.POINTER(C.c_void_p)]
     L.lv_free_device.argtypes = [C.c_void_p]
+    L.lv_gen_lfr.argtypes = [C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_double, C.c_int32,
+                             C.c_int32, C.c_double, C.c_uint64, P64, C.POINTER(P32), C.POINTER(P32),
+                             C.POINTER(PF), C.POINTER(P32)]
     L.lv_trim_device_memory.argtypes = [C.c_int32]
     L.lv_modularity_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64,
                                         C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_char_p,
                                         C.c_int32]
+    L.lv_batch_create.argtypes = [P32, P32, PF, C.c_int32, C.c_int64, P32, C.c_int32,
+                                  C.POINTER(_Opts), C.POINTER(C.c_void_p)]
+    L.lv_batch_create_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64,
+                                         P32, C.c_int32, C.POINTER(_Opts), C.POINTER(C.c_void_p)]
+    L.lv_batch_run.argtypes = [C.c_void_p, C.c_float]
+    L.lv_batch_get_results.argtypes = [C.c_void_p, P32, C.POINTER(C.c_double), P32, P32]
+    L.lv_batch_get_graph_stats.argtypes = [C.c_void_p, P32, P64, P64, C.POINTER(C.c_double)]
+    L.lv_batch_get_stats.argtypes = [C.c_void_p, C.POINTER(C.c_double), P64, P64, P32]
+    L.lv_batch_last_error.restype = C.c_char_p
+    L.lv_batch_last_error.argtypes = [C.c_void_p]
+    L.lv_batch_destroy.argtypes = [C.c_void_p]
     _lib = L
     return L
 
@@ -249,6 +266,20 @@ def gen_planted(V: int = 10000, blocks: int = 64, d_in: float = 16.0, d_out: flo
                             C.byref(E), C.byref(rp), C.byref(cl), C.byref(w)))
     return Graph(_take_host(rp, V + 1, np.int32), _take_host(cl, E.value, np.int32),
                  _take_host(w, E.value, np.float32))
+
+
+def gen_lfr(V: int = 1000000, mu: float = 0.3, seed: int = 0, tau1: float = 2.5,
+            mean_degree: float = 20.0, kmax: int = 2000, tau2: float = 1.5, cmin: int = 50,
+            cmax: int = 5000):
+    """LFR-like graph (lv_gen_lfr): returns (Graph, planted community array)."""
+    L = lib()
+    E = C.c_int64()
+    rp, cl, w, cm = P32(), P32(), PF(), P32()
+    _check(L.lv_gen_lfr(V, tau1, mean_degree, kmax, tau2, cmin, cmax, mu, seed, C.byref(E), C.byref(rp),
+                        C.byref(cl), C.byref(w), C.byref(cm)))
+    g = Graph(_take_host(rp, V + 1, np.int32), _take_host(cl, E.value, np.int32),
+              _take_host(w, E.value, np.float32))
+    return g, _take_host(cm, V, np.int32)
 
 
 class DeviceGraph:
@@ -410,3 +441,179 @@ class Louvain:
 
     def clear_stats(self) -> None:
         self._c(lib().lv_clear_stats(self._h))
+
+
+# ---------------------------------------------------------------------------
+# batches of independent graphs (lv_batch_*)
+# ---------------------------------------------------------------------------
+def concat_graphs(graphs):
+    """Block-diagonal CSR of a list of Graphs: (rowptr, col, w, graph_ptr)."""
+    vs = np.array([g.V for g in graphs], dtype=np.int64)
+    es = np.array([g.E for g in graphs], dtype=np.int64)
+    gptr = np.zeros(len(graphs) + 1, dtype=np.int64)
+    np.cumsum(vs, out=gptr[1:])
+    eptr = np.zeros(len(graphs) + 1, dtype=np.int64)
+    np.cumsum(es, out=eptr[1:])
+    if gptr[-1] >= 2**31 - len(graphs) - 1 or eptr[-1] >= 2**31:
+        raise ValueError("batch exceeds int32 vertex ids or entry offsets")
+    rowptr = np.empty(int(gptr[-1]) + 1, dtype=np.int32)
+    col = np.empty(int(eptr[-1]), dtype=np.int32)
+    w = np.empty(int(eptr[-1]), dtype=np.float32)
+    rowptr[0] = 0
+    for i, g in enumerate(graphs):
+        v0, v1, e0, e1 = int(gptr[i]), int(gptr[i + 1]), int(eptr[i]), int(eptr[i + 1])
+        rowptr[v0 + 1:v1 + 1] = g.rowptr[1:] + e0
+        col[e0:e1] = g.col + v0
+        w[e0:e1] = g.w
+    return rowptr, col, w, gptr.astype(np.int32)
+
+
+class Batch:
+    """Many independent graphs, each run through the level loop of lv_run in
+    one persistent launch (lv_batch_run).  Build it from a list of Graphs or
+    from a block-diagonal CSR plus graph_ptr (vertex offsets of the graphs);
+    device_csr=(rowptr, col, w) device pointers borrows a resident CSR."""
+
+    def __init__(self, graphs=None, *, rowptr=None, col=None, w=None, graph_ptr=None,
+                 device: int = 0, max_sweeps: int = 0, device_csr: tuple | None = None,
+                 num_vertices: int | None = None, num_entries: int | None = None):
+        L = lib()
+        opts = _Opts()
+        L.lv_default_opts(C.byref(opts))
+        opts.device = device
+        opts.max_sweeps = max_sweeps
+        if graphs is not None:
+            rowptr, col, w, graph_ptr = concat_graphs(graphs)
+        self.graph_ptr = _i32(graph_ptr)
+        self.G = len(self.graph_ptr) - 1
+        self._b = C.c_void_p()
+        if device_csr is not None:
+            d_rp, d_cl, d_w = device_csr
+            self.V, self.E = int(num_vertices), int(num_entries)
+            rc = L.lv_batch_create_device(C.c_void_p(d_rp), C.c_void_p(d_cl), C.c_void_p(d_w), self.V,
+                                          self.E, _ptr(self.graph_ptr, C.c_int32), self.G,
+                                          C.byref(opts), C.byref(self._b))
+        else:
+            rp, cl = _i32(rowptr), _i32(col)
+            ww = np.ascontiguousarray(w, dtype=np.float32)
+            self.V, self.E = len(rp) - 1, len(cl)
+            rc = L.lv_batch_create(_ptr(rp, C.c_int32), _ptr(cl, C.c_int32), _ptr(ww, C.c_float),
+                                   self.V, self.E, _ptr(self.graph_ptr, C.c_int32), self.G,
+                                   C.byref(opts), C.byref(self._b))
+        if rc != LV_OK:
+            raise LouvainError(rc, status_string(rc))
+
+    def _c(self, code: int) -> None:
+        if code != LV_OK:
+            detail = lib().lv_batch_last_error(self._b)
+            raise LouvainError(code, status_string(code) + (f" ({detail.decode()})" if detail else ""))
+
+    def close(self) -> None:
+        if self._b:
+            lib().lv_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def run(self, min_gain: float, check: bool = True) -> int:
+        """Run every graph; returns the lv_status (raises unless check=False)."""
+        rc = lib().lv_batch_run(self._b, min_gain)
+        if check:
+            self._c(rc)
+        return rc
+
+    def results(self) -> dict:
+        comm = np.empty(self.V, np.int32)
+        q = np.empty(self.G, np.float64)
+        nc = np.empty(self.G, np.int32)
+        st = np.empty(self.G, np.int32)
+        self._c(lib().lv_batch_get_results(self._b, _ptr(comm, C.c_int32), _ptr(q, C.c_double),
+                                           _ptr(nc, C.c_int32), _ptr(st, C.c_int32)))
+        return {"communities": comm, "modularity": q, "num_communities": nc, "status": st}
+
+    def graph_stats(self) -> dict:
+        lv = np.empty(self.G, np.int32)
+        sw = np.empty(self.G, np.int64)
+        es = np.empty(self.G, np.int64)
+        lat = np.empty(self.G, np.float64)
+        self._c(lib().lv_batch_get_graph_stats(self._b, _ptr(lv, C.c_int32), _ptr(sw, C.c_int64),
+                                               _ptr(es, C.c_int64), _ptr(lat, C.c_double)))
+        return {"levels": lv, "sweeps": sw, "edge_sweeps": es, "latency_ms": lat}
+
+    def stats(self) -> dict:
+        ms, es, vs, ctas = C.c_double(), C.c_int64(), C.c_int64(), C.c_int32()
+        self._c(lib().lv_batch_get_stats(self._b, C.byref(ms), C.byref(es), C.byref(vs), C.byref(ctas)))
+        return {"device_ms": ms.value, "edge_sweeps": es.value, "vertex_sweeps": vs.value,
+                "ctas": ctas.value}
+
+    def split(self, communities: np.ndarray) -> list:
+        """Per-graph views of a communities array."""
+        return [communities[self.graph_ptr[g]:self.graph_ptr[g + 1]] for g in range(self.G)]
+
+
+def assign_shards(entries, world: int) -> list:
+    """Graphs of a batch over `world` GPUs: largest first, each to the GPU with
+    the fewest entries so far (ties to the lower rank).  Returns one list of
+    graph indices per rank, each in increasing order."""
+    order = sorted(range(len(entries)), key=lambda g: (-int(entries[g]), g))
+    load = [0] * world
+    out = [[] for _ in range(world)]
+    for g in order:
+        r = min(range(world), key=lambda i: (load[i], i))
+        out[r].append(g)
+        load[r] += int(entries[g])
+    return [sorted(x) for x in out]
+
+
+def _run_local(graphs, min_gain, device, max_sweeps):
+    b = Batch(graphs, device=device, max_sweeps=max_sweeps)
+    try:
+        b.run(min_gain, check=False)
+        r = b.results()
+        gs = b.graph_stats()
+        parts = b.split(r["communities"])
+        return [{"communities": parts[i].copy(), "modularity": float(r["modularity"][i]),
+                 "num_communities": int(r["num_communities"][i]), "status": int(r["status"][i]),
+                 "levels": int(gs["levels"][i]), "sweeps": int(gs["sweeps"][i]),
+                 "edge_sweeps": int(gs["edge_sweeps"][i]), "latency_ms": float(gs["latency_ms"][i])}
+                for i in range(len(graphs))]
+    finally:
+        b.close()
+
+
+def run_batch_sharded(graphs, min_gain: float, *, max_sweeps: int = 0, device: int | None = None,
+                      runner=None) -> list:
+    """Run a batch of graphs over all ranks of the default torch.distributed
+    process group: each rank runs its shard (assign_shards, by entry count) as
+    one lv_batch on its GPU, and every rank gets all graphs' results in input
+    order.  Graphs are independent, so the only exchange is the final gather of
+    results.  runner(graphs, min_gain, device, max_sweeps) -> list of per-graph
+    dicts replaces the local lv_batch run (for tests)."""
+    import torch.distributed as dist
+    world = dist.get_world_size() if dist.is_initialized() else 1
+    rank = dist.get_rank() if dist.is_initialized() else 0
+    if device is None:
+        device = int(os.environ.get("LOCAL_RANK", "0"))
+    mine = assign_shards([g.E for g in graphs], world)[rank]
+    res = (runner or _run_local)([graphs[i] for i in mine], min_gain, device, max_sweeps)
+    local = list(zip(mine, res))
+    if world > 1:
+        gathered = [None] * world
+        dist.all_gather_object(gathered, local)
+    else:
+        gathered = [local]
+    out = [None] * len(graphs)
+    for part in gathered:
+        for i, r in part:
+            out[i] = r
+    return out

@@ -521,6 +521,48 @@ __device__ __forceinline__ void group_reduce_best(const MoveCtx &m, Best &b, int
     b.eo = eo;
 }
 
+// u128 -> double, round to nearest even (as the host's conversion): the top 64
+// significant bits with every lower bit folded into bit 0 round the same way
+// as the full value, then an exact power-of-two scale.
+__device__ __forceinline__ double u128_to_double_rn(u64 hi, u64 lo) {
+    if (hi == 0) return __ull2double_rn(lo);
+    const int lz = __clzll((long long)hi);
+    const u64 top = lz ? ((hi << lz) | (lo >> (64 - lz))) : hi;
+    const u64 rest = lz ? (lo << lz) : lo;
+    return ldexp(__ull2double_rn(top | (rest != 0 ? 1ull : 0ull)), 64 - lz);
+}
+
+// Q = e_own / T - sum(Sigma_tot^2) / T^2 with the host's FP64 operations, each
+// correctly rounded, so the value equals the host's bit for bit
+// (calculateModularity, modularity_optimisation.cu:395-401, in exact parts).
+__device__ __forceinline__ double q_from_parts_dev(u64 T, u64 e_own, u64 s2_hi, u64 s2_lo) {
+    const double td = __ull2double_rn(T);
+    const double a = __ddiv_rn(__ull2double_rn(e_own), td);
+    const double b = __ddiv_rn(u128_to_double_rn(s2_hi, s2_lo), __dmul_rn(td, td));
+    return __dsub_rn(a, b);
+}
+
+// Fixed-point analysis of one float32 weight (the oracle's weight_bits):
+// need = fractional bits of its exact binary value, top = floor(log2 w) + 1024
+// (0 for a zero weight); bad = 1 for a negative, NaN or infinite weight.
+__device__ __forceinline__ void weight_bits_dev(float wf, int &need, int &top, int &bad) {
+    const uint32_t bits = __float_as_uint(wf);
+    const uint32_t ex = (bits >> 23) & 0xFF, man = bits & 0x7FFFFF;
+    need = 0;
+    top = 0;
+    bad = 0;
+    if (ex == 0xFF) { bad = 1; return; }
+    if ((bits & 0x7FFFFFFFu) == 0) return;
+    if (bits >> 31) { bad = 1; return; }
+    uint32_t m;
+    int ee, t;
+    if (ex == 0) { m = man; ee = -149; t = (31 - __clz(man)) - 149; }
+    else { m = man | 0x800000u; ee = (int)ex - 150; t = (int)ex - 127; }
+    ee += __ffs(m) - 1;
+    need = ee < 0 ? -ee : 0;
+    top = t + 1024;
+}
+
 __device__ __forceinline__ u64 warp_sum_u64(u64 x) {
     for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(FULL, x, off);
     return x;

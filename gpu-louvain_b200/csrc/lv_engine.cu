@@ -220,6 +220,29 @@ int dalloc(lv_handle *h, T **p, size_t n) {
     return LV_OK;
 }
 
+}  // namespace
+
+// The pool for other handle types of the library (lv_batch).
+cudaError_t lv::pool_alloc(int dev, void **p, size_t bytes, cudaStream_t s) {
+    *p = nullptr;
+    cudaMemPool_t pool = device_pool(dev);
+    const cudaError_t e = pool ? cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, s)
+                               : cudaMalloc(p, bytes ? bytes : 1);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+    }
+    return e;
+}
+
+void lv::pool_free(int dev, void *p, cudaStream_t s) {
+    if (!p) return;
+    if (device_pool(dev)) cudaFreeAsync(p, s);
+    else cudaFree(p);
+}
+
+namespace {
+
 // Stream-ordered free (after the handle's queued work); the memory returns
 // to the device pool.
 template <typename T>
@@ -706,24 +729,10 @@ struct LoopState {
     int32_t pad;
 };
 
-// u128 -> double, round to nearest even (as the host's conversion): the top 64
-// significant bits with every lower bit folded into bit 0 round the same way
-// as the full value, then an exact power-of-two scale.
-__device__ double u128_to_double_rn(u64 hi, u64 lo) {
-    if (hi == 0) return __ull2double_rn(lo);
-    const int lz = __clzll((long long)hi);
-    const u64 top = lz ? ((hi << lz) | (lo >> (64 - lz))) : hi;
-    const u64 rest = lz ? (lo << lz) : lo;
-    return ldexp(__ull2double_rn(top | (rest != 0 ? 1ull : 0ull)), 64 - lz);
-}
-
 __global__ void sweep_end_kernel(cudaGraphConditionalHandle cond, const Totals *t, LoopState *ls) {
     if (threadIdx.x != 0) return;
     ls->e_own += t->dE;
-    const double td = __ull2double_rn(ls->T);
-    const double a = __ddiv_rn(__ull2double_rn(ls->e_own), td);
-    const double b = __ddiv_rn(u128_to_double_rn(t->s2[0], t->s2[1]), __dmul_rn(td, td));
-    const double q = __dsub_rn(a, b);
+    const double q = q_from_parts_dev(ls->T, ls->e_own, t->s2[0], t->s2[1]);
     ls->sweeps += 1;
     ls->moves_total += t->moves;
     const double gain = __dsub_rn(q, ls->q_before);

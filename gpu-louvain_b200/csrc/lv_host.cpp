@@ -261,6 +261,12 @@ int lv_print_communities(const char *path, const int32_t *orig2comm, int32_t V0,
 // ---------------------------------------------------------------------------
 namespace {
 
+int ceil_log2_host(int64_t x) {
+    int r = 0;
+    while ((int64_t(1) << r) < x) ++r;
+    return r < 1 ? 1 : r;
+}
+
 // Parallel LSD radix sort of 64-bit keys whose significant bits are < nbits.
 void radix_sort_u64(std::vector<uint64_t> &a, int nbits) {
     const size_t n = a.size();
@@ -412,4 +418,135 @@ int lv_gen_planted(int32_t V, int32_t blocks, double d_in, double d_out, uint64_
     return keys_to_csr(keys, 32, V, weight_mode, seed, Eout, rowptr, col, w);
 }
 
+
+// LFR-like benchmark graph (the construction of Lancichinetti, Fortunato and
+// Radicchi, Phys. Rev. E 78, 046110 (2008), simplified): degrees from a
+// power law of exponent tau1 on [kmin, kmax] with kmin chosen for the mean
+// degree, community sizes from a power law of exponent tau2 on [cmin, cmax]
+// (the last community absorbs the remainder), each vertex with
+// round((1 - mu) d) stubs inside its community (at most size - 1) and the
+// rest outside; stubs are paired uniformly at random (intra stubs within
+// their community, inter stubs over the whole graph), self-loops and repeated
+// pairs are dropped, and vertex ids are a random permutation of the
+// community order.  Unit weights.  comm_out (may be NULL) receives each
+// vertex's planted community (malloc'd, V entries).
+int lv_gen_lfr(int32_t V, double tau1, double mean_degree, int32_t kmax, double tau2, int32_t cmin,
+               int32_t cmax, double mu, uint64_t seed, int64_t *Eout, int32_t **rowptr, int32_t **col,
+               float **w, int32_t **comm_out) {
+    if (V < 2 || tau1 <= 1.0 || tau2 <= 1.0 || mean_degree < 1.0 || kmax < 2 || cmin < 2 || cmax < cmin ||
+        mu < 0.0 || mu > 1.0 || !Eout || !rowptr || !col || !w)
+        return LV_ERR_INVALID;
+    if (V >= (1 << 26)) return LV_ERR_TOO_LARGE;
+    // continuous power-law sample on [a, b] with exponent t from u in [0, 1)
+    auto plaw = [](double u, double a, double b, double t) {
+        const double e = 1.0 - t;
+        const double lo = std::pow(a, e), hi = std::pow(b, e);
+        return std::pow(lo + u * (hi - lo), 1.0 / e);
+    };
+    auto unit = [](uint64_t r) { return (double)(r >> 11) * 0x1.0p-53; };
+    // kmin for the requested mean (bisection on the continuous mean)
+    auto mean_of = [&](double a) {
+        const double e1 = 1.0 - tau1, e2 = 2.0 - tau1, b = (double)kmax;
+        return (e1 / e2) * (std::pow(b, e2) - std::pow(a, e2)) / (std::pow(b, e1) - std::pow(a, e1));
+    };
+    double lo = 1.0, hi = (double)kmax;
+    for (int it = 0; it < 100; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (mean_of(mid) < mean_degree) lo = mid;
+        else hi = mid;
+    }
+    const double kmin = 0.5 * (lo + hi);
+    const uint64_t kdeg = lvrng::stream_key(seed, 11), kcom = lvrng::stream_key(seed, 12),
+                   kperm = lvrng::stream_key(seed, 13), kin = lvrng::stream_key(seed, 14),
+                   kout = lvrng::stream_key(seed, 15);
+    // community sizes
+    std::vector<int32_t> csize;
+    int64_t tot = 0;
+    for (uint64_t i = 0; tot < V; ++i) {
+        int32_t c = (int32_t)std::lround(plaw(unit(lvrng::draw(kcom, i)), cmin, cmax, tau2));
+        if (c > V - tot) c = (int32_t)(V - tot);
+        csize.push_back(c);
+        tot += c;
+    }
+    if (csize.size() > 1 && csize.back() < cmin) {
+        csize[csize.size() - 2] += csize.back();
+        csize.pop_back();
+    }
+    const int32_t nc = (int32_t)csize.size();
+    std::vector<int32_t> cstart((size_t)nc + 1, 0);
+    for (int32_t c = 0; c < nc; ++c) cstart[(size_t)c + 1] = cstart[(size_t)c] + csize[(size_t)c];
+    // community-order position -> vertex id: sort by random keys
+    const int vb = ceil_log2_host(V);
+    std::vector<uint64_t> pk((size_t)V);
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < V; ++i) pk[(size_t)i] = ((lvrng::draw(kperm, (uint64_t)i) >> vb) << vb) | (uint64_t)i;
+    radix_sort_u64(pk, 64);
+    std::vector<int32_t> vid((size_t)V);   // position -> vertex id
+    for (int32_t i = 0; i < V; ++i) vid[(size_t)(pk[(size_t)i] & ((1ull << vb) - 1))] = i;
+    // degrees and stubs; position p is in community cpos[p]
+    std::vector<int32_t> cpos((size_t)V);
+    for (int32_t c = 0; c < nc; ++c)
+        for (int32_t p = cstart[(size_t)c]; p < cstart[(size_t)c + 1]; ++p) cpos[(size_t)p] = c;
+    std::vector<int32_t> din((size_t)V), dout((size_t)V);
+#pragma omp parallel for schedule(static)
+    for (int32_t p = 0; p < V; ++p) {
+        int32_t d = (int32_t)std::lround(plaw(unit(lvrng::draw(kdeg, (uint64_t)p)), kmin, (double)kmax, tau1));
+        if (d < 1) d = 1;
+        int32_t a = (int32_t)std::lround((1.0 - mu) * d);
+        const int32_t cap = csize[(size_t)cpos[(size_t)p]] - 1;
+        if (a > cap) a = cap;
+        din[(size_t)p] = a;
+        dout[(size_t)p] = d - a;
+    }
+    const int cb = ceil_log2_host(nc);
+    const int rb = 64 - vb - cb;
+    if (rb < 12) return LV_ERR_TOO_LARGE;
+    std::vector<uint64_t> sin, sout;
+    {
+        int64_t ni = 0, no = 0;
+        for (int32_t p = 0; p < V; ++p) { ni += din[(size_t)p]; no += dout[(size_t)p]; }
+        sin.reserve((size_t)ni);
+        sout.reserve((size_t)no);
+        uint64_t j = 0;
+        for (int32_t p = 0; p < V; ++p) {
+            for (int32_t s = 0; s < din[(size_t)p]; ++s, ++j) {
+                const uint64_t r = lvrng::draw(kin, j) >> (64 - rb);
+                sin.push_back(((uint64_t)cpos[(size_t)p] << (64 - cb)) | (r << vb) | (uint64_t)p);
+            }
+        }
+        j = 0;
+        for (int32_t p = 0; p < V; ++p)
+            for (int32_t s = 0; s < dout[(size_t)p]; ++s, ++j)
+                sout.push_back(((lvrng::draw(kout, j) >> vb) << vb) | (uint64_t)p);
+    }
+    radix_sort_u64(sin, 64);
+    radix_sort_u64(sout, 64);
+    const uint64_t vmask = (1ull << vb) - 1;
+    std::vector<uint64_t> keys;
+    keys.reserve((sin.size() + sout.size()) / 2 + 1);
+    auto add = [&](uint64_t a, uint64_t b) {
+        const int32_t u = vid[(size_t)(a & vmask)], v = vid[(size_t)(b & vmask)];
+        if (u == v) return;
+        const uint32_t x = (uint32_t)(u < v ? u : v), y = (uint32_t)(u < v ? v : u);
+        keys.push_back(((uint64_t)x << 32) | y);
+    };
+    for (size_t i = 0; i + 1 < sin.size();) {
+        if ((sin[i] >> (64 - cb)) != (sin[i + 1] >> (64 - cb))) {   // odd stub count: skip one
+            ++i;
+            continue;
+        }
+        add(sin[i], sin[i + 1]);
+        i += 2;
+    }
+    for (size_t i = 0; i + 1 < sout.size(); i += 2) add(sout[i], sout[i + 1]);
+    radix_sort_u64(keys, 64);
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    if (comm_out) {
+        int32_t *cm = (int32_t *)std::malloc(sizeof(int32_t) * (size_t)V);
+        if (!cm) return LV_ERR_NOMEM;
+        for (int32_t p = 0; p < V; ++p) cm[vid[(size_t)p]] = cpos[(size_t)p];
+        *comm_out = cm;
+    }
+    return keys_to_csr(keys, 32, V, 0, seed, Eout, rowptr, col, w);
+}
 }  // extern "C"

@@ -59,6 +59,11 @@ struct HubGlobal {
     int32_t *ovf_count = nullptr;         // length of ovf_list (reset by the host per use)
 };
 
+// Device memory from the library's per-device stream-ordered pool (freed
+// memory stays mapped for the next handle).
+cudaError_t pool_alloc(int dev, void **p, size_t bytes, cudaStream_t s);
+void pool_free(int dev, void *p, cudaStream_t s);
+
 // Count of engine kernel launches (all handles, all devices of the process).
 void note_launches(int n);
 long long launches_total();

@@ -209,19 +209,11 @@ __global__ void to_fixed_kernel(const WT *w, int64_t E, double scale, int64_t *o
 __global__ void weight_scan_kernel(const float *__restrict__ w, int64_t E, int32_t *out) {
     int need = 0, top = 0, bad = 0;
     for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < E; e += (int64_t)gridDim.x * 256) {
-        const uint32_t bits = __float_as_uint(w[e]);
-        const uint32_t ex = (bits >> 23) & 0xFF, man = bits & 0x7FFFFF;
-        if (ex == 0xFF) { bad = 1; continue; }
-        if ((bits & 0x7FFFFFFFu) == 0) continue;
-        if (bits >> 31) { bad = 1; continue; }
-        uint32_t m;
-        int ee, t;
-        if (ex == 0) { m = man; ee = -149; t = (31 - __clz(man)) - 149; }
-        else { m = man | 0x800000u; ee = (int)ex - 150; t = (int)ex - 127; }
-        ee += __ffs(m) - 1;
-        const int n = ee < 0 ? -ee : 0;
+        int n, t, b;
+        weight_bits_dev(w[e], n, t, b);
         need = max(need, n);
-        top = max(top, t + 1024);
+        top = max(top, t);
+        bad |= b;
     }
     for (int off = 16; off > 0; off >>= 1) {
         need = max(need, __shfl_xor_sync(FULL, need, off));

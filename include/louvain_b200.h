@@ -178,6 +178,15 @@ int lv_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed, double a, dou
  * intra-block and round(V*d_out/2) inter-block uniform draws. */
 int lv_gen_planted(int32_t V, int32_t blocks, double d_in, double d_out, uint64_t seed,
                    int32_t weight_mode, int64_t *E, int32_t **rowptr, int32_t **col, float **w);
+/* LFR-like benchmark graph (Lancichinetti-Fortunato-Radicchi construction,
+ * simplified): power-law degrees (exponent tau1, mean mean_degree, at most
+ * kmax), power-law community sizes (exponent tau2, in [cmin, cmax]), mixing
+ * parameter mu (fraction of each vertex's stubs outside its community),
+ * random stub pairing, unit weights, vertex ids permuted.  comm (may be NULL)
+ * receives the planted community of each vertex (malloc'd). */
+int lv_gen_lfr(int32_t V, double tau1, double mean_degree, int32_t kmax, double tau2, int32_t cmin,
+               int32_t cmax, double mu, uint64_t seed, int64_t *E, int32_t **rowptr, int32_t **col,
+               float **w, int32_t **comm);
 /* R-MAT drawn on the device into device buffers allocated by the library
  * (free with lv_free_device); same graph as lv_gen_rmat. */
 int lv_gen_rmat_device(int32_t scale, int32_t edge_factor, uint64_t seed, double a, double b,
@@ -211,6 +220,50 @@ int lv_modularity_noalloc(const int32_t *d_rowptr, const int32_t *d_col, const f
                           int64_t E, const int32_t *d_comm, void *stream, double *q, char *err,
                           int32_t err_len);
 
+/* ---- batches of independent graphs ----
+ * No counterpart in the reference, whose CLI runs one graph per process.  A
+ * batch is one block-diagonal CSR of num_graphs graphs: graph g owns vertices
+ * graph_ptr[g] .. graph_ptr[g+1]-1 (graph_ptr is a HOST array of num_graphs+1
+ * nondecreasing offsets, graph_ptr[0] = 0, graph_ptr[num_graphs] = V) and its
+ * rows reference only its own vertices.  lv_batch_run runs the level loop of
+ * lv_run on every graph in one persistent launch (one CTA per graph at a time,
+ * largest graphs first); each graph's communities, modularity, level and sweep
+ * counts equal those of lv_create + lv_run on that graph alone.  Each graph
+ * gets its own fixed-point scale, as lv_create would choose it.  Whole-CSR
+ * errors (offsets, column range, weights, a graph of more than
+ * LV_BATCH_MAX_GRAPH_VERTICES vertices) fail lv_batch_create; per-graph
+ * errors (a row that leaves its graph, a total weight beyond the fixed grid,
+ * a failed device check) are reported per graph, and lv_batch_run then
+ * returns LV_ERR_DEVICE with the other graphs' results still valid.  opts:
+ * device and max_sweeps are used. */
+#define LV_BATCH_MAX_GRAPH_VERTICES (1 << 29)   /* per graph of a batch */
+typedef struct lv_batch lv_batch;
+int lv_batch_create(const int32_t *rowptr, const int32_t *col, const float *w, int32_t V, int64_t E,
+                    const int32_t *graph_ptr, int32_t num_graphs, const lv_opts *opts, lv_batch **out);
+/* Same for a CSR resident in device memory (borrowed until lv_batch_destroy);
+ * graph_ptr is still a host array. */
+int lv_batch_create_device(const int32_t *d_rowptr, const int32_t *d_col, const float *d_w, int32_t V,
+                           int64_t E, const int32_t *graph_ptr, int32_t num_graphs, const lv_opts *opts,
+                           lv_batch **out);
+/* Run every graph from singleton communities (each run starts afresh). */
+int lv_batch_run(lv_batch *b, float min_gain);
+/* communities[V]: final community of each vertex, numbered 0 .. n_g - 1 within
+ * its graph (-1 for a failed graph); modularity[G], num_communities[G] (n_g),
+ * status[G] (lv_status per graph).  Any pointer may be NULL. */
+int lv_batch_get_results(lv_batch *b, int32_t *communities, double *modularity, int32_t *num_communities,
+                         int32_t *status);
+/* Per graph: levels, sweeps, edge-sweeps (sum over sweeps of the level's CSR
+ * size) and device latency from the graph's start to its end inside the
+ * launch (ms).  Any pointer may be NULL. */
+int lv_batch_get_graph_stats(lv_batch *b, int32_t *levels, int64_t *sweeps, int64_t *edge_sweeps,
+                             double *latency_ms);
+/* Last run: device time of the launch (ms, CUDA events), total edge-sweeps
+ * and vertex-sweeps (sums over sweeps of the level's entries / vertices), and
+ * the number of CTAs launched.  Any pointer may be NULL. */
+int lv_batch_get_stats(lv_batch *b, double *device_ms, int64_t *edge_sweeps, int64_t *vertex_sweeps,
+                       int32_t *ctas);
+const char *lv_batch_last_error(const lv_batch *b);
+int lv_batch_destroy(lv_batch *b);
 #ifdef __cplusplus
 }
 #endif
