@@ -26,6 +26,18 @@ threads) on the same workload; each step is one level-0 sweep.
 Multi-GPU: the path does not shard (one graph per GPU); --gpus N runs N
 independent replicas under torchrun (weak scaling, no collective on the
 data path; the only collectives are the timing barrier and max/sum).
+
+Other workloads (not the default line):
+  --workload batch : 4096 seeded planted-partition graphs (V log-uniform in
+          [100, 50000], 4-256 blocks, intra degree 8-24, inter 1-4) run by
+          lv_batch_run in one persistent launch; value = graphs/s, with
+          per-graph latency p50/p99, edge-sweeps/s, the single-graph engine
+          run graph by graph on a sample (sequential launches) and the CPU
+          oracle on the same sample.  Under torchrun the graphs are sharded
+          over the ranks by entry count.
+  --workload lfr   : held-out LFR-like graphs (4M vertices, mu 0.2/0.35/0.5):
+          the learned active-set mode against plain sweeps; value = plain
+          time / learned time, with the modularity difference per graph.
 """
 import argparse
 import json
@@ -567,6 +579,88 @@ def run_reference(args, ranks: Ranks):
     }
 
 
+# ---------------------------------------------------------------------------
+# learned active set: held-out LFR-like graphs, learned vs plain sweeps
+# ---------------------------------------------------------------------------
+LFR_EVAL_SEED = 9001
+LFR_EVAL_MU = (0.2, 0.35, 0.5)
+
+
+def run_lfr(args, ranks: Ranks):
+    import numpy as np
+    import torch
+    lvb = load_pkg()
+    dev = ranks.local
+    torch.cuda.set_device(dev)
+    model, thr = lvb.load_active_model(args.active_model)
+    import json as _json
+    with open(args.active_model or os.path.join(ROOT, "gpu-louvain_b200", "active_set_lfr.json")) as f:
+        meta = _json.load(f)
+    K = int(meta.get("full_every", 4))
+    lfr = meta["training"]["lfr"]
+    per_mu = []
+    t_plain = t_learned = 0.0
+    sampler = ClockSampler(gpu_index_for(dev))
+    for mu in LFR_EVAL_MU:
+        g, _ = lvb.gen_lfr(args.lfr_vertices, mu, seed=LFR_EVAL_SEED + ranks.rank, **lfr)
+        res = {}
+        for mode in ("plain", "learned"):
+            kw = {"active_set": True, "active_full_every": K} if mode == "learned" else {}
+            with lvb.Louvain(g, device=dev, **kw) as e:
+                if mode == "learned":
+                    e.set_active_model(model, thr)
+                for _ in range(args.warmup):
+                    e.reset()
+                    e.run(MIN_GAIN)
+                e.clear_stats()
+                ranks.barrier()
+                if mu == LFR_EVAL_MU[0] and mode == "plain":
+                    sampler.start()
+                ts = []
+                for _ in range(args.steps):
+                    e.reset()
+                    t0 = time.perf_counter()
+                    q = e.run(MIN_GAIN)
+                    ts.append(time.perf_counter() - t0)
+                st = e.stats()
+                a = e.active_stats()
+                m, nc = e.original_to_community()
+            res[mode] = {"s": min(ts), "q": q, "communities": int(nc),
+                         "levels": st["levels"] // args.steps, "sweeps": st["sweeps"] // args.steps,
+                         "evaluated_per_run": a["evaluated"] // args.steps if mode == "learned" else None,
+                         "full_sweeps": a["full_sweeps"] // args.steps if mode == "learned" else None,
+                         "recall": a["last_recall"] if mode == "learned" else None,
+                         "fell_back": a["fell_back"] if mode == "learned" else None}
+        t_plain += res["plain"]["s"]
+        t_learned += res["learned"]["s"]
+        per_mu.append({"mu": mu, "V": g.V, "E_csr": g.E, "plain_ms": res["plain"]["s"] * 1e3,
+                       "learned_ms": res["learned"]["s"] * 1e3,
+                       "speedup": res["plain"]["s"] / res["learned"]["s"],
+                       "q_plain": res["plain"]["q"], "q_learned": res["learned"]["q"],
+                       "dq": res["learned"]["q"] - res["plain"]["q"],
+                       "plain": res["plain"], "learned": res["learned"]})
+    clocks = sampler.stop()
+    _, secs, _ = combine(ranks, 1.0, t_learned)
+    speed = t_plain / t_learned
+    return {
+        "metric": "learned active-set vs plain Louvain on held-out LFR-like graphs (speed-up at |dQ|<=1e-3)",
+        "value": speed, "unit": "x (plain time / learned time)", "n_gpus": ranks.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_learned * 1e3 / len(LFR_EVAL_MU),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (bf16 predictor)",
+        "data": "synthetic (seeded LFR-like graphs generated on the host; held-out seeds)",
+        "config": {"workload": f"lfr{args.lfr_vertices}_learned_vs_plain", "vertices": args.lfr_vertices,
+                   "mu": list(LFR_EVAL_MU), "seed": LFR_EVAL_SEED, "lfr": lfr, "min_gain": MIN_GAIN,
+                   "full_every": K, "logit_threshold": thr, "model": os.path.basename(
+                       args.active_model or "active_set_lfr.json"), "parallelism": f"replicas{ranks.world}"},
+        "max_abs_dq": max(abs(r["dq"]) for r in per_mu),
+        "per_graph": per_mu,
+        "e2e": None,
+        "gpu_launches": None,
+        "clocks": clocks,
+        "cpu_baseline": None,
+    }
+
+
 def run_reference_batch(args, ranks: Ranks):
     """Reference arm of the batched workload: the CPU restatement of the rule
     (the oracle, all host threads), rank 0 only, one step = full runs of a
@@ -618,9 +712,12 @@ def main():
     ap.add_argument("--cpu-sweeps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--trace", action="store_true", help="per-level / per-sweep lines on stderr")
-    ap.add_argument("--workload", default="rmat", choices=["rmat", "batch"],
+    ap.add_argument("--workload", default="rmat", choices=["rmat", "batch", "lfr"],
                     help="rmat: one R-MAT graph per GPU (default); batch: thousands of planted-"
-                         "partition graphs per launch, sharded over the GPUs")
+                         "partition graphs per launch, sharded over the GPUs; lfr: learned "
+                         "active-set vs plain sweeps on held-out LFR-like graphs")
+    ap.add_argument("--lfr-vertices", type=int, default=4000000)
+    ap.add_argument("--active-model", default=None, help="predictor JSON (default: the packaged one)")
     ap.add_argument("--batch-graphs", type=int, default=4096)
     ap.add_argument("--batch-seq-sample", type=int, default=64,
                     help="graphs run one by one through the single-graph engine for comparison")
@@ -630,7 +727,8 @@ def main():
         line = run_reference_batch(args, ranks) if args.workload == "batch" else run_reference(args, ranks)
     else:
         ranks = Ranks()
-        line = run_batch(args, ranks) if args.workload == "batch" else run_ours(args, ranks)
+        line = (run_batch(args, ranks) if args.workload == "batch"
+                else run_lfr(args, ranks) if args.workload == "lfr" else run_ours(args, ranks))
     if ranks.rank == 0 and line is not None:
         print(json.dumps(line), flush=True)
     ranks.close()

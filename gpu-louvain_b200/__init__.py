@@ -58,7 +58,8 @@ class LouvainError(RuntimeError):
 class _Opts(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("device", C.c_int32), ("max_sweeps", C.c_int32),
                 ("profile", C.c_int32), ("verify", C.c_int32), ("trace", C.c_int32),
-                ("sweep_graph", C.c_int32), ("reserved", C.c_int32 * 9)]
+                ("sweep_graph", C.c_int32), ("active_set", C.c_int32), ("active_full_every", C.c_int32),
+                ("active_min_recall", C.c_float), ("trace_sample", C.c_float), ("reserved", C.c_int32 * 5)]
 
 
 class _Stats(C.Structure):
@@ -85,7 +86,8 @@ EXPORTED = [
     "lv_free_device", "lv_modularity_noalloc", "lv_trim_device_memory",
     "lv_batch_create", "lv_batch_create_device", "lv_batch_run", "lv_batch_get_results",
     "lv_batch_get_graph_stats", "lv_batch_get_stats", "lv_batch_last_error", "lv_batch_destroy",
-    "lv_gen_lfr",
+    "lv_gen_lfr", "lv_set_active_model", "lv_get_traces", "lv_get_active_stats", "lv_active_train",
+    "lv_active_predict",
 ]
 
 _lib = None
@@ -165,6 +167,14 @@ def lib() -> C.CDLL:
     L.lv_batch_last_error.restype = C.c_char_p
     L.lv_batch_last_error.argtypes = [C.c_void_p]
     L.lv_batch_destroy.argtypes = [C.c_void_p]
+    PU16 = C.POINTER(C.c_uint16)
+    PU8 = C.POINTER(C.c_uint8)
+    L.lv_set_active_model.argtypes = [C.c_void_p, PU16, C.c_int32, C.c_float]
+    L.lv_get_traces.argtypes = [C.c_void_p, PF, PU8, C.c_int64, P64]
+    L.lv_get_active_stats.argtypes = [C.c_void_p, P64, P64, P64, C.POINTER(C.c_double), P32]
+    L.lv_active_train.argtypes = [PF, PU8, C.c_int64, C.c_int32, C.c_int32, C.c_float, C.c_float,
+                                  C.c_uint64, C.c_int32, PU16, PF]
+    L.lv_active_predict.argtypes = [PU16, PF, C.c_int64, C.c_int32, PF]
     _lib = L
     return L
 
@@ -321,7 +331,9 @@ class Louvain:
 
     def __init__(self, graph: Graph | None = None, *, device: int = 0, max_sweeps: int = 0,
                  profile: bool = False, verify: bool = False, trace: bool = False,
-                 device_csr: tuple | None = None, sweep_graph: bool = True):
+                 device_csr: tuple | None = None, sweep_graph: bool = True,
+                 active_set: bool = False, active_full_every: int = 0, active_min_recall: float = 0.0,
+                 trace_sample: float = 0.0):
         L = lib()
         opts = _Opts()
         L.lv_default_opts(C.byref(opts))
@@ -331,6 +343,10 @@ class Louvain:
         opts.verify = 1 if verify else 0
         opts.trace = 1 if trace else 0
         opts.sweep_graph = 1 if sweep_graph else 0
+        opts.active_set = 1 if active_set else 0
+        opts.active_full_every = active_full_every
+        opts.active_min_recall = active_min_recall
+        opts.trace_sample = trace_sample
         h = C.c_void_p()
         if device_csr is not None:
             rp, cl, w, V, E = device_csr
@@ -441,6 +457,68 @@ class Louvain:
 
     def clear_stats(self) -> None:
         self._c(lib().lv_clear_stats(self._h))
+
+    def set_active_model(self, model, logit_threshold: float) -> None:
+        """Predictor for active_set=True: LV_ACTIVE_MODEL_SIZE bf16 bit patterns."""
+        m = np.ascontiguousarray(model, dtype=np.uint16)
+        self._c(lib().lv_set_active_model(self._h, _ptr(m, C.c_uint16), len(m), logit_threshold))
+
+    def traces(self):
+        """(features [n, 4] float32, labels [n] uint8) recorded with trace_sample > 0."""
+        n = C.c_int64()
+        self._c(lib().lv_get_traces(self._h, None, None, 0, C.byref(n)))
+        x = np.empty((n.value, ACTIVE_FEATURES), np.float32)
+        y = np.empty(n.value, np.uint8)
+        self._c(lib().lv_get_traces(self._h, _ptr(x, C.c_float), _ptr(y, C.c_uint8), n.value, C.byref(n)))
+        return x, y
+
+    def active_stats(self) -> dict:
+        ev, fs, as_, fb = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int32()
+        rc = C.c_double()
+        self._c(lib().lv_get_active_stats(self._h, C.byref(ev), C.byref(fs), C.byref(as_), C.byref(rc),
+                                          C.byref(fb)))
+        return {"evaluated": ev.value, "full_sweeps": fs.value, "active_sweeps": as_.value,
+                "last_recall": rc.value, "fell_back": bool(fb.value)}
+
+
+# ---------------------------------------------------------------------------
+# learned active-set predictor (lv_active_*)
+# ---------------------------------------------------------------------------
+ACTIVE_FEATURES = 4
+ACTIVE_HIDDEN = 16
+ACTIVE_MODEL_SIZE = ACTIVE_HIDDEN * ACTIVE_FEATURES + 2 * ACTIVE_HIDDEN + 1
+
+
+def active_train(x, y, *, epochs: int = 4, batch: int = 8192, lr: float = 1e-2, pos_weight: float = 1.0,
+                 seed: int = 0, device: int = 0):
+    """Train the move predictor on traces; returns (bf16 model as uint16, per-epoch loss)."""
+    xx = np.ascontiguousarray(x, dtype=np.float32)
+    yy = np.ascontiguousarray(y, dtype=np.uint8)
+    model = np.empty(ACTIVE_MODEL_SIZE, np.uint16)
+    loss = np.empty(epochs, np.float32)
+    _check(lib().lv_active_train(_ptr(xx, C.c_float), _ptr(yy, C.c_uint8), len(yy), epochs, batch, lr,
+                                 pos_weight, seed, device, _ptr(model, C.c_uint16), _ptr(loss, C.c_float)))
+    return model, loss
+
+
+def active_predict(model, x, device: int = 0) -> np.ndarray:
+    """Logits of the predictor (the engine's inference kernel) for features x [n, 4]."""
+    m = np.ascontiguousarray(model, dtype=np.uint16)
+    xx = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty(len(xx), np.float32)
+    _check(lib().lv_active_predict(_ptr(m, C.c_uint16), _ptr(xx, C.c_float), len(xx), device,
+                                   _ptr(out, C.c_float)))
+    return out
+
+
+def load_active_model(path: str | None = None):
+    """(model uint16[97], logit threshold) from a JSON file written by
+    train_active_set.py (default: the packaged LFR model)."""
+    import json
+    path = path or os.path.join(_HERE, "active_set_lfr.json")
+    with open(path) as f:
+        d = json.load(f)
+    return np.array(d["model_bf16"], dtype=np.uint16), float(d["logit_threshold"])
 
 
 # ---------------------------------------------------------------------------

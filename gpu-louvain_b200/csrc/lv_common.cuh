@@ -147,6 +147,7 @@ struct StateView {
     u64 *S;
     u64 T;
     int *err;
+    float *feat;   // learned active set: 2 features per vertex, written when set
 };
 
 // Exact 64-bit add to a table value.  In shared memory a 64-bit atomicAdd
@@ -482,6 +483,24 @@ __device__ __forceinline__ int32_t move_decision(const MoveCtx &m, const Best &b
         return b.c;
     }
     return m.own;
+}
+
+// Features of the learned active set, recorded at v's evaluation when
+// st.feat is set: the fraction of k_v into the own community and the best
+// move's gain relative to T k_v, (G_best - T e_own) / (T k_v) in [-1, 1]
+// (from the FP64 estimate; the exact rule never reads them).
+__device__ __forceinline__ void record_features(const StateView &st, int32_t v, const MoveCtx &m,
+                                                const Best &b) {
+    if (!st.feat) return;
+    float own = 0.0f, gain = 0.0f;
+    if (m.kv > 0) {
+        const double eo = (double)b.eo;
+        own = (float)(eo / m.kvd);
+        const double g = (b.c == m.own ? 0.0 : b.gd) - m.Td * eo;
+        gain = (float)fmin(1.0, fmax(-1.0, g / (m.Td * m.kvd)));
+    }
+    st.feat[2 * (size_t)v] = own;
+    st.feat[2 * (size_t)v + 1] = gain;
 }
 
 // Butterfly reduction inside aligned groups of `width` lanes; every lane of

@@ -145,6 +145,26 @@ struct lv_handle {
     bool e_own_valid = false;
     std::vector<cudaEvent_t> ev_free;
     std::vector<Pending> pend;
+
+    // learned active set and move traces
+    float *feat = nullptr;          // [2 V0] features recorded by the move kernels
+    uint8_t *moved = nullptr;       // [V0] moved in the previous sweep
+    uint8_t *pred = nullptr;        // [V0] proposed by the predictor
+    int32_t *comm_prev = nullptr;   // [V0] communities before the sweep
+    int32_t *alist = nullptr;       // [V0] proposed vertices, at their class's offset
+    int32_t *acnt = nullptr;        // [NCLS] proposed vertices per class
+    u64 *actr = nullptr;            // [4] movers, proposed movers, trace rows
+    uint16_t *model = nullptr;      // [LV_ACTIVE_MODEL_SIZE] bf16 parameters
+    bool has_model = false;
+    float logit_thr = 0.0f;
+    float *tr_x = nullptr;          // trace rows: features, vertex, label
+    int32_t *tr_v = nullptr;
+    uint8_t *tr_y = nullptr;
+    int64_t tr_cap = 0, tr_rows = 0;
+    uint64_t tr_sweep = 0;
+    int64_t act_evaluated = 0, act_full = 0, act_active = 0;
+    double act_recall = -1.0;
+    int32_t act_fell_back = 0;
 };
 
 namespace {
@@ -340,7 +360,7 @@ GraphView<u64> view_of<u64>(lv_handle *h) {
 }
 
 StateView state_of(lv_handle *h) {
-    return StateView{h->comm, h->newc, h->size, h->k, h->S, h->T, &h->tot_d->err};
+    return StateView{h->comm, h->newc, h->size, h->k, h->S, h->T, &h->tot_d->err, h->feat};
 }
 
 // ---------------------------------------------------------------------------
@@ -831,7 +851,199 @@ int sweep_loop_graph(lv_handle *h, float min_gain, double q_start, int *ch, int 
     return LV_OK;
 }
 
+// ---------------------------------------------------------------------------
+// learned active set (lv_opts.active_set) and move traces (trace_sample)
+// ---------------------------------------------------------------------------
+// Levels with fewer vertices than this run plain sweeps in learned mode: their
+// sweeps are short and the device-side sweep loop (no host round trip per
+// sweep) is cheaper than proposing.
+constexpr int32_t ACTIVE_MIN_VERTICES = 1 << 16;
+
+bool learned_mode(const lv_handle *h) {
+    return h->opts.trace_sample > 0.0f || (h->opts.active_set != 0 && h->V >= ACTIVE_MIN_VERTICES);
+}
+
+int ensure_active(lv_handle *h) {
+    if (h->feat) return LV_OK;
+    const size_t V = (size_t)h->V0 + 1;
+    LV_TRY(dalloc(h, &h->feat, 2 * V));
+    LV_TRY(dalloc(h, &h->moved, V));
+    LV_TRY(dalloc(h, &h->pred, V));
+    LV_TRY(dalloc(h, &h->comm_prev, V));
+    LV_TRY(dalloc(h, &h->alist, V));
+    LV_TRY(dalloc(h, &h->acnt, (size_t)NCLS));
+    LV_TRY(dalloc(h, &h->actr, 4));
+    LV_CUDA(h, cudaMemsetAsync(h->actr, 0, 4 * sizeof(u64), h->stream));
+    if (h->opts.trace_sample > 0.0f) {
+        const double r = h->opts.trace_sample < 1.0f ? h->opts.trace_sample : 1.0;
+        h->tr_cap = (int64_t)std::ceil(r * (double)h->V0 * 48.0) + 1024;
+        LV_TRY(dalloc(h, &h->tr_x, (size_t)h->tr_cap * LV_ACTIVE_FEATURES));
+        LV_TRY(dalloc(h, &h->tr_v, (size_t)h->tr_cap));
+        LV_TRY(dalloc(h, &h->tr_y, (size_t)h->tr_cap));
+    }
+    return LV_OK;
+}
+
+// One sweep over the proposed vertices only (per-class counts cnt, lists at
+// the classes' offsets in alist); giants are always in the list.
+template <typename WT>
+void enqueue_sweep_active(lv_handle *h, const int32_t *cnt) {
+    GraphView<WT> g = view_of<WT>(h);
+    StateView st = state_of(h);
+    u64 *dE = &h->tot_d->dE;
+    Timer tm(h, 100);
+    int64_t verts = 0;
+    for (int b = 0; b < NBUCKETS; ++b) {
+        const int c0 = b, c1 = (b < 6) ? b + 1 : NCLS;
+        int64_t any = 0;
+        for (int c = c0; c < c1; ++c) any += cnt[c];
+        if (!any) continue;
+        if (b < 4) {
+            launch_move_class<WT>(b, g, st, h->alist + h->cls_off[b], cnt[b], h->di, dE, h->stream);
+        } else {
+            for (int c = c0; c < c1; ++c) {
+                if (c == CLS_HG || !cnt[c]) continue;
+                const int32_t maxdeg = c == CLS_B4 ? 84 : (c == CLS_B5 ? 319 : (c == CLS_H1 ? 1024 : HG_MIN_DEG));
+                launch_move_wide<WT>(g, st, h->alist + h->cls_off[c], cnt[c], h->fb, h->di, dE, h->stream, maxdeg);
+            }
+            if (b == 6 && cnt[CLS_HG]) launch_move_giants<WT>(g, st, h->hub_move.view, h->fb, h->di, dE, h->stream);
+        }
+        for (int c = c0; c < c1; ++c)
+            launch_correction<WT>(c, g, st, h->alist + h->cls_off[c], cnt[c], h->di, dE, h->stream);
+        for (int c = c0; c < c1; ++c) launch_commit(st, h->alist + h->cls_off[c], cnt[c], &h->tot_d->moves, h->stream);
+        verts += any;
+    }
+    tm.bytes = 20.0 * (double)verts;
+    tm.stop();
+}
+
+// One sweep of the learned / traced loop: full (every vertex) or over the
+// proposed vertices; predict = run the predictor first (the proposal of an
+// active sweep, or the flags whose recall a full sweep measures).
+int sweep_learned(lv_handle *h, bool full, bool predict, int64_t *moves, double *q, int64_t *movers,
+                  int64_t *hits) {
+    LV_TRY(reset_totals(h));
+    LV_CUDA(h, cudaMemsetAsync(h->actr, 0, 2 * sizeof(u64), h->stream));
+    const int32_t n = h->cls_off[NCLS];
+    ActiveClassOffsets co;
+    for (int c = 0; c <= NCLS; ++c) co.off[c] = h->cls_off[c];
+    const int32_t *rowend = h->cur_rowend ? h->cur_rowend : h->cur_rowptr + 1;
+    int32_t cnt[NCLS];
+    if (predict) {
+        if (!full) LV_CUDA(h, cudaMemsetAsync(h->acnt, 0, NCLS * sizeof(int32_t), h->stream));
+        launch_active_select(h->list, n, co, h->cur_rowptr, rowend, h->feat, h->moved, h->model, h->logit_thr,
+                             CLS_HG, full ? nullptr : h->alist, h->acnt, h->pred, h->stream);
+        if (!full) {
+            LV_CUDA(h, cudaMemcpyAsync(h->small_h, h->acnt, NCLS * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                       h->stream));
+            LV_TRY(sync(h));
+            for (int c = 0; c < NCLS; ++c) cnt[c] = h->small_h[c];
+        }
+    }
+    const bool tracing = h->opts.trace_sample > 0.0f && h->tr_x;
+    if (tracing && h->tr_sweep > 0) {
+        const double r = h->opts.trace_sample < 1.0f ? h->opts.trace_sample : 1.0;
+        const u64 thr = r >= 1.0 ? ~0ull : (u64)(r * 18446744073709551616.0);
+        launch_trace_sample(h->V, h->cur_rowptr, rowend, h->feat, h->moved, thr,
+                            0x7A11ull * (h->tr_sweep + 1) ^ ((u64)h->level << 40), h->tr_x, h->tr_v, h->tr_cap,
+                            h->actr + 2, h->stream);
+    }
+    LV_CUDA(h, cudaMemcpyAsync(h->comm_prev, h->comm, sizeof(int32_t) * (size_t)h->V, cudaMemcpyDeviceToDevice,
+                               h->stream));
+    if (full) {
+        if (h->cur_w) enqueue_sweep<u64>(h); else enqueue_sweep<float>(h);
+        h->act_evaluated += n;
+        h->act_full += 1;
+    } else {
+        if (h->cur_w) enqueue_sweep_active<u64>(h, cnt); else enqueue_sweep_active<float>(h, cnt);
+        for (int c = 0; c < NCLS; ++c) h->act_evaluated += cnt[c];
+        h->act_active += 1;
+    }
+    {
+        Timer tm(h, 101);
+        launch_s2(h->S, h->V, h->tot_d->s2, h->stream);
+        tm.stop();
+    }
+    launch_active_moved(h->comm, h->comm_prev, h->V, h->moved, predict && full ? h->pred : nullptr, h->actr,
+                        h->stream);
+    if (tracing && h->tr_sweep > 0)
+        launch_trace_label(h->tr_v, h->moved, h->tr_rows, h->actr + 2, h->tr_cap, h->tr_y, h->stream);
+    u64 ctr[3];
+    LV_CUDA(h, cudaMemcpyAsync(ctr, h->actr, 3 * sizeof(u64), cudaMemcpyDeviceToHost, h->stream));
+    LV_TRY(read_totals(h));
+    if (tracing) {
+        if (h->tr_sweep > 0) h->tr_rows = (int64_t)ctr[2] < h->tr_cap ? (int64_t)ctr[2] : h->tr_cap;
+        h->tr_sweep += 1;
+    }
+    h->e_own_cur += h->tot_h->dE;
+    Totals t = *h->tot_h;
+    t.e_own = h->e_own_cur;
+    *moves = (int64_t)t.moves;
+    *movers = (int64_t)ctr[0];
+    *hits = (int64_t)ctr[1];
+    *q = q_from_totals(h->T, t);
+    h->st.sweeps += 1;
+    h->st.edge_sweeps += h->E;
+    h->st.moves += *moves;
+    return LV_OK;
+}
+
+// optimiseModularity with the learned proposal: the first sweep of a level
+// and every active_full_every-th sweep evaluate every vertex; the others only
+// the proposed ones.  A full sweep after a proposal measures its recall
+// (proposed movers / movers); below active_min_recall the plain sweep takes
+// over for the rest of the level.  An active sweep that gains less than
+// min_gain (or moves nothing) is followed by a full sweep, and the level ends
+// as the plain loop does, on a full sweep.  Without a model (trace recording
+// only) every sweep is full and the result equals the plain loop's.
+int optimise_level_learned(lv_handle *h, float min_gain, int32_t *changed) {
+    LV_TRY(ensure_active(h));
+    LV_CUDA(h, cudaMemsetAsync(h->feat, 0, sizeof(float) * 2 * (size_t)h->V, h->stream));
+    LV_CUDA(h, cudaMemsetAsync(h->moved, 0, (size_t)h->V, h->stream));
+    h->tr_sweep = 0;
+    double q_before = 0, q_after = 0;
+    LV_TRY(modularity(h, &q_before));
+    const bool learned = h->opts.active_set != 0 && h->has_model;
+    const int K = h->opts.active_full_every > 0 ? h->opts.active_full_every : 4;
+    const double rmin = h->opts.active_min_recall > 0.0f ? (double)h->opts.active_min_recall : 0.9;
+    bool plain_rest = !learned, force_full = true;
+    int since_full = 0, sweeps = 0, ch = 0;
+    for (;;) {
+        if (h->opts.max_sweeps > 0 && sweeps >= h->opts.max_sweeps) break;
+        const bool full = force_full || plain_rest || since_full + 1 >= K;
+        const bool predict = learned && !plain_rest && sweeps > 0;
+        int64_t moves = 0, movers = 0, hits = 0;
+        LV_TRY(sweep_learned(h, full, predict, &moves, &q_after, &movers, &hits));
+        sweeps++;
+        const double gain = q_after - q_before;
+        if (gain > 0) ch = 1;
+        q_before = q_after;
+        const bool stall = !(gain >= (double)min_gain) || moves == 0;
+        if (full) {
+            since_full = 0;
+            force_full = false;
+            if (predict) {
+                h->act_recall = movers > 0 ? (double)hits / (double)movers : 1.0;
+                if (h->act_recall < rmin) {
+                    plain_rest = true;
+                    h->act_fell_back = 1;
+                }
+            }
+            if (stall) break;
+        } else {
+            since_full++;
+            if (stall) force_full = true;
+        }
+    }
+    launch_compose_map(h->orig2comm, h->comm, h->V0, h->stream);
+    h->st.levels += 1;
+    h->st.final_vertices = h->V;
+    if (changed) *changed = ch;
+    return sync(h);
+}
+
 int optimise_level(lv_handle *h, float min_gain, int32_t *changed) {
+    if (learned_mode(h)) return optimise_level_learned(h, min_gain, changed);
     double q_before = 0, q_after = 0;
     LV_TRY(modularity(h, &q_before));
     if (h->opts.sweep_graph && !h->opts.profile && !h->opts.verify && !h->opts.trace) {
@@ -1183,6 +1395,9 @@ int lv_destroy(lv_handle *h) {
         dfree(h, h->lvl_start[b]); dfree(h, h->lvl_end[b]); dfree(h, h->lvl_col[b]); dfree(h, h->lvl_w[b]);
     }
     dfree(h, h->tot_d);
+    dfree(h, h->feat); dfree(h, h->moved); dfree(h, h->pred); dfree(h, h->comm_prev); dfree(h, h->alist);
+    dfree(h, h->acnt); dfree(h, h->actr); dfree(h, h->model); dfree(h, h->tr_x); dfree(h, h->tr_v);
+    dfree(h, h->tr_y);
     {
         LoopState *ld = (LoopState *)h->loop_d;
         dfree(h, ld);
@@ -1404,6 +1619,42 @@ int lv_get_scale(lv_handle *h, int32_t *scale, uint64_t *total_weight, int32_t *
     return LV_OK;
 }
 
+int lv_set_active_model(lv_handle *h, const uint16_t *model, int32_t n_params, float logit_threshold) {
+    if (!h || !model || n_params != LV_ACTIVE_MODEL_SIZE) return LV_ERR_INVALID;
+    cudaSetDevice(h->device);
+    if (!h->model) LV_TRY(dalloc(h, &h->model, (size_t)LV_ACTIVE_MODEL_SIZE));
+    LV_CUDA(h, cudaMemcpyAsync(h->model, model, sizeof(uint16_t) * LV_ACTIVE_MODEL_SIZE, cudaMemcpyHostToDevice,
+                               h->stream));
+    h->logit_thr = logit_threshold;
+    h->has_model = true;
+    return sync(h);
+}
+
+int lv_get_traces(lv_handle *h, float *features, uint8_t *labels, int64_t cap, int64_t *n) {
+    if (!h || cap < 0) return LV_ERR_INVALID;
+    cudaSetDevice(h->device);
+    const int64_t rows = h->tr_rows;
+    if (n) *n = rows;
+    const int64_t m = rows < cap ? rows : cap;
+    if (m > 0 && features)
+        LV_CUDA(h, cudaMemcpyAsync(features, h->tr_x, sizeof(float) * LV_ACTIVE_FEATURES * (size_t)m,
+                                   cudaMemcpyDeviceToHost, h->stream));
+    if (m > 0 && labels)
+        LV_CUDA(h, cudaMemcpyAsync(labels, h->tr_y, (size_t)m, cudaMemcpyDeviceToHost, h->stream));
+    return sync(h);
+}
+
+int lv_get_active_stats(lv_handle *h, int64_t *evaluated, int64_t *full_sweeps, int64_t *active_sweeps,
+                        double *last_recall, int32_t *fell_back) {
+    if (!h) return LV_ERR_INVALID;
+    if (evaluated) *evaluated = h->act_evaluated;
+    if (full_sweeps) *full_sweeps = h->act_full;
+    if (active_sweeps) *active_sweeps = h->act_active;
+    if (last_recall) *last_recall = h->act_recall;
+    if (fell_back) *fell_back = h->act_fell_back;
+    return LV_OK;
+}
+
 int lv_get_stats(lv_handle *h, lv_stats *s) {
     if (!h || !s) return LV_ERR_INVALID;
     LV_TRY(sync(h));
@@ -1425,6 +1676,9 @@ int lv_clear_stats(lv_handle *h) {
     std::memset(&h->st, 0, sizeof(h->st));
     std::memset(&h->cst, 0, sizeof(h->cst));
     h->launch_base = launches_total();
+    h->act_evaluated = h->act_full = h->act_active = 0;
+    h->act_recall = -1.0;
+    h->act_fell_back = 0;
     return LV_OK;
 }
 

@@ -72,7 +72,10 @@ __global__ void __launch_bounds__(256) move_group_kernel(GraphView<WT> g, StateV
     if (active) eval_slots<(CAP / G > 1 ? (LV_U_EVAL < 2 ? LV_U_EVAL : 2) : 1), false, false>(keys, vals, nullptr, CAP, lane, G, m, st.S, st.size, b);
     group_reduce_best(m, b, G);
     u64 delta = 0;
-    if (active && lane == 0) st.newc[v] = move_decision(m, b, &delta);
+    if (active && lane == 0) {
+        st.newc[v] = move_decision(m, b, &delta);
+        record_features(st, v, m, b);
+    }
     block_add_total<256>(delta, dE);
 }
 
@@ -258,6 +261,7 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
         if (lane == 0) {
             u64 delta = 0;
             st.newc[v] = move_decision(m, b, &delta);
+            record_features(st, v, m, b);
             delta_acc += delta;
         }
         __syncwarp();
@@ -373,6 +377,7 @@ __global__ void __launch_bounds__(THREADS) move_fallback_kernel(GraphView<WT> g,
             if (decide) {
                 u64 delta = 0;
                 st.newc[v] = move_decision(m, t, &delta);
+                record_features(st, v, m, t);
                 delta_acc += delta;
                 if (src >= 0) {
                     hg.nocc[src] = 0;
@@ -489,6 +494,7 @@ __global__ void __launch_bounds__(THREADS) giant_merge_kernel(StateView st, HubG
         if (threadIdx.x == 0) {
             u64 delta = 0;
             st.newc[v] = move_decision(m, b, &delta);
+            record_features(st, v, m, b);
             delta_sum += delta;
             nocc = 0;
             hg.nocc[h] = 0;

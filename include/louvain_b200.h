@@ -55,7 +55,21 @@ typedef struct lv_opts {
                               trip per sweep); used when profile, verify and
                               trace are 0.  0: one host round trip per sweep.
                               Results are identical.                      */
-    int32_t reserved[9];
+    int32_t active_set;    /* 1: learned active-set sweeps on levels of at
+                              least 65536 vertices (needs a model,
+                              lv_set_active_model); results then differ from
+                              the plain method (final modularity close to it).
+                              0 (default): plain sweeps                    */
+    int32_t active_full_every; /* learned mode: every this many sweeps a full
+                              sweep measures the predictor's recall
+                              (default 0 = 4)                              */
+    float active_min_recall;   /* learned mode: below this recall the plain
+                              sweep takes over for the rest of the level
+                              (default 0 = 0.9)                            */
+    float trace_sample;    /* > 0: record move traces (features before each
+                              sweep and whether the vertex then moved) for
+                              this fraction of vertices per sweep           */
+    int32_t reserved[5];
 } lv_opts;
 
 /* Per-run counters; times in milliseconds (device time, CUDA events). */
@@ -220,6 +234,41 @@ int lv_modularity_noalloc(const int32_t *d_rowptr, const int32_t *d_col, const f
                           int64_t E, const int32_t *d_comm, void *stream, double *q, char *err,
                           int32_t err_len);
 
+/* ---- learned active-set proposal ----
+ * No counterpart in the reference.  A per-vertex move predictor (MLP with
+ * LV_ACTIVE_FEATURES inputs, LV_ACTIVE_HIDDEN ReLU units and one logit;
+ * bf16 weights, fp32 accumulation) proposes which vertices to evaluate in a
+ * sweep.  Parameters, as bf16 bit patterns, in the order W1[HIDDEN][FEATURES],
+ * b1[HIDDEN], W2[HIDDEN], b2.  Features of a vertex: log2(1 + degree) / 16,
+ * the fraction of its weight into its own community and its best move's gain
+ * relative to T k (both from its last evaluation), and whether it moved in the
+ * previous sweep. */
+#define LV_ACTIVE_FEATURES 4
+#define LV_ACTIVE_HIDDEN 16
+#define LV_ACTIVE_MODEL_SIZE (LV_ACTIVE_HIDDEN * LV_ACTIVE_FEATURES + 2 * LV_ACTIVE_HIDDEN + 1)
+/* Model for lv_opts.active_set = 1; a vertex is proposed when its logit
+ * exceeds logit_threshold. */
+int lv_set_active_model(lv_handle *h, const uint16_t *model, int32_t n_params, float logit_threshold);
+/* Move traces recorded with lv_opts.trace_sample > 0: features[n][FEATURES]
+ * and labels[n] (1 = moved in the sweep after sampling); up to cap rows are
+ * copied, *n receives the number of complete rows available. */
+int lv_get_traces(lv_handle *h, float *features, uint8_t *labels, int64_t cap, int64_t *n);
+/* Learned-mode counters since the handle's creation or lv_clear_stats: vertices evaluated,
+ * full and active sweeps, the last measured recall, and whether the plain
+ * sweep took over in some level. */
+int lv_get_active_stats(lv_handle *h, int64_t *evaluated, int64_t *full_sweeps, int64_t *active_sweeps,
+                        double *last_recall, int32_t *fell_back);
+/* Train the predictor on traces (features[n][FEATURES], labels[n]) with
+ * mini-batch Adam on the weighted binary cross-entropy (positives weighted
+ * by pos_weight) on `device`; hand-written CUDA kernels, reproducible for a
+ * seed.  model_out receives LV_ACTIVE_MODEL_SIZE bf16 parameters,
+ * epoch_loss (may be NULL) the mean loss of each epoch. */
+int lv_active_train(const float *features, const uint8_t *labels, int64_t n, int32_t epochs, int32_t batch,
+                    float lr, float pos_weight, uint64_t seed, int32_t device, uint16_t *model_out,
+                    float *epoch_loss);
+/* Logits of the predictor for features[n][FEATURES] (the engine's inference
+ * arithmetic). */
+int lv_active_predict(const uint16_t *model, const float *features, int64_t n, int32_t device, float *logits);
 /* ---- batches of independent graphs ----
  * No counterpart in the reference, whose CLI runs one graph per process.  A
  * batch is one block-diagonal CSR of num_graphs graphs: graph g owns vertices

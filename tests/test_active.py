@@ -1,0 +1,134 @@
+"""Learned active-set proposal: trace recorder, predictor kernels, learned sweeps.
+
+The learned mode is an approximation of the plain method by design (only the
+proposed vertices are evaluated), so its parity bar is the one the method
+states: final modularity within 1e-3 of the plain run on the same graph, with
+every move still decided by the exact rule.  Everything else is exact:
+recording traces does not change the plain run, a predictor that proposes
+nothing falls back to the plain sweep and reproduces the plain result bit for
+bit, and the inference kernel equals an fp32 reference of the MLP to within
+1e-5 (fp32 rounding of the 16 hidden sums)."""
+import numpy as np
+import pytest
+
+
+def bf16_to_f32(bits):
+    return (np.asarray(bits, np.uint32) << 16).view(np.float32)
+
+
+def f32_to_bf16(x):
+    u = np.asarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    u = u + 0x7FFF + ((u >> 16) & 1)
+    return (u >> 16).astype(np.uint16)
+
+
+def mlp_reference(model_bits, x):
+    """fp32 forward pass of the predictor: relu(W1 x + b1), then W2 . h + b2."""
+    w = bf16_to_f32(model_bits).astype(np.float64)
+    H, F = 16, 4
+    W1 = w[:H * F].reshape(H, F)
+    b1 = w[H * F:H * F + H]
+    W2 = w[H * F + H:H * F + 2 * H]
+    b2 = w[-1]
+    h = np.maximum(x.astype(np.float64) @ W1.T + b1, 0.0)
+    return h @ W2 + b2
+
+
+def test_model_layout(lvb):
+    assert lvb.ACTIVE_MODEL_SIZE == 97
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(1000).astype(np.float32)
+    b = f32_to_bf16(x)
+    assert np.allclose(bf16_to_f32(b), x, rtol=2 ** -8)
+
+
+@pytest.mark.gpu
+def test_predict_matches_fp32_reference(lvb):
+    rng = np.random.default_rng(1)
+    model = f32_to_bf16(rng.standard_normal(lvb.ACTIVE_MODEL_SIZE).astype(np.float32))
+    x = rng.uniform(-1, 1, (50000, 4)).astype(np.float32)
+    got = lvb.active_predict(model, x)
+    ref = mlp_reference(model, x)
+    assert np.allclose(got, ref, rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.gpu
+def test_train_reduces_loss_and_is_reproducible(lvb):
+    rng = np.random.default_rng(2)
+    x = rng.uniform(0, 1, (200000, 4)).astype(np.float32)
+    y = ((x[:, 1] < 0.5) & (x[:, 3] > 0.3)).astype(np.uint8)
+    m1, l1 = lvb.active_train(x, y, epochs=5, batch=4096, seed=3)
+    m2, l2 = lvb.active_train(x, y, epochs=5, batch=4096, seed=3)
+    assert np.array_equal(m1, m2) and np.array_equal(l1, l2)
+    assert l1[-1] < 0.6 * l1[0]
+    acc = ((lvb.active_predict(m1, x) > 0) == (y == 1)).mean()
+    assert acc > 0.9
+
+
+@pytest.mark.gpu
+def test_trace_recording_leaves_plain_run_unchanged(lvb):
+    g, _ = lvb.gen_lfr(100000, 0.3, seed=5)
+    with lvb.Louvain(g) as e:
+        q0 = e.run(1e-6)
+        m0 = e.original_to_community()[0]
+    with lvb.Louvain(g, trace_sample=0.2) as e:
+        q1 = e.run(1e-6)
+        m1 = e.original_to_community()[0]
+        x, y = e.traces()
+    assert q0 == q1 and np.array_equal(m0, m1)
+    assert len(y) > 10000 and set(np.unique(y)) <= {0, 1} and 0 < y.mean() < 1
+    assert np.isfinite(x).all()
+    assert (x[:, 1] >= 0).all() and (x[:, 1] <= 1.0 + 1e-6).all()
+    assert (np.abs(x[:, 2]) <= 1.0).all() and set(np.unique(x[:, 3])) <= {0.0, 1.0}
+
+
+@pytest.mark.gpu
+def test_null_predictor_falls_back_to_plain(lvb):
+    g, _ = lvb.gen_lfr(100000, 0.3, seed=6)
+    with lvb.Louvain(g) as e:
+        q0 = e.run(1e-6)
+        m0 = e.original_to_community()[0]
+    model = np.zeros(lvb.ACTIVE_MODEL_SIZE, np.uint16)
+    model[-1] = f32_to_bf16(np.float32(-30.0))     # b2: every logit -30
+    with lvb.Louvain(g, active_set=True) as e:
+        e.set_active_model(model, 0.0)
+        q1 = e.run(1e-6)
+        m1 = e.original_to_community()[0]
+        st = e.active_stats()
+    assert st["fell_back"] and st["last_recall"] == 0.0
+    assert q1 == q0 and np.array_equal(m0, m1)
+
+
+@pytest.mark.gpu
+def test_learned_mode_within_tolerance(lvb):
+    # train on traces of two graphs, evaluate on a third seed
+    xs, ys = [], []
+    for s in (11, 12):
+        g, _ = lvb.gen_lfr(200000, 0.25 + 0.1 * (s - 11), seed=s)
+        with lvb.Louvain(g, trace_sample=0.2) as e:
+            e.run(1e-6)
+            x, y = e.traces()
+        xs.append(x)
+        ys.append(y)
+    x, y = np.concatenate(xs), np.concatenate(ys)
+    model, loss = lvb.active_train(x, y, epochs=4, seed=1)
+    z = lvb.active_predict(model, x)
+    pos = np.sort(z[y == 1])
+    thr = float(pos[int(0.03 * len(pos))]) - 1e-6
+    g, _ = lvb.gen_lfr(300000, 0.3, seed=13)
+    with lvb.Louvain(g) as e:
+        q0 = e.run(1e-6)
+        ev_plain = e.stats()["edge_sweeps"]
+    runs = []
+    for _ in range(2):
+        with lvb.Louvain(g, active_set=True) as e:
+            e.set_active_model(model, thr)
+            q = e.run(1e-6)
+            runs.append((q, e.original_to_community()[0], e.active_stats(), e.stats()))
+    (q1, m1, st1, s1), (q2, m2, _, _) = runs
+    assert q1 == q2 and np.array_equal(m1, m2)          # deterministic
+    assert abs(q1 - q0) <= 1e-3
+    assert st1["active_sweeps"] > 0
+    # fewer vertex evaluations than sweeps x vertices
+    assert st1["evaluated"] < s1["sweeps"] * g.V
+    assert ev_plain > 0
