@@ -59,7 +59,8 @@ class _Opts(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("device", C.c_int32), ("max_sweeps", C.c_int32),
                 ("profile", C.c_int32), ("verify", C.c_int32), ("trace", C.c_int32),
                 ("sweep_graph", C.c_int32), ("active_set", C.c_int32), ("active_full_every", C.c_int32),
-                ("active_min_recall", C.c_float), ("trace_sample", C.c_float), ("reserved", C.c_int32 * 5)]
+                ("active_min_recall", C.c_float), ("trace_sample", C.c_float), ("active_start", C.c_float),
+                ("reserved", C.c_int32 * 4)]
 
 
 class _Stats(C.Structure):
@@ -333,7 +334,7 @@ class Louvain:
                  profile: bool = False, verify: bool = False, trace: bool = False,
                  device_csr: tuple | None = None, sweep_graph: bool = True,
                  active_set: bool = False, active_full_every: int = 0, active_min_recall: float = 0.0,
-                 trace_sample: float = 0.0):
+                 trace_sample: float = 0.0, active_start: float = 0.0):
         L = lib()
         opts = _Opts()
         L.lv_default_opts(C.byref(opts))
@@ -347,6 +348,7 @@ class Louvain:
         opts.active_full_every = active_full_every
         opts.active_min_recall = active_min_recall
         opts.trace_sample = trace_sample
+        opts.active_start = active_start
         h = C.c_void_p()
         if device_csr is not None:
             rp, cl, w, V, E = device_csr

@@ -988,8 +988,10 @@ int sweep_learned(lv_handle *h, bool full, bool predict, int64_t *moves, double 
     return LV_OK;
 }
 
-// optimiseModularity with the learned proposal: the first sweep of a level
-// and every active_full_every-th sweep evaluate every vertex; the others only
+// optimiseModularity with the learned proposal: sweeps are full until one
+// moves fewer than active_start of the level's vertices (the early sweeps,
+// where most vertices move, stay exactly the plain method's); after that
+// every active_full_every-th sweep evaluates every vertex and the others only
 // the proposed ones.  A full sweep after a proposal measures its recall
 // (proposed movers / movers); below active_min_recall the plain sweep takes
 // over for the rest of the level.  An active sweep that gains less than
@@ -1006,12 +1008,13 @@ int optimise_level_learned(lv_handle *h, float min_gain, int32_t *changed) {
     const bool learned = h->opts.active_set != 0 && h->has_model;
     const int K = h->opts.active_full_every > 0 ? h->opts.active_full_every : 4;
     const double rmin = h->opts.active_min_recall > 0.0f ? (double)h->opts.active_min_recall : 0.9;
-    bool plain_rest = !learned, force_full = true;
+    const double start = h->opts.active_start > 0.0f ? (double)h->opts.active_start : 0.05;
+    bool plain_rest = !learned, force_full = true, proposing = false;
     int since_full = 0, sweeps = 0, ch = 0;
     for (;;) {
         if (h->opts.max_sweeps > 0 && sweeps >= h->opts.max_sweeps) break;
-        const bool full = force_full || plain_rest || since_full + 1 >= K;
-        const bool predict = learned && !plain_rest && sweeps > 0;
+        const bool full = force_full || plain_rest || !proposing || since_full + 1 >= K;
+        const bool predict = learned && !plain_rest && proposing;
         int64_t moves = 0, movers = 0, hits = 0;
         LV_TRY(sweep_learned(h, full, predict, &moves, &q_after, &movers, &hits));
         sweeps++;
@@ -1022,6 +1025,7 @@ int optimise_level_learned(lv_handle *h, float min_gain, int32_t *changed) {
         if (full) {
             since_full = 0;
             force_full = false;
+            if ((double)movers < start * (double)h->V) proposing = true;
             if (predict) {
                 h->act_recall = movers > 0 ? (double)hits / (double)movers : 1.0;
                 if (h->act_recall < rmin) {

@@ -69,7 +69,10 @@ typedef struct lv_opts {
     float trace_sample;    /* > 0: record move traces (features before each
                               sweep and whether the vertex then moved) for
                               this fraction of vertices per sweep           */
-    int32_t reserved[5];
+    float active_start;    /* learned mode: proposals start after a full
+                              sweep moved less than this fraction of the
+                              level's vertices (default 0 = 0.05)          */
+    int32_t reserved[4];
 } lv_opts;
 
 /* Per-run counters; times in milliseconds (device time, CUDA events). */

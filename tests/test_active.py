@@ -114,7 +114,7 @@ def test_learned_mode_within_tolerance(lvb):
     model, loss = lvb.active_train(x, y, epochs=4, seed=1)
     z = lvb.active_predict(model, x)
     pos = np.sort(z[y == 1])
-    thr = float(pos[int(0.03 * len(pos))]) - 1e-6
+    thr = float(pos[int(0.01 * len(pos))]) - 1e-6
     g, _ = lvb.gen_lfr(300000, 0.3, seed=13)
     with lvb.Louvain(g) as e:
         q0 = e.run(1e-6)
