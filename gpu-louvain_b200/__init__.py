@@ -461,12 +461,12 @@ class Louvain:
         self._c(lib().lv_clear_stats(self._h))
 
     def set_active_model(self, model, logit_threshold: float) -> None:
-        """Predictor for active_set=True: LV_ACTIVE_MODEL_SIZE bf16 bit patterns."""
+        """Predictor for active_set=True: ACTIVE_MODEL_SIZE bf16 bit patterns."""
         m = np.ascontiguousarray(model, dtype=np.uint16)
         self._c(lib().lv_set_active_model(self._h, _ptr(m, C.c_uint16), len(m), logit_threshold))
 
     def traces(self):
-        """(features [n, 4] float32, labels [n] uint8) recorded with trace_sample > 0."""
+        """(features [n, ACTIVE_FEATURES] float32, labels [n] uint8) recorded with trace_sample > 0."""
         n = C.c_int64()
         self._c(lib().lv_get_traces(self._h, None, None, 0, C.byref(n)))
         x = np.empty((n.value, ACTIVE_FEATURES), np.float32)
@@ -486,7 +486,7 @@ class Louvain:
 # ---------------------------------------------------------------------------
 # learned active-set predictor (lv_active_*)
 # ---------------------------------------------------------------------------
-ACTIVE_FEATURES = 4
+ACTIVE_FEATURES = 5
 ACTIVE_HIDDEN = 16
 ACTIVE_MODEL_SIZE = ACTIVE_HIDDEN * ACTIVE_FEATURES + 2 * ACTIVE_HIDDEN + 1
 
@@ -504,7 +504,7 @@ def active_train(x, y, *, epochs: int = 4, batch: int = 8192, lr: float = 1e-2, 
 
 
 def active_predict(model, x, device: int = 0) -> np.ndarray:
-    """Logits of the predictor (the engine's inference kernel) for features x [n, 4]."""
+    """Logits of the predictor (the engine's inference kernel) for features x [n, ACTIVE_FEATURES]."""
     m = np.ascontiguousarray(model, dtype=np.uint16)
     xx = np.ascontiguousarray(x, dtype=np.float32)
     out = np.empty(len(xx), np.float32)
@@ -514,7 +514,7 @@ def active_predict(model, x, device: int = 0) -> np.ndarray:
 
 
 def load_active_model(path: str | None = None):
-    """(model uint16[97], logit threshold) from a JSON file written by
+    """(model uint16[ACTIVE_MODEL_SIZE], logit threshold) from a JSON file written by
     train_active_set.py (default: the packaged LFR model)."""
     import json
     path = path or os.path.join(_HERE, "active_set_lfr.json")

@@ -1,5 +1,5 @@
 // lv_active.cu -- learned active-set proposal: the per-vertex move predictor
-// (a 4-16-1 MLP, bf16 weights, fp32 accumulation), its inference and
+// (a 5-16-1 MLP, bf16 weights, fp32 accumulation), its inference and
 // compaction kernels, the move-trace recorder and the training kernels.
 //
 // The plain method evaluates every vertex in every sweep.  After the first
@@ -14,8 +14,9 @@
 //   x1 = weight from v into its own community / k_v   (last evaluation)
 //   x2 = (G_best - T e_own) / (T k_v), clamped to [-1, 1] (last evaluation)
 //   x3 = 1 if v moved in the previous sweep
+//   x4 = fraction of v's row entries whose vertex moved in the previous sweep
 // Model: h = relu(W1 x + b1) (16 units), logit = W2 . h + b2; parameters in
-// the order W1[16][4], b1[16], W2[16], b2 (LV_ACTIVE_MODEL_SIZE = 97).
+// the order W1[16][5], b1[16], W2[16], b2 (LV_ACTIVE_MODEL_SIZE = 113).
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -55,11 +56,12 @@ __device__ __forceinline__ float mlp_logit(const float *w, const float *x) {
 }
 
 __device__ __forceinline__ void vertex_features(int32_t deg, const float *feat, const uint8_t *moved,
-                                                int32_t v, float *x) {
+                                                const int32_t *nmoved, int32_t v, float *x) {
     x[0] = log2f(1.0f + (float)deg) * 0.0625f;
     x[1] = feat[2 * (size_t)v];
     x[2] = feat[2 * (size_t)v + 1];
     x[3] = moved[v] ? 1.0f : 0.0f;
+    x[4] = fminf(1.0f, (float)nmoved[v] / (float)(deg > 0 ? deg : 1));
 }
 
 __device__ __forceinline__ int class_at(const ActiveClassOffsets &co, int32_t p) {
@@ -78,6 +80,7 @@ __global__ void __launch_bounds__(256) active_select_kernel(const int32_t *__res
                                                             const int32_t *__restrict__ rowend,
                                                             const float *__restrict__ feat,
                                                             const uint8_t *__restrict__ moved,
+                                                            const int32_t *__restrict__ nmoved,
                                                             const uint16_t *__restrict__ model, float logit_thr,
                                                             int keep_cls, int32_t *alist, int32_t *acnt,
                                                             uint8_t *pred) {
@@ -97,7 +100,7 @@ __global__ void __launch_bounds__(256) active_select_kernel(const int32_t *__res
             act = true;
         } else {
             float x[NF];
-            vertex_features(rowend[v] - rowptr[v], feat, moved, v, x);
+            vertex_features(rowend[v] - rowptr[v], feat, moved, nmoved, v, x);
             act = mlp_logit(w, x) > logit_thr;
         }
         if (pred) pred[v] = act ? 1 : 0;
@@ -137,7 +140,8 @@ __global__ void __launch_bounds__(256) active_moved_kernel(const int32_t *__rest
 __global__ void __launch_bounds__(256) trace_sample_kernel(int32_t V, const int32_t *__restrict__ rowptr,
                                                            const int32_t *__restrict__ rowend,
                                                            const float *__restrict__ feat,
-                                                           const uint8_t *__restrict__ moved, u64 thr, u64 key,
+                                                           const uint8_t *__restrict__ moved,
+                                                           const int32_t *__restrict__ nmoved, u64 thr, u64 key,
                                                            float *tx, int32_t *tv, int64_t cap, u64 *tcount) {
     for (int32_t v = blockIdx.x * 256 + threadIdx.x; v < V; v += gridDim.x * 256) {
         u64 z = key + (u64)v * 0x9E3779B97F4A7C15ull;
@@ -148,7 +152,7 @@ __global__ void __launch_bounds__(256) trace_sample_kernel(int32_t V, const int3
         const u64 idx = atomicAdd(tcount, 1ull);
         if ((int64_t)idx >= cap) continue;
         float x[NF];
-        vertex_features(rowend[v] - rowptr[v], feat, moved, v, x);
+        vertex_features(rowend[v] - rowptr[v], feat, moved, nmoved, v, x);
         for (int f = 0; f < NF; ++f) tx[idx * NF + f] = x[f];
         tv[idx] = v;
     }
@@ -163,6 +167,31 @@ __global__ void trace_label_kernel(const int32_t *__restrict__ tv, const uint8_t
         ty[i] = moved[tv[i]];
 }
 
+// nmoved[x] += 1 for every row entry (v, x), x != v, of every vertex v that
+// moved in the sweep: a warp takes 32 vertices and walks the movers' rows
+// with its lanes.
+__global__ void __launch_bounds__(256) nbr_moved_kernel(const int32_t *__restrict__ rowptr,
+                                                        const int32_t *__restrict__ rowend,
+                                                        const int32_t *__restrict__ col, int32_t V,
+                                                        const uint8_t *__restrict__ moved, int32_t *nmoved) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * 8;
+    for (int64_t base = ((int64_t)blockIdx.x * 8 + (threadIdx.x >> 5)) * 32; base < V; base += warps * 32) {
+        const int64_t v = base + lane;
+        unsigned bal = __ballot_sync(FULL, v < V && moved[v]);
+        while (bal) {
+            const int src = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const int32_t u = (int32_t)(base + src);
+            const int32_t r1 = rowend[u];
+            for (int32_t e = rowptr[u] + lane; e < r1; e += 32) {
+                const int32_t x = col[e];
+                if (x != u) atomicAdd(nmoved + x, 1);
+            }
+        }
+    }
+}
+
 inline unsigned grid_of(int64_t n, int64_t cap = 148 * 16) {
     int64_t b = (n + 255) / 256;
     if (b < 1) b = 1;
@@ -172,12 +201,12 @@ inline unsigned grid_of(int64_t n, int64_t cap = 148 * 16) {
 }  // namespace
 
 void launch_active_select(const int32_t *list, int32_t n, const ActiveClassOffsets &co, const int32_t *rowptr,
-                          const int32_t *rowend, const float *feat, const uint8_t *moved, const uint16_t *model,
-                          float logit_thr, int keep_cls, int32_t *alist, int32_t *acnt, uint8_t *pred,
-                          cudaStream_t s) {
+                          const int32_t *rowend, const float *feat, const uint8_t *moved, const int32_t *nmoved,
+                          const uint16_t *model, float logit_thr, int keep_cls, int32_t *alist, int32_t *acnt,
+                          uint8_t *pred, cudaStream_t s) {
     if (n <= 0) return;
-    active_select_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(list, n, co, rowptr, rowend, feat, moved, model,
-                                                                    logit_thr, keep_cls, alist, acnt, pred);
+    active_select_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(list, n, co, rowptr, rowend, feat, moved, nmoved,
+                                                                    model, logit_thr, keep_cls, alist, acnt, pred);
     note_launches(1);
 }
 
@@ -189,10 +218,19 @@ void launch_active_moved(const int32_t *comm, const int32_t *prev, int32_t V, ui
 }
 
 void launch_trace_sample(int32_t V, const int32_t *rowptr, const int32_t *rowend, const float *feat,
-                         const uint8_t *moved, u64 thr, u64 key, float *tx, int32_t *tv, int64_t cap,
-                         u64 *tcount, cudaStream_t s) {
+                         const uint8_t *moved, const int32_t *nmoved, u64 thr, u64 key, float *tx, int32_t *tv,
+                         int64_t cap, u64 *tcount, cudaStream_t s) {
     if (V <= 0) return;
-    trace_sample_kernel<<<grid_of(V), 256, 0, s>>>(V, rowptr, rowend, feat, moved, thr, key, tx, tv, cap, tcount);
+    trace_sample_kernel<<<grid_of(V), 256, 0, s>>>(V, rowptr, rowend, feat, moved, nmoved, thr, key, tx, tv, cap,
+                                                   tcount);
+    note_launches(1);
+}
+
+void launch_nbr_moved(const int32_t *rowptr, const int32_t *rowend, const int32_t *col, int32_t V,
+                      const uint8_t *moved, int32_t *nmoved, cudaStream_t s) {
+    if (V <= 0) return;
+    cudaMemsetAsync(nmoved, 0, sizeof(int32_t) * (size_t)V, s);
+    nbr_moved_kernel<<<grid_of(((int64_t)V + 7) / 8), 256, 0, s>>>(rowptr, rowend, col, V, moved, nmoved);
     note_launches(1);
 }
 

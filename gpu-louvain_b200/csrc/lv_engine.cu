@@ -149,6 +149,7 @@ struct lv_handle {
     // learned active set and move traces
     float *feat = nullptr;          // [2 V0] features recorded by the move kernels
     uint8_t *moved = nullptr;       // [V0] moved in the previous sweep
+    int32_t *nmoved = nullptr;      // [V0] row entries whose vertex moved in the previous sweep
     uint8_t *pred = nullptr;        // [V0] proposed by the predictor
     int32_t *comm_prev = nullptr;   // [V0] communities before the sweep
     int32_t *alist = nullptr;       // [V0] proposed vertices, at their class's offset
@@ -868,6 +869,7 @@ int ensure_active(lv_handle *h) {
     const size_t V = (size_t)h->V0 + 1;
     LV_TRY(dalloc(h, &h->feat, 2 * V));
     LV_TRY(dalloc(h, &h->moved, V));
+    LV_TRY(dalloc(h, &h->nmoved, V));
     LV_TRY(dalloc(h, &h->pred, V));
     LV_TRY(dalloc(h, &h->comm_prev, V));
     LV_TRY(dalloc(h, &h->alist, V));
@@ -931,7 +933,7 @@ int sweep_learned(lv_handle *h, bool full, bool predict, int64_t *moves, double 
     int32_t cnt[NCLS];
     if (predict) {
         if (!full) LV_CUDA(h, cudaMemsetAsync(h->acnt, 0, NCLS * sizeof(int32_t), h->stream));
-        launch_active_select(h->list, n, co, h->cur_rowptr, rowend, h->feat, h->moved, h->model, h->logit_thr,
+        launch_active_select(h->list, n, co, h->cur_rowptr, rowend, h->feat, h->moved, h->nmoved, h->model, h->logit_thr,
                              CLS_HG, full ? nullptr : h->alist, h->acnt, h->pred, h->stream);
         if (!full) {
             LV_CUDA(h, cudaMemcpyAsync(h->small_h, h->acnt, NCLS * sizeof(int32_t), cudaMemcpyDeviceToHost,
@@ -944,7 +946,7 @@ int sweep_learned(lv_handle *h, bool full, bool predict, int64_t *moves, double 
     if (tracing && h->tr_sweep > 0) {
         const double r = h->opts.trace_sample < 1.0f ? h->opts.trace_sample : 1.0;
         const u64 thr = r >= 1.0 ? ~0ull : (u64)(r * 18446744073709551616.0);
-        launch_trace_sample(h->V, h->cur_rowptr, rowend, h->feat, h->moved, thr,
+        launch_trace_sample(h->V, h->cur_rowptr, rowend, h->feat, h->moved, h->nmoved, thr,
                             0x7A11ull * (h->tr_sweep + 1) ^ ((u64)h->level << 40), h->tr_x, h->tr_v, h->tr_cap,
                             h->actr + 2, h->stream);
     }
@@ -966,6 +968,7 @@ int sweep_learned(lv_handle *h, bool full, bool predict, int64_t *moves, double 
     }
     launch_active_moved(h->comm, h->comm_prev, h->V, h->moved, predict && full ? h->pred : nullptr, h->actr,
                         h->stream);
+    launch_nbr_moved(h->cur_rowptr, rowend, h->cur_col, h->V, h->moved, h->nmoved, h->stream);
     if (tracing && h->tr_sweep > 0)
         launch_trace_label(h->tr_v, h->moved, h->tr_rows, h->actr + 2, h->tr_cap, h->tr_y, h->stream);
     u64 ctr[3];
@@ -1002,6 +1005,7 @@ int optimise_level_learned(lv_handle *h, float min_gain, int32_t *changed) {
     LV_TRY(ensure_active(h));
     LV_CUDA(h, cudaMemsetAsync(h->feat, 0, sizeof(float) * 2 * (size_t)h->V, h->stream));
     LV_CUDA(h, cudaMemsetAsync(h->moved, 0, (size_t)h->V, h->stream));
+    LV_CUDA(h, cudaMemsetAsync(h->nmoved, 0, sizeof(int32_t) * (size_t)h->V, h->stream));
     h->tr_sweep = 0;
     double q_before = 0, q_after = 0;
     LV_TRY(modularity(h, &q_before));
@@ -1399,7 +1403,7 @@ int lv_destroy(lv_handle *h) {
         dfree(h, h->lvl_start[b]); dfree(h, h->lvl_end[b]); dfree(h, h->lvl_col[b]); dfree(h, h->lvl_w[b]);
     }
     dfree(h, h->tot_d);
-    dfree(h, h->feat); dfree(h, h->moved); dfree(h, h->pred); dfree(h, h->comm_prev); dfree(h, h->alist);
+    dfree(h, h->feat); dfree(h, h->moved); dfree(h, h->nmoved); dfree(h, h->pred); dfree(h, h->comm_prev); dfree(h, h->alist);
     dfree(h, h->acnt); dfree(h, h->actr); dfree(h, h->model); dfree(h, h->tr_x); dfree(h, h->tr_v);
     dfree(h, h->tr_y);
     {

@@ -69,14 +69,17 @@ struct ActiveClassOffsets {
     int32_t off[NCLS + 1];
 };
 void launch_active_select(const int32_t *list, int32_t n, const ActiveClassOffsets &co, const int32_t *rowptr,
-                          const int32_t *rowend, const float *feat, const uint8_t *moved, const uint16_t *model,
-                          float logit_thr, int keep_cls, int32_t *alist, int32_t *acnt, uint8_t *pred,
-                          cudaStream_t s);
+                          const int32_t *rowend, const float *feat, const uint8_t *moved, const int32_t *nmoved,
+                          const uint16_t *model, float logit_thr, int keep_cls, int32_t *alist, int32_t *acnt,
+                          uint8_t *pred, cudaStream_t s);
+// nmoved[x] = number of row entries of x whose vertex moved (recomputed)
+void launch_nbr_moved(const int32_t *rowptr, const int32_t *rowend, const int32_t *col, int32_t V,
+                      const uint8_t *moved, int32_t *nmoved, cudaStream_t s);
 void launch_active_moved(const int32_t *comm, const int32_t *prev, int32_t V, uint8_t *moved, const uint8_t *pred,
                          u64 *counts, cudaStream_t s);
 void launch_trace_sample(int32_t V, const int32_t *rowptr, const int32_t *rowend, const float *feat,
-                         const uint8_t *moved, u64 thr, u64 key, float *tx, int32_t *tv, int64_t cap,
-                         u64 *tcount, cudaStream_t s);
+                         const uint8_t *moved, const int32_t *nmoved, u64 thr, u64 key, float *tx, int32_t *tv,
+                         int64_t cap, u64 *tcount, cudaStream_t s);
 void launch_trace_label(const int32_t *tv, const uint8_t *moved, int64_t r0, const u64 *tcount, int64_t cap,
                         uint8_t *ty, cudaStream_t s);
 

@@ -5,7 +5,7 @@ Move traces come from plain Louvain runs on seeded LFR-like graphs (power-law
 degrees with exponent 2.5, mean 20, max 2000; power-law community sizes with
 exponent 1.5 in [50, 5000]; mixing parameter mu uniform in [0.1, 0.5]).  Each
 run records, for a sample of vertices before every sweep, the predictor's
-four features and whether the vertex then moved (lv_opts.trace_sample).  The
+five features and whether the vertex then moved (lv_opts.trace_sample).  The
 MLP is trained on the GPU with the library's own kernels (lv_active_train);
 the logit threshold is the largest one whose recall of movers on held-out
 graphs reaches --target-recall.  The result is a JSON file with the bf16
@@ -106,7 +106,7 @@ def main():
         "full_every": a.full_every,
         "thresholds_by_recall": alt,
         "features": ["log2(1+degree)/16", "own-community weight fraction", "relative best gain",
-                     "moved in previous sweep"],
+                     "moved in previous sweep", "fraction of neighbours that moved in previous sweep"],
         "hidden": lvb.ACTIVE_HIDDEN,
         "training": {"graphs": a.seeds, "holdout_graphs": a.holdout, "vertices": a.vertices,
                      "graph_seeds": [TRAIN_SEED0, TRAIN_SEED0 + a.seeds + a.holdout - 1],

@@ -244,9 +244,10 @@ int lv_modularity_noalloc(const int32_t *d_rowptr, const int32_t *d_col, const f
  * sweep.  Parameters, as bf16 bit patterns, in the order W1[HIDDEN][FEATURES],
  * b1[HIDDEN], W2[HIDDEN], b2.  Features of a vertex: log2(1 + degree) / 16,
  * the fraction of its weight into its own community and its best move's gain
- * relative to T k (both from its last evaluation), and whether it moved in the
- * previous sweep. */
-#define LV_ACTIVE_FEATURES 4
+ * relative to T k (both from its last evaluation), whether it moved in the
+ * previous sweep, and the fraction of its row entries whose vertex moved in
+ * the previous sweep. */
+#define LV_ACTIVE_FEATURES 5
 #define LV_ACTIVE_HIDDEN 16
 #define LV_ACTIVE_MODEL_SIZE (LV_ACTIVE_HIDDEN * LV_ACTIVE_FEATURES + 2 * LV_ACTIVE_HIDDEN + 1)
 /* Model for lv_opts.active_set = 1; a vertex is proposed when its logit
