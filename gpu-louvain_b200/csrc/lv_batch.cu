@@ -39,11 +39,15 @@
 namespace lv {
 namespace {
 
+// 512 threads and 2 CTAs per SM (64 registers): 16 warps per graph shorten
+// the largest graphs' latency, which bounds the launch, and 32 resident warps
+// per SM raise throughput; measured against 256 x 3 (80 registers) on the
+// 4096-graph batch: 469 ms vs 713 ms per launch.
 #ifndef LV_BATCH_THREADS
-#define LV_BATCH_THREADS 256
+#define LV_BATCH_THREADS 512
 #endif
 #ifndef LV_BATCH_MINB
-#define LV_BATCH_MINB 3
+#define LV_BATCH_MINB 2
 #endif
 constexpr int BT = LV_BATCH_THREADS;   // threads per CTA
 constexpr int BW = BT / 32;            // warps per CTA
