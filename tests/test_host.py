@@ -84,3 +84,26 @@ def test_cli_usage(lvb):
     assert r.stdout == "Usage: ./gpulouvain -f mtx-matrix-file -g min-gain [-v]\n"
     r = subprocess.run([lvb.CLI_PATH, "-f", "x.mtx"], capture_output=True, text=True)
     assert r.returncode == 1
+
+
+def test_lfr_generator(lvb):
+    """LFR-like graphs: symmetric simple CSR, the requested mean degree (less
+    the dropped repeated pairs and odd stubs), the maximum degree, community
+    sizes within bounds, and about 1 - mu of the entries inside communities;
+    a seed names one graph."""
+    V, mu = 50000, 0.3
+    g, comm = lvb.gen_lfr(V, mu, seed=4)
+    g2, comm2 = lvb.gen_lfr(V, mu, seed=4)
+    assert np.array_equal(g.rowptr, g2.rowptr) and np.array_equal(g.col, g2.col)
+    assert np.array_equal(comm, comm2)
+    deg = np.diff(g.rowptr)
+    row = np.repeat(np.arange(V), deg)
+    assert (g.col != row).all()                                   # no self-loops
+    fwd = set(zip(row.tolist(), g.col.tolist()))
+    assert len(fwd) == g.E and all((b, a) in fwd for a, b in list(fwd)[:20000])
+    assert 17.0 < deg.mean() < 21.0 and deg.max() <= 2000
+    sizes = np.bincount(comm)
+    assert sizes.min() >= 50 and sizes.max() <= 5000 + 50
+    intra = (comm[row] == comm[g.col]).mean()
+    assert abs(intra - (1 - mu)) < 0.05
+    assert (g.w == 1.0).all()
