@@ -597,6 +597,8 @@ def run_lfr(args, ranks: Ranks):
     with open(args.active_model or os.path.join(ROOT, "gpu-louvain_b200", "active_set_lfr.json")) as f:
         meta = _json.load(f)
     K = int(meta.get("full_every", 4))
+    start = float(meta.get("active_start", 0.0))
+    min_recall = float(meta.get("min_recall", 0.0))
     lfr = meta["training"]["lfr"]
     per_mu = []
     t_plain = t_learned = 0.0
@@ -605,7 +607,8 @@ def run_lfr(args, ranks: Ranks):
         g, _ = lvb.gen_lfr(args.lfr_vertices, mu, seed=LFR_EVAL_SEED + ranks.rank, **lfr)
         res = {}
         for mode in ("plain", "learned"):
-            kw = {"active_set": True, "active_full_every": K} if mode == "learned" else {}
+            kw = ({"active_set": True, "active_full_every": K, "active_start": start,
+                   "active_min_recall": min_recall} if mode == "learned" else {})
             with lvb.Louvain(g, device=dev, **kw) as e:
                 if mode == "learned":
                     e.set_active_model(model, thr)
@@ -650,7 +653,8 @@ def run_lfr(args, ranks: Ranks):
         "data": "synthetic (seeded LFR-like graphs generated on the host; held-out seeds)",
         "config": {"workload": f"lfr{args.lfr_vertices}_learned_vs_plain", "vertices": args.lfr_vertices,
                    "mu": list(LFR_EVAL_MU), "seed": LFR_EVAL_SEED, "lfr": lfr, "min_gain": MIN_GAIN,
-                   "full_every": K, "logit_threshold": thr, "model": os.path.basename(
+                   "full_every": K, "active_start": start, "min_recall": min_recall,
+                   "logit_threshold": thr, "model": os.path.basename(
                        args.active_model or "active_set_lfr.json"), "parallelism": f"replicas{ranks.world}"},
         "max_abs_dq": max(abs(r["dq"]) for r in per_mu),
         "per_graph": per_mu,

@@ -75,8 +75,10 @@ def main():
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=1e-2)
-    ap.add_argument("--target-recall", type=float, default=0.97)
+    ap.add_argument("--target-recall", type=float, default=0.99)
     ap.add_argument("--full-every", type=int, default=4, help="recommended lv_opts.active_full_every")
+    ap.add_argument("--active-start", type=float, default=0.2, help="recommended lv_opts.active_start")
+    ap.add_argument("--min-recall", type=float, default=0.01, help="recommended lv_opts.active_min_recall")
     ap.add_argument("--min-gain", type=float, default=1e-6)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--seed", type=int, default=7)
@@ -104,6 +106,8 @@ def main():
         "model_bf16": [int(v) for v in model],
         "logit_threshold": thr,
         "full_every": a.full_every,
+        "active_start": a.active_start,
+        "min_recall": a.min_recall,
         "thresholds_by_recall": alt,
         "features": ["log2(1+degree)/16", "own-community weight fraction", "relative best gain",
                      "moved in previous sweep", "fraction of neighbours that moved in previous sweep"],
