@@ -138,3 +138,29 @@ def test_learned_mode_is_exact_and_deterministic(lvb, orc):
     o.close()
     assert st1["full_sweeps"] > 0 and st1["evaluated"] <= s1["sweeps"] * g.V
     assert abs(q1 - q0) <= 5e-3
+
+
+def test_packaged_model_and_threshold_rule(lvb):
+    """The packaged predictor has the library's parameter count and the
+    settings it was measured with; pick_threshold keeps the requested share of
+    positives above the threshold."""
+    import importlib.util
+    import os
+    model, thr = lvb.load_active_model()
+    assert model.dtype == np.uint16 and len(model) == lvb.ACTIVE_MODEL_SIZE
+    assert np.isfinite(bf16_to_f32(model)).all() and np.isfinite(thr)
+    import json
+    with open(os.path.join(os.path.dirname(lvb.__file__), "active_set_lfr.json")) as f:
+        meta = json.load(f)
+    for k in ("full_every", "active_start", "min_recall", "thresholds_by_recall", "training"):
+        assert k in meta
+    path = os.path.join(os.path.dirname(lvb.__file__), "train_active_set.py")
+    spec = importlib.util.spec_from_file_location("train_active_set", path)
+    T = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(T)
+    rng = np.random.default_rng(3)
+    z = rng.standard_normal(10000).astype(np.float32)
+    y = (rng.uniform(size=10000) < 0.3).astype(np.uint8)
+    for target in (0.9, 0.97, 0.99):
+        t = T.pick_threshold(z, y, target)
+        assert ((z > t) & (y == 1)).sum() >= target * (y == 1).sum()
