@@ -88,7 +88,7 @@ EXPORTED = [
     "lv_batch_create", "lv_batch_create_device", "lv_batch_run", "lv_batch_get_results",
     "lv_batch_get_graph_stats", "lv_batch_get_stats", "lv_batch_last_error", "lv_batch_destroy",
     "lv_gen_lfr", "lv_set_active_model", "lv_get_traces", "lv_get_active_stats", "lv_active_train",
-    "lv_active_predict",
+    "lv_active_predict", "lv_write_csr", "lv_read_csr",
 ]
 
 _lib = None
@@ -139,6 +139,8 @@ def lib() -> C.CDLL:
     L.lv_get_class_stats.argtypes = [C.c_void_p, C.POINTER(_ClassStats)]
     L.lv_read_mtx.argtypes = [C.c_char_p, P32, P64, C.POINTER(P32), C.POINTER(P32), C.POINTER(PF), PF]
     L.lv_write_mtx.argtypes = [C.c_char_p, C.c_int32, C.c_int64, P32, P32, PF]
+    L.lv_write_csr.argtypes = [C.c_char_p, C.c_int32, C.c_int64, P32, P32, PF, C.c_float]
+    L.lv_read_csr.argtypes = [C.c_char_p, P32, P64, C.POINTER(P32), C.POINTER(P32), C.POINTER(PF), PF]
     L.lv_free_host.argtypes = [C.c_void_p]
     L.lv_print_communities.argtypes = [C.c_char_p, P32, C.c_int32, C.c_int32]
     L.lv_gen_rmat.argtypes = [C.c_int32, C.c_int32, C.c_uint64, C.c_double, C.c_double, C.c_double,
@@ -205,10 +207,9 @@ def _ptr(a: np.ndarray, t):
 def _take_host(ptr, n: int, dtype) -> np.ndarray:
     """Copy a malloc'd C array into numpy and free it."""
     L = lib()
+    buf = np.empty(n if n > 0 else 0, dtype=dtype)
     if n > 0:
-        buf = np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype, copy=True)
-    else:
-        buf = np.zeros(0, dtype=dtype)
+        C.memmove(buf.ctypes.data, ptr, n * buf.itemsize)
     L.lv_free_host(C.cast(ptr, C.c_void_p))
     return buf
 
@@ -244,6 +245,25 @@ def read_mtx(path: str) -> Graph:
     rp, cl, w = P32(), P32(), PF()
     m = C.c_float()
     _check(L.lv_read_mtx(path.encode(), C.byref(V), C.byref(E), C.byref(rp), C.byref(cl), C.byref(w),
+                         C.byref(m)))
+    return Graph(_take_host(rp, V.value + 1, np.int32), _take_host(cl, E.value, np.int32),
+                 _take_host(w, E.value, np.float32), m_ref=m.value)
+
+
+def write_csr(path: str, g: Graph) -> None:
+    """Binary CSR cache file (lv_write_csr)."""
+    _check(lib().lv_write_csr(path.encode(), g.V, g.E, _ptr(g.rowptr, C.c_int32), _ptr(g.col, C.c_int32),
+                              _ptr(g.w, C.c_float), g.m_ref if g.m_ref is not None else 0.0))
+
+
+def read_csr(path: str) -> Graph:
+    """Graph from a binary CSR cache file (lv_read_csr)."""
+    L = lib()
+    V = C.c_int32()
+    E = C.c_int64()
+    rp, cl, w = P32(), P32(), PF()
+    m = C.c_float()
+    _check(L.lv_read_csr(path.encode(), C.byref(V), C.byref(E), C.byref(rp), C.byref(cl), C.byref(w),
                          C.byref(m)))
     return Graph(_take_host(rp, V.value + 1, np.int32), _take_host(cl, E.value, np.int32),
                  _take_host(w, E.value, np.float32), m_ref=m.value)

@@ -7,13 +7,35 @@
 // scopes follow the reference: totalTime adds the device set-up (allocation,
 // host->device copy, M) to the algorithm time (level loop + final modularity);
 // reading the file is not timed.
+//
+// Not in the reference: -d N selects the CUDA device, and -c keeps a binary
+// CSR cache beside the file (<file>.lvcsr, lv_write_csr): when the cache is
+// newer than the file it is read instead of parsing the text again.
 #include <getopt.h>
+#include <sys/stat.h>
 
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 
 #include "../../include/louvain_b200.h"
+
+// The CSR of `file`, through the cache <file>.lvcsr when use_cache is set.
+static int read_graph(const char *file, bool use_cache, int32_t *V, int64_t *E, int32_t **rowptr, int32_t **col,
+                      float **w) {
+    if (!use_cache) return lv_read_mtx(file, V, E, rowptr, col, w, nullptr);
+    const std::string cache = std::string(file) + ".lvcsr";
+    struct stat sf, sc;
+    if (stat(file, &sf) == 0 && stat(cache.c_str(), &sc) == 0 && sc.st_mtime >= sf.st_mtime &&
+        lv_read_csr(cache.c_str(), V, E, rowptr, col, w, nullptr) == LV_OK)
+        return LV_OK;
+    float m_ref = 0;
+    const int rc = lv_read_mtx(file, V, E, rowptr, col, w, &m_ref);
+    if (rc == LV_OK && lv_write_csr(cache.c_str(), *V, *E, *rowptr, *col, *w, m_ref) != LV_OK)
+        std::fprintf(stderr, "gpulouvain: could not write the cache %s\n", cache.c_str());
+    return rc;
+}
 
 static void usage() {
     std::printf("Usage: ./gpulouvain -f mtx-matrix-file -g min-gain [-v]\n");
@@ -23,15 +45,16 @@ static void usage() {
 int main(int argc, char *argv[]) {
     const char *file = nullptr;
     float min_gain = 0;
-    bool have_f = false, have_g = false, verbose = false;
+    bool have_f = false, have_g = false, verbose = false, use_cache = false;
     int device = 0;
     int opt;
-    while ((opt = getopt(argc, argv, "f:g:vd:")) != -1) {
+    while ((opt = getopt(argc, argv, "f:g:vd:c")) != -1) {
         switch (opt) {
         case 'g': have_g = true; min_gain = std::strtof(optarg, nullptr); break;
         case 'v': verbose = true; break;
         case 'f': have_f = true; file = optarg; break;
         case 'd': device = std::atoi(optarg); break;
+        case 'c': use_cache = true; break;
         default: usage();
         }
     }
@@ -41,7 +64,7 @@ int main(int argc, char *argv[]) {
     int64_t E = 0;
     int32_t *rowptr = nullptr, *col = nullptr;
     float *w = nullptr;
-    int rc = lv_read_mtx(file, &V, &E, &rowptr, &col, &w, nullptr);
+    int rc = read_graph(file, use_cache, &V, &E, &rowptr, &col, &w);
     if (rc != LV_OK) {
         std::fprintf(stderr, "gpulouvain: cannot read %s: %s\n", file, lv_status_string(rc));
         return EXIT_FAILURE;

@@ -75,11 +75,194 @@ inline bool parse_f32(const char *&p, const char *end, float *out) {
     return true;
 }
 
+// The entries of the data section as the reference reads them: a stream of
+// whitespace-separated tokens, `v1 v2 [w]` per entry (utils.cu:20-31).
+int parse_entries(const char *p, const char *end, long long nnz, bool pattern, int32_t V, int32_t *ea,
+                  int32_t *eb, float *ew) {
+    for (long long i = 0; i < nnz; ++i) {
+        long long a, b;
+        float wv = 1.0f;
+        if (!parse_i64(p, end, &a) || !parse_i64(p, end, &b)) return LV_ERR_IO;
+        if (!pattern && !parse_f32(p, end, &wv)) return LV_ERR_IO;
+        a -= 1;
+        b -= 1;
+        if (a < 0 || b < 0 || a >= V || b >= V) return LV_ERR_INVALID;
+        ea[i] = (int32_t)a;
+        eb[i] = (int32_t)b;
+        ew[i] = wv;
+    }
+    return LV_OK;
+}
+
+constexpr int PARSE_SEQUENTIAL = -1;
+
+// Tokens on the line [p, eol), up to 4.
+inline int line_tokens(const char *p, const char *eol) {
+    int n = 0;
+    bool in = false;
+    for (; p < eol && n < 4; ++p) {
+        const bool ws = *p == ' ' || *p == '\t' || *p == '\r';
+        if (!ws && !in) ++n;
+        in = !ws;
+    }
+    return n;
+}
+
+// The same entries parsed by all host threads.  The data section is cut into
+// byte ranges at line starts; a first pass counts each range's entries, a
+// second parses them into their file-order positions.  This equals the
+// token-stream reading when every non-blank line holds exactly one entry (2
+// tokens for pattern files, 3 otherwise); on any other layout, and on any
+// parse or range error (whose code depends on file order), the caller falls
+// back to the sequential reading (PARSE_SEQUENTIAL).  Small files are read
+// sequentially.
+int parse_entries_parallel(const char *p, const char *end, long long nnz, bool pattern, int32_t V,
+                           int32_t *ea, int32_t *eb, float *ew) {
+    const size_t n = (size_t)(end - p);
+    const int T = omp_get_max_threads();
+    if (T < 2 || n < ((size_t)1 << 22) || nnz < 100000) return PARSE_SEQUENTIAL;
+    const int want = pattern ? 2 : 3;
+    std::vector<const char *> cut((size_t)T + 1);
+    cut[0] = p;
+    cut[(size_t)T] = end;
+    for (int t = 1; t < T; ++t) {
+        const char *c = p + n / (size_t)T * (size_t)t;
+        if (c < cut[(size_t)t - 1]) c = cut[(size_t)t - 1];
+        const char *nl = c < end ? (const char *)std::memchr(c, '\n', (size_t)(end - c)) : nullptr;
+        cut[(size_t)t] = nl ? nl + 1 : end;
+    }
+    std::vector<long long> cnt((size_t)T, 0);
+    std::vector<int> bad((size_t)T, 0);
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+    for (int t = 0; t < T; ++t) {
+        const char *q = cut[(size_t)t], *e = cut[(size_t)t + 1];
+        long long c = 0;
+        while (q < e) {
+            const char *nl = (const char *)std::memchr(q, '\n', (size_t)(e - q));
+            const char *eol = nl ? nl : e;
+            const int k = line_tokens(q, eol);
+            if (k == want) ++c;
+            else if (k != 0) { bad[(size_t)t] = 1; break; }
+            q = nl ? nl + 1 : e;
+        }
+        cnt[(size_t)t] = c;
+    }
+    long long total = 0;
+    std::vector<long long> first((size_t)T + 1, 0);
+    for (int t = 0; t < T; ++t) {
+        if (bad[(size_t)t]) return PARSE_SEQUENTIAL;
+        first[(size_t)t] = total;
+        total += cnt[(size_t)t];
+    }
+    if (total < nnz) return PARSE_SEQUENTIAL;
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+    for (int t = 0; t < T; ++t) {
+        const char *q = cut[(size_t)t], *e = cut[(size_t)t + 1];
+        long long i = first[(size_t)t];
+        while (q < e && i < nnz) {
+            const char *nl = (const char *)std::memchr(q, '\n', (size_t)(e - q));
+            const char *eol = nl ? nl : e;
+            if (line_tokens(q, eol) != 0) {
+                const char *r = q;
+                long long a, b;
+                float wv = 1.0f;
+                if (!parse_i64(r, eol, &a) || !parse_i64(r, eol, &b) || (!pattern && !parse_f32(r, eol, &wv)) ||
+                    a < 1 || b < 1 || a > V || b > V) {
+                    bad[(size_t)t] = 1;
+                    break;
+                }
+                ea[i] = (int32_t)(a - 1);
+                eb[i] = (int32_t)(b - 1);
+                ew[i] = wv;
+                ++i;
+            }
+            q = nl ? nl + 1 : e;
+        }
+    }
+    for (int t = 0; t < T; ++t)
+        if (bad[(size_t)t]) return PARSE_SEQUENTIAL;
+    return LV_OK;
+}
+
+constexpr char CSR_MAGIC[8] = {'L', 'V', 'C', 'S', 'R', '0', '0', '1'};
+struct CsrHeader {
+    char magic[8];
+    int64_t V;
+    int64_t E;
+    float m_ref;
+    uint32_t pad;
+};
+
 }  // namespace
 
 extern "C" {
 
 void lv_free_host(void *p) { std::free(p); }
+
+int lv_write_csr(const char *path, int32_t V, int64_t E, const int32_t *rowptr, const int32_t *col, const float *w,
+                 float m_ref) {
+    if (!path || V < 0 || E < 0 || !rowptr || (E > 0 && (!col || !w))) return LV_ERR_INVALID;
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return LV_ERR_IO;
+    CsrHeader h{};
+    std::memcpy(h.magic, CSR_MAGIC, 8);
+    h.V = V;
+    h.E = E;
+    h.m_ref = m_ref;
+    bool ok = std::fwrite(&h, sizeof h, 1, f) == 1 &&
+              std::fwrite(rowptr, sizeof(int32_t), (size_t)V + 1, f) == (size_t)V + 1 &&
+              (E == 0 || (std::fwrite(col, sizeof(int32_t), (size_t)E, f) == (size_t)E &&
+                          std::fwrite(w, sizeof(float), (size_t)E, f) == (size_t)E));
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? LV_OK : LV_ERR_IO;
+}
+
+int lv_read_csr(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr, int32_t **col, float **w,
+                float *m_ref) {
+    if (!path || !Vout || !Eout || !rowptr || !col || !w) return LV_ERR_INVALID;
+    Mapped m;
+    m.fd = open(path, O_RDONLY);
+    if (m.fd < 0) return LV_ERR_IO;
+    struct stat sb;
+    if (fstat(m.fd, &sb) != 0 || (size_t)sb.st_size < sizeof(CsrHeader)) return LV_ERR_IO;
+    m.n = (size_t)sb.st_size;
+    void *mp = mmap(nullptr, m.n, PROT_READ, MAP_PRIVATE, m.fd, 0);
+    if (mp == MAP_FAILED) return LV_ERR_IO;
+    m.p = (const char *)mp;
+    CsrHeader h;
+    std::memcpy(&h, m.p, sizeof h);
+    if (std::memcmp(h.magic, CSR_MAGIC, 8) != 0 || h.V < 0 || h.V > 0x7ffffffeLL || h.E < 0 || h.E > 0x7fffffffLL)
+        return LV_ERR_IO;
+    const size_t need = sizeof h + 4 * ((size_t)h.V + 1) + 8 * (size_t)h.E;
+    if (m.n != need) return LV_ERR_IO;
+    int32_t *rp = (int32_t *)std::malloc(4 * ((size_t)h.V + 1));
+    int32_t *cl = (int32_t *)std::malloc(4 * (size_t)(h.E > 0 ? h.E : 1));
+    float *wt = (float *)std::malloc(4 * (size_t)(h.E > 0 ? h.E : 1));
+    if (!rp || !cl || !wt) {
+        std::free(rp); std::free(cl); std::free(wt);
+        return LV_ERR_NOMEM;
+    }
+    const char *q = m.p + sizeof h;
+    std::memcpy(rp, q, 4 * ((size_t)h.V + 1));
+    q += 4 * ((size_t)h.V + 1);
+    std::memcpy(cl, q, 4 * (size_t)h.E);
+    q += 4 * (size_t)h.E;
+    std::memcpy(wt, q, 4 * (size_t)h.E);
+    bool okp = rp[0] == 0 && (int64_t)rp[h.V] == h.E;
+    for (int64_t v = 0; okp && v < h.V; ++v) okp = rp[v + 1] >= rp[v];
+    for (int64_t e = 0; okp && e < h.E; ++e) okp = cl[e] >= 0 && cl[e] < h.V;
+    if (!okp) {
+        std::free(rp); std::free(cl); std::free(wt);
+        return LV_ERR_IO;
+    }
+    *Vout = (int32_t)h.V;
+    *Eout = h.E;
+    *rowptr = rp;
+    *col = cl;
+    *w = wt;
+    if (m_ref) *m_ref = h.m_ref;
+    return LV_OK;
+}
 
 int lv_read_mtx(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr_out,
                 int32_t **col_out, float **w_out, float *m_ref) {
@@ -125,18 +308,9 @@ int lv_read_mtx(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr
     const int32_t V = (int32_t)cols;
     std::vector<int32_t> ea((size_t)nnz), eb((size_t)nnz);
     std::vector<float> ew((size_t)nnz);
-    for (long long i = 0; i < nnz; ++i) {
-        long long a, b;
-        float wv = 1.0f;
-        if (!parse_i64(p, end, &a) || !parse_i64(p, end, &b)) return LV_ERR_IO;
-        if (!pattern && !parse_f32(p, end, &wv)) return LV_ERR_IO;
-        a -= 1;
-        b -= 1;
-        if (a < 0 || b < 0 || a >= V || b >= V) return LV_ERR_INVALID;
-        ea[(size_t)i] = (int32_t)a;
-        eb[(size_t)i] = (int32_t)b;
-        ew[(size_t)i] = wv;
-    }
+    int prc = parse_entries_parallel(p, end, nnz, pattern, V, ea.data(), eb.data(), ew.data());
+    if (prc == PARSE_SEQUENTIAL) prc = parse_entries(p, end, nnz, pattern, V, ea.data(), eb.data(), ew.data());
+    if (prc != LV_OK) return prc;
     // degrees: v1 gets (v2,w); v2 gets (v1,w) unless self-loop (utils.cu:32-46)
     std::vector<int64_t> deg((size_t)V + 1, 0);
     int64_t E = 0;

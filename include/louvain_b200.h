@@ -167,11 +167,24 @@ int lv_clear_stats(lv_handle *h);
 /* ---- host-side I/O (no GPU needed) ---- */
 
 /* readInputData (utils.cu:9-62): symmetric Matrix Market -> CSR in file
- * order (both directions for off-diagonal entries, self-loops once).
+ * order (both directions for off-diagonal entries, self-loops once).  The
+ * file is memory-mapped; large files with one entry per line are parsed by
+ * all host threads, other layouts by the reference's token-stream reading
+ * (same result either way).
  * Arrays are malloc'd; release with lv_free_host.  m_ref receives M as the
  * reference accumulates it (FP32, sequential). */
 int lv_read_mtx(const char *path, int32_t *V, int64_t *E, int32_t **rowptr, int32_t **col,
                 float **w, float *m_ref);
+/* Binary CSR file, a cache for lv_read_mtx's output (no counterpart in the
+ * reference, which parses the text file on every run): header "LVCSR001",
+ * V and E (int64), m_ref (float), then rowptr[V+1], col[E] (int32) and w[E]
+ * (float32), little-endian.  lv_read_csr checks the header, the file size,
+ * the offsets and the column range (LV_ERR_IO otherwise); arrays are
+ * malloc'd (lv_free_host). */
+int lv_write_csr(const char *path, int32_t V, int64_t E, const int32_t *rowptr, const int32_t *col,
+                 const float *w, float m_ref);
+int lv_read_csr(const char *path, int32_t *V, int64_t *E, int32_t **rowptr, int32_t **col, float **w,
+                float *m_ref);
 /* Write an undirected edge list as symmetric Matrix Market (i > j, 1-based). */
 int lv_write_mtx(const char *path, int32_t V, int64_t n_edges, const int32_t *u, const int32_t *v,
                  const float *w);

@@ -107,3 +107,66 @@ def test_lfr_generator(lvb):
     intra = (comm[row] == comm[g.col]).mean()
     assert abs(intra - (1 - mu)) < 0.05
     assert (g.w == 1.0).all()
+
+
+def _same_csr(r, o):
+    rp, cl, w, m = o
+    return (np.array_equal(r.rowptr, rp) and np.array_equal(r.col, cl) and np.array_equal(r.w, w)
+            and r.m_ref == m)
+
+
+def test_parallel_reader_matches_token_stream(lvb, orc, tmp_path):
+    """Files large enough for the multi-threaded reading (one entry per line)
+    give exactly the oracle's token-stream reading; so do layouts that force
+    the sequential reading (an entry split over two lines), CRLF line ends,
+    pattern files and a header line with trailing blanks."""
+    g = lvb.gen_rmat(15, seed=3)
+    p = tmp_path / "big.mtx"
+    lvb.write_mtx(str(p), g)
+    assert p.stat().st_size > (1 << 22)
+    assert _same_csr(lvb.read_mtx(str(p)), orc.read_mtx(str(p)))
+    text = p.read_text()
+    head, body = text.split("\n", 2)[:2], text.split("\n", 2)[2]
+    lines = body.split("\n")
+    # an entry split over two lines (sequential reading)
+    a, b, w = lines[5].split()
+    split = "\n".join(head) + "\n" + "\n".join(lines[:5] + [a + " " + b, w] + lines[6:])
+    q = tmp_path / "split.mtx"
+    q.write_text(split)
+    assert _same_csr(lvb.read_mtx(str(q)), orc.read_mtx(str(q)))
+    # CRLF line ends
+    q2 = tmp_path / "crlf.mtx"
+    q2.write_bytes(text.replace("\n", "\r\n").encode())
+    assert _same_csr(lvb.read_mtx(str(q2)), orc.read_mtx(str(q2)))
+    # pattern file: two tokens per line
+    pat = "%%MatrixMarket matrix coordinate pattern symmetric\n" + head[1] + "   \n" + "\n".join(
+        " ".join(l.split()[:2]) for l in lines if l.strip())
+    q3 = tmp_path / "pattern.mtx"
+    q3.write_text(pat + "\n")
+    r3 = lvb.read_mtx(str(q3))
+    assert _same_csr(r3, orc.read_mtx(str(q3))) and (r3.w == 1.0).all()
+    # an out-of-range vertex far into the file is still an error
+    bad = lines[:]
+    bad[len(bad) // 2] = f"{g.V + 7} 1 1.0"
+    q4 = tmp_path / "range.mtx"
+    q4.write_text("\n".join(head) + "\n" + "\n".join(bad))
+    with pytest.raises(lvb.LouvainError) as ex:
+        lvb.read_mtx(str(q4))
+    assert ex.value.status == lvb.LV_ERR_INVALID
+
+
+def test_csr_cache_roundtrip(lvb, tmp_path):
+    g = lvb.gen_planted(3000, 16, 12.0, 2.0, 5, "uniform")
+    g.m_ref = 1234.5
+    p = str(tmp_path / "g.lvcsr")
+    lvb.write_csr(p, g)
+    r = lvb.read_csr(p)
+    assert np.array_equal(r.rowptr, g.rowptr) and np.array_equal(r.col, g.col) and np.array_equal(r.w, g.w)
+    assert r.m_ref == np.float32(1234.5)
+    raw = open(p, "rb").read()
+    for broken in (raw[:-4], b"XXXXXXXX" + raw[8:], raw[:64] + (b"\xff" * 4) + raw[68:]):
+        q = str(tmp_path / "broken.lvcsr")
+        open(q, "wb").write(broken)
+        with pytest.raises(lvb.LouvainError) as ex:
+            lvb.read_csr(q)
+        assert ex.value.status == lvb.LV_ERR_IO
