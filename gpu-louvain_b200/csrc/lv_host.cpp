@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -386,6 +387,7 @@ int lv_write_mtx(const char *path, int32_t V, int64_t n_edges, const int32_t *u,
 int lv_print_communities(const char *path, const int32_t *orig2comm, int32_t V0,
                          int32_t num_communities) {
     if (V0 < 0 || num_communities < 0 || (V0 > 0 && !orig2comm)) return LV_ERR_INVALID;
+    // counting sort of the vertices by community (members in increasing id)
     std::vector<int64_t> start((size_t)num_communities + 1, 0);
     for (int32_t v = 0; v < V0; ++v) {
         const int32_t c = orig2comm[v];
@@ -400,32 +402,57 @@ int lv_print_communities(const char *path, const int32_t *orig2comm, int32_t V0,
     }
     FILE *f = path ? std::fopen(path, "w") : stdout;
     if (!f) return LV_ERR_IO;
-    std::vector<char> out;
-    out.reserve(1 << 22);
-    char tmp[32];
-    auto flush = [&]() {
-        if (!out.empty()) std::fwrite(out.data(), 1, out.size(), f);
-        out.clear();
-    };
-    auto put_int = [&](int64_t x) {
-        int n = std::snprintf(tmp, sizeof(tmp), "%lld", (long long)x);
-        out.insert(out.end(), tmp, tmp + n);
-    };
-    put_int(num_communities);
-    out.push_back('\n');
-    for (int32_t c = 0; c < num_communities; ++c) {
-        put_int((int64_t)c + 1);
-        for (int64_t i = start[(size_t)c]; i < start[(size_t)c + 1]; ++i) {
-            out.push_back(' ');
-            put_int((int64_t)mem[(size_t)i] + 1);
-        }
-        out.push_back('\n');
-        if (out.size() > (1 << 21)) flush();
+    // the lines of consecutive community ranges are formatted by all host
+    // threads into their own buffers (ranges of about equal member counts),
+    // then written in order
+    const int T = omp_get_max_threads();
+    const int64_t per = ((int64_t)V0 + num_communities) / (T > 0 ? T : 1) + 1;
+    std::vector<int32_t> cut((size_t)T + 1, num_communities);
+    cut[0] = 0;
+    for (int t = 1, c = 0; t < T; ++t) {
+        while (c < num_communities && start[(size_t)c] + c < per * t) ++c;
+        cut[(size_t)t] = c;
     }
-    flush();
+    // decimal digits of x >= 0 at p; returns the end
+    auto put_int = [](char *p, int64_t x) {
+        char tmp[24];
+        int n = 0;
+        do {
+            tmp[n++] = (char)('0' + x % 10);
+            x /= 10;
+        } while (x > 0);
+        while (n > 0) *p++ = tmp[--n];
+        return p;
+    };
+    std::vector<std::unique_ptr<char[]>> buf((size_t)T);
+    std::vector<size_t> len((size_t)T, 0);
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+    for (int t = 0; t < T; ++t) {
+        const int32_t c0 = cut[(size_t)t], c1 = cut[(size_t)t + 1];
+        if (c1 <= c0) continue;
+        // at most 11 characters per number plus a separator
+        buf[(size_t)t].reset(new char[(size_t)(start[(size_t)c1] - start[(size_t)c0] + (c1 - c0)) * 12]);
+        char *const o = buf[(size_t)t].get();
+        char *q = o;
+        for (int32_t c = c0; c < c1; ++c) {
+            q = put_int(q, (int64_t)c + 1);
+            for (int64_t i = start[(size_t)c]; i < start[(size_t)c + 1]; ++i) {
+                *q++ = ' ';
+                q = put_int(q, (int64_t)mem[(size_t)i] + 1);
+            }
+            *q++ = '\n';
+        }
+        len[(size_t)t] = (size_t)(q - o);
+    }
+    char head[32];
+    char *he = put_int(head, num_communities);
+    *he++ = '\n';
+    bool ok = std::fwrite(head, 1, (size_t)(he - head), f) == (size_t)(he - head);
+    for (int t = 0; t < T && ok; ++t)
+        ok = len[(size_t)t] == 0 || std::fwrite(buf[(size_t)t].get(), 1, len[(size_t)t], f) == len[(size_t)t];
     std::fflush(f);
-    if (path) std::fclose(f);
-    return LV_OK;
+    if (path) ok = (std::fclose(f) == 0) && ok;
+    return ok ? LV_OK : LV_ERR_IO;
 }
 
 }  // extern "C"

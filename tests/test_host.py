@@ -170,3 +170,21 @@ def test_csr_cache_roundtrip(lvb, tmp_path):
         with pytest.raises(lvb.LouvainError) as ex:
             lvb.read_csr(q)
         assert ex.value.status == lvb.LV_ERR_IO
+
+
+def test_print_communities_large_matches_python(lvb, tmp_path):
+    """The multi-threaded writer gives the reference's format byte for byte:
+    the community count, then "c+1 m1+1 m2+1 ..." per community with members
+    in increasing id (empty communities print just their number)."""
+    rng = np.random.default_rng(8)
+    V, nc = 200000, 50000
+    m = rng.integers(0, nc, V).astype(np.int32)
+    p = str(tmp_path / "map.txt")
+    lvb.print_communities(m, nc, p)
+    order = np.argsort(m, kind="stable")
+    bounds = np.searchsorted(m[order], np.arange(nc + 1))
+    lines = [str(nc)]
+    for c in range(nc):
+        mem = order[bounds[c]:bounds[c + 1]] + 1
+        lines.append(" ".join([str(c + 1)] + [str(x) for x in mem]))
+    assert open(p).read() == "\n".join(lines) + "\n"
