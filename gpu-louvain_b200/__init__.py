@@ -60,7 +60,7 @@ class _Opts(C.Structure):
                 ("profile", C.c_int32), ("verify", C.c_int32), ("trace", C.c_int32),
                 ("sweep_graph", C.c_int32), ("active_set", C.c_int32), ("active_full_every", C.c_int32),
                 ("active_min_recall", C.c_float), ("trace_sample", C.c_float), ("active_start", C.c_float),
-                ("reserved", C.c_int32 * 4)]
+                ("wide_weights", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class _Stats(C.Structure):
@@ -74,7 +74,7 @@ class _Stats(C.Structure):
 class _ClassStats(C.Structure):
     _fields_ = [("launches", C.c_int64 * NUM_CLASSES), ("vertices", C.c_int64 * NUM_CLASSES),
                 ("edges", C.c_int64 * NUM_CLASSES), ("ms", C.c_double * NUM_CLASSES),
-                ("bytes", C.c_double * NUM_CLASSES)]
+                ("bytes", C.c_double * NUM_CLASSES), ("stored_bytes", C.c_double * NUM_CLASSES)]
 
 
 EXPORTED = [
@@ -88,7 +88,7 @@ EXPORTED = [
     "lv_batch_create", "lv_batch_create_device", "lv_batch_run", "lv_batch_get_results",
     "lv_batch_get_graph_stats", "lv_batch_get_stats", "lv_batch_last_error", "lv_batch_destroy",
     "lv_gen_lfr", "lv_set_active_model", "lv_get_traces", "lv_get_active_stats", "lv_active_train",
-    "lv_active_predict", "lv_write_csr", "lv_read_csr",
+    "lv_active_predict", "lv_write_csr", "lv_read_csr", "lv_write_csr_stamped", "lv_read_csr_stamp",
 ]
 
 _lib = None
@@ -141,6 +141,9 @@ def lib() -> C.CDLL:
     L.lv_write_mtx.argtypes = [C.c_char_p, C.c_int32, C.c_int64, P32, P32, PF]
     L.lv_write_csr.argtypes = [C.c_char_p, C.c_int32, C.c_int64, P32, P32, PF, C.c_float]
     L.lv_read_csr.argtypes = [C.c_char_p, P32, P64, C.POINTER(P32), C.POINTER(P32), C.POINTER(PF), PF]
+    L.lv_write_csr_stamped.argtypes = [C.c_char_p, C.c_int32, C.c_int64, P32, P32, PF, C.c_float, C.c_int64,
+                                       C.c_int64]
+    L.lv_read_csr_stamp.argtypes = [C.c_char_p, P64, P64]
     L.lv_free_host.argtypes = [C.c_void_p]
     L.lv_print_communities.argtypes = [C.c_char_p, P32, C.c_int32, C.c_int32]
     L.lv_gen_rmat.argtypes = [C.c_int32, C.c_int32, C.c_uint64, C.c_double, C.c_double, C.c_double,
@@ -354,7 +357,7 @@ class Louvain:
                  profile: bool = False, verify: bool = False, trace: bool = False,
                  device_csr: tuple | None = None, sweep_graph: bool = True,
                  active_set: bool = False, active_full_every: int = 0, active_min_recall: float = 0.0,
-                 trace_sample: float = 0.0, active_start: float = 0.0):
+                 trace_sample: float = 0.0, active_start: float = 0.0, wide_weights: bool = False):
         L = lib()
         opts = _Opts()
         L.lv_default_opts(C.byref(opts))
@@ -369,6 +372,7 @@ class Louvain:
         opts.active_min_recall = active_min_recall
         opts.trace_sample = trace_sample
         opts.active_start = active_start
+        opts.wide_weights = 1 if wide_weights else 0
         h = C.c_void_p()
         if device_csr is not None:
             rp, cl, w, V, E = device_csr
@@ -437,8 +441,13 @@ class Louvain:
         self._c(lib().lv_get_level_info(self._h, C.byref(V), C.byref(E), C.byref(lvl)))
         return V.value, E.value, lvl.value
 
-    def original_to_community(self):
-        out = np.empty(self.V0, np.int32)
+    def original_to_community(self, out: np.ndarray | None = None):
+        """(map, number of communities); out (int32, V0 entries, contiguous),
+        e.g. a pinned buffer, receives the map instead of a new array."""
+        if out is None:
+            out = np.empty(self.V0, np.int32)
+        elif out.dtype != np.int32 or out.shape != (self.V0,) or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous int32 array of V0 entries")
         nc = C.c_int32()
         self._c(lib().lv_get_original_to_community(self._h, _ptr(out, C.c_int32), C.byref(nc)))
         return out, nc.value

@@ -9,8 +9,9 @@
 // reading the file is not timed.
 //
 // Not in the reference: -d N selects the CUDA device, and -c keeps a binary
-// CSR cache beside the file (<file>.lvcsr, lv_write_csr): when the cache is
-// newer than the file it is read instead of parsing the text again.
+// CSR cache beside the file (<file>.lvcsr, lv_write_csr_stamped): the cache
+// records the text file's size and modification time (nanoseconds) and is
+// read instead of the text only while both still match the file.
 #include <getopt.h>
 #include <sys/stat.h>
 
@@ -26,13 +27,18 @@ static int read_graph(const char *file, bool use_cache, int32_t *V, int64_t *E, 
                       float **w) {
     if (!use_cache) return lv_read_mtx(file, V, E, rowptr, col, w, nullptr);
     const std::string cache = std::string(file) + ".lvcsr";
-    struct stat sf, sc;
-    if (stat(file, &sf) == 0 && stat(cache.c_str(), &sc) == 0 && sc.st_mtime >= sf.st_mtime &&
-        lv_read_csr(cache.c_str(), V, E, rowptr, col, w, nullptr) == LV_OK)
+    struct stat sf;
+    const bool have_stat = stat(file, &sf) == 0;
+    const int64_t size = have_stat ? (int64_t)sf.st_size : 0;
+    const int64_t mtime_ns = have_stat ? (int64_t)sf.st_mtim.tv_sec * 1000000000LL + sf.st_mtim.tv_nsec : 0;
+    int64_t c_size = 0, c_mtime = 0;
+    if (have_stat && lv_read_csr_stamp(cache.c_str(), &c_size, &c_mtime) == LV_OK && c_size == size &&
+        c_mtime == mtime_ns && lv_read_csr(cache.c_str(), V, E, rowptr, col, w, nullptr) == LV_OK)
         return LV_OK;
     float m_ref = 0;
     const int rc = lv_read_mtx(file, V, E, rowptr, col, w, &m_ref);
-    if (rc == LV_OK && lv_write_csr(cache.c_str(), *V, *E, *rowptr, *col, *w, m_ref) != LV_OK)
+    if (rc == LV_OK && have_stat &&
+        lv_write_csr_stamped(cache.c_str(), *V, *E, *rowptr, *col, *w, m_ref, size, mtime_ns) != LV_OK)
         std::fprintf(stderr, "gpulouvain: could not write the cache %s\n", cache.c_str());
     return rc;
 }

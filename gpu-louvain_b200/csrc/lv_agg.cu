@@ -178,8 +178,9 @@ __global__ void __launch_bounds__(256) merge_group_kernel(const int32_t *__restr
                                                           int32_t n, const int32_t *__restrict__ mstart,
                                                           const int32_t *__restrict__ P,
                                                           const int32_t *__restrict__ newid,
-                                                          int32_t *vkey, u64 *vw, int32_t *newdeg,
-                                                          int32_t *epos_new, int *err) {
+                                                          int32_t *vkey, u64 *vw, uint32_t *vw32,
+                                                          int32_t *newdeg, int32_t *epos_new, int *err,
+                                                          int *hiflag) {
     constexpr int GPB = 256 / G;
     constexpr int LG = (CAP == 64) ? 6 : (CAP == 128) ? 7 : 8;
     static_assert((1 << LG) == CAP, "CAP");
@@ -216,6 +217,7 @@ __global__ void __launch_bounds__(256) merge_group_kernel(const int32_t *__restr
     const int wl = threadIdx.x & 31;
     const unsigned gmask = (G == 32) ? FULL : (((1u << G) - 1u) << (wl & ~(G - 1)));
     int32_t cnt = 0;
+    u64 hi = 0;
 #pragma unroll
     for (int s0 = 0; s0 < CAP; s0 += G) {
         const int s = s0 + lane;
@@ -223,11 +225,15 @@ __global__ void __launch_bounds__(256) merge_group_kernel(const int32_t *__restr
         const unsigned bal = __ballot_sync(FULL, occ) & gmask;
         if (occ) {
             const int32_t pos = a + cnt + __popc(bal & ((1u << wl) - 1u));
+            const u64 x = vals[s];
             vkey[pos] = keys[s];
-            vw[pos] = vals[s];
+            vw[pos] = x;
+            vw32[pos] = (uint32_t)x;
+            if (keys[s] != self) hi |= x >> 32;   // the self-loop is read as uint64 only
         }
         cnt += __popc(bal);
     }
+    if (hi) atomicOr(hiflag, 1);
     if (active && lane == 0) {
         const int32_t nid = newid[c];
         newdeg[nid] = cnt;
@@ -240,12 +246,14 @@ __global__ void __launch_bounds__(T) merge_cta_kernel(const int32_t *__restrict_
                                                       const int32_t *__restrict__ mstart,
                                                       const int32_t *__restrict__ P,
                                                       const int32_t *__restrict__ newid,
-                                                      int32_t *vkey, u64 *vw, int32_t *newdeg,
-                                                      int32_t *epos_new, int *err) {
+                                                      int32_t *vkey, u64 *vw, uint32_t *vw32,
+                                                      int32_t *newdeg, int32_t *epos_new, int *err,
+                                                      int *hiflag) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     u64 *vals = reinterpret_cast<u64 *>(smem_raw);
     int32_t *keys = reinterpret_cast<int32_t *>(vals + CAPMAX);
     __shared__ int32_t cnt;
+    u64 hi = 0;
     for (int s = threadIdx.x; s < CAPMAX; s += T) { keys[s] = -1; vals[s] = 0; }
     if (threadIdx.x == 0) cnt = 0;
     __syncthreads();
@@ -269,8 +277,11 @@ __global__ void __launch_bounds__(T) merge_cta_kernel(const int32_t *__restrict_
             const int32_t key = keys[s];
             if (key >= 0) {
                 const int32_t pos = a + atomicAdd(&cnt, 1);
+                const u64 x = vals[s];
                 vkey[pos] = key;
-                vw[pos] = vals[s];
+                vw[pos] = x;
+                vw32[pos] = (uint32_t)x;
+                if (key != self) hi |= x >> 32;   // the self-loop is read as uint64 only
                 keys[s] = -1;
                 vals[s] = 0;
             }
@@ -284,6 +295,7 @@ __global__ void __launch_bounds__(T) merge_cta_kernel(const int32_t *__restrict_
         }
         __syncthreads();
     }
+    if (hi) atomicOr(hiflag, 1);
 }
 
 // Global-table merge for communities whose degree bound exceeds 4096: one CTA
@@ -335,23 +347,32 @@ __global__ void __launch_bounds__(HG_INSERT_THREADS) mergeg_insert_kernel(
 __global__ void __launch_bounds__(256) mergeg_emit_kernel(HubGlobal hg,
                                                           const int32_t *__restrict__ mstart,
                                                           const int32_t *__restrict__ P,
-                                                          int32_t *vkey, u64 *vw) {
+                                                          const int32_t *__restrict__ newid,
+                                                          int32_t *vkey, u64 *vw, uint32_t *vw32,
+                                                          int *hiflag) {
     const int32_t bidx = blockIdx.x;
     const int32_t h = hg.schunk_hub[bidx];
     const int32_t c = hg.hubs[h];
     const int32_t a = P[mstart[c]];
+    const int32_t self = newid[c];
     int32_t *keys = hg.keys + hg.tbl_off[h];
     u64 *vals = hg.vals + hg.tbl_off[h];
     const int32_t *occ = hg.occ + hg.occ_off[h];
     const int32_t s0 = hg.schunk_s0[bidx];
     const int32_t n = min(hg.nocc[h] - s0, HG_SLOT_CHUNK);
+    u64 hi = 0;
     for (int32_t i = threadIdx.x; i < n; i += 256) {
         const int32_t sl = occ[s0 + i];
-        vkey[a + s0 + i] = keys[sl];
-        vw[a + s0 + i] = vals[sl];
+        const int32_t key = keys[sl];
+        const u64 x = vals[sl];
+        vkey[a + s0 + i] = key;
+        vw[a + s0 + i] = x;
+        vw32[a + s0 + i] = (uint32_t)x;
+        if (key != self) hi |= x >> 32;   // the self-loop is read as uint64 only
         keys[sl] = -1;
         vals[sl] = 0;
     }
+    if (hi) atomicOr(hiflag, 1);
 }
 
 __global__ void mergeg_finish_kernel(HubGlobal hg, const int32_t *__restrict__ mstart,
@@ -455,36 +476,37 @@ void agg_new_vertices(const int32_t *size, const u64 *S, int32_t V, const AggBuf
 }
 
 void agg_merge_class(int acls, const AggBuffers &ab, const int32_t *P, const int32_t *list,
-                     int32_t n, int32_t *vkey, u64 *vw, int *err, int sms, cudaStream_t s) {
+                     int32_t n, int32_t *vkey, u64 *vw, uint32_t *vw32, int *err, int *hiflag, int sms,
+                     cudaStream_t s) {
     if (n <= 0) return;
     switch (acls) {
     case AC1:
         merge_group_kernel<8, 64><<<nblocks(n, 32), 256, 0, s>>>(list, n, ab.mstart, P, ab.flag, vkey,
-                                                                  vw, ab.newdeg, ab.epos_new, err); note_launches(1);
+                                                                  vw, vw32, ab.newdeg, ab.epos_new, err, hiflag); note_launches(1);
         break;
     case AC2:
         merge_group_kernel<32, 256><<<nblocks(n, 8), 256, 0, s>>>(list, n, ab.mstart, P, ab.flag, vkey,
-                                                                   vw, ab.newdeg, ab.epos_new, err); note_launches(1);
+                                                                   vw, vw32, ab.newdeg, ab.epos_new, err, hiflag); note_launches(1);
         break;
     case AC3:
         merge_cta_kernel<A3_T, A3_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a3), A3_T,
-                                         A3_CAP * 12, s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw,
-                                                           ab.newdeg, ab.epos_new, err); note_launches(1);
+                                         A3_CAP * 12, s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw, vw32,
+                                                           ab.newdeg, ab.epos_new, err, hiflag); note_launches(1);
         break;
     case AC4:
         merge_cta_kernel<A4_T, A4_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a4), A4_T,
-                                         A4_CAP * 12, s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw,
-                                                           ab.newdeg, ab.epos_new, err); note_launches(1);
+                                         A4_CAP * 12, s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw, vw32,
+                                                           ab.newdeg, ab.epos_new, err, hiflag); note_launches(1);
         break;
     default: break;
     }
 }
 
 void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *P, int32_t *vkey,
-                      u64 *vw, int *err, cudaStream_t s) {
+                      u64 *vw, uint32_t *vw32, int *err, int *hiflag, cudaStream_t s) {
     if (hg.nhubs <= 0) return;
     mergeg_insert_kernel<<<hg.n_echunks, HG_INSERT_THREADS, HG_INSERT_SMEM, s>>>(hg, ab.mstart, P, ab.flag, vkey, vw, err); note_launches(1);
-    mergeg_emit_kernel<<<hg.n_schunks, 256, 0, s>>>(hg, ab.mstart, P, vkey, vw); note_launches(1);
+    mergeg_emit_kernel<<<hg.n_schunks, 256, 0, s>>>(hg, ab.mstart, P, ab.flag, vkey, vw, vw32, hiflag); note_launches(1);
     mergeg_finish_kernel<<<grid_for(hg.nhubs), 256, 0, s>>>(hg, ab.mstart, P, ab.flag, ab.newdeg, ab.epos_new); note_launches(1);
 }
 

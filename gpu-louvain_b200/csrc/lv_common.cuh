@@ -121,11 +121,13 @@ __device__ __forceinline__ uint32_t table_hash(int32_t key, int lg) {
 // Weight access: level 0 reads float32 and maps it onto the fixed grid
 // (exact: w * 2^scale is a power-of-two scaling, then round-to-nearest-even,
 // the same rule as the host's llrint(ldexp(w, scale))); later levels read the
-// stored uint64 sums.
+// stored uint64 sums, or their 32-bit copy when every sum of the level is
+// below 2^32.
 __device__ __forceinline__ u64 wfix(const float *w, int64_t e, double scale) {
     return (u64)__double2ll_rn(__dmul_rn((double)__ldg(w + e), scale));
 }
 __device__ __forceinline__ u64 wfix(const u64 *w, int64_t e, double) { return __ldg(w + e); }
+__device__ __forceinline__ u64 wfix(const uint32_t *w, int64_t e, double) { return (u64)__ldg(w + e); }
 
 // A level's graph: row v is col/w[rowptr[v] .. rowend[v]).  Level 0 is a
 // plain CSR (rowend = rowptr + 1); aggregated levels keep each merged row
@@ -204,6 +206,49 @@ __device__ __forceinline__ int32_t table_insert_claim(int32_t *keys, u64 *vals, 
             int32_t prev = atomicCAS(keys + s, -1, key);
             if (prev < 0) { table_add(vals + s, w); return (int32_t)s; }
             if (prev == key) { table_add(vals + s, w); return -1; }
+        }
+        s = (s + 1u) & mask;
+    }
+    atomicOr(err, DEVERR_HASH_FULL);
+    return -1;
+}
+
+// Shared table whose sums are kept as two 32-bit counters of 16-bit pieces:
+// lo[s] sums w & 0xFFFF and hi[s] sums w >> 16 of weights below 2^32, so the
+// value hi * 2^16 + lo is the exact 64-bit sum as long as a slot takes at
+// most 65537 additions (a row or chunk of at most 65536 entries).  Both adds
+// are fire-and-forget shared atomics (no returned value to wait for, no
+// carry), which is what the move phase's rows need once weights fit 32 bits
+// (level 0 with a fixed-point grid below 2^32 and every aggregated level
+// whose merged sums, self-loops aside, stay below 2^32).
+struct PieceTable {
+    int32_t *keys;
+    uint32_t *lo;
+    uint32_t *hi;
+};
+constexpr int PIECE_MAX_ADDS = 65536;   // rows or chunks longer than this need 64-bit sums
+
+__device__ __forceinline__ void piece_add(const PieceTable &t, uint32_t s, u64 w) {
+    atomicAdd(t.lo + s, (uint32_t)w & 0xFFFFu);
+    atomicAdd(t.hi + s, (uint32_t)(w >> 16));
+}
+
+__device__ __forceinline__ u64 piece_value(const PieceTable &t, uint32_t s) {
+    return ((u64)t.hi[s] << 16) + (u64)t.lo[s];
+}
+
+// Insert (key, w) into a piece table (move-phase hash, linear probing,
+// bounded by the capacity); returns the slot newly claimed for key, or -1.
+__device__ __forceinline__ int32_t piece_insert(const PieceTable &t, int lg, int32_t key, u64 w, int *err) {
+    const uint32_t mask = (1u << lg) - 1u;
+    uint32_t s = hash_slot(key, lg);
+    for (uint32_t p = 0; p <= mask; ++p) {
+        const int32_t k = ((volatile int32_t *)t.keys)[s];
+        if (k == key) { piece_add(t, s, w); return -1; }
+        if (k < 0) {
+            const int32_t prev = atomicCAS(t.keys + s, -1, key);
+            if (prev < 0) { piece_add(t, s, w); return (int32_t)s; }
+            if (prev == key) { piece_add(t, s, w); return -1; }
         }
         s = (s + 1u) & mask;
     }
@@ -308,6 +353,46 @@ __device__ __forceinline__ void insert_row(const GraphView<WT> &g, const int32_t
                 table_insert_occ(keys, vals, lg, cc[u], ww[u], err, occ, nocc);
             } else {
                 table_insert(keys, vals, lg, cc[u], ww[u], err);
+            }
+        }
+    }
+}
+
+// insert_row for piece tables (weights below 2^32, at most PIECE_MAX_ADDS
+// entries): OCC records every newly claimed slot in occ[] (the first occ_cap
+// of them; *nocc counts them all).
+template <int U, bool OCC, typename WT>
+__device__ __forceinline__ void insert_row_piece(const GraphView<WT> &g, const int32_t *__restrict__ comm,
+                                                 int32_t v, int32_t own, int32_t r0, int32_t r1, int lane,
+                                                 int stride, const PieceTable &t, int lg, int *err,
+                                                 int32_t *occ, int32_t *nocc, int32_t occ_cap, u64 &e_own) {
+    for (int32_t base = r0 + lane; base < r1; base += U * stride) {
+        int32_t jj[U];
+        u64 ww[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int32_t e = base + u * stride;
+            jj[u] = -1;
+            ww[u] = 0;
+            if (e < r1) {
+                jj[u] = __ldg(g.col + e);
+                ww[u] = wfix(g.w, e, g.scale);
+            }
+        }
+        int32_t cc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(comm + jj[u]) : -1;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (cc[u] < 0) continue;
+            if (cc[u] == own) {
+                e_own += ww[u];
+            } else {
+                const int32_t claimed = piece_insert(t, lg, cc[u], ww[u], err);
+                if (OCC && claimed >= 0) {
+                    const int32_t i = atomicAdd(nocc, 1);
+                    if (i < occ_cap) occ[i] = claimed;
+                }
             }
         }
     }

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -31,9 +32,10 @@ void agg_permute(int cls, const GraphView<WT> &g, const AggBuffers &ab, const in
 void agg_new_vertices(const int32_t *size, const u64 *S, int32_t V, const AggBuffers &ab,
                       const int32_t *P, u64 *knew, cudaStream_t s);
 void agg_merge_class(int acls, const AggBuffers &ab, const int32_t *P, const int32_t *list,
-                     int32_t n, int32_t *vkey, u64 *vw, int *err, int sms, cudaStream_t s);
+                     int32_t n, int32_t *vkey, u64 *vw, uint32_t *vw32, int *err, int *hiflag, int sms,
+                     cudaStream_t s);
 void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *P, int32_t *vkey,
-                      u64 *vw, int *err, cudaStream_t s);
+                      u64 *vw, uint32_t *vw32, int *err, int *hiflag, cudaStream_t s);
 void agg_row_bounds(const AggBuffers &ab, int32_t Vn, int32_t *start, int32_t *end, cudaStream_t s);
 void launch_gather_degrees(const int32_t *rowptr, const int32_t *rowend, const int32_t *list,
                            int32_t n, int32_t *out, cudaStream_t s);
@@ -61,7 +63,8 @@ struct Totals {
 struct Pending {
     int kind;   // 0..NCLS-1 class, 100 move phase, 101 modularity, 102 aggregate, 103 setup
     cudaEvent_t a, b;
-    double bytes;
+    double bytes;    // algorithmic: 12 per edge + 20 per vertex
+    double sbytes;   // as stored: 8 + weight width per edge + 20 per vertex
     int64_t verts, edges;
 };
 
@@ -90,6 +93,7 @@ struct lv_handle {
     double scale_d = 1.0;
     u64 T = 0;
     int exact = 1;
+    bool w0_narrow = false;   // level-0 fixed-point weights are all below 2^32
 
     int level = 0;
     int32_t V = 0;
@@ -97,12 +101,17 @@ struct lv_handle {
     // current level: row v = cur_col/cur_w[cur_rowptr[v] .. cur_rowend[v])
     int32_t *cur_rowptr = nullptr, *cur_rowend = nullptr, *cur_col = nullptr;
     u64 *cur_w = nullptr;   // nullptr at level 0 (float input weights)
+    uint32_t *cur_w32 = nullptr;   // 32-bit copy of cur_w when every sum other than the
+                                   // self-loops is below 2^32; the move kernels (which
+                                   // skip self-loops) then read it, the modularity pass
+                                   // and the aggregation read cur_w
 
     // aggregated levels, ping-pong: rows stay where the merge wrote them
     int32_t *lvl_start[2] = {nullptr, nullptr};
     int32_t *lvl_end[2] = {nullptr, nullptr};
     int32_t *lvl_col[2] = {nullptr, nullptr};
     u64 *lvl_w[2] = {nullptr, nullptr};
+    uint32_t *lvl_w32[2] = {nullptr, nullptr};
     int cur_buf = -1;
 
     int32_t *comm = nullptr, *newc = nullptr, *size = nullptr, *orig2comm = nullptr;
@@ -291,7 +300,7 @@ struct Timer {
     lv_handle *h;
     int kind;
     cudaEvent_t a = nullptr;
-    double bytes = 0;
+    double bytes = 0, sbytes = 0;
     int64_t verts = 0, edges = 0;
     Timer(lv_handle *hh, int k) : h(hh), kind(k) {
         if (h->capturing) return;   // graph bodies hold no event nodes
@@ -302,7 +311,7 @@ struct Timer {
         if (!a) return;
         cudaEvent_t b = ev_get(h);
         cudaEventRecord(b, h->stream);
-        h->pend.push_back(Pending{kind, a, b, bytes, verts, edges});
+        h->pend.push_back(Pending{kind, a, b, bytes, sbytes, verts, edges});
     }
 };
 
@@ -314,6 +323,7 @@ void resolve_events(lv_handle *h) {
             h->cst.launches[p.kind] += 1;
             h->cst.ms[p.kind] += ms;
             h->cst.bytes[p.kind] += p.bytes;
+            h->cst.stored_bytes[p.kind] += p.sbytes;
             h->cst.vertices[p.kind] += p.verts;
             h->cst.edges[p.kind] += p.edges;
         } else if (p.kind == 100) {
@@ -358,6 +368,33 @@ GraphView<float> view_of<float>(lv_handle *h) {
 template <>
 GraphView<u64> view_of<u64>(lv_handle *h) {
     return GraphView<u64>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->cur_w, h->scale_d};
+}
+template <>
+GraphView<uint32_t> view_of<uint32_t>(lv_handle *h) {
+    return GraphView<uint32_t>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->cur_w32, h->scale_d};
+}
+
+// Calls F<WT>(args...) with the weight type the move phase reads at the
+// current level: float32 input at level 0, the 32-bit copy of the sums when
+// every sum other than the self-loops is below 2^32 (the move kernels skip
+// self-loops), the uint64 sums otherwise.
+#define LV_BY_WEIGHT(h, F, ...)                                  \
+    do {                                                         \
+        if ((h)->cur_w32) F<uint32_t>(__VA_ARGS__);              \
+        else if ((h)->cur_w) F<u64>(__VA_ARGS__);                \
+        else F<float>(__VA_ARGS__);                              \
+    } while (0)
+
+// Every weight the move phase reads is below 2^32: the 32-bit view of an
+// aggregated level, or level 0 when its fixed-point weights fit 32 bits
+// (the move kernels then keep their table sums in 16-bit-piece counters).
+// opts.wide_weights keeps 64-bit sums everywhere.
+template <typename WT>
+bool narrow_weights(const lv_handle *h) {
+    if (h->opts.wide_weights) return false;
+    if (std::is_same<WT, uint32_t>::value) return true;
+    if (std::is_same<WT, float>::value) return h->w0_narrow;
+    return false;
 }
 
 StateView state_of(lv_handle *h) {
@@ -602,13 +639,14 @@ void enqueue_sweep(lv_handle *h) {
             tc = new Timer(h, b);
             tc->verts = hg0 - lo;
             tc->edges = edges;
-            tc->bytes = (8.0 + wbytes) * (double)edges + 20.0 * (double)(hg0 - lo);
+            tc->bytes = 12.0 * (double)edges + 20.0 * (double)(hg0 - lo);
+            tc->sbytes = (8.0 + wbytes) * (double)edges + 20.0 * (double)(hg0 - lo);
         }
         if (b < 4)
-            launch_move_class<WT>(b, g, st, h->list + lo, hi - lo, h->di, dE, h->stream);
+            launch_move_class<WT>(b, g, st, h->list + lo, hi - lo, h->di, dE, h->stream, narrow_weights<WT>(h));
         else if (hg0 > lo)
             launch_move_wide<WT>(g, st, h->list + lo, hg0 - lo, h->fb, h->di, dE, h->stream,
-                                 b == 6 ? HG_MIN_DEG : (b == 4 ? 84 : 319));
+                                 b == 6 ? HG_MIN_DEG : (b == 4 ? 84 : 319), narrow_weights<WT>(h));
         if (tc) {
             tc->stop();
             delete tc;
@@ -619,9 +657,10 @@ void enqueue_sweep(lv_handle *h) {
                 tc = new Timer(h, 7);
                 tc->verts = hi - hg0;
                 tc->edges = h->cls_edges[CLS_HG];
-                tc->bytes = (8.0 + wbytes) * (double)tc->edges + 20.0 * (double)tc->verts;
+                tc->bytes = 12.0 * (double)tc->edges + 20.0 * (double)tc->verts;
+                tc->sbytes = (8.0 + wbytes) * (double)tc->edges + 20.0 * (double)tc->verts;
             }
-            launch_move_giants<WT>(g, st, h->hub_move.view, h->fb, h->di, dE, h->stream);
+            launch_move_giants<WT>(g, st, h->hub_move.view, h->fb, h->di, dE, h->stream, narrow_weights<WT>(h));
             if (tc) {
                 tc->stop();
                 delete tc;
@@ -634,7 +673,8 @@ void enqueue_sweep(lv_handle *h) {
         launch_commit(st, h->list + lo, hi - lo, &h->tot_d->moves, h->stream);
         sweep_verts += hi - lo;
     }
-    tm.bytes = (8.0 + wbytes) * (double)h->E + 20.0 * (double)sweep_verts;
+    tm.bytes = 12.0 * (double)h->E + 20.0 * (double)sweep_verts;
+    tm.sbytes = (8.0 + wbytes) * (double)h->E + 20.0 * (double)sweep_verts;
     tm.stop();
     h->st.move_bytes += tm.bytes;
 }
@@ -691,7 +731,7 @@ int sweep_and_q(lv_handle *h, int64_t *moves, double *q) {
         LV_TRY(modularity(h, &q0));
     }
     LV_TRY(reset_totals(h));
-    if (h->cur_w) enqueue_sweep<u64>(h); else enqueue_sweep<float>(h);
+    LV_BY_WEIGHT(h, enqueue_sweep, h);
     {
         Timer tm(h, 101);
         launch_s2(h->S, h->V, h->tot_d->s2, h->stream);
@@ -807,7 +847,7 @@ int sweep_loop_graph(lv_handle *h, float min_gain, double q_start, int *ch, int 
         if (ok) {
             h->capturing = true;
             cudaMemsetAsync(h->tot_d, 0, offsetof(Totals, err), h->stream);
-            if (h->cur_w) enqueue_sweep<u64>(h); else enqueue_sweep<float>(h);
+            LV_BY_WEIGHT(h, enqueue_sweep, h);
             launch_s2(h->S, h->V, h->tot_d->s2, h->stream);
             sweep_end_kernel<<<1, 32, 0, h->stream>>>(cond, h->tot_d, ld);
             note_launches(1);
@@ -901,14 +941,16 @@ void enqueue_sweep_active(lv_handle *h, const int32_t *cnt) {
         for (int c = c0; c < c1; ++c) any += cnt[c];
         if (!any) continue;
         if (b < 4) {
-            launch_move_class<WT>(b, g, st, h->alist + h->cls_off[b], cnt[b], h->di, dE, h->stream);
+            launch_move_class<WT>(b, g, st, h->alist + h->cls_off[b], cnt[b], h->di, dE, h->stream,
+                                  narrow_weights<WT>(h));
         } else {
             for (int c = c0; c < c1; ++c) {
                 if (c == CLS_HG || !cnt[c]) continue;
                 const int32_t maxdeg = c == CLS_B4 ? 84 : (c == CLS_B5 ? 319 : (c == CLS_H1 ? 1024 : HG_MIN_DEG));
-                launch_move_wide<WT>(g, st, h->alist + h->cls_off[c], cnt[c], h->fb, h->di, dE, h->stream, maxdeg);
+                launch_move_wide<WT>(g, st, h->alist + h->cls_off[c], cnt[c], h->fb, h->di, dE, h->stream, maxdeg,
+                                     narrow_weights<WT>(h));
             }
-            if (b == 6 && cnt[CLS_HG]) launch_move_giants<WT>(g, st, h->hub_move.view, h->fb, h->di, dE, h->stream);
+            if (b == 6 && cnt[CLS_HG]) launch_move_giants<WT>(g, st, h->hub_move.view, h->fb, h->di, dE, h->stream, narrow_weights<WT>(h));
         }
         for (int c = c0; c < c1; ++c)
             launch_correction<WT>(c, g, st, h->alist + h->cls_off[c], cnt[c], h->di, dE, h->stream);
@@ -953,11 +995,11 @@ int sweep_learned(lv_handle *h, bool full, bool predict, int64_t *moves, double 
     LV_CUDA(h, cudaMemcpyAsync(h->comm_prev, h->comm, sizeof(int32_t) * (size_t)h->V, cudaMemcpyDeviceToDevice,
                                h->stream));
     if (full) {
-        if (h->cur_w) enqueue_sweep<u64>(h); else enqueue_sweep<float>(h);
+        LV_BY_WEIGHT(h, enqueue_sweep, h);
         h->act_evaluated += n;
         h->act_full += 1;
     } else {
-        if (h->cur_w) enqueue_sweep_active<u64>(h, cnt); else enqueue_sweep_active<float>(h, cnt);
+        LV_BY_WEIGHT(h, enqueue_sweep_active, h, cnt);
         for (int c = 0; c < NCLS; ++c) h->act_evaluated += cnt[c];
         h->act_active += 1;
     }
@@ -1110,6 +1152,7 @@ int ensure_agg(lv_handle *h) {
         LV_TRY(dalloc(h, &h->lvl_end[b], V + 1));
         LV_TRY(dalloc(h, &h->lvl_col[b], E));
         LV_TRY(dalloc(h, &h->lvl_w[b], E));
+        LV_TRY(dalloc(h, &h->lvl_w32[b], E));
     }
     h->agg_ready = true;
     return LV_OK;
@@ -1124,6 +1167,8 @@ int aggregate_t(lv_handle *h) {
     const int nb = (h->cur_buf == 0) ? 1 : 0;
     int32_t *vkey = h->lvl_col[nb];
     u64 *vw = h->lvl_w[nb];
+    uint32_t *vw32 = h->lvl_w32[nb];
+    int32_t *hiflag = ab.scalars + 12;   // set when a merged sum is 2^32 or more
     agg_prepare(h->cur_rowptr, h->cur_rowend, h->comm, h->size, V, ab, h->mslot, h->degm, h->P,
                 h->stream);
     LV_CUDA(h, cudaMemcpyAsync(h->small_h, ab.scalars, sizeof(int32_t) * (2 + NAC),
@@ -1150,15 +1195,17 @@ int aggregate_t(lv_handle *h) {
         agg_permute<WT>(c, g, ab, h->mslot, h->P, h->list + h->cls_off[c],
                         h->cls_off[c + 1] - h->cls_off[c], vkey, vw, h->di.sms, h->stream);
     agg_new_vertices(h->size, h->S, V, ab, h->P, h->k, h->stream);
+    LV_CUDA(h, cudaMemsetAsync(hiflag, 0, sizeof(int32_t), h->stream));
     for (int c = 0; c < NAC - 1; ++c)
-        agg_merge_class(c, ab, h->P, ab.clist + aoff[c], aoff[c + 1] - aoff[c], vkey, vw,
-                        &h->tot_d->err, h->di.sms, h->stream);
-    agg_merge_global(h->hub_agg.view, ab, h->P, vkey, vw, &h->tot_d->err, h->stream);
+        agg_merge_class(c, ab, h->P, ab.clist + aoff[c], aoff[c + 1] - aoff[c], vkey, vw, vw32,
+                        &h->tot_d->err, hiflag, h->di.sms, h->stream);
+    agg_merge_global(h->hub_agg.view, ab, h->P, vkey, vw, vw32, &h->tot_d->err, hiflag, h->stream);
     agg_row_bounds(ab, newV, h->lvl_start[nb], h->lvl_end[nb], h->stream);
     // E' = number of stored entries (P is free again after the merges)
     scan_exclusive_i32(ab.newdeg, h->P, newV, h->P + newV, ab.scan_tmp, h->stream);
     LV_CUDA(h, cudaMemcpyAsync(h->small_h, h->P + newV, sizeof(int32_t), cudaMemcpyDeviceToHost,
                                h->stream));
+    LV_CUDA(h, cudaMemcpyAsync(h->small_h + 1, hiflag, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
     launch_compose_map(h->orig2comm, ab.flag, h->V0, h->stream);
     LV_CUDA(h, cudaMemcpyAsync(h->tot_h, h->tot_d, sizeof(Totals), cudaMemcpyDeviceToHost, h->stream));
     tm.stop();
@@ -1168,11 +1215,13 @@ int aggregate_t(lv_handle *h) {
                      h->st.aggregate_ms);
     LV_TRY(check_device_error(h, h->tot_h->err));
     const int64_t newE = h->small_h[0];
+    const bool wide = h->small_h[1] != 0;
     h->cur_buf = nb;
     h->cur_rowptr = h->lvl_start[nb];
     h->cur_rowend = h->lvl_end[nb];
     h->cur_col = h->lvl_col[nb];
     h->cur_w = h->lvl_w[nb];
+    h->cur_w32 = (wide || h->opts.wide_weights) ? nullptr : h->lvl_w32[nb];
     h->V = newV;
     h->E = newE;
     h->level += 1;
@@ -1196,6 +1245,7 @@ int to_level0(lv_handle *h) {
     h->cur_rowend = h->in_rowptr + 1;
     h->cur_col = h->in_col;
     h->cur_w = nullptr;
+    h->cur_w32 = nullptr;
     h->cur_buf = -1;
     h->e_own_valid = false;
     launch_iota_i32(h->orig2comm, h->V0, h->stream);
@@ -1271,6 +1321,8 @@ int finish_create(lv_handle *h) {
     if (s < 0) return fail(h, LV_ERR_TOO_LARGE, "total edge weight exceeds the fixed-point range");
     h->scale = s;
     h->exact = (s == need);
+    // every fixed-point weight is at most 2^(top + 1 + scale) (rounding included)
+    h->w0_narrow = !h->small_h[1] || top + 1 + s <= 31;
     h->scale_d = std::ldexp(1.0, s);
     u64 *tw = (u64 *)(h->tot_d);   // reuse e_own slot
     launch_total_weight(h->in_w, h->E0, h->scale_d, tw, h->stream);

@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -185,13 +186,15 @@ int parse_entries_parallel(const char *p, const char *end, long long nnz, bool p
     return LV_OK;
 }
 
-constexpr char CSR_MAGIC[8] = {'L', 'V', 'C', 'S', 'R', '0', '0', '1'};
+constexpr char CSR_MAGIC[8] = {'L', 'V', 'C', 'S', 'R', '0', '0', '2'};
 struct CsrHeader {
     char magic[8];
     int64_t V;
     int64_t E;
     float m_ref;
     uint32_t pad;
+    int64_t src_size;       // size of the file the CSR was read from (0: unknown)
+    int64_t src_mtime_ns;   // its modification time in nanoseconds (0: unknown)
 };
 
 }  // namespace
@@ -200,8 +203,8 @@ extern "C" {
 
 void lv_free_host(void *p) { std::free(p); }
 
-int lv_write_csr(const char *path, int32_t V, int64_t E, const int32_t *rowptr, const int32_t *col, const float *w,
-                 float m_ref) {
+int lv_write_csr_stamped(const char *path, int32_t V, int64_t E, const int32_t *rowptr, const int32_t *col,
+                         const float *w, float m_ref, int64_t src_size, int64_t src_mtime_ns) {
     if (!path || V < 0 || E < 0 || !rowptr || (E > 0 && (!col || !w))) return LV_ERR_INVALID;
     FILE *f = std::fopen(path, "wb");
     if (!f) return LV_ERR_IO;
@@ -210,12 +213,32 @@ int lv_write_csr(const char *path, int32_t V, int64_t E, const int32_t *rowptr, 
     h.V = V;
     h.E = E;
     h.m_ref = m_ref;
+    h.src_size = src_size;
+    h.src_mtime_ns = src_mtime_ns;
     bool ok = std::fwrite(&h, sizeof h, 1, f) == 1 &&
               std::fwrite(rowptr, sizeof(int32_t), (size_t)V + 1, f) == (size_t)V + 1 &&
               (E == 0 || (std::fwrite(col, sizeof(int32_t), (size_t)E, f) == (size_t)E &&
                           std::fwrite(w, sizeof(float), (size_t)E, f) == (size_t)E));
     ok = (std::fclose(f) == 0) && ok;
     return ok ? LV_OK : LV_ERR_IO;
+}
+
+int lv_write_csr(const char *path, int32_t V, int64_t E, const int32_t *rowptr, const int32_t *col, const float *w,
+                 float m_ref) {
+    return lv_write_csr_stamped(path, V, E, rowptr, col, w, m_ref, 0, 0);
+}
+
+int lv_read_csr_stamp(const char *path, int64_t *src_size, int64_t *src_mtime_ns) {
+    if (!path || !src_size || !src_mtime_ns) return LV_ERR_INVALID;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return LV_ERR_IO;
+    CsrHeader h;
+    const bool ok = std::fread(&h, sizeof h, 1, f) == 1 && std::memcmp(h.magic, CSR_MAGIC, 8) == 0;
+    std::fclose(f);
+    if (!ok) return LV_ERR_IO;
+    *src_size = h.src_size;
+    *src_mtime_ns = h.src_mtime_ns;
+    return LV_OK;
 }
 
 int lv_read_csr(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr, int32_t **col, float **w,
@@ -384,9 +407,12 @@ int lv_write_mtx(const char *path, int32_t V, int64_t n_edges, const int32_t *u,
     return rc == 0 ? LV_OK : LV_ERR_IO;
 }
 
-int lv_print_communities(const char *path, const int32_t *orig2comm, int32_t V0,
-                         int32_t num_communities) {
-    if (V0 < 0 || num_communities < 0 || (V0 > 0 && !orig2comm)) return LV_ERR_INVALID;
+// The lines of consecutive community ranges are formatted by all host
+// threads into their own buffers (ranges of about equal member counts), then
+// written in order.  Every buffer is allocated before the threads start, so
+// an allocation failure returns LV_ERR_NOMEM instead of ending the process.
+static int print_communities_impl(const char *path, const int32_t *orig2comm, int32_t V0,
+                                  int32_t num_communities) {
     // counting sort of the vertices by community (members in increasing id)
     std::vector<int64_t> start((size_t)num_communities + 1, 0);
     for (int32_t v = 0; v < V0; ++v) {
@@ -400,18 +426,22 @@ int lv_print_communities(const char *path, const int32_t *orig2comm, int32_t V0,
         std::vector<int64_t> pos(start.begin(), start.end() - 1);
         for (int32_t v = 0; v < V0; ++v) mem[(size_t)pos[(size_t)orig2comm[v]]++] = v;
     }
-    FILE *f = path ? std::fopen(path, "w") : stdout;
-    if (!f) return LV_ERR_IO;
-    // the lines of consecutive community ranges are formatted by all host
-    // threads into their own buffers (ranges of about equal member counts),
-    // then written in order
-    const int T = omp_get_max_threads();
-    const int64_t per = ((int64_t)V0 + num_communities) / (T > 0 ? T : 1) + 1;
+    const int T = omp_get_max_threads() > 0 ? omp_get_max_threads() : 1;
+    const int64_t per = ((int64_t)V0 + num_communities) / T + 1;
     std::vector<int32_t> cut((size_t)T + 1, num_communities);
     cut[0] = 0;
     for (int t = 1, c = 0; t < T; ++t) {
         while (c < num_communities && start[(size_t)c] + c < per * t) ++c;
         cut[(size_t)t] = c;
+    }
+    // at most 11 characters per number plus a separator
+    std::vector<std::unique_ptr<char[]>> buf((size_t)T);
+    for (int t = 0; t < T; ++t) {
+        const int32_t c0 = cut[(size_t)t], c1 = cut[(size_t)t + 1];
+        if (c1 <= c0) continue;
+        buf[(size_t)t].reset(new (std::nothrow)
+                                 char[(size_t)(start[(size_t)c1] - start[(size_t)c0] + (c1 - c0)) * 12]);
+        if (!buf[(size_t)t]) return LV_ERR_NOMEM;
     }
     // decimal digits of x >= 0 at p; returns the end
     auto put_int = [](char *p, int64_t x) {
@@ -424,14 +454,11 @@ int lv_print_communities(const char *path, const int32_t *orig2comm, int32_t V0,
         while (n > 0) *p++ = tmp[--n];
         return p;
     };
-    std::vector<std::unique_ptr<char[]>> buf((size_t)T);
     std::vector<size_t> len((size_t)T, 0);
 #pragma omp parallel for num_threads(T) schedule(static, 1)
     for (int t = 0; t < T; ++t) {
         const int32_t c0 = cut[(size_t)t], c1 = cut[(size_t)t + 1];
         if (c1 <= c0) continue;
-        // at most 11 characters per number plus a separator
-        buf[(size_t)t].reset(new char[(size_t)(start[(size_t)c1] - start[(size_t)c0] + (c1 - c0)) * 12]);
         char *const o = buf[(size_t)t].get();
         char *q = o;
         for (int32_t c = c0; c < c1; ++c) {
@@ -444,6 +471,8 @@ int lv_print_communities(const char *path, const int32_t *orig2comm, int32_t V0,
         }
         len[(size_t)t] = (size_t)(q - o);
     }
+    FILE *f = path ? std::fopen(path, "w") : stdout;
+    if (!f) return LV_ERR_IO;
     char head[32];
     char *he = put_int(head, num_communities);
     *he++ = '\n';
@@ -453,6 +482,16 @@ int lv_print_communities(const char *path, const int32_t *orig2comm, int32_t V0,
     std::fflush(f);
     if (path) ok = (std::fclose(f) == 0) && ok;
     return ok ? LV_OK : LV_ERR_IO;
+}
+
+int lv_print_communities(const char *path, const int32_t *orig2comm, int32_t V0,
+                         int32_t num_communities) {
+    if (V0 < 0 || num_communities < 0 || (V0 > 0 && !orig2comm)) return LV_ERR_INVALID;
+    try {
+        return print_communities_impl(path, orig2comm, V0, num_communities);
+    } catch (const std::bad_alloc &) {
+        return LV_ERR_NOMEM;
+    }
 }
 
 }  // extern "C"

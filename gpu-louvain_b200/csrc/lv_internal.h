@@ -130,7 +130,9 @@ struct FallbackSet {
 struct DeviceInfo {
     int sms = 148;
     int occ_warp = 4;   // resident CTAs per SM of the warp kernel
+    int occ_warp_narrow = 4;   // ... of its narrow-weight form
     int occ_fbq[NFBQ] = {1, 1, 1, 1};   // ... of the row fallback kernels
+    int occ_fbq_narrow[NFBQ] = {1, 1, 1, 1};   // ... and of their narrow-weight form
     int occ_merge_s = 1;                 // ... of the small giant-merge kernel
 };
 void init_kernel_attributes(DeviceInfo &di);
@@ -140,16 +142,17 @@ void init_kernel_attributes(DeviceInfo &di);
 // Classes B0..B3 (degree <= 32): group kernels.
 template <typename WT>
 void launch_move_class(int cls, const GraphView<WT> &g, const StateView &st, const int32_t *list,
-                       int32_t n, const DeviceInfo &di, u64 *dE, cudaStream_t s);
+                       int32_t n, const DeviceInfo &di, u64 *dE, cudaStream_t s, bool narrow);
 // 32 < degree <= 8192 (the vertices of one update bucket): warp kernel +
 // fallback.  Degree > 8192: staged chunks + merge (hg describes the giants).
+// narrow: every weight the kernels read is below 2^32 (piece-counter tables).
 template <typename WT>
 void launch_move_wide(const GraphView<WT> &g, const StateView &st, const int32_t *list, int32_t n,
                       const FallbackSet &fb, const DeviceInfo &di, u64 *dE, cudaStream_t s,
-                      int32_t max_degree);
+                      int32_t max_degree, bool narrow);
 template <typename WT>
 void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGlobal &hg,
-                        const FallbackSet &fb, const DeviceInfo &di, u64 *dE, cudaStream_t s);
+                        const FallbackSet &fb, const DeviceInfo &di, u64 *dE, cudaStream_t s, bool narrow);
 // Exact correction of dE for neighbours that moved in the same sub-round.
 template <typename WT>
 void launch_correction(int cls, const GraphView<WT> &g, const StateView &st, const int32_t *list,

@@ -79,6 +79,62 @@ __global__ void __launch_bounds__(256) move_group_kernel(GraphView<WT> g, StateV
     block_add_total<256>(delta, dE);
 }
 
+// move_group_kernel for weights below 2^32: the group's table keeps its sums
+// in 16-bit-piece counters (fire-and-forget adds).
+template <int G, int CAP, typename WT>
+__global__ void __launch_bounds__(256) move_group_narrow_kernel(GraphView<WT> g, StateView st,
+                                                                const int32_t *__restrict__ list,
+                                                                int32_t n, u64 *dE) {
+    constexpr int GPB = 256 / G;
+    constexpr int LG = ilog2_c(CAP);
+    static_assert((1 << LG) == CAP, "CAP must be a power of two");
+    __shared__ uint32_t slo[GPB * CAP], shi[GPB * CAP];
+    __shared__ int32_t skeys[GPB * CAP];
+    const int grp = threadIdx.x / G;
+    const int lane = threadIdx.x % G;
+    const int idx = blockIdx.x * GPB + grp;
+    PieceTable t;
+    t.keys = skeys + grp * CAP;
+    t.lo = slo + grp * CAP;
+    t.hi = shi + grp * CAP;
+#pragma unroll
+    for (int s = lane; s < CAP; s += G) { t.keys[s] = -1; t.lo[s] = 0; t.hi[s] = 0; }
+    __syncwarp();
+    const bool active = idx < n;
+    int32_t v = 0, own = 0;
+    u64 e_own = 0;
+    if (active) {
+        v = list[idx];
+        own = __ldg(st.comm + v);
+        insert_row_piece<(CAP > 32 ? LV_U_CTA : LV_U_GROUP), false>(g, st.comm, v, own, g.rowptr[v], g.rowend[v],
+                                                                     lane, G, t, LG, st.err, nullptr, nullptr, 0,
+                                                                     e_own);
+    }
+    __syncwarp();
+    const MoveCtx m = move_ctx(own, active ? __ldg(st.size + own) == 1 : false, st.T,
+                               active ? __ldg(st.k + v) : 0, active ? __ldg(st.S + own) : 0);
+    Best b = best_init(own);
+    b.eo = e_own;
+    if (active) {
+#pragma unroll
+        for (int s = lane; s < CAP; s += G) {
+            const int32_t c = t.keys[s];
+            if (c < 0) continue;
+            const bool cand = c != own;
+            const u64 Sc = cand ? __ldg(st.S + c) : 0;
+            const int32_t szc = (cand && guard_needs_size(m, c)) ? __ldg(st.size + c) : 0;
+            eval_loaded(c, piece_value(t, (uint32_t)s), Sc, szc, m, b);
+        }
+    }
+    group_reduce_best(m, b, G);
+    u64 delta = 0;
+    if (active && lane == 0) {
+        st.newc[v] = move_decision(m, b, &delta);
+        record_features(st, v, m, b);
+    }
+    block_add_total<256>(delta, dE);
+}
+
 // CTA-wide reduction of a Best; the result is valid in thread 0.
 template <int THREADS>
 __device__ __forceinline__ void cta_reduce_best(const MoveCtx &m, Best &b) {
@@ -269,6 +325,141 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
     if (lane == 0 && delta_acc) atomicAdd(dE, delta_acc);
 }
 
+// The warp kernel for weights below 2^32 (see PieceTable): the same work
+// mapping and overflow rule as move_warp_kernel, with the table sums kept in
+// 16-bit-piece counters (fire-and-forget adds, no carry) and the claimed slots
+// listed, so that evaluation and clearing visit only the vertex's distinct
+// neighbour communities (a few dozen on aggregated levels) instead of the
+// whole table.  A vertex with more than WARP_OCC_CAP distinct communities is
+// evaluated over the whole table.
+constexpr int WARP_OCC_CAP = 128;
+constexpr int WARP_NSMEM = 8 * (WARP_CAP * 12 + WARP_OCC_CAP * 4 + 16);
+
+template <typename WT>
+__global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, StateView st,
+                                                               const int32_t *__restrict__ list, int32_t n,
+                                                               FallbackSet fs, u64 *dE) {
+    constexpr int NW = 8;
+    constexpr int LG = ilog2_c(WARP_CAP);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char *base = smem_raw + (size_t)wid * (WARP_CAP * 12 + WARP_OCC_CAP * 4 + 16);
+    PieceTable t;
+    t.lo = reinterpret_cast<uint32_t *>(base);
+    t.hi = t.lo + WARP_CAP;
+    t.keys = reinterpret_cast<int32_t *>(t.hi + WARP_CAP);
+    int32_t *occ = t.keys + WARP_CAP;
+    int32_t *nocc = occ + WARP_OCC_CAP;
+    for (int s = lane; s < WARP_CAP; s += 32) { t.keys[s] = -1; t.lo[s] = 0; t.hi[s] = 0; }
+    if (lane == 0) *nocc = 0;
+    __syncwarp();
+    u64 delta_acc = 0;
+    const int32_t nwarps = gridDim.x * NW;
+    int32_t idx = blockIdx.x * NW + wid;
+    int32_t nv = 0, nr0 = 0, nr1 = 0, nown = 0;
+    if (idx < n) {
+        nv = list[idx];
+        nr0 = g.rowptr[nv];
+        nr1 = g.rowend[nv];
+        nown = __ldg(st.comm + nv);
+    }
+    for (; idx < n; idx += nwarps) {
+        const int32_t v = nv, r0 = nr0, r1 = nr1, own = nown;
+        if (idx + nwarps < n) {
+            nv = list[idx + nwarps];
+            nr0 = g.rowptr[nv];
+            nr1 = g.rowend[nv];
+            nown = __ldg(st.comm + nv);
+        }
+        const int32_t d = r1 - r0;
+        if (d > WARP_LIMIT && fs.hint[v]) {
+            if (lane == 0) enqueue_fallback(fs, v, d, st.err);
+            continue;
+        }
+        const int32_t sz_own = __ldg(st.size + own);
+        const u64 k_v = __ldg(st.k + v), s_own = __ldg(st.S + own);
+        int lg = ceil_log2_i(2 * (int64_t)d);
+        lg = lg < 5 ? 5 : (lg > LG ? LG : lg);
+        u64 e_own = 0;
+        bool overflow = false;
+        // U chunks of 32 edges per step; the claim count is read after every
+        // step, so at most WARP_LIMIT + 32 U slots are ever claimed
+        constexpr int U = LV_U_WARP;
+        for (int32_t b0 = r0 + lane; b0 < r1 + lane; b0 += 32 * U) {
+            int32_t jj[U];
+            u64 ww[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int32_t e = b0 + 32 * u;
+                jj[u] = -1;
+                ww[u] = 0;
+                if (e < r1) { jj[u] = __ldg(g.col + e); ww[u] = wfix(g.w, e, g.scale); }
+            }
+            int32_t cc[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(st.comm + jj[u]) : -1;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (cc[u] < 0) continue;
+                if (cc[u] == own) {
+                    e_own += ww[u];
+                } else {
+                    const int32_t claimed = piece_insert(t, lg, cc[u], ww[u], st.err);
+                    if (claimed >= 0) {
+                        const int32_t i = atomicAdd(nocc, 1);
+                        if (i < WARP_OCC_CAP) occ[i] = claimed;
+                    }
+                }
+            }
+            __syncwarp();
+            if (*nocc > WARP_LIMIT) { overflow = true; break; }
+        }
+        __syncwarp();
+        const int nslots = 1 << lg;
+        const int32_t nd = *nocc;
+        __syncwarp();
+        if (lane == 0) *nocc = 0;
+        if (overflow) {
+            for (int s2 = lane; s2 < nslots; s2 += 32) {
+                if (t.keys[s2] >= 0) { t.keys[s2] = -1; t.lo[s2] = 0; t.hi[s2] = 0; }
+            }
+            if (lane == 0) {
+                fs.hint[v] = 1;
+                enqueue_fallback(fs, v, d, st.err);
+            }
+            __syncwarp();
+            continue;
+        }
+        const MoveCtx m = move_ctx(own, sz_own == 1, st.T, k_v, s_own);
+        Best b = best_init(own);
+        b.eo = e_own;
+        const bool listed = nd <= WARP_OCC_CAP;
+        const int32_t nscan = listed ? nd : nslots;
+        for (int32_t i = lane; i < nscan; i += 32) {
+            const int32_t sl = listed ? occ[i] : i;
+            const int32_t c = t.keys[sl];
+            if (c < 0) continue;
+            const u64 ec = piece_value(t, (uint32_t)sl);
+            t.keys[sl] = -1;
+            t.lo[sl] = 0;
+            t.hi[sl] = 0;
+            const bool cand = c != own;
+            const u64 Sc = cand ? __ldg(st.S + c) : 0;
+            const int32_t szc = (cand && guard_needs_size(m, c)) ? __ldg(st.size + c) : 0;
+            eval_loaded(c, ec, Sc, szc, m, b);
+        }
+        group_reduce_best(m, b, 32);
+        if (lane == 0) {
+            u64 delta = 0;
+            st.newc[v] = move_decision(m, b, &delta);
+            record_features(st, v, m, b);
+            delta_acc += delta;
+        }
+        __syncwarp();
+    }
+    if (lane == 0 && delta_acc) atomicAdd(dE, delta_acc);
+}
+
 // Fallback CTAs.  PART = false: items are whole rows of degree <= CAP / 2
 // (small and medium queues).  PART = true: key-space partitions of a row or
 // of a giant's staged pairs (large queue).  The occupied list holds CAP / 2
@@ -392,6 +583,70 @@ __global__ void __launch_bounds__(THREADS) move_fallback_kernel(GraphView<WT> g,
     if (threadIdx.x == 0 && delta_acc) atomicAdd(dE, delta_acc);
 }
 
+// The row queues' fallback CTAs for weights below 2^32: whole rows of degree
+// <= CAP / 2 in a piece table (fire-and-forget adds), evaluated over the
+// claimed-slot list.
+template <typename WT, int THREADS, int CAP>
+__global__ void __launch_bounds__(THREADS) move_rowq_narrow_kernel(GraphView<WT> g, StateView st, Fallback fb,
+                                                                   uint8_t *hint, u64 *dE) {
+    constexpr int OCC_CAP = CAP / 2;
+    static_assert(OCC_CAP <= PIECE_MAX_ADDS, "rows of the queue fit the piece counters");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PieceTable t;
+    t.lo = reinterpret_cast<uint32_t *>(smem_raw);
+    t.hi = t.lo + CAP;
+    t.keys = reinterpret_cast<int32_t *>(t.hi + CAP);
+    int32_t *occ = t.keys + CAP;
+    __shared__ int32_t nocc, item_sh;
+    for (int s = threadIdx.x; s < CAP; s += THREADS) { t.keys[s] = -1; t.lo[s] = 0; t.hi[s] = 0; }
+    if (threadIdx.x == 0) nocc = 0;
+    __syncthreads();
+    const int32_t count = min(*fb.count, fb.cap);
+    u64 delta_acc = 0;
+    for (;;) {
+        if (threadIdx.x == 0) item_sh = atomicAdd(fb.next, 1);
+        __syncthreads();
+        const int32_t item = item_sh;
+        if (item >= count) break;
+        const int32_t v = fb.v[item];
+        const int32_t own = __ldg(st.comm + v);
+        const int32_t r0 = g.rowptr[v], r1 = g.rowend[v];
+        int lg = ceil_log2_i(2 * (int64_t)(r1 - r0));
+        lg = lg < 3 ? 3 : lg;
+        u64 e_own = 0;
+        insert_row_piece<LV_U_FB, true>(g, st.comm, v, own, r0, r1, threadIdx.x, THREADS, t, lg, st.err, occ,
+                                        &nocc, OCC_CAP, e_own);
+        __syncthreads();
+        const int32_t nd = min(nocc, OCC_CAP);
+        const MoveCtx m = move_ctx(own, __ldg(st.size + own) == 1, st.T, __ldg(st.k + v), __ldg(st.S + own));
+        Best b = best_init(own);
+        b.eo = e_own;
+        for (int32_t i = threadIdx.x; i < nd; i += THREADS) {
+            const int32_t sl = occ[i];
+            const int32_t c = t.keys[sl];
+            const u64 ec = piece_value(t, (uint32_t)sl);
+            t.keys[sl] = -1;
+            t.lo[sl] = 0;
+            t.hi[sl] = 0;
+            const bool cand = c != own;
+            const u64 Sc = cand ? __ldg(st.S + c) : 0;
+            const int32_t szc = (cand && guard_needs_size(m, c)) ? __ldg(st.size + c) : 0;
+            eval_loaded(c, ec, Sc, szc, m, b);
+        }
+        cta_reduce_best<THREADS>(m, b);
+        if (threadIdx.x == 0) {
+            nocc = 0;
+            u64 delta = 0;
+            st.newc[v] = move_decision(m, b, &delta);
+            record_features(st, v, m, b);
+            delta_acc += delta;
+            hint[v] = nd > HINT_SET ? 1 : 0;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && delta_acc) atomicAdd(dE, delta_acc);
+}
+
 // ------------------------------------------------------------------------
 // giants (degree > 8192): staged two-level reduction
 // ------------------------------------------------------------------------
@@ -403,6 +658,47 @@ __global__ void __launch_bounds__(THREADS) move_fallback_kernel(GraphView<WT> g,
 //     decide its move; a giant with more staged pairs than the table holds
 //     is queued as key-space partitions of its staged pairs (fallback items
 //     with src = h), which the fallback kernel then decides.
+// giant_stage_kernel for weights below 2^32: the chunk's table keeps its sums
+// in 16-bit-piece counters (fire-and-forget adds; a chunk has STAGE_CHUNK
+// entries, far below PIECE_MAX_ADDS).
+template <typename WT>
+__global__ void __launch_bounds__(STAGE_THREADS) giant_stage_narrow_kernel(GraphView<WT> g, StateView st,
+                                                                           HubGlobal hg) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int LCAP = 2 * STAGE_CHUNK;
+    constexpr int LLG = ilog2_c(LCAP);
+    static_assert(STAGE_CHUNK <= PIECE_MAX_ADDS, "chunks fit the piece counters");
+    PieceTable t;
+    t.lo = reinterpret_cast<uint32_t *>(smem_raw);
+    t.hi = t.lo + LCAP;
+    t.keys = reinterpret_cast<int32_t *>(t.hi + LCAP);
+    int32_t *locc = t.keys + LCAP;
+    __shared__ int32_t lnocc, base;
+    for (int s = threadIdx.x; s < LCAP; s += STAGE_THREADS) { t.keys[s] = -1; t.lo[s] = 0; t.hi[s] = 0; }
+    if (threadIdx.x == 0) lnocc = 0;
+    __syncthreads();
+    const int32_t h = hg.echunk_hub[blockIdx.x];
+    const int32_t v = hg.hubs[h];
+    const int32_t r1 = g.rowend[v];
+    const int32_t e0 = g.rowptr[v] + hg.echunk_e0[blockIdx.x];
+    const int32_t e1 = min(e0 + STAGE_CHUNK, r1);
+    const int32_t own = __ldg(st.comm + v);
+    u64 e_own = 0;
+    insert_row_piece<LV_U_STAGE, true>(g, st.comm, v, own, e0, e1, threadIdx.x, STAGE_THREADS, t, LLG, st.err,
+                                       locc, &lnocc, STAGE_CHUNK, e_own);
+    block_add_total<STAGE_THREADS>(e_own, hg.eown + h);   // contains the barrier
+    const int32_t n = lnocc;
+    if (threadIdx.x == 0) base = atomicAdd(hg.nocc + h, n);
+    __syncthreads();
+    int32_t *sk = hg.stage_key + hg.occ_off[h] + base;
+    u64 *sv = hg.stage_val + hg.occ_off[h] + base;
+    for (int32_t i = threadIdx.x; i < n; i += STAGE_THREADS) {
+        const int32_t sl = locc[i];
+        sk[i] = t.keys[sl];
+        sv[i] = piece_value(t, (uint32_t)sl);
+    }
+}
+
 template <typename WT>
 __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_kernel(GraphView<WT> g, StateView st,
                                                                     HubGlobal hg) {
@@ -717,17 +1013,24 @@ template <typename WT, int B>
 static void set_row_queue_attrs(DeviceInfo &di) {
     constexpr int T = FBQ_THREADS(B), CAP = 2 * FBQ_MAXDEG(B), SM = FBQ_SMEM(B);
     cudaFuncSetAttribute(move_fallback_kernel<WT, T, CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+    cudaFuncSetAttribute(move_rowq_narrow_kernel<WT, T, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
     int o = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_fallback_kernel<WT, T, CAP, false>, T, SM);
     di.occ_fbq[B] = o > 0 ? o : 1;
+    o = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_rowq_narrow_kernel<WT, T, CAP>, T, SM);
+    di.occ_fbq_narrow[B] = o > 0 ? o : 1;
 }
 
 template <typename WT, int B>
 static void launch_row_queue(const GraphView<WT> &g, const StateView &st, const FallbackSet &fs,
-                             const DeviceInfo &di, u64 *dE, cudaStream_t s) {
+                             const DeviceInfo &di, u64 *dE, cudaStream_t s, bool narrow) {
     constexpr int T = FBQ_THREADS(B), CAP = 2 * FBQ_MAXDEG(B), SM = FBQ_SMEM(B);
-    move_fallback_kernel<WT, T, CAP, false><<<di.sms * di.occ_fbq[B], T, SM, s>>>(g, st, fs.q[B], HubGlobal(),
-                                                                                fs.hint, dE);
+    if (narrow)
+        move_rowq_narrow_kernel<WT, T, CAP><<<di.sms * di.occ_fbq_narrow[B], T, SM, s>>>(g, st, fs.q[B], fs.hint, dE);
+    else
+        move_fallback_kernel<WT, T, CAP, false><<<di.sms * di.occ_fbq[B], T, SM, s>>>(g, st, fs.q[B], HubGlobal(),
+                                                                                    fs.hint, dE);
     note_launches(1);
 }
 
@@ -740,10 +1043,15 @@ static void set_attrs_for(DeviceInfo &di) {
     cudaFuncSetAttribute(move_fallback_kernel<WT, FB_THREADS, FB_CAP, true>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM);
     cudaFuncSetAttribute(giant_stage_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM);
+    cudaFuncSetAttribute(giant_stage_narrow_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM);
     cudaFuncSetAttribute(move_warp_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_SMEM);
+    cudaFuncSetAttribute(move_warp_narrow_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_NSMEM);
     int o = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_warp_kernel<WT>, 256, WARP_SMEM);
     di.occ_warp = o > 0 ? o : 1;
+    o = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_warp_narrow_kernel<WT>, 256, WARP_NSMEM);
+    di.occ_warp_narrow = o > 0 ? o : 1;
 }
 
 void init_kernel_attributes(DeviceInfo &di) {
@@ -751,6 +1059,7 @@ void init_kernel_attributes(DeviceInfo &di) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&di.sms, cudaDevAttrMultiProcessorCount, dev);
     set_attrs_for<u64>(di);
+    set_attrs_for<uint32_t>(di);
     set_attrs_for<float>(di);
     cudaFuncSetAttribute(giant_merge_kernel<HG_MERGE_THREADS, HG_MERGE_CAP>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, HG_MERGE_SMEM);
@@ -764,15 +1073,22 @@ void init_kernel_attributes(DeviceInfo &di) {
 
 template <typename WT>
 void launch_move_class(int cls, const GraphView<WT> &g, const StateView &st, const int32_t *list,
-                       int32_t n, const DeviceInfo &di, u64 *dE, cudaStream_t s) {
+                       int32_t n, const DeviceInfo &di, u64 *dE, cudaStream_t s, bool narrow) {
     if (n <= 0) return;
+#define LV_GROUP(G, CAP)                                                                              \
+    do {                                                                                              \
+        if (narrow) move_group_narrow_kernel<G, CAP, WT><<<nblocks(n, 256 / G), 256, 0, s>>>(g, st, list, n, dE); \
+        else move_group_kernel<G, CAP, WT><<<nblocks(n, 256 / G), 256, 0, s>>>(g, st, list, n, dE);   \
+        note_launches(1);                                                                             \
+    } while (0)
     switch (cls) {
-    case CLS_B0: move_group_kernel<4, 8, WT><<<nblocks(n, 64), 256, 0, s>>>(g, st, list, n, dE); note_launches(1); break;
-    case CLS_B1: move_group_kernel<8, 16, WT><<<nblocks(n, 32), 256, 0, s>>>(g, st, list, n, dE); note_launches(1); break;
-    case CLS_B2: move_group_kernel<16, 32, WT><<<nblocks(n, 16), 256, 0, s>>>(g, st, list, n, dE); note_launches(1); break;
-    case CLS_B3: move_group_kernel<32, 64, WT><<<nblocks(n, 8), 256, 0, s>>>(g, st, list, n, dE); note_launches(1); break;
+    case CLS_B0: LV_GROUP(4, 8); break;
+    case CLS_B1: LV_GROUP(8, 16); break;
+    case CLS_B2: LV_GROUP(16, 32); break;
+    case CLS_B3: LV_GROUP(32, 64); break;
     default: break;
     }
+#undef LV_GROUP
 }
 
 template <typename WT>
@@ -785,10 +1101,12 @@ static void launch_fallback_large(const GraphView<WT> &g, const StateView &st, c
 
 template <typename WT>
 void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGlobal &hg,
-                        const FallbackSet &fs, const DeviceInfo &di, u64 *dE, cudaStream_t s) {
+                        const FallbackSet &fs, const DeviceInfo &di, u64 *dE, cudaStream_t s, bool narrow) {
     if (hg.nhubs <= 0) return;
     cudaMemsetAsync(fs.q[NFBQ].count, 0, 2 * sizeof(int32_t), s);   // count, next
-    giant_stage_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg); note_launches(1);
+    if (narrow) giant_stage_narrow_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg);
+    else giant_stage_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg);
+    note_launches(1);
 #if LV_MERGE_SMALL
     giant_merge_kernel<MERGE_S_THREADS, MERGE_S_CAP>
         <<<(unsigned)imin64(hg.nhubs, (int64_t)di.sms * di.occ_merge_s), MERGE_S_THREADS, MERGE_S_CAP * 14, s>>>(
@@ -808,18 +1126,24 @@ void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGl
 template <typename WT>
 void launch_move_wide(const GraphView<WT> &g, const StateView &st, const int32_t *list, int32_t n,
                       const FallbackSet &fs, const DeviceInfo &di, u64 *dE, cudaStream_t s,
-                      int32_t max_degree) {
+                      int32_t max_degree, bool narrow) {
     if (n <= 0) return;
     // the queues' (count, next) pairs are contiguous
     cudaMemsetAsync(fs.q[0].count, 0, 2 * (NFBQ + 1) * sizeof(int32_t), s);
-    const unsigned grid = (unsigned)imin64((n + 7) / 8, (int64_t)di.sms * di.occ_warp);
-    move_warp_kernel<WT><<<grid, 256, WARP_SMEM, s>>>(g, st, list, n, fs, dE); note_launches(1);
+    if (narrow) {
+        const unsigned grid = (unsigned)imin64((n + 7) / 8, (int64_t)di.sms * di.occ_warp_narrow);
+        move_warp_narrow_kernel<WT><<<grid, 256, WARP_NSMEM, s>>>(g, st, list, n, fs, dE);
+    } else {
+        const unsigned grid = (unsigned)imin64((n + 7) / 8, (int64_t)di.sms * di.occ_warp);
+        move_warp_kernel<WT><<<grid, 256, WARP_SMEM, s>>>(g, st, list, n, fs, dE);
+    }
+    note_launches(1);
     if (max_degree <= WARP_LIMIT) return;   // no vertex can overflow its warp table
     launch_fallback_large<WT>(g, st, HubGlobal(), fs, di, dE, s);
-    launch_row_queue<WT, 3>(g, st, fs, di, dE, s);
-    launch_row_queue<WT, 2>(g, st, fs, di, dE, s);
-    launch_row_queue<WT, 1>(g, st, fs, di, dE, s);
-    launch_row_queue<WT, 0>(g, st, fs, di, dE, s);
+    launch_row_queue<WT, 3>(g, st, fs, di, dE, s, narrow);
+    launch_row_queue<WT, 2>(g, st, fs, di, dE, s, narrow);
+    launch_row_queue<WT, 1>(g, st, fs, di, dE, s, narrow);
+    launch_row_queue<WT, 0>(g, st, fs, di, dE, s, narrow);
 }
 
 template <typename WT>
@@ -894,21 +1218,21 @@ void launch_s2(const u64 *S, int32_t V, u64 *total_hi_lo, cudaStream_t s) {
 
 template void launch_move_class<float>(int, const GraphView<float> &, const StateView &,
                                        const int32_t *, int32_t, const DeviceInfo &, u64 *,
-                                       cudaStream_t);
+                                       cudaStream_t, bool);
 template void launch_move_class<u64>(int, const GraphView<u64> &, const StateView &,
                                      const int32_t *, int32_t, const DeviceInfo &, u64 *,
-                                     cudaStream_t);
+                                     cudaStream_t, bool);
 template void launch_move_wide<float>(const GraphView<float> &, const StateView &, const int32_t *,
                                       int32_t, const FallbackSet &, const DeviceInfo &, u64 *,
-                                      cudaStream_t, int32_t);
+                                      cudaStream_t, int32_t, bool);
 template void launch_move_wide<u64>(const GraphView<u64> &, const StateView &, const int32_t *,
                                     int32_t, const FallbackSet &, const DeviceInfo &, u64 *,
-                                    cudaStream_t, int32_t);
+                                    cudaStream_t, int32_t, bool);
 template void launch_move_giants<float>(const GraphView<float> &, const StateView &,
                                         const HubGlobal &, const FallbackSet &, const DeviceInfo &,
-                                        u64 *, cudaStream_t);
+                                        u64 *, cudaStream_t, bool);
 template void launch_move_giants<u64>(const GraphView<u64> &, const StateView &, const HubGlobal &,
-                                      const FallbackSet &, const DeviceInfo &, u64 *, cudaStream_t);
+                                      const FallbackSet &, const DeviceInfo &, u64 *, cudaStream_t, bool);
 template void launch_correction<float>(int, const GraphView<float> &, const StateView &,
                                        const int32_t *, int32_t, const DeviceInfo &, u64 *,
                                        cudaStream_t);
@@ -919,6 +1243,21 @@ template void launch_row_reduce<float>(int, int, const GraphView<float> &, const
                                        u64 *, const int32_t *, int32_t, const DeviceInfo &,
                                        cudaStream_t);
 template void launch_row_reduce<u64>(int, int, const GraphView<u64> &, const int32_t *, u64 *,
+                                     u64 *, const int32_t *, int32_t, const DeviceInfo &,
+                                     cudaStream_t);
+
+template void launch_move_class<uint32_t>(int, const GraphView<uint32_t> &, const StateView &,
+                                     const int32_t *, int32_t, const DeviceInfo &, u64 *,
+                                     cudaStream_t, bool);
+template void launch_move_wide<uint32_t>(const GraphView<uint32_t> &, const StateView &, const int32_t *,
+                                    int32_t, const FallbackSet &, const DeviceInfo &, u64 *,
+                                    cudaStream_t, int32_t, bool);
+template void launch_move_giants<uint32_t>(const GraphView<uint32_t> &, const StateView &, const HubGlobal &,
+                                      const FallbackSet &, const DeviceInfo &, u64 *, cudaStream_t, bool);
+template void launch_correction<uint32_t>(int, const GraphView<uint32_t> &, const StateView &,
+                                     const int32_t *, int32_t, const DeviceInfo &, u64 *,
+                                     cudaStream_t);
+template void launch_row_reduce<uint32_t>(int, int, const GraphView<uint32_t> &, const int32_t *, u64 *,
                                      u64 *, const int32_t *, int32_t, const DeviceInfo &,
                                      cudaStream_t);
 

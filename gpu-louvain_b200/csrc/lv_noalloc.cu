@@ -17,7 +17,6 @@
 // lv_modularity return.
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 
 #include "../../include/louvain_b200.h"
 #include "lv_internal.h"
@@ -42,10 +41,6 @@ static_assert(sizeof(NoallocHeader) <= NOALLOC_HEADER_BYTES, "header fits its sl
 constexpr size_t NOALLOC_BYTES = NOALLOC_HEADER_BYTES + sizeof(u64) * (size_t)LV_NOALLOC_MAX_VERTICES;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
-
-constexpr int NOALLOC_MAX_DEVICES = 64;
-std::mutex g_noalloc_mu;
-void *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
 
 __global__ void noalloc_clear_kernel(u64 *words, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256)
@@ -101,22 +96,19 @@ int noalloc_fail(char *err, int32_t err_len, int code, const char *msg) {
     return code;
 }
 
-// Device address of the scratch array on the current device, resolved once
-// per device (the host-side name of the array is not a device address).
-int noalloc_scratch(int dev, void **out, char *err, int32_t err_len) {
-    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
-        return noalloc_fail(err, err_len, LV_ERR_INVALID, "device ordinal beyond the supported range");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            return noalloc_fail(err, err_len, LV_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
-        }
-        g_noalloc_ptr[dev] = p;
+// Device address of the scratch array on the current device.  The host-side
+// name of the array is not a device address, so every call asks the runtime
+// for it (a cheap lookup) instead of keeping it: an address kept across calls
+// would dangle after the caller resets the device (cudaDeviceReset reloads the
+// module, possibly elsewhere).
+int noalloc_scratch(void **out, char *err, int32_t err_len) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return noalloc_fail(err, err_len, LV_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
     }
-    *out = g_noalloc_ptr[dev];
+    *out = p;
     return LV_OK;
 }
 
@@ -142,6 +134,8 @@ extern "C" int lv_modularity_noalloc(const int32_t *d_rowptr, const int32_t *d_c
     if (err && err_len > 0) err[0] = '\0';
     if (!q || V < 0 || E < 0 || (V > 0 && (!d_rowptr || !d_comm)) || (E > 0 && (!d_col || !d_w)))
         return noalloc_fail(err, err_len, LV_ERR_INVALID, "invalid argument");
+    // a CSR without vertices has no entries (lv_create_device rejects it too)
+    if (V == 0 && E > 0) return noalloc_fail(err, err_len, LV_ERR_INVALID, "malformed CSR: entries without vertices");
     if (V > LV_NOALLOC_MAX_VERTICES) {
         char msg[160];
         std::snprintf(msg, sizeof msg,
@@ -156,7 +150,7 @@ extern "C" int lv_modularity_noalloc(const int32_t *d_rowptr, const int32_t *d_c
         return noalloc_fail(err, err_len, LV_ERR_NO_DEVICE, "no usable CUDA device");
     }
     void *base = nullptr;
-    int rc = noalloc_scratch(dev, &base, err, err_len);
+    int rc = noalloc_scratch(&base, err, err_len);
     if (rc != LV_OK) return rc;
     cudaStream_t s = (cudaStream_t)stream;
     NoallocHeader *dh = (NoallocHeader *)base;

@@ -72,7 +72,15 @@ typedef struct lv_opts {
     float active_start;    /* learned mode: proposals start after a full
                               sweep moved less than this fraction of the
                               level's vertices (default 0 = 0.05)          */
-    int32_t reserved[4];
+    int32_t wide_weights;  /* 1: the move phase reads aggregated levels as
+                              uint64 sums and sums every table in 64 bits;
+                              0 (default): when every weight it reads is
+                              below 2^32 (level 0 whose fixed-point weights
+                              fit, aggregated levels whose merged sums other
+                              than the self-loops, which the move phase
+                              skips, fit) it reads 32-bit values and sums in
+                              16-bit-piece counters.  Same results.       */
+    int32_t reserved[3];
 } lv_opts;
 
 /* Per-run counters; times in milliseconds (device time, CUDA events). */
@@ -99,7 +107,12 @@ typedef struct lv_class_stats {
     int64_t vertices[LV_NUM_CLASSES];
     int64_t edges[LV_NUM_CLASSES];
     double ms[LV_NUM_CLASSES];
-    double bytes[LV_NUM_CLASSES];   /* algorithmic bytes: 8+w per edge, 20 per vertex */
+    double bytes[LV_NUM_CLASSES];   /* algorithmic bytes: 12 per edge, 20 per vertex
+                                       (col, weight and community gather as 4 bytes
+                                       each; row offset, own community, k_i,
+                                       Sigma_tot[own] and new community)           */
+    double stored_bytes[LV_NUM_CLASSES]; /* the same with the stored weight width:
+                                            8 + 4 or 8 bytes per edge            */
 } lv_class_stats;
 
 void lv_default_opts(lv_opts *opts);
@@ -176,15 +189,22 @@ int lv_clear_stats(lv_handle *h);
 int lv_read_mtx(const char *path, int32_t *V, int64_t *E, int32_t **rowptr, int32_t **col,
                 float **w, float *m_ref);
 /* Binary CSR file, a cache for lv_read_mtx's output (no counterpart in the
- * reference, which parses the text file on every run): header "LVCSR001",
- * V and E (int64), m_ref (float), then rowptr[V+1], col[E] (int32) and w[E]
- * (float32), little-endian.  lv_read_csr checks the header, the file size,
- * the offsets and the column range (LV_ERR_IO otherwise); arrays are
- * malloc'd (lv_free_host). */
+ * reference, which parses the text file on every run): header "LVCSR002",
+ * V and E (int64), m_ref (float), 4 pad bytes, the size and the modification
+ * time in nanoseconds of the file the CSR came from (int64; 0 = unknown),
+ * then rowptr[V+1], col[E] (int32) and w[E] (float32), little-endian.
+ * lv_read_csr checks the header, the file size, the offsets and the column
+ * range (LV_ERR_IO otherwise); arrays are malloc'd (lv_free_host).
+ * lv_write_csr writes a zero source stamp; lv_write_csr_stamped records
+ * one, and lv_read_csr_stamp reads it back (header only), so a cache can be
+ * trusted only when its source's size and modification time still match. */
 int lv_write_csr(const char *path, int32_t V, int64_t E, const int32_t *rowptr, const int32_t *col,
                  const float *w, float m_ref);
+int lv_write_csr_stamped(const char *path, int32_t V, int64_t E, const int32_t *rowptr, const int32_t *col,
+                         const float *w, float m_ref, int64_t src_size, int64_t src_mtime_ns);
 int lv_read_csr(const char *path, int32_t *V, int64_t *E, int32_t **rowptr, int32_t **col, float **w,
                 float *m_ref);
+int lv_read_csr_stamp(const char *path, int64_t *src_size, int64_t *src_mtime_ns);
 /* Write an undirected edge list as symmetric Matrix Market (i > j, 1-based). */
 int lv_write_mtx(const char *path, int32_t V, int64_t n_edges, const int32_t *u, const int32_t *v,
                  const float *w);
@@ -232,18 +252,20 @@ void lv_free_device(void *p);
  * device-wide synchronisation of cudaMalloc / cudaFree.  Returns the same
  * modularity as lv_create_device + lv_set_communities + lv_modularity for a
  * level-0 device CSR (as lv_create_device takes it) and a device array
- * d_comm of V community ids in [0, V).
+ * d_comm of V community ids in [0, V).  V = 0 with E > 0 is a malformed CSR
+ * (LV_ERR_INVALID), as for lv_create_device.
  *
  * Working memory is a fixed array inside the library (about 8 MiB per
  * device, held by every GPU that loads the library until exit), so V may be
  * at most LV_NOALLOC_MAX_VERTICES; larger V returns LV_ERR_TOO_LARGE.  No
  * device memory is allocated.  Runs on the calling thread's current device
  * and on `stream` (a cudaStream_t; NULL = the default stream), and
- * synchronises that stream before returning.  The first call on a device
- * looks up the array's device address; make that first call before any
- * stream capture on that device.  All calls on one device share the array:
- * calls that overlap on the GPU (other threads or streams) race and must be
- * serialised by the caller.  On failure a message is written to err (may be
+ * synchronises that stream before returning.  Every call looks up the
+ * array's device address on the current device (nothing is kept between
+ * calls, so a device reset between calls is harmless).  All calls on one
+ * device share the array, which keeps the last call's contents (each call
+ * clears what it sums into), so calls that overlap on the GPU (other threads
+ * or streams) race and must be serialised by the caller.  On failure a message is written to err (may be
  * NULL) of err_len bytes. */
 #define LV_NOALLOC_MAX_VERTICES (1 << 20)
 int lv_modularity_noalloc(const int32_t *d_rowptr, const int32_t *d_col, const float *d_w, int32_t V,

@@ -678,6 +678,161 @@ int orc_read_mtx(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowpt
 
 void orc_free(void *p) { free(p); }
 
+/* ------------------------------------------------------------------ */
+/* seeded R-MAT input (the benchmark graph, generated without the      */
+/* product library)                                                    */
+/* ------------------------------------------------------------------ */
+
+/* Counter-based draws: splitmix64's finaliser (Steele, Lea, Flood 2014)
+ * applied to key + i * golden ratio, key = mix(seed ^ (stream << 32)).  The
+ * R-MAT recursion (Chakrabarti, Zhan, Faloutsos 2004) takes, for bit level l
+ * (most significant first), 32 bits of draw(key_{l/2}, i): quadrant
+ * q = [x >= a] + [x >= a+b] + [x >= a+b+c] gives the row bit q >> 1 and the
+ * column bit q & 1.  Self-loops and repeated pairs are dropped and the
+ * graph is symmetrised with ascending rows.  Weight of pair (lo, hi):
+ * (m + 2^23) * 2^-24 from 24 bits of draw(key_w, lo << 32 | hi), uniform on
+ * [0.5, 1.5) and exact in float32.  The same seed gives the same graph as
+ * the engine's generators. */
+static uint64_t rng_mix(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static uint64_t rng_key(uint64_t seed, uint64_t stream) { return rng_mix(seed ^ (stream << 32)); }
+static uint64_t rng_draw(uint64_t key, uint64_t i) { return rng_mix(key + i * 0x9E3779B97F4A7C15ull); }
+
+/* LSD radix sort of n keys on their low nbits bits (tmp holds n keys). */
+static void radix_sort_keys(uint64_t *a, uint64_t *tmp, int64_t n, int nbits, int nt) {
+    int64_t *hist = (int64_t *)malloc(sizeof(int64_t) * (size_t)nt * 256);
+    for (int shift = 0; shift < nbits; shift += 8) {
+        memset(hist, 0, sizeof(int64_t) * (size_t)nt * 256);
+#pragma omp parallel num_threads(nt)
+        {
+            int t = 0;
+#ifdef _OPENMP
+            t = omp_get_thread_num();
+#endif
+            int64_t lo = n * t / nt, hi = n * (t + 1) / nt;
+            int64_t *h = hist + (size_t)t * 256;
+            for (int64_t i = lo; i < hi; i++) h[(a[i] >> shift) & 255]++;
+        }
+        int64_t run = 0;
+        for (int d = 0; d < 256; d++)
+            for (int t = 0; t < nt; t++) {
+                int64_t c = hist[(size_t)t * 256 + d];
+                hist[(size_t)t * 256 + d] = run;
+                run += c;
+            }
+#pragma omp parallel num_threads(nt)
+        {
+            int t = 0;
+#ifdef _OPENMP
+            t = omp_get_thread_num();
+#endif
+            int64_t lo = n * t / nt, hi = n * (t + 1) / nt;
+            int64_t *h = hist + (size_t)t * 256;
+            for (int64_t i = lo; i < hi; i++) tmp[h[(a[i] >> shift) & 255]++] = a[i];
+        }
+        memcpy(a, tmp, sizeof(uint64_t) * (size_t)n);
+    }
+    free(hist);
+}
+
+int orc_gen_rmat(int scale, int edge_factor, uint64_t seed, double a, double b, double c,
+                 int unit_weights, int nthreads, int32_t *Vout, int64_t *Eout, int32_t **rowptr,
+                 int32_t **col, float **w) {
+    if (scale < 1 || scale > 30 || edge_factor < 1 || !Vout || !Eout || !rowptr || !col || !w)
+        return ORC_EINVAL;
+    int nt = nthreads > 0 ? nthreads : 1;
+    const int64_t n = (int64_t)edge_factor << scale;
+    const uint32_t ta = (uint32_t)(a * 4294967296.0), tb = (uint32_t)((a + b) * 4294967296.0),
+                   tc = (uint32_t)((a + b + c) * 4294967296.0);
+    uint64_t keys_l[16];
+    for (int i = 0; i < 16; i++) keys_l[i] = rng_key(seed, (uint64_t)(1 + i));
+    uint64_t *keys = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)n);
+    uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)n);
+    int64_t *cnt = (int64_t *)calloc((size_t)nt + 1, sizeof(int64_t));
+    if (!keys || !tmp || !cnt) { free(keys); free(tmp); free(cnt); return ORC_ENOMEM; }
+#pragma omp parallel num_threads(nt)
+    {
+        int t = 0;
+#ifdef _OPENMP
+        t = omp_get_thread_num();
+#endif
+        int64_t lo = n * t / nt, hi = n * (t + 1) / nt, k = lo;
+        for (int64_t i = lo; i < hi; i++) {
+            uint32_t u = 0, v = 0;
+            for (int pr = 0; 2 * pr < scale; pr++) {
+                uint64_t r = rng_draw(keys_l[pr], (uint64_t)i);
+                for (int half = 0; half < 2 && 2 * pr + half < scale; half++) {
+                    uint32_t x = (uint32_t)(r >> (32 * half));
+                    uint32_t q = (uint32_t)(x >= ta) + (uint32_t)(x >= tb) + (uint32_t)(x >= tc);
+                    u = (u << 1) | (q >> 1);
+                    v = (v << 1) | (q & 1u);
+                }
+            }
+            if (u == v) continue;
+            uint32_t lo32 = u < v ? u : v, hi32 = u < v ? v : u;
+            keys[k++] = ((uint64_t)lo32 << scale) | hi32;
+        }
+        cnt[t + 1] = k - lo;
+    }
+    int64_t m = 0;
+    for (int t = 0; t < nt; t++) {
+        int64_t lo = n * t / nt;
+        if (m != lo) memmove(keys + m, keys + lo, sizeof(uint64_t) * (size_t)cnt[t + 1]);
+        m += cnt[t + 1];
+    }
+    free(cnt);
+    radix_sort_keys(keys, tmp, m, 2 * scale, nt);
+    free(tmp);
+    int64_t nk = 0;
+    for (int64_t i = 0; i < m; i++)
+        if (nk == 0 || keys[i] != keys[nk - 1]) keys[nk++] = keys[i];
+    const int32_t V = (int32_t)(1u << scale);
+    const int64_t E = 2 * nk;
+    if (E > INT32_MAX) { free(keys); return ORC_ETOOLARGE; }
+    const uint64_t mask = ((uint64_t)1 << scale) - 1;
+    int64_t *dlo = (int64_t *)calloc((size_t)V + 1, sizeof(int64_t));
+    int64_t *dhi = (int64_t *)calloc((size_t)V + 1, sizeof(int64_t));
+    int32_t *rp = (int32_t *)malloc(sizeof(int32_t) * ((size_t)V + 1));
+    int32_t *cl = (int32_t *)malloc(sizeof(int32_t) * (size_t)(E > 0 ? E : 1));
+    float *wt = (float *)malloc(sizeof(float) * (size_t)(E > 0 ? E : 1));
+    if (!dlo || !dhi || !rp || !cl || !wt) {
+        free(keys); free(dlo); free(dhi); free(rp); free(cl); free(wt);
+        return ORC_ENOMEM;
+    }
+    for (int64_t i = 0; i < nk; i++) {
+        dhi[keys[i] >> scale]++;   /* a row's larger neighbours */
+        dlo[keys[i] & mask]++;     /* ... and its smaller ones */
+    }
+    /* row v: smaller neighbours (ascending), then larger ones (ascending) */
+    int64_t acc = 0;
+    for (int32_t v = 0; v < V; v++) {
+        rp[v] = (int32_t)acc;
+        int64_t d_lo = dlo[v], d_hi = dhi[v];
+        dlo[v] = acc;           /* cursor of the smaller neighbours */
+        dhi[v] = acc + d_lo;    /* cursor of the larger neighbours */
+        acc += d_lo + d_hi;
+    }
+    rp[V] = (int32_t)acc;
+    const uint64_t wkey = rng_key(seed, 0xFFFF);
+    for (int64_t i = 0; i < nk; i++) {
+        int32_t x = (int32_t)(keys[i] >> scale), y = (int32_t)(keys[i] & mask);
+        float wv = 1.0f;
+        if (!unit_weights) {
+            uint64_t h = rng_draw(wkey, ((uint64_t)(uint32_t)x << 32) | (uint32_t)y);
+            wv = (float)((uint32_t)(h >> 40) + 8388608u) * 5.9604644775390625e-08f;
+        }
+        int64_t px = dhi[x]++, py = dlo[y]++;
+        cl[px] = y; wt[px] = wv;
+        cl[py] = x; wt[py] = wv;
+    }
+    free(keys); free(dlo); free(dhi);
+    *Vout = V; *Eout = E; *rowptr = rp; *col = cl; *w = wt;
+    return ORC_OK;
+}
+
 double orc_modularity_f64(int32_t V, const int32_t *rowptr, const int32_t *col,
                           const float *w, const int32_t *comm) {
     double T = 0, eown = 0;

@@ -97,6 +97,15 @@ int orc_read_mtx(const char *path, int32_t *V, int64_t *E, int32_t **rowptr,
                  int32_t **col, float **w, float *m_ref);
 void orc_free(void *p);
 
+/* Seeded R-MAT graph (scale, edge factor, a, b, c), symmetrised without
+ * self-loops or repeated pairs, ascending rows; unit weights or weights
+ * uniform on [0.5, 1.5) exact in float32.  The same seed gives the same CSR
+ * as the engine's generators, so baselines can build the benchmark input
+ * without loading the product library.  Arrays are malloc'd (orc_free). */
+int orc_gen_rmat(int scale, int edge_factor, uint64_t seed, double a, double b, double c,
+                 int unit_weights, int nthreads, int32_t *V, int64_t *E, int32_t **rowptr,
+                 int32_t **col, float **w);
+
 /* Modularity in FP64 of an arbitrary partition of the level-0 graph given as
  * float weights (a plain recomputation, used to check printed maps). */
 double orc_modularity_f64(int32_t V, const int32_t *rowptr, const int32_t *col,

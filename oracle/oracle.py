@@ -61,6 +61,9 @@ def lib():
         L.orc_read_mtx.argtypes = [C.c_char_p, P32, P64, C.POINTER(P32), C.POINTER(P32),
                                    C.POINTER(PF), PF]
         L.orc_free.argtypes = [C.c_void_p]
+        L.orc_gen_rmat.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_double, C.c_double, C.c_double,
+                                   C.c_int, C.c_int, P32, P64, C.POINTER(P32), C.POINTER(P32),
+                                   C.POINTER(PF)]
         L.orc_modularity_f64.restype = C.c_double
         L.orc_modularity_f64.argtypes = [C.c_int32, P32, P32, PF, P32]
         _lib = L
@@ -93,6 +96,27 @@ def read_mtx(path: str):
         L.orc_free(C.cast(ptr, C.c_void_p))
         out.append(arr)
     return out[0], out[1], out[2], m.value
+
+
+def _take(ptr, n, dt):
+    """Copy a malloc'd oracle array into numpy and free it."""
+    arr = np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+    lib().orc_free(C.cast(ptr, C.c_void_p))
+    return arr
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, seed: int = 1, a: float = 0.57, b: float = 0.19,
+             c: float = 0.19, weights: str = "uniform", nthreads: int = 0):
+    """Seeded R-MAT graph as (rowptr, col, w): the same CSR as the engine's
+    generators for the same arguments, built without the product library."""
+    V, E = C.c_int32(), C.c_int64()
+    rp, cl, w = P32(), P32(), PF()
+    rc = lib().orc_gen_rmat(scale, edge_factor, seed, a, b, c, 1 if weights == "unit" else 0,
+                            nthreads if nthreads > 0 else (os.cpu_count() or 1), C.byref(V), C.byref(E),
+                            C.byref(rp), C.byref(cl), C.byref(w))
+    if rc:
+        raise RuntimeError(f"orc_gen_rmat failed: {rc}")
+    return (_take(rp, V.value + 1, np.int32), _take(cl, E.value, np.int32), _take(w, E.value, np.float32))
 
 
 def modularity_f64(rowptr, col, w, comm) -> float:

@@ -96,6 +96,24 @@ def test_batch_matches_oracle(lvb, orc, gnp, min_gain):
     _check_against_oracle(lvb, orc, _mixed_batch(lvb, gnp), min_gain)
 
 
+def _upper_bound_batch(lvb):
+    """Graphs at the batched workload's bounds: 50,000 vertices, 4 to 256
+    blocks, expected intra-block degree 8 to 24 and inter-block degree 1 to
+    4, unit weights (one grid-weight variant), plus the smallest graphs."""
+    specs = [(50000, 256, 24.0, 4.0, "unit"), (50000, 4, 24.0, 4.0, "unit"), (50000, 256, 8.0, 1.0, "unit"),
+             (50000, 128, 16.0, 4.0, "uniform"), (49999, 255, 23.5, 3.9, "unit"), (25000, 256, 24.0, 4.0, "unit"),
+             (12000, 64, 20.0, 3.0, "unit"), (100, 4, 24.0, 4.0, "unit"), (100, 100, 8.0, 1.0, "unit"),
+             (101, 4, 8.0, 1.0, "unit")]
+    return [lvb.gen_planted(V, B, di, do, seed=900 + i, weights=wt) for i, (V, B, di, do, wt) in enumerate(specs)]
+
+
+@pytest.mark.gpu
+def test_batch_upper_bounds_match_oracle(lvb, orc):
+    graphs = _upper_bound_batch(lvb)
+    assert max(g.V for g in graphs) == 50000
+    _check_against_oracle(lvb, orc, graphs, 1e-6)
+
+
 @pytest.mark.gpu
 def test_batch_max_sweeps_matches_oracle(lvb, orc, gnp):
     graphs = _mixed_batch(lvb, gnp)[:12]

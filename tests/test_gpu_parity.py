@@ -154,6 +154,11 @@ def test_full_run_matches_oracle(lvb, orc, graphs, name):
     e.reset()
     assert e.run(gain) == q1
     assert np.array_equal(e.original_to_community()[0], o2c1)
+    e.close()
+    # aggregated levels read as uint64 sums instead of their 32-bit copy
+    with lvb.Louvain(lvb.Graph(rp, cl, w), wide_weights=True) as ew:
+        assert ew.run(gain) == q1
+        assert np.array_equal(ew.original_to_community()[0], o2c1)
 
 
 def test_megahub_matches_oracle(lvb, orc):
@@ -355,6 +360,31 @@ def test_cli_output(lvb, orc, tmp_path):
     assert np.array_equal(got, o2c)
     r2 = subprocess.run([lvb.CLI_PATH, "-f", p, "-g", "0.01"], capture_output=True, text=True)
     assert r2.stdout.split("\n")[0] == lines[0] and len(r2.stdout.split("\n")) == 3
+
+
+def test_cli_cache_follows_source(lvb, tmp_path):
+    """gpulouvain -c reuses <file>.lvcsr only while the text file's size and
+    modification time match the ones recorded in the cache: a file replaced
+    by another graph with an older modification time is parsed again."""
+    p = str(tmp_path / "g.mtx")
+    first = lvb.gen_planted(1500, 12, 12.0, 2.0, 1)
+    lvb.write_mtx(p, first)
+    r1 = subprocess.run([lvb.CLI_PATH, "-f", p, "-g", "0.01", "-c"], capture_output=True, text=True)
+    assert r1.returncode == 0, r1.stderr
+    assert os.path.exists(p + ".lvcsr")
+    r1b = subprocess.run([lvb.CLI_PATH, "-f", p, "-g", "0.01", "-c"], capture_output=True, text=True)
+    assert r1b.stdout.split("\n")[0] == r1.stdout.split("\n")[0]
+    second = lvb.gen_planted(1800, 9, 14.0, 1.0, 2)
+    lvb.write_mtx(p, second)
+    old = os.stat(p + ".lvcsr").st_mtime - 3600
+    os.utime(p, (old, old))        # older than the cache, as after cp -p / tar / rsync -t
+    r2 = subprocess.run([lvb.CLI_PATH, "-f", p, "-g", "0.01", "-c"], capture_output=True, text=True)
+    r3 = subprocess.run([lvb.CLI_PATH, "-f", p, "-g", "0.01"], capture_output=True, text=True)
+    assert r2.returncode == 0 and r3.returncode == 0
+    assert r2.stdout.split("\n")[0] == r3.stdout.split("\n")[0]
+    e = lvb.Louvain(lvb.read_mtx(p))
+    assert r3.stdout.split("\n")[0] == "%f" % e.run(0.01)
+    e.close()
 
 
 # ---------------------------------------------------------------------------

@@ -172,6 +172,26 @@ def test_csr_cache_roundtrip(lvb, tmp_path):
         assert ex.value.status == lvb.LV_ERR_IO
 
 
+def test_csr_cache_source_stamp(lvb, tmp_path):
+    import ctypes as C
+    g = lvb.gen_planted(500, 8, 10.0, 2.0, 3)
+    p = str(tmp_path / "s.lvcsr")
+    L = lvb.lib()
+    P32 = C.POINTER(C.c_int32)
+    rc = L.lv_write_csr_stamped(p.encode(), g.V, g.E, g.rowptr.ctypes.data_as(P32), g.col.ctypes.data_as(P32),
+                                g.w.ctypes.data_as(C.POINTER(C.c_float)), 1.0, 123456, 1700000000123456789)
+    assert rc == lvb.LV_OK
+    size, mt = C.c_int64(), C.c_int64()
+    assert L.lv_read_csr_stamp(p.encode(), C.byref(size), C.byref(mt)) == lvb.LV_OK
+    assert (size.value, mt.value) == (123456, 1700000000123456789)
+    r = lvb.read_csr(p)
+    assert np.array_equal(r.rowptr, g.rowptr) and np.array_equal(r.col, g.col)
+    lvb.write_csr(p, g)           # unstamped
+    assert L.lv_read_csr_stamp(p.encode(), C.byref(size), C.byref(mt)) == lvb.LV_OK
+    assert (size.value, mt.value) == (0, 0)
+    assert L.lv_read_csr_stamp(str(tmp_path / "missing").encode(), C.byref(size), C.byref(mt)) == lvb.LV_ERR_IO
+
+
 def test_print_communities_large_matches_python(lvb, tmp_path):
     """The multi-threaded writer gives the reference's format byte for byte:
     the community count, then "c+1 m1+1 m2+1 ..." per community with members
