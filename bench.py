@@ -295,10 +295,10 @@ def class_table_of(cs):
             for c in range(len(CLASS_NAMES))}
 
 
-def profiled_run(lvb, dg, dev, wide_weights=False):
+def profiled_run(lvb, dg, dev, wide_weights=False, knobs=None):
     """One untimed run with per-class CUDA events (host loop per sweep)."""
     prof = lvb.Louvain(device_csr=(dg.rowptr, dg.col, dg.w, dg.V, dg.E), device=dev, profile=True,
-                       wide_weights=wide_weights)
+                       wide_weights=wide_weights, **(knobs or {}))
     prof.run(MIN_GAIN)
     cs = prof.class_stats()
     pst = prof.stats()
@@ -330,10 +330,18 @@ def run_ours(args, ranks: Ranks):
     scale = args.scale
     dg = lvb.gen_rmat_device(scale, EDGE_FACTOR, SEED, device=dev)
     V, E = dg.V, dg.E
+    # --- autotuning of the work-mapping knobs (untimed; results identical) ---
+    tuning, knobs = None, {}
+    if not args.no_tune:
+        t0 = time.perf_counter()
+        tuning = lvb.tune(device_csr=(dg.rowptr, dg.col, dg.w, V, E), device=dev, min_gain=MIN_GAIN,
+                          cache=os.path.join(ROOT, "_build", "tune_cache.json") if args.tune_cache else None)
+        tuning["tuning_s"] = round(time.perf_counter() - t0, 1)
+        knobs = {"giant_degree": tuning["giant_degree"], "warp_limit": tuning["warp_limit"]}
     # --- value: resident inputs ---
     # timed runs use the default path (each level's sweep loop as one CUDA
     # graph); the per-class split comes from a separate profiled run below
-    eng = lvb.Louvain(device_csr=(dg.rowptr, dg.col, dg.w, V, E), device=dev, trace=args.trace)
+    eng = lvb.Louvain(device_csr=(dg.rowptr, dg.col, dg.w, V, E), device=dev, trace=args.trace, **knobs)
     for _ in range(args.warmup):
         eng.reset()
         eng.run(MIN_GAIN)
@@ -361,13 +369,13 @@ def run_ours(args, ranks: Ranks):
     units, secs, value = combine(ranks, float(st["edge_sweeps"]), ms / 1e3)
     eng.close()
     # the first level-0 sweep's community vector (checked against the oracle)
-    e1 = lvb.Louvain(device_csr=(dg.rowptr, dg.col, dg.w, V, E), device=dev)
+    e1 = lvb.Louvain(device_csr=(dg.rowptr, dg.col, dg.w, V, E), device=dev, **knobs)
     first_moves = e1.sweep()
     first_comm = e1.communities()
     e1.close()
     # one untimed profiled run (per-class CUDA events, one host round trip per
     # sweep) for the roofline and the class / phase split
-    cs, pst, o2c_prof = profiled_run(lvb, dg, dev)
+    cs, pst, o2c_prof = profiled_run(lvb, dg, dev, knobs=knobs)
     assert np.array_equal(o2c_prof, o2c), "profiled run differs"
     # roofline of the dominant kernel class
     dom = max(range(len(CLASS_NAMES)), key=lambda c: cs["ms"][c])
@@ -396,7 +404,7 @@ def run_ours(args, ranks: Ranks):
 
     def e2e_step():
         t_a = time.perf_counter()
-        with lvb.Louvain(host_graph, device=dev) as e:
+        with lvb.Louvain(host_graph, device=dev, **knobs) as e:
             t_b = time.perf_counter()
             e.run(MIN_GAIN)
             t_c = time.perf_counter()
@@ -474,6 +482,8 @@ def run_ours(args, ranks: Ranks):
         "clocks": clocks,
         "cpu_baseline": cpu,
         "parity": parity,
+        "tuning": ({k: tuning[k] for k in ("giant_degree", "warp_limit", "ms", "default_ms", "cached",
+                                           "tuning_s", "trials")} if tuning else None),
     }
     return line
 
@@ -496,12 +506,27 @@ def batch_graph_params(i: int):
     return V, blocks, float(r.uniform(8.0, 24.0)), float(r.uniform(1.0, 4.0))
 
 
+def batch_seed(i: int) -> int:
+    return BATCH_SEED * 1000003 + i
+
+
 def batch_graphs(lvb, indices):
+    """Graph objects of the given batch indices (samples)."""
     out = []
     for i in indices:
         V, blocks, d_in, d_out = batch_graph_params(i)
-        out.append(lvb.gen_planted(V, blocks, d_in, d_out, seed=BATCH_SEED * 1000003 + i))
+        out.append(lvb.gen_planted(V, blocks, d_in, d_out, seed=batch_seed(i)))
     return out
+
+
+def batch_csr(lvb, indices):
+    """Block-diagonal CSR of the given batch indices, generated by all host
+    threads: (rowptr, col, w, graph_ptr)."""
+    params = []
+    for i in indices:
+        V, blocks, d_in, d_out = batch_graph_params(i)
+        params.append((V, blocks, d_in, d_out, batch_seed(i)))
+    return lvb.gen_planted_batch(params)
 
 
 def batch_shard(lvb, n_graphs: int, ranks: Ranks):
@@ -519,10 +544,9 @@ def run_batch(args, ranks: Ranks):
     torch.cuda.set_device(dev)
     mine = batch_shard(lvb, args.batch_graphs, ranks)
     t_gen = time.perf_counter()
-    graphs = batch_graphs(lvb, mine)
+    rp, cl, w, gptr = batch_csr(lvb, mine)
     t_gen = time.perf_counter() - t_gen
-    rp, cl, w, gptr = lvb.concat_graphs(graphs)
-    V, E, G = len(rp) - 1, len(cl), len(graphs)
+    V, E, G = len(rp) - 1, len(cl), len(mine)
     h_rp = torch.from_numpy(rp).pin_memory().numpy()
     h_cl = torch.from_numpy(cl).pin_memory().numpy()
     h_w = torch.from_numpy(w).pin_memory().numpy()
@@ -580,9 +604,10 @@ def run_batch(args, ranks: Ranks):
     n_seq = min(args.batch_seq_sample, G)
     pick = sorted(set(int(x) for x in np.linspace(0, G - 1, n_seq))) if G else []
     parts = [gptr[i:i + 2] for i in range(G)]
+    sample = dict(zip(pick, batch_graphs(lvb, [mine[i] for i in pick])))
     t0 = time.perf_counter()
     for i in pick:
-        with lvb.Louvain(graphs[i], device=dev) as e:
+        with lvb.Louvain(sample[i], device=dev) as e:
             q = e.run(MIN_GAIN)
             m, _ = e.original_to_community()
         assert q == res["modularity"][i] and np.array_equal(m, res["communities"][parts[i][0]:parts[i][1]])
@@ -595,7 +620,7 @@ def run_batch(args, ranks: Ranks):
         nt = host_threads()
         t0 = time.perf_counter()
         for i in pick:
-            o = orc.Oracle(graphs[i].rowptr, graphs[i].col, graphs[i].w, nt)
+            o = orc.Oracle(sample[i].rowptr, sample[i].col, sample[i].w, nt)
             o.run(MIN_GAIN)
             o.close()
         dt = time.perf_counter() - t0
@@ -632,6 +657,57 @@ def run_batch(args, ranks: Ranks):
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
+
+
+def batch_summary(args, ranks: Ranks):
+    """Compact driver-visible summary of the batched workload (the 4096-graph
+    batch in one persistent launch, device-timed, 1 warm-up + 2 timed runs)."""
+    import numpy as np
+    import torch
+    lvb = load_pkg()
+    dev = ranks.local
+    torch.cuda.set_device(dev)
+    t_gen = time.perf_counter()
+    rp, cl, w, gptr = batch_csr(lvb, range(args.batch_graphs))
+    t_gen = time.perf_counter() - t_gen
+    G = args.batch_graphs
+    with lvb.Batch(rowptr=rp, col=cl, w=w, graph_ptr=gptr, device=dev) as b:
+        b.run(MIN_GAIN)
+        dev_ms, es = 0.0, 0
+        lat = []
+        for _ in range(2):
+            b.run(MIN_GAIN)
+            st = b.stats()
+            dev_ms += st["device_ms"]
+            es += st["edge_sweeps"]
+            lat.append(b.graph_stats()["latency_ms"])
+        ok = bool((b.results()["status"] == lvb.LV_OK).all())
+    lat = np.concatenate(lat)
+    return {"workload": f"batch{G}_planted", "graphs_per_s": 2 * G / (dev_ms * 1e-3),
+            "ms_per_launch": dev_ms / 2, "edge_sweeps_per_s": es / (dev_ms * 1e-3),
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "max": float(lat.max())},
+            "all_ok": ok, "V_total": len(rp) - 1, "E_csr_total": len(cl), "generation_s": round(t_gen, 1),
+            "note": "lv_batch_run, one persistent launch per run, device time (1 warm-up + 2 timed runs); "
+                    "bench.py --workload batch gives the full line"}
+
+
+def learned_summary(args, ranks: Ranks):
+    """Compact driver-visible summary of the learned active-set form against
+    the plain method on the held-out 4M-vertex LFR-like graphs."""
+    import copy
+    a = copy.copy(args)
+    a.steps, a.warmup = 2, 1
+    line = run_lfr(a, ranks)
+    return {"workload": line["config"]["workload"], "speedup": line["value"],
+            "max_abs_dq": line["max_abs_dq"], "target": "speed-up >= 1.5 at |dQ| <= 1e-3",
+            "per_graph": [{"mu": r["mu"], "plain_ms": round(r["plain_ms"], 2), "learned_ms": round(r["learned_ms"], 2),
+                           "speedup": round(r["speedup"], 3), "dq": r["dq"],
+                           "recall": r["learned"]["recall"], "fell_back": r["learned"]["fell_back"]}
+                          for r in line["per_graph"]],
+            "settings": {k: line["config"][k] for k in ("full_every", "active_start", "min_recall")},
+            "note": "plain vs learned on the same handle options, best of 2 timed runs each; "
+                    "bench.py --workload lfr gives the full line"}
 
 
 def run_reference(args, ranks: Ranks):
@@ -840,6 +916,12 @@ def main():
                     help="graphs run one by one through the single-graph engine for comparison")
     ap.add_argument("--profile-only", action="store_true",
                     help="one profiled run of the R-MAT graph and its class split (for ncu launch lists)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="default workload: run with the default work-mapping knobs (no autotuning)")
+    ap.add_argument("--tune-cache", action="store_true",
+                    help="keep the autotuner's choice in _build/tune_cache.json between runs")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload: skip the learned and batched summaries added to the line")
     ap.add_argument("--wide-weights", action="store_true",
                     help="with --profile-only: 64-bit table sums and weights at every level (lv_opts.wide_weights)")
     args = ap.parse_args()
@@ -851,6 +933,15 @@ def main():
         line = (run_batch(args, ranks) if args.workload == "batch"
                 else run_lfr(args, ranks) if args.workload == "lfr"
                 else run_profile_only(args, ranks) if args.profile_only else run_ours(args, ranks))
+        if (args.workload == "rmat" and not args.profile_only and not args.no_extras and ranks.world == 1
+                and line is not None):
+            # the metric also names the learned form and the batched form:
+            # compact summaries of both ride on the default line
+            for key, fn in (("learned", learned_summary), ("batch", batch_summary)):
+                try:
+                    line[key] = fn(args, ranks)
+                except Exception as ex:   # the headline line is printed regardless
+                    line[key] = {"error": f"{type(ex).__name__}: {ex}"}
     if ranks.rank == 0 and line is not None:
         print(json.dumps(line), flush=True)
     ranks.close()

@@ -60,7 +60,8 @@ class _Opts(C.Structure):
                 ("profile", C.c_int32), ("verify", C.c_int32), ("trace", C.c_int32),
                 ("sweep_graph", C.c_int32), ("active_set", C.c_int32), ("active_full_every", C.c_int32),
                 ("active_min_recall", C.c_float), ("trace_sample", C.c_float), ("active_start", C.c_float),
-                ("wide_weights", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("wide_weights", C.c_int32), ("giant_degree", C.c_int32), ("warp_limit", C.c_int32),
+                ("reserved", C.c_int32 * 1)]
 
 
 class _Stats(C.Structure):
@@ -88,7 +89,8 @@ EXPORTED = [
     "lv_batch_create", "lv_batch_create_device", "lv_batch_run", "lv_batch_get_results",
     "lv_batch_get_graph_stats", "lv_batch_get_stats", "lv_batch_last_error", "lv_batch_destroy",
     "lv_gen_lfr", "lv_set_active_model", "lv_get_traces", "lv_get_active_stats", "lv_active_train",
-    "lv_active_predict", "lv_write_csr", "lv_read_csr", "lv_write_csr_stamped", "lv_read_csr_stamp",
+    "lv_active_predict", "lv_write_csr", "lv_read_csr", "lv_write_csr_stamped", "lv_read_csr_stamp", "lv_gen_planted_batch", "lv_read_mtx_device",
+    "lv_csr_from_entries_device", "lv_read_mtx_entries", "lv_get_level_classes", "lv_get_device_name",
 ]
 
 _lib = None
@@ -144,6 +146,17 @@ def lib() -> C.CDLL:
     L.lv_write_csr_stamped.argtypes = [C.c_char_p, C.c_int32, C.c_int64, P32, P32, PF, C.c_float, C.c_int64,
                                        C.c_int64]
     L.lv_read_csr_stamp.argtypes = [C.c_char_p, P64, P64]
+    L.lv_get_level_classes.argtypes = [C.c_void_p, P32, P64]
+    L.lv_read_mtx_entries.argtypes = [C.c_char_p, P32, P64, C.POINTER(P32), C.POINTER(P32), C.POINTER(PF)]
+    L.lv_get_device_name.argtypes = [C.c_int32, C.c_char_p, C.c_int32]
+    L.lv_read_mtx_device.argtypes = [C.c_char_p, C.c_int32, P32, P64, C.POINTER(C.c_void_p),
+                                     C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), PF]
+    L.lv_csr_from_entries_device.argtypes = [C.c_int32, C.c_int32, C.c_int64, P32, P32, PF, P64,
+                                             C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                             C.POINTER(C.c_void_p)]
+    L.lv_gen_planted_batch.argtypes = [C.c_int32, P32, P32, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                       C.POINTER(C.c_uint64), C.c_int32, P32, P64, C.POINTER(P32),
+                                       C.POINTER(P32), C.POINTER(PF), C.POINTER(P32)]
     L.lv_free_host.argtypes = [C.c_void_p]
     L.lv_print_communities.argtypes = [C.c_char_p, P32, C.c_int32, C.c_int32]
     L.lv_gen_rmat.argtypes = [C.c_int32, C.c_int32, C.c_uint64, C.c_double, C.c_double, C.c_double,
@@ -302,6 +315,27 @@ def gen_planted(V: int = 10000, blocks: int = 64, d_in: float = 16.0, d_out: flo
                  _take_host(w, E.value, np.float32))
 
 
+def gen_planted_batch(params, weights: str = "unit"):
+    """Block-diagonal CSR (rowptr, col, w, graph_ptr) of planted-partition
+    graphs, one per (V, blocks, d_in, d_out, seed) in params, generated by all
+    host threads; graph i equals gen_planted(*params[i]) offset by
+    graph_ptr[i]."""
+    G = len(params)
+    Vs = np.array([p[0] for p in params], np.int32)
+    Bs = np.array([p[1] for p in params], np.int32)
+    di = np.array([p[2] for p in params], np.float64)
+    do = np.array([p[3] for p in params], np.float64)
+    sd = np.array([p[4] for p in params], np.uint64)
+    Vt, Et = C.c_int32(), C.c_int64()
+    rp, cl, w, gp = P32(), P32(), PF(), P32()
+    _check(lib().lv_gen_planted_batch(G, _ptr(Vs, C.c_int32), _ptr(Bs, C.c_int32), _ptr(di, C.c_double),
+                                      _ptr(do, C.c_double), _ptr(sd, C.c_uint64),
+                                      1 if weights == "uniform" else 0, C.byref(Vt), C.byref(Et), C.byref(rp),
+                                      C.byref(cl), C.byref(w), C.byref(gp)))
+    return (_take_host(rp, Vt.value + 1, np.int32), _take_host(cl, Et.value, np.int32),
+            _take_host(w, Et.value, np.float32), _take_host(gp, G + 1, np.int32))
+
+
 def gen_lfr(V: int = 1000000, mu: float = 0.3, seed: int = 0, tau1: float = 2.5,
             mean_degree: float = 20.0, kmax: int = 2000, tau2: float = 1.5, cmin: int = 50,
             cmax: int = 5000):
@@ -344,6 +378,39 @@ def gen_rmat_device(scale: int, edge_factor: int = 16, seed: int = 1, a: float =
     return DeviceGraph(V.value, E.value, rp.value, cl.value, w.value, device)
 
 
+def device_name(device: int = 0) -> str:
+    buf = C.create_string_buffer(256)
+    _check(lib().lv_get_device_name(device, buf, 256))
+    return buf.value.decode()
+
+
+def read_mtx_device(path: str, device: int = 0) -> DeviceGraph:
+    """Matrix Market file -> CSR built on the device (lv_read_mtx_device);
+    the same CSR as read_mtx.  m_ref is set on the returned object."""
+    L = lib()
+    V, E = C.c_int32(), C.c_int64()
+    rp, cl, w = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    m = C.c_float()
+    _check(L.lv_read_mtx_device(path.encode(), device, C.byref(V), C.byref(E), C.byref(rp), C.byref(cl),
+                                C.byref(w), C.byref(m)))
+    g = DeviceGraph(V.value, E.value, rp.value, cl.value, w.value, device)
+    g.m_ref = m.value
+    return g
+
+
+def csr_from_entries_device(V: int, v1, v2, w, device: int = 0) -> DeviceGraph:
+    """CSR on the device from 0-based entries in file order
+    (lv_csr_from_entries_device)."""
+    a, b = _i32(v1), _i32(v2)
+    ww = np.ascontiguousarray(w, dtype=np.float32)
+    E = C.c_int64()
+    rp, cl, dw = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    _check(lib().lv_csr_from_entries_device(device, V, len(a), _ptr(a, C.c_int32), _ptr(b, C.c_int32),
+                                            _ptr(ww, C.c_float), C.byref(E), C.byref(rp), C.byref(cl),
+                                            C.byref(dw)))
+    return DeviceGraph(V, E.value, rp.value, cl.value, dw.value, device)
+
+
 def print_communities(orig2comm: np.ndarray, num_communities: int, path: str | None = None) -> None:
     o = _i32(orig2comm)
     _check(lib().lv_print_communities(path.encode() if path else None, _ptr(o, C.c_int32), len(o),
@@ -357,7 +424,8 @@ class Louvain:
                  profile: bool = False, verify: bool = False, trace: bool = False,
                  device_csr: tuple | None = None, sweep_graph: bool = True,
                  active_set: bool = False, active_full_every: int = 0, active_min_recall: float = 0.0,
-                 trace_sample: float = 0.0, active_start: float = 0.0, wide_weights: bool = False):
+                 trace_sample: float = 0.0, active_start: float = 0.0, wide_weights: bool = False,
+                 giant_degree: int = 0, warp_limit: int = 0):
         L = lib()
         opts = _Opts()
         L.lv_default_opts(C.byref(opts))
@@ -373,6 +441,8 @@ class Louvain:
         opts.trace_sample = trace_sample
         opts.active_start = active_start
         opts.wide_weights = 1 if wide_weights else 0
+        opts.giant_degree = giant_degree
+        opts.warp_limit = warp_limit
         h = C.c_void_p()
         if device_csr is not None:
             rp, cl, w, V, E = device_csr
@@ -480,6 +550,13 @@ class Louvain:
         st = _Stats()
         self._c(lib().lv_get_stats(self._h, C.byref(st)))
         return {k: getattr(st, k) for k, _ in _Stats._fields_}
+
+    def level_classes(self):
+        """(vertices, entries) per work class of the current level."""
+        v = np.zeros(NUM_CLASSES, np.int32)
+        e = np.zeros(NUM_CLASSES, np.int64)
+        self._c(lib().lv_get_level_classes(self._h, _ptr(v, C.c_int32), _ptr(e, C.c_int64)))
+        return v, e
 
     def class_stats(self) -> dict:
         st = _ClassStats()
@@ -726,3 +803,9 @@ def run_batch_sharded(graphs, min_gain: float, *, max_sweeps: int = 0, device: i
         for i, r in part:
             out[i] = r
     return out
+
+
+def tune(graph=None, **kw) -> dict:
+    """Choose the work-mapping knobs for a graph on this GPU (autotune.tune)."""
+    import importlib
+    return importlib.import_module(__name__ + ".autotune").tune(graph, **kw)

@@ -73,7 +73,8 @@ __device__ __forceinline__ int class_at(const ActiveClassOffsets &co, int32_t p)
 
 // One position of the level's vertex list per thread.  Vertices of class
 // >= keep_cls are always active.  alist != nullptr: active vertices are
-// compacted into alist at their class's offset (acnt[c] counts them);
+// compacted into alist at their class's offset (acnt[c] counts them) and,
+// when fresh is given, marked fresh (evaluated since the last full sweep);
 // pred != nullptr: pred[v] = active.
 __global__ void __launch_bounds__(256) active_select_kernel(const int32_t *__restrict__ list, int32_t n,
                                                             ActiveClassOffsets co, const int32_t *__restrict__ rowptr,
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(256) active_select_kernel(const int32_t *__res
                                                             const int32_t *__restrict__ nmoved,
                                                             const uint16_t *__restrict__ model, float logit_thr,
                                                             int keep_cls, int32_t *alist, int32_t *acnt,
-                                                            uint8_t *pred) {
+                                                            uint8_t *pred, uint8_t *fresh) {
     __shared__ float w[NP];
     __shared__ int32_t lc[NCLS], base[NCLS];
     load_model(model, w);
@@ -104,7 +105,10 @@ __global__ void __launch_bounds__(256) active_select_kernel(const int32_t *__res
             act = mlp_logit(w, x) > logit_thr;
         }
         if (pred) pred[v] = act ? 1 : 0;
-        if (alist && act) rank = atomicAdd(&lc[c], 1);
+        if (alist && act) {
+            rank = atomicAdd(&lc[c], 1);
+            if (fresh) fresh[v] = 1;
+        }
     }
     if (!alist) return;
     __syncthreads();
@@ -113,23 +117,35 @@ __global__ void __launch_bounds__(256) active_select_kernel(const int32_t *__res
     if (act) alist[co.off[c] + base[c] + rank] = v;
 }
 
-// moved[v] = comm[v] != prev[v]; counts[0] += movers, counts[1] += movers
-// with pred[v] set (when pred is given).
+// moved[v] = comm[v] != prev[v]; counts[0] += movers.  When pred is given
+// (a full sweep measuring the predictor), the recall counts only the fresh
+// vertices (evaluated in an active sweep since the last full sweep, whose
+// features are current): counts[3] += fresh movers, counts[1] += fresh
+// movers with pred[v] set; fresh is then cleared.
 __global__ void __launch_bounds__(256) active_moved_kernel(const int32_t *__restrict__ comm,
                                                            const int32_t *__restrict__ prev, int32_t V,
                                                            uint8_t *moved, const uint8_t *__restrict__ pred,
-                                                           u64 *counts) {
-    u64 m = 0, hit = 0;
+                                                           uint8_t *fresh, u64 *counts) {
+    u64 m = 0, fm = 0, hit = 0;
     for (int32_t v = blockIdx.x * 256 + threadIdx.x; v < V; v += gridDim.x * 256) {
         const bool mv = comm[v] != prev[v];
         moved[v] = mv ? 1 : 0;
         m += mv ? 1 : 0;
-        if (pred && mv && pred[v]) hit += 1;
+        if (pred) {
+            const bool f = fresh[v] != 0;
+            if (f) fresh[v] = 0;
+            if (mv && f) {
+                fm += 1;
+                if (pred[v]) hit += 1;
+            }
+        }
     }
     m = warp_sum_u64(m);
+    fm = warp_sum_u64(fm);
     hit = warp_sum_u64(hit);
     if ((threadIdx.x & 31) == 0) {
         if (m) atomicAdd(counts, m);
+        if (fm) atomicAdd(counts + 3, fm);
         if (hit) atomicAdd(counts + 1, hit);
     }
 }
@@ -203,17 +219,18 @@ inline unsigned grid_of(int64_t n, int64_t cap = 148 * 16) {
 void launch_active_select(const int32_t *list, int32_t n, const ActiveClassOffsets &co, const int32_t *rowptr,
                           const int32_t *rowend, const float *feat, const uint8_t *moved, const int32_t *nmoved,
                           const uint16_t *model, float logit_thr, int keep_cls, int32_t *alist, int32_t *acnt,
-                          uint8_t *pred, cudaStream_t s) {
+                          uint8_t *pred, uint8_t *fresh, cudaStream_t s) {
     if (n <= 0) return;
     active_select_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(list, n, co, rowptr, rowend, feat, moved, nmoved,
-                                                                    model, logit_thr, keep_cls, alist, acnt, pred);
+                                                                    model, logit_thr, keep_cls, alist, acnt, pred,
+                                                                    fresh);
     note_launches(1);
 }
 
 void launch_active_moved(const int32_t *comm, const int32_t *prev, int32_t V, uint8_t *moved, const uint8_t *pred,
-                         u64 *counts, cudaStream_t s) {
+                         uint8_t *fresh, u64 *counts, cudaStream_t s) {
     if (V <= 0) return;
-    active_moved_kernel<<<grid_of(V), 256, 0, s>>>(comm, prev, V, moved, pred, counts);
+    active_moved_kernel<<<grid_of(V), 256, 0, s>>>(comm, prev, V, moved, pred, fresh, counts);
     note_launches(1);
 }
 

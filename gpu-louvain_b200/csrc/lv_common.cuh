@@ -64,11 +64,15 @@ enum WorkClass {
     CLS_HG,       // > 8192      edge chunks staged and merged (bucket 6)
     NCLS
 };
-constexpr int HG_MIN_DEG = 8192;   // giants: degree above this
+// Giants: degree above giant_degree (a tuning knob, lv_opts.giant_degree:
+// default HG_MIN_DEG, at least HG_MIN_DEG_LO so that CLS_H1 is unchanged, at
+// most HG_MIN_DEG_HI so that a warp's row fits its piece counters).
+constexpr int HG_MIN_DEG = 8192;
+constexpr int HG_MIN_DEG_LO = 1024, HG_MIN_DEG_HI = 65536;
 // class -> update bucket
 __host__ __device__ constexpr int class_bucket(int c) { return c < CLS_H1 ? c : 6; }
 
-__host__ __device__ __forceinline__ int degree_class(int32_t d) {
+__host__ __device__ __forceinline__ int degree_class(int32_t d, int32_t giant_degree = HG_MIN_DEG) {
     if (d <= 0) return -1;
     if (d <= 4) return CLS_B0;
     if (d <= 8) return CLS_B1;
@@ -77,7 +81,7 @@ __host__ __device__ __forceinline__ int degree_class(int32_t d) {
     if (d <= 84) return CLS_B4;
     if (d <= 319) return CLS_B5;
     if (d <= 1024) return CLS_H1;
-    if (d <= HG_MIN_DEG) return CLS_H2;
+    if (d <= giant_degree) return CLS_H2;
     return CLS_HG;
 }
 

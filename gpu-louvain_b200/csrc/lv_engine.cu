@@ -94,6 +94,7 @@ struct lv_handle {
     u64 T = 0;
     int exact = 1;
     bool w0_narrow = false;   // level-0 fixed-point weights are all below 2^32
+    int32_t giant_degree = HG_MIN_DEG;   // work-mapping knobs (lv_opts.giant_degree, warp_limit)
 
     int level = 0;
     int32_t V = 0;
@@ -160,6 +161,7 @@ struct lv_handle {
     uint8_t *moved = nullptr;       // [V0] moved in the previous sweep
     int32_t *nmoved = nullptr;      // [V0] row entries whose vertex moved in the previous sweep
     uint8_t *pred = nullptr;        // [V0] proposed by the predictor
+    uint8_t *fresh = nullptr;       // [V0] evaluated in an active sweep since the last full sweep
     int32_t *comm_prev = nullptr;   // [V0] communities before the sweep
     int32_t *alist = nullptr;       // [V0] proposed vertices, at their class's offset
     int32_t *acnt = nullptr;        // [NCLS] proposed vertices per class
@@ -573,7 +575,7 @@ int compute_k(lv_handle *h) {
 int level_setup(lv_handle *h) {
     Timer t(h, 103);
     int32_t *counts = h->cls_scratch, *cursors = h->cls_scratch + CLASS_COUNT_WORDS;
-    launch_class_count(h->cur_rowptr, h->cur_rowend, h->V, counts, h->stream);
+    launch_class_count(h->cur_rowptr, h->cur_rowend, h->V, h->giant_degree, counts, h->stream);
     LV_CUDA(h, cudaMemcpyAsync(h->small_h, counts, sizeof(int32_t) * CLASS_COUNT_WORDS,
                                cudaMemcpyDeviceToHost, h->stream));
     LV_TRY(sync(h));
@@ -583,13 +585,14 @@ int level_setup(lv_handle *h) {
         h->cls_off[c + 1] = h->cls_off[c] + h->small_h[c];
         h->cls_edges[c] = (int64_t)esum[c];
     }
-    launch_class_scatter(h->cur_rowptr, h->cur_rowend, h->V, h->cls_off, cursors, h->list, h->fb.hint,
+    launch_class_scatter(h->cur_rowptr, h->cur_rowend, h->V, h->giant_degree, h->fb.warp_limit, h->cls_off,
+                         cursors, h->list, h->fb.hint,
                          h->stream);
     if (h->level == 0) {
         LV_TRY(compute_k<float>(h));
     }
     launch_level_init(h->comm, h->newc, h->size, h->k, h->S, h->V, h->stream);
-    // giants (degree > HG_MIN_DEG): staging areas and global tables
+    // giants (degree > giant_degree): staging areas and global tables
     const int32_t nh = h->cls_off[CLS_HG + 1] - h->cls_off[CLS_HG];
     std::vector<int32_t> ids(nh), deg(nh);
     if (nh > 0) {
@@ -646,7 +649,7 @@ void enqueue_sweep(lv_handle *h) {
             launch_move_class<WT>(b, g, st, h->list + lo, hi - lo, h->di, dE, h->stream, narrow_weights<WT>(h));
         else if (hg0 > lo)
             launch_move_wide<WT>(g, st, h->list + lo, hg0 - lo, h->fb, h->di, dE, h->stream,
-                                 b == 6 ? HG_MIN_DEG : (b == 4 ? 84 : 319), narrow_weights<WT>(h));
+                                 b == 6 ? h->giant_degree : (b == 4 ? 84 : 319), narrow_weights<WT>(h));
         if (tc) {
             tc->stop();
             delete tc;
@@ -911,6 +914,8 @@ int ensure_active(lv_handle *h) {
     LV_TRY(dalloc(h, &h->moved, V));
     LV_TRY(dalloc(h, &h->nmoved, V));
     LV_TRY(dalloc(h, &h->pred, V));
+    LV_TRY(dalloc(h, &h->fresh, V));
+    LV_CUDA(h, cudaMemsetAsync(h->fresh, 0, V, h->stream));
     LV_TRY(dalloc(h, &h->comm_prev, V));
     LV_TRY(dalloc(h, &h->alist, V));
     LV_TRY(dalloc(h, &h->acnt, (size_t)NCLS));
@@ -946,7 +951,7 @@ void enqueue_sweep_active(lv_handle *h, const int32_t *cnt) {
         } else {
             for (int c = c0; c < c1; ++c) {
                 if (c == CLS_HG || !cnt[c]) continue;
-                const int32_t maxdeg = c == CLS_B4 ? 84 : (c == CLS_B5 ? 319 : (c == CLS_H1 ? 1024 : HG_MIN_DEG));
+                const int32_t maxdeg = c == CLS_B4 ? 84 : (c == CLS_B5 ? 319 : (c == CLS_H1 ? 1024 : h->giant_degree));
                 launch_move_wide<WT>(g, st, h->alist + h->cls_off[c], cnt[c], h->fb, h->di, dE, h->stream, maxdeg,
                                      narrow_weights<WT>(h));
             }
@@ -965,9 +970,10 @@ void enqueue_sweep_active(lv_handle *h, const int32_t *cnt) {
 // proposed vertices; predict = run the predictor first (the proposal of an
 // active sweep, or the flags whose recall a full sweep measures).
 int sweep_learned(lv_handle *h, bool full, bool predict, int64_t *moves, double *q, int64_t *movers,
-                  int64_t *hits) {
+                  int64_t *hits, int64_t *fresh_movers) {
     LV_TRY(reset_totals(h));
     LV_CUDA(h, cudaMemsetAsync(h->actr, 0, 2 * sizeof(u64), h->stream));
+    LV_CUDA(h, cudaMemsetAsync(h->actr + 3, 0, sizeof(u64), h->stream));
     const int32_t n = h->cls_off[NCLS];
     ActiveClassOffsets co;
     for (int c = 0; c <= NCLS; ++c) co.off[c] = h->cls_off[c];
@@ -976,7 +982,7 @@ int sweep_learned(lv_handle *h, bool full, bool predict, int64_t *moves, double 
     if (predict) {
         if (!full) LV_CUDA(h, cudaMemsetAsync(h->acnt, 0, NCLS * sizeof(int32_t), h->stream));
         launch_active_select(h->list, n, co, h->cur_rowptr, rowend, h->feat, h->moved, h->nmoved, h->model, h->logit_thr,
-                             CLS_HG, full ? nullptr : h->alist, h->acnt, h->pred, h->stream);
+                             CLS_HG, full ? nullptr : h->alist, h->acnt, h->pred, h->fresh, h->stream);
         if (!full) {
             LV_CUDA(h, cudaMemcpyAsync(h->small_h, h->acnt, NCLS * sizeof(int32_t), cudaMemcpyDeviceToHost,
                                        h->stream));
@@ -1008,13 +1014,13 @@ int sweep_learned(lv_handle *h, bool full, bool predict, int64_t *moves, double 
         launch_s2(h->S, h->V, h->tot_d->s2, h->stream);
         tm.stop();
     }
-    launch_active_moved(h->comm, h->comm_prev, h->V, h->moved, predict && full ? h->pred : nullptr, h->actr,
-                        h->stream);
+    launch_active_moved(h->comm, h->comm_prev, h->V, h->moved, predict && full ? h->pred : nullptr, h->fresh,
+                        h->actr, h->stream);
     launch_nbr_moved(h->cur_rowptr, rowend, h->cur_col, h->V, h->moved, h->nmoved, h->stream);
     if (tracing && h->tr_sweep > 0)
         launch_trace_label(h->tr_v, h->moved, h->tr_rows, h->actr + 2, h->tr_cap, h->tr_y, h->stream);
-    u64 ctr[3];
-    LV_CUDA(h, cudaMemcpyAsync(ctr, h->actr, 3 * sizeof(u64), cudaMemcpyDeviceToHost, h->stream));
+    u64 ctr[4];
+    LV_CUDA(h, cudaMemcpyAsync(ctr, h->actr, 4 * sizeof(u64), cudaMemcpyDeviceToHost, h->stream));
     LV_TRY(read_totals(h));
     if (tracing) {
         if (h->tr_sweep > 0) h->tr_rows = (int64_t)ctr[2] < h->tr_cap ? (int64_t)ctr[2] : h->tr_cap;
@@ -1026,6 +1032,7 @@ int sweep_learned(lv_handle *h, bool full, bool predict, int64_t *moves, double 
     *moves = (int64_t)t.moves;
     *movers = (int64_t)ctr[0];
     *hits = (int64_t)ctr[1];
+    *fresh_movers = (int64_t)ctr[3];
     *q = q_from_totals(h->T, t);
     h->st.sweeps += 1;
     h->st.edge_sweeps += h->E;
@@ -1037,9 +1044,10 @@ int sweep_learned(lv_handle *h, bool full, bool predict, int64_t *moves, double 
 // moves fewer than active_start of the level's vertices (the early sweeps,
 // where most vertices move, stay exactly the plain method's); after that
 // every active_full_every-th sweep evaluates every vertex and the others only
-// the proposed ones.  A full sweep after a proposal measures its recall
-// (proposed movers / movers); below active_min_recall the plain sweep takes
-// over for the rest of the level.  An active sweep that gains less than
+// the proposed ones.  A full sweep after a proposal measures its recall over
+// the vertices evaluated since the previous full sweep (movers the predictor
+// proposes now / movers among them); below active_min_recall the plain sweep
+// takes over for the rest of the level.  An active sweep that gains less than
 // min_gain (or moves nothing) is followed by a full sweep, and the level ends
 // as the plain loop does, on a full sweep.  Without a model (trace recording
 // only) every sweep is full and the result equals the plain loop's.
@@ -1048,6 +1056,7 @@ int optimise_level_learned(lv_handle *h, float min_gain, int32_t *changed) {
     LV_CUDA(h, cudaMemsetAsync(h->feat, 0, sizeof(float) * 2 * (size_t)h->V, h->stream));
     LV_CUDA(h, cudaMemsetAsync(h->moved, 0, (size_t)h->V, h->stream));
     LV_CUDA(h, cudaMemsetAsync(h->nmoved, 0, sizeof(int32_t) * (size_t)h->V, h->stream));
+    LV_CUDA(h, cudaMemsetAsync(h->fresh, 0, (size_t)h->V, h->stream));
     h->tr_sweep = 0;
     double q_before = 0, q_after = 0;
     LV_TRY(modularity(h, &q_before));
@@ -1061,8 +1070,8 @@ int optimise_level_learned(lv_handle *h, float min_gain, int32_t *changed) {
         if (h->opts.max_sweeps > 0 && sweeps >= h->opts.max_sweeps) break;
         const bool full = force_full || plain_rest || !proposing || since_full + 1 >= K;
         const bool predict = learned && !plain_rest && proposing;
-        int64_t moves = 0, movers = 0, hits = 0;
-        LV_TRY(sweep_learned(h, full, predict, &moves, &q_after, &movers, &hits));
+        int64_t moves = 0, movers = 0, hits = 0, fresh_movers = 0;
+        LV_TRY(sweep_learned(h, full, predict, &moves, &q_after, &movers, &hits, &fresh_movers));
         sweeps++;
         const double gain = q_after - q_before;
         if (gain > 0) ch = 1;
@@ -1073,7 +1082,10 @@ int optimise_level_learned(lv_handle *h, float min_gain, int32_t *changed) {
             force_full = false;
             if ((double)movers < start * (double)h->V) proposing = true;
             if (predict) {
-                h->act_recall = movers > 0 ? (double)hits / (double)movers : 1.0;
+                // recall over the movers whose features are current (evaluated
+                // since the last full sweep): what the predictor caught, not
+                // the moves it postponed
+                h->act_recall = fresh_movers > 0 ? (double)hits / (double)fresh_movers : 1.0;
                 if (h->act_recall < rmin) {
                     plain_rest = true;
                     h->act_fell_back = 1;
@@ -1267,7 +1279,7 @@ int finish_create(lv_handle *h) {
     LV_TRY(dalloc(h, &h->cls_scratch, V + SCRATCH_OFF + 16));
     {
         // fallback work lists of the move phase.  Only vertices of degree
-        // > WARP_LIMIT are queued (at most E / WARP_LIMIT of them at any
+        // > warp_limit are queued (at most E / warp_limit of them at any
         // level); a large item covers FB_KEYS edges of a vertex of degree
         // > FBQ_MAXDEG(NFBQ - 1), or as many staged pairs of a giant.
         FallbackSet &fs = h->fb;
@@ -1275,7 +1287,7 @@ int finish_create(lv_handle *h) {
         LV_TRY(dalloc(h, &counters, 2 * (NFBQ + 1)));
         LV_TRY(dalloc(h, &fs.hint, V + 1));
         LV_CUDA(h, cudaMemsetAsync(fs.hint, 0, V + 1, h->stream));
-        const size_t cap_row = (size_t)(h->E0 / WARP_LIMIT) + 64;
+        const size_t cap_row = (size_t)(h->E0 / fs.warp_limit) + 64;
         const size_t cap_large = (size_t)(2 * (h->E0 / FBQ_MAXDEG(NFBQ - 1) + h->E0 / FB_KEYS)) + 64;
         for (int q = 0; q <= NFBQ; ++q) {
             Fallback &f = fs.q[q];
@@ -1355,6 +1367,19 @@ int begin_create(const lv_opts *opts, int32_t V, int64_t E, lv_handle **out, lv_
         delete h;
         return LV_ERR_INVALID;
     }
+    // work-mapping knobs (0 = default); results never depend on them
+    if (h->opts.giant_degree != 0 &&
+        (h->opts.giant_degree < HG_MIN_DEG_LO || h->opts.giant_degree > HG_MIN_DEG_HI)) {
+        delete h;
+        return LV_ERR_INVALID;
+    }
+    if (h->opts.warp_limit != 0 && (h->opts.warp_limit < WARP_LIMIT_MIN || h->opts.warp_limit > WARP_LIMIT_MAX)) {
+        delete h;
+        return LV_ERR_INVALID;
+    }
+    h->giant_degree = h->opts.giant_degree ? h->opts.giant_degree : HG_MIN_DEG;
+    h->fb.warp_limit = h->opts.warp_limit ? h->opts.warp_limit : WARP_LIMIT;
+    h->fb.hint_set = (h->fb.warp_limit * 3) / 4;
     h->device = h->opts.device;
     cudaSetDevice(h->device);
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -1453,9 +1478,11 @@ int lv_destroy(lv_handle *h) {
     dfree(h, h->mslot); dfree(h, h->degm); dfree(h, h->P);
     for (int b = 0; b < 2; ++b) {
         dfree(h, h->lvl_start[b]); dfree(h, h->lvl_end[b]); dfree(h, h->lvl_col[b]); dfree(h, h->lvl_w[b]);
+        dfree(h, h->lvl_w32[b]);
     }
     dfree(h, h->tot_d);
-    dfree(h, h->feat); dfree(h, h->moved); dfree(h, h->nmoved); dfree(h, h->pred); dfree(h, h->comm_prev); dfree(h, h->alist);
+    dfree(h, h->feat); dfree(h, h->moved); dfree(h, h->nmoved); dfree(h, h->pred); dfree(h, h->fresh);
+    dfree(h, h->comm_prev); dfree(h, h->alist);
     dfree(h, h->acnt); dfree(h, h->actr); dfree(h, h->model); dfree(h, h->tr_x); dfree(h, h->tr_v);
     dfree(h, h->tr_y);
     {
@@ -1613,6 +1640,26 @@ int lv_get_level_info(lv_handle *h, int32_t *V, int64_t *E, int32_t *level) {
     if (V) *V = h->V;
     if (E) *E = h->E;
     if (level) *level = h->level;
+    return LV_OK;
+}
+
+int lv_get_level_classes(lv_handle *h, int32_t *vertices, int64_t *entries) {
+    if (!h) return LV_ERR_INVALID;
+    for (int c = 0; c < NCLS; ++c) {
+        if (vertices) vertices[c] = h->cls_off[c + 1] - h->cls_off[c];
+        if (entries) entries[c] = h->cls_edges[c];
+    }
+    return LV_OK;
+}
+
+int lv_get_device_name(int32_t device, char *name, int32_t len) {
+    if (!name || len <= 0) return LV_ERR_INVALID;
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, device) != cudaSuccess) {
+        cudaGetLastError();
+        return LV_ERR_NO_DEVICE;
+    }
+    std::snprintf(name, (size_t)len, "%s (sm_%d%d, %d SMs)", p.name, p.major, p.minor, p.multiProcessorCount);
     return LV_OK;
 }
 

@@ -288,9 +288,14 @@ int lv_read_csr(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr
     return LV_OK;
 }
 
-int lv_read_mtx(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr_out,
-                int32_t **col_out, float **w_out, float *m_ref) {
-    if (!path || !Vout || !Eout || !rowptr_out || !col_out || !w_out) return LV_ERR_INVALID;
+}  // extern "C"
+
+namespace {
+
+// The header and the entries of a Matrix Market file, in file order
+// (0-based): the vertex count is the size line's second number.
+int read_mtx_entries(const char *path, int32_t *Vout, std::vector<int32_t> &ea, std::vector<int32_t> &eb,
+                     std::vector<float> &ew) {
     Mapped m;
     m.fd = open(path, O_RDONLY);
     if (m.fd < 0) return LV_ERR_IO;
@@ -330,11 +335,40 @@ int lv_read_mtx(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr
     if (cols < 0 || nnz < 0) return LV_ERR_IO;
     if (cols > 0x7ffffffeLL) return LV_ERR_TOO_LARGE;
     const int32_t V = (int32_t)cols;
-    std::vector<int32_t> ea((size_t)nnz), eb((size_t)nnz);
-    std::vector<float> ew((size_t)nnz);
+    ea.resize((size_t)nnz);
+    eb.resize((size_t)nnz);
+    ew.resize((size_t)nnz);
     int prc = parse_entries_parallel(p, end, nnz, pattern, V, ea.data(), eb.data(), ew.data());
     if (prc == PARSE_SEQUENTIAL) prc = parse_entries(p, end, nnz, pattern, V, ea.data(), eb.data(), ew.data());
     if (prc != LV_OK) return prc;
+    *Vout = V;
+    return LV_OK;
+}
+
+// M as the reference accumulates it: a sequential float sum of every entry's
+// weight, counted twice for off-diagonal entries, halved (utils.cu:36-46).
+float reference_m(const std::vector<int32_t> &ea, const std::vector<int32_t> &eb, const std::vector<float> &ew) {
+    float M = 0;
+    for (size_t i = 0; i < ea.size(); ++i) {
+        if (ea[i] != eb[i]) M += ew[i];
+        M += ew[i];
+    }
+    return M / 2;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lv_read_mtx(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr_out,
+                int32_t **col_out, float **w_out, float *m_ref) {
+    if (!path || !Vout || !Eout || !rowptr_out || !col_out || !w_out) return LV_ERR_INVALID;
+    int32_t V = 0;
+    std::vector<int32_t> ea, eb;
+    std::vector<float> ew;
+    const int prc = read_mtx_entries(path, &V, ea, eb, ew);
+    if (prc != LV_OK) return prc;
+    const long long nnz = (long long)ea.size();
     // degrees: v1 gets (v2,w); v2 gets (v1,w) unless self-loop (utils.cu:32-46)
     std::vector<int64_t> deg((size_t)V + 1, 0);
     int64_t E = 0;
@@ -386,6 +420,57 @@ int lv_read_mtx(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr
     *col_out = cl;
     *w_out = wt;
     if (m_ref) *m_ref = M;
+    return LV_OK;
+}
+
+int lv_read_mtx_entries(const char *path, int32_t *Vout, int64_t *nnz_out, int32_t **v1, int32_t **v2, float **w) {
+    if (!path || !Vout || !nnz_out || !v1 || !v2 || !w) return LV_ERR_INVALID;
+    int32_t V = 0;
+    std::vector<int32_t> ea, eb;
+    std::vector<float> ew;
+    try {
+        const int prc = read_mtx_entries(path, &V, ea, eb, ew);
+        if (prc != LV_OK) return prc;
+    } catch (const std::bad_alloc &) {
+        return LV_ERR_NOMEM;
+    }
+    const size_t n = ea.size() > 0 ? ea.size() : 1;
+    int32_t *a = (int32_t *)std::malloc(sizeof(int32_t) * n), *b = (int32_t *)std::malloc(sizeof(int32_t) * n);
+    float *x = (float *)std::malloc(sizeof(float) * n);
+    if (!a || !b || !x) {
+        std::free(a); std::free(b); std::free(x);
+        return LV_ERR_NOMEM;
+    }
+    if (!ea.empty()) {
+        std::memcpy(a, ea.data(), sizeof(int32_t) * ea.size());
+        std::memcpy(b, eb.data(), sizeof(int32_t) * eb.size());
+        std::memcpy(x, ew.data(), sizeof(float) * ew.size());
+    }
+    *Vout = V;
+    *nnz_out = (int64_t)ea.size();
+    *v1 = a;
+    *v2 = b;
+    *w = x;
+    return LV_OK;
+}
+
+int lv_read_mtx_device(const char *path, int32_t device, int32_t *Vout, int64_t *Eout, int32_t **d_rowptr,
+                       int32_t **d_col, float **d_w, float *m_ref) {
+    if (!path || !Vout || !Eout || !d_rowptr || !d_col || !d_w) return LV_ERR_INVALID;
+    int32_t V = 0;
+    std::vector<int32_t> ea, eb;
+    std::vector<float> ew;
+    try {
+        const int prc = read_mtx_entries(path, &V, ea, eb, ew);
+        if (prc != LV_OK) return prc;
+    } catch (const std::bad_alloc &) {
+        return LV_ERR_NOMEM;
+    }
+    const int rc = lv_csr_from_entries_device(device, V, (int64_t)ea.size(), ea.data(), eb.data(), ew.data(), Eout,
+                                              d_rowptr, d_col, d_w);
+    if (rc != LV_OK) return rc;
+    *Vout = V;
+    if (m_ref) *m_ref = reference_m(ea, eb, ew);
     return LV_OK;
 }
 
@@ -636,13 +721,18 @@ int lv_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed, double a, dou
     return rc;
 }
 
-int lv_gen_planted(int32_t V, int32_t blocks, double d_in, double d_out, uint64_t seed,
-                   int32_t weight_mode, int64_t *Eout, int32_t **rowptr, int32_t **col, float **w) {
-    if (V < 1 || blocks < 1 || blocks > V || d_in < 0 || d_out < 0 || !Eout || !rowptr || !col || !w)
-        return LV_ERR_INVALID;
+}  // extern "C"
+
+namespace {
+
+// The sorted, unique undirected pairs (lo << 32 | hi) of a planted-partition
+// draw; false for invalid arguments.
+bool planted_keys(int32_t V, int32_t blocks, double d_in, double d_out, uint64_t seed,
+                  std::vector<uint64_t> &keys) {
+    if (V < 1 || blocks < 1 || blocks > V || d_in < 0 || d_out < 0) return false;
     const int64_t m_in = (int64_t)std::llround((double)V * d_in / 2.0);
     const int64_t m_out = (int64_t)std::llround((double)V * d_out / 2.0);
-    std::vector<uint64_t> keys;
+    keys.clear();
     keys.reserve((size_t)(m_in + m_out));
     const uint64_t k1 = lvrng::stream_key(seed, 1), k2 = lvrng::stream_key(seed, 2);
     for (int64_t i = 0; i < m_in + m_out; ++i) {
@@ -655,7 +745,99 @@ int lv_gen_planted(int32_t V, int32_t blocks, double d_in, double d_out, uint64_
     }
     std::sort(keys.begin(), keys.end());
     keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lv_gen_planted(int32_t V, int32_t blocks, double d_in, double d_out, uint64_t seed,
+                   int32_t weight_mode, int64_t *Eout, int32_t **rowptr, int32_t **col, float **w) {
+    if (!Eout || !rowptr || !col || !w) return LV_ERR_INVALID;
+    std::vector<uint64_t> keys;
+    if (!planted_keys(V, blocks, d_in, d_out, seed, keys)) return LV_ERR_INVALID;
     return keys_to_csr(keys, 32, V, weight_mode, seed, Eout, rowptr, col, w);
+}
+
+int lv_gen_planted_batch(int32_t G, const int32_t *V, const int32_t *blocks, const double *d_in,
+                         const double *d_out, const uint64_t *seeds, int32_t weight_mode, int32_t *Vtot,
+                         int64_t *Etot, int32_t **rowptr, int32_t **col, float **w, int32_t **graph_ptr) {
+    if (G < 0 || !Vtot || !Etot || !rowptr || !col || !w || !graph_ptr ||
+        (G > 0 && (!V || !blocks || !d_in || !d_out || !seeds)))
+        return LV_ERR_INVALID;
+    struct One {
+        int32_t *rp = nullptr, *cl = nullptr;
+        float *wt = nullptr;
+        int64_t E = 0;
+        int rc = LV_OK;
+    };
+    std::vector<One> parts((size_t)G);
+    try {
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int32_t i = 0; i < G; ++i) {
+            std::vector<uint64_t> keys;
+            One &o = parts[(size_t)i];
+            try {
+                if (!planted_keys(V[i], blocks[i], d_in[i], d_out[i], seeds[i], keys)) o.rc = LV_ERR_INVALID;
+                else o.rc = keys_to_csr(keys, 32, V[i], weight_mode, seeds[i], &o.E, &o.rp, &o.cl, &o.wt);
+            } catch (const std::bad_alloc &) {
+                o.rc = LV_ERR_NOMEM;
+            }
+        }
+    } catch (const std::bad_alloc &) {
+        return LV_ERR_NOMEM;
+    }
+    int rc = LV_OK;
+    int64_t nv = 0, ne = 0;
+    for (int32_t i = 0; i < G; ++i) {
+        if (parts[(size_t)i].rc != LV_OK && rc == LV_OK) rc = parts[(size_t)i].rc;
+        nv += V[i];
+        ne += parts[(size_t)i].E;
+    }
+    if (rc == LV_OK && (nv >= 0x7fffffffLL - G || ne > 0x7fffffffLL)) rc = LV_ERR_TOO_LARGE;
+    int32_t *rp = nullptr, *cl = nullptr, *gp = nullptr;
+    float *wt = nullptr;
+    if (rc == LV_OK) {
+        rp = (int32_t *)std::malloc(sizeof(int32_t) * ((size_t)nv + 1));
+        cl = (int32_t *)std::malloc(sizeof(int32_t) * (size_t)(ne > 0 ? ne : 1));
+        wt = (float *)std::malloc(sizeof(float) * (size_t)(ne > 0 ? ne : 1));
+        gp = (int32_t *)std::malloc(sizeof(int32_t) * ((size_t)G + 1));
+        if (!rp || !cl || !wt || !gp) rc = LV_ERR_NOMEM;
+    }
+    if (rc == LV_OK) {
+        std::vector<int64_t> v0((size_t)G + 1, 0), e0((size_t)G + 1, 0);
+        for (int32_t i = 0; i < G; ++i) {
+            v0[(size_t)i + 1] = v0[(size_t)i] + V[i];
+            e0[(size_t)i + 1] = e0[(size_t)i] + parts[(size_t)i].E;
+        }
+        rp[0] = 0;
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int32_t i = 0; i < G; ++i) {
+            const One &o = parts[(size_t)i];
+            const int64_t vb = v0[(size_t)i], eb = e0[(size_t)i];
+            for (int32_t v = 1; v <= V[i]; ++v) rp[vb + v] = (int32_t)(eb + o.rp[v]);
+            for (int64_t e = 0; e < o.E; ++e) {
+                cl[eb + e] = (int32_t)(vb + o.cl[e]);
+                wt[eb + e] = o.wt[e];
+            }
+        }
+        for (int32_t i = 0; i <= G; ++i) gp[i] = (int32_t)v0[(size_t)i];
+    }
+    for (One &o : parts) {
+        std::free(o.rp); std::free(o.cl); std::free(o.wt);
+    }
+    if (rc != LV_OK) {
+        std::free(rp); std::free(cl); std::free(wt); std::free(gp);
+        return rc;
+    }
+    *Vtot = (int32_t)nv;
+    *Etot = ne;
+    *rowptr = rp;
+    *col = cl;
+    *w = wt;
+    *graph_ptr = gp;
+    return LV_OK;
 }
 
 

@@ -71,12 +71,12 @@ struct ActiveClassOffsets {
 void launch_active_select(const int32_t *list, int32_t n, const ActiveClassOffsets &co, const int32_t *rowptr,
                           const int32_t *rowend, const float *feat, const uint8_t *moved, const int32_t *nmoved,
                           const uint16_t *model, float logit_thr, int keep_cls, int32_t *alist, int32_t *acnt,
-                          uint8_t *pred, cudaStream_t s);
+                          uint8_t *pred, uint8_t *fresh, cudaStream_t s);
 // nmoved[x] = number of row entries of x whose vertex moved (recomputed)
 void launch_nbr_moved(const int32_t *rowptr, const int32_t *rowend, const int32_t *col, int32_t V,
                       const uint8_t *moved, int32_t *nmoved, cudaStream_t s);
 void launch_active_moved(const int32_t *comm, const int32_t *prev, int32_t V, uint8_t *moved, const uint8_t *pred,
-                         u64 *counts, cudaStream_t s);
+                         uint8_t *fresh, u64 *counts, cudaStream_t s);
 void launch_trace_sample(int32_t V, const int32_t *rowptr, const int32_t *rowend, const float *feat,
                          const uint8_t *moved, const int32_t *nmoved, u64 thr, u64 key, float *tx, int32_t *tv,
                          int64_t cap, u64 *tcount, cudaStream_t s);
@@ -117,13 +117,19 @@ struct Fallback {
     int32_t *cnt = nullptr;     // distinct communities seen by the item
 };
 
-// The three fallback queues and the per-vertex hint "had more than
-// WARP_LIMIT distinct neighbour communities at its last evaluation" (such a
-// vertex skips the warp attempt; the hint only routes work, results do not
-// depend on it).
+// The fallback queues and the per-vertex hint "had more than 3/4 of
+// warp_limit distinct neighbour communities at its last evaluation" (such a
+// vertex of degree > warp_limit skips the warp attempt; the hint only routes
+// work, results do not depend on it).  warp_limit: distinct communities after
+// which the warp kernel hands a vertex to a fallback CTA (a tuning knob,
+// lv_opts.warp_limit, at most WARP_LIMIT_MAX so that every claim fits the
+// warp table).
+constexpr int WARP_LIMIT_MIN = 32, WARP_LIMIT_MAX = 384;
 struct FallbackSet {
     Fallback q[NFBQ + 1];   // row queues by degree, then the large queue
     uint8_t *hint = nullptr;
+    int32_t warp_limit = 352;
+    int32_t hint_set = 264;   // hint = distinct count above this
 };
 
 // Launch geometry helpers (filled once per device).
@@ -177,11 +183,11 @@ void scan_exclusive_i32(const int32_t *in, int32_t *out, int64_t n, int32_t *tot
 // The count buffer holds CLASS_COUNT_WORDS int32: NCLS vertex counts, then
 // (8-byte aligned) NCLS uint64 edge totals.
 constexpr int CLASS_COUNT_WORDS = NCLS + (NCLS & 1) + 2 * NCLS;
-void launch_class_count(const int32_t *rowptr, const int32_t *rowend, int32_t V, int32_t *counts,
-                        cudaStream_t s);
-void launch_class_scatter(const int32_t *rowptr, const int32_t *rowend, int32_t V,
-                          const int32_t *offsets, int32_t *cursors, int32_t *list, uint8_t *hint,
-                          cudaStream_t s);
+void launch_class_count(const int32_t *rowptr, const int32_t *rowend, int32_t V, int32_t giant_degree,
+                        int32_t *counts, cudaStream_t s);
+void launch_class_scatter(const int32_t *rowptr, const int32_t *rowend, int32_t V, int32_t giant_degree,
+                          int32_t warp_limit, const int32_t *offsets, int32_t *cursors, int32_t *list,
+                          uint8_t *hint, cudaStream_t s);
 void launch_fill_i32(int32_t *p, int64_t n, int32_t v, cudaStream_t s);
 void launch_iota_i32(int32_t *p, int64_t n, cudaStream_t s);
 void launch_level_init(int32_t *comm, int32_t *newc, int32_t *size, const u64 *k, u64 *S,

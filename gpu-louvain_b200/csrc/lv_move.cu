@@ -186,7 +186,6 @@ __device__ __forceinline__ void cta_reduce_best(const MoveCtx &m, Best &b) {
 //    its partial best; the CTA that finishes the last item of v combines the
 //    P partials (the items of v are contiguous) and decides.
 // Results do not depend on which path decides a vertex.
-constexpr int HINT_SET = (WARP_LIMIT * 3) / 4;   // hint = distinct count above this
 
 __device__ __forceinline__ uint32_t part_of(int32_t c, int32_t P) {
     const uint32_t hsh = (uint32_t)c * 0x85EBCA6Bu;
@@ -255,7 +254,7 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
             nown = __ldg(st.comm + nv);
         }
         const int32_t d = r1 - r0;
-        if (d > WARP_LIMIT && fs.hint[v]) {
+        if (d > fs.warp_limit && fs.hint[v]) {
             if (lane == 0) enqueue_fallback(fs, v, d, st.err);
             continue;
         }
@@ -293,7 +292,7 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
                     else claimed = table_insert_claim(keys, vals, lg, cc[u], ww[u], st.err);
                 }
                 nclaim += __popc(__ballot_sync(FULL, claimed >= 0));
-                if (nclaim > WARP_LIMIT) { overflow = true; break; }
+                if (nclaim > fs.warp_limit) { overflow = true; break; }
             }
         }
         __syncwarp();
@@ -372,7 +371,7 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
             nown = __ldg(st.comm + nv);
         }
         const int32_t d = r1 - r0;
-        if (d > WARP_LIMIT && fs.hint[v]) {
+        if (d > fs.warp_limit && fs.hint[v]) {
             if (lane == 0) enqueue_fallback(fs, v, d, st.err);
             continue;
         }
@@ -412,7 +411,7 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
                 }
             }
             __syncwarp();
-            if (*nocc > WARP_LIMIT) { overflow = true; break; }
+            if (*nocc > fs.warp_limit) { overflow = true; break; }
         }
         __syncwarp();
         const int nslots = 1 << lg;
@@ -468,7 +467,7 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
 template <typename WT, int THREADS, int CAP, bool PART>
 __global__ void __launch_bounds__(THREADS) move_fallback_kernel(GraphView<WT> g, StateView st,
                                                                 Fallback fb, HubGlobal hg,
-                                                                uint8_t *hint, u64 *dE) {
+                                                                uint8_t *hint, int32_t hint_set, u64 *dE) {
     constexpr int OCC_CAP = CAP / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     u64 *vals = reinterpret_cast<u64 *>(smem_raw);
@@ -574,7 +573,7 @@ __global__ void __launch_bounds__(THREADS) move_fallback_kernel(GraphView<WT> g,
                     hg.nocc[src] = 0;
                     hg.eown[src] = 0;
                 } else {
-                    hint[v] = distinct > HINT_SET ? 1 : 0;
+                    hint[v] = distinct > hint_set ? 1 : 0;
                 }
             }
         }
@@ -588,7 +587,7 @@ __global__ void __launch_bounds__(THREADS) move_fallback_kernel(GraphView<WT> g,
 // claimed-slot list.
 template <typename WT, int THREADS, int CAP>
 __global__ void __launch_bounds__(THREADS) move_rowq_narrow_kernel(GraphView<WT> g, StateView st, Fallback fb,
-                                                                   uint8_t *hint, u64 *dE) {
+                                                                   uint8_t *hint, int32_t hint_set, u64 *dE) {
     constexpr int OCC_CAP = CAP / 2;
     static_assert(OCC_CAP <= PIECE_MAX_ADDS, "rows of the queue fit the piece counters");
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -640,7 +639,7 @@ __global__ void __launch_bounds__(THREADS) move_rowq_narrow_kernel(GraphView<WT>
             st.newc[v] = move_decision(m, b, &delta);
             record_features(st, v, m, b);
             delta_acc += delta;
-            hint[v] = nd > HINT_SET ? 1 : 0;
+            hint[v] = nd > hint_set ? 1 : 0;
         }
         __syncthreads();
     }
@@ -1027,10 +1026,11 @@ static void launch_row_queue(const GraphView<WT> &g, const StateView &st, const 
                              const DeviceInfo &di, u64 *dE, cudaStream_t s, bool narrow) {
     constexpr int T = FBQ_THREADS(B), CAP = 2 * FBQ_MAXDEG(B), SM = FBQ_SMEM(B);
     if (narrow)
-        move_rowq_narrow_kernel<WT, T, CAP><<<di.sms * di.occ_fbq_narrow[B], T, SM, s>>>(g, st, fs.q[B], fs.hint, dE);
+        move_rowq_narrow_kernel<WT, T, CAP><<<di.sms * di.occ_fbq_narrow[B], T, SM, s>>>(g, st, fs.q[B], fs.hint,
+                                                                                        fs.hint_set, dE);
     else
         move_fallback_kernel<WT, T, CAP, false><<<di.sms * di.occ_fbq[B], T, SM, s>>>(g, st, fs.q[B], HubGlobal(),
-                                                                                    fs.hint, dE);
+                                                                                    fs.hint, fs.hint_set, dE);
     note_launches(1);
 }
 
@@ -1095,7 +1095,7 @@ template <typename WT>
 static void launch_fallback_large(const GraphView<WT> &g, const StateView &st, const HubGlobal &hg,
                                   const FallbackSet &fs, const DeviceInfo &di, u64 *dE, cudaStream_t s) {
     move_fallback_kernel<WT, FB_THREADS, FB_CAP, true><<<di.sms, FB_THREADS, FB_SMEM, s>>>(
-        g, st, fs.q[NFBQ], hg, fs.hint, dE);
+        g, st, fs.q[NFBQ], hg, fs.hint, fs.hint_set, dE);
     note_launches(1);
 }
 
@@ -1138,7 +1138,7 @@ void launch_move_wide(const GraphView<WT> &g, const StateView &st, const int32_t
         move_warp_kernel<WT><<<grid, 256, WARP_SMEM, s>>>(g, st, list, n, fs, dE);
     }
     note_launches(1);
-    if (max_degree <= WARP_LIMIT) return;   // no vertex can overflow its warp table
+    if (max_degree <= fs.warp_limit) return;   // no vertex can overflow its warp table
     launch_fallback_large<WT>(g, st, HubGlobal(), fs, di, dE, s);
     launch_row_queue<WT, 3>(g, st, fs, di, dE, s, narrow);
     launch_row_queue<WT, 2>(g, st, fs, di, dE, s, narrow);

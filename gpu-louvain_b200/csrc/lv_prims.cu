@@ -100,14 +100,14 @@ __global__ void __launch_bounds__(SCAN_THREADS) scan_apply_kernel(const int32_t 
 // uint64 edge totals per class.
 __global__ void __launch_bounds__(256) class_count_kernel(const int32_t *__restrict__ rowptr,
                                                           const int32_t *__restrict__ rowend,
-                                                          int32_t V, int32_t *counts) {
+                                                          int32_t V, int32_t giant_degree, int32_t *counts) {
     __shared__ int32_t c[NCLS];
     __shared__ u64 es[NCLS];
     if (threadIdx.x < NCLS) { c[threadIdx.x] = 0; es[threadIdx.x] = 0; }
     __syncthreads();
     for (int32_t v = blockIdx.x * 256 + threadIdx.x; v < V; v += gridDim.x * 256) {
         const int32_t d = rowend[v] - rowptr[v];
-        const int cls = degree_class(d);
+        const int cls = degree_class(d, giant_degree);
         if (cls >= 0) {
             atomicAdd(c + cls, 1);
             atomicAdd(es + cls, (u64)d);
@@ -126,19 +126,19 @@ struct ClassOffsets {
 };
 
 // Also sets the move phase's fallback hint: at the start of a level every
-// vertex is a singleton community, so a row with more than WARP_LIMIT
+// vertex is a singleton community, so a row with more than warp_limit
 // entries has (up to duplicates) more distinct neighbour communities.
 __global__ void __launch_bounds__(256) class_scatter_kernel(const int32_t *__restrict__ rowptr,
                                                             const int32_t *__restrict__ rowend,
-                                                            int32_t V, ClassOffsets offs,
-                                                            int32_t *cursors, int32_t *list,
+                                                            int32_t V, int32_t giant_degree, int32_t warp_limit,
+                                                            ClassOffsets offs, int32_t *cursors, int32_t *list,
                                                             uint8_t *hint) {
     const int lane = threadIdx.x & 31;
     for (int32_t base = blockIdx.x * 256; base < V; base += gridDim.x * 256) {
         const int32_t v = base + threadIdx.x;
         const int32_t d = v < V ? rowend[v] - rowptr[v] : 0;
-        const int cls = v < V ? degree_class(d) : -1;
-        if (v < V) hint[v] = d > WARP_LIMIT ? 1 : 0;
+        const int cls = v < V ? degree_class(d, giant_degree) : -1;
+        if (v < V) hint[v] = d > warp_limit ? 1 : 0;
         const unsigned peers = __match_any_sync(FULL, cls);
         const int leader = __ffs(peers) - 1;
         int32_t pos = 0;
@@ -285,21 +285,23 @@ void scan_exclusive_i32(const int32_t *in, int32_t *out, int64_t n, int32_t *tot
     scan_apply_kernel<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, tmp); note_launches(1);
 }
 
-void launch_class_count(const int32_t *rowptr, const int32_t *rowend, int32_t V, int32_t *counts,
-                        cudaStream_t s) {
+void launch_class_count(const int32_t *rowptr, const int32_t *rowend, int32_t V, int32_t giant_degree,
+                        int32_t *counts, cudaStream_t s) {
     cudaMemsetAsync(counts, 0, sizeof(int32_t) * CLASS_COUNT_WORDS, s);
     if (V <= 0) return;
-    class_count_kernel<<<grid_for(V), 256, 0, s>>>(rowptr, rowend, V, counts); note_launches(1);
+    class_count_kernel<<<grid_for(V), 256, 0, s>>>(rowptr, rowend, V, giant_degree, counts); note_launches(1);
 }
 
-void launch_class_scatter(const int32_t *rowptr, const int32_t *rowend, int32_t V,
-                          const int32_t *offsets, int32_t *cursors, int32_t *list, uint8_t *hint,
-                          cudaStream_t s) {
+void launch_class_scatter(const int32_t *rowptr, const int32_t *rowend, int32_t V, int32_t giant_degree,
+                          int32_t warp_limit, const int32_t *offsets, int32_t *cursors, int32_t *list,
+                          uint8_t *hint, cudaStream_t s) {
     cudaMemsetAsync(cursors, 0, sizeof(int32_t) * NCLS, s);
     if (V <= 0) return;
     ClassOffsets o;
     for (int c = 0; c < NCLS; ++c) o.off[c] = offsets[c];
-    class_scatter_kernel<<<grid_for(V), 256, 0, s>>>(rowptr, rowend, V, o, cursors, list, hint); note_launches(1);
+    class_scatter_kernel<<<grid_for(V), 256, 0, s>>>(rowptr, rowend, V, giant_degree, warp_limit, o, cursors, list,
+                                                     hint);
+    note_launches(1);
 }
 
 void launch_fill_i32(int32_t *p, int64_t n, int32_t v, cudaStream_t s) {

@@ -80,7 +80,14 @@ typedef struct lv_opts {
                               than the self-loops, which the move phase
                               skips, fit) it reads 32-bit values and sums in
                               16-bit-piece counters.  Same results.       */
-    int32_t reserved[3];
+    int32_t giant_degree;  /* work mapping (results never depend on it): a
+                              vertex of degree above this is decided by the
+                              staged-chunk path instead of a warp; 0 =
+                              default 8192, else 1024..65536              */
+    int32_t warp_limit;    /* work mapping: distinct neighbour communities
+                              after which a warp hands its vertex to a
+                              fallback CTA; 0 = default 352, else 32..384  */
+    int32_t reserved[1];
 } lv_opts;
 
 /* Per-run counters; times in milliseconds (device time, CUDA events). */
@@ -169,6 +176,12 @@ int lv_get_communities(lv_handle *h, int32_t *out);
  * recomputed), e.g. to drive lv_aggregate from a given community vector. */
 int lv_set_communities(lv_handle *h, const int32_t *comm);
 int lv_get_level_info(lv_handle *h, int32_t *V, int64_t *E, int32_t *level);
+/* The current level's work classes (LV_NUM_CLASSES entries each): vertices
+ * and CSR entries per class (degree (0,4], (4,8], (8,16], (16,32], (32,84],
+ * (84,319], (319,1024], (1024,giant_degree], above giant_degree). */
+int lv_get_level_classes(lv_handle *h, int32_t *vertices, int64_t *entries);
+/* "name (sm_XY, N SMs)" of a CUDA device (the autotuner's cache key). */
+int lv_get_device_name(int32_t device, char *name, int32_t len);
 /* Test hook: current level CSR; weights as fixed-point integers
  * (value = wfix / 2^scale).  Any pointer may be NULL. */
 int lv_get_csr(lv_handle *h, int32_t *rowptr, int32_t *col, int64_t *wfix);
@@ -188,6 +201,26 @@ int lv_clear_stats(lv_handle *h);
  * reference accumulates it (FP32, sequential). */
 int lv_read_mtx(const char *path, int32_t *V, int64_t *E, int32_t **rowptr, int32_t **col,
                 float **w, float *m_ref);
+/* lv_read_mtx with the CSR built on the device (no counterpart in the
+ * reference, whose CSR is built on the host, utils.cu:32-59): the file is
+ * parsed on the host as lv_read_mtx parses it, and lv_csr_from_entries_device
+ * builds the same CSR (same rows, same order) in device memory allocated by
+ * the library on `device` (free with lv_free_device).  m_ref (may be NULL)
+ * as for lv_read_mtx. */
+int lv_read_mtx_device(const char *path, int32_t device, int32_t *V, int64_t *E, int32_t **d_rowptr,
+                       int32_t **d_col, float **d_w, float *m_ref);
+/* The parsed entries of a Matrix Market file in file order (0-based
+ * v1[i], v2[i], w[i]; unit weights for pattern files) and the vertex count:
+ * what lv_read_mtx reads before building its CSR.  Arrays are malloc'd
+ * (lv_free_host). */
+int lv_read_mtx_entries(const char *path, int32_t *V, int64_t *nnz, int32_t **v1, int32_t **v2, float **w);
+/* CSR on the device from nnz Matrix Market entries (host arrays, 0-based,
+ * file order) with the reference's conventions: entry (v1, v2, w) appends
+ * (v2, w) to row v1 and, unless v1 == v2, (v1, w) to row v2; rows keep file
+ * order.  Directed entries are numbered by a scan and stably radix-sorted by
+ * row on the device.  Entries outside [0, V) give LV_ERR_INVALID. */
+int lv_csr_from_entries_device(int32_t device, int32_t V, int64_t nnz, const int32_t *v1, const int32_t *v2,
+                               const float *w, int64_t *E, int32_t **d_rowptr, int32_t **d_col, float **d_w);
 /* Binary CSR file, a cache for lv_read_mtx's output (no counterpart in the
  * reference, which parses the text file on every run): header "LVCSR002",
  * V and E (int64), m_ref (float), 4 pad bytes, the size and the modification
@@ -228,6 +261,14 @@ int lv_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed, double a, dou
  * intra-block and round(V*d_out/2) inter-block uniform draws. */
 int lv_gen_planted(int32_t V, int32_t blocks, double d_in, double d_out, uint64_t seed,
                    int32_t weight_mode, int64_t *E, int32_t **rowptr, int32_t **col, float **w);
+/* G planted-partition graphs (graph i as lv_gen_planted(V[i], blocks[i],
+ * d_in[i], d_out[i], seeds[i], weight_mode)) generated by all host threads
+ * into one block-diagonal CSR: graph i's vertices are
+ * [graph_ptr[i], graph_ptr[i+1]) and its columns are offset by graph_ptr[i]
+ * (the layout lv_batch_create takes).  Arrays are malloc'd (lv_free_host). */
+int lv_gen_planted_batch(int32_t G, const int32_t *V, const int32_t *blocks, const double *d_in,
+                         const double *d_out, const uint64_t *seeds, int32_t weight_mode, int32_t *Vtot,
+                         int64_t *Etot, int32_t **rowptr, int32_t **col, float **w, int32_t **graph_ptr);
 /* LFR-like benchmark graph (Lancichinetti-Fortunato-Radicchi construction,
  * simplified): power-law degrees (exponent tau1, mean mean_degree, at most
  * kmax), power-law community sizes (exponent tau2, in [cmin, cmax]), mixing

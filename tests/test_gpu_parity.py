@@ -426,3 +426,28 @@ def test_engine_matches_reference_goldens(lvb, case):
         a = sorted(zip(rcl[rrp[v]:rrp[v + 1]].tolist(), rw[rrp[v]:rrp[v + 1]].tolist()))
         b = sorted(zip(pcl[prp[v]:prp[v + 1]].tolist(), (pwf[prp[v]:prp[v + 1]] / 2.0 ** s).tolist()))
         assert a == b
+
+
+@pytest.mark.parametrize("name", ["rmat15", "hubs"])
+def test_work_mapping_knobs_do_not_change_results(lvb, graphs, name):
+    """The autotuner's knobs (giant threshold, warp overflow limit, 64-bit
+    sums) move work between kernels; every setting gives the same sweeps."""
+    rp, cl, w, gain = graphs[name]
+    runs = []
+    for kw in ({}, {"giant_degree": 1024}, {"giant_degree": 65536}, {"warp_limit": 32},
+               {"warp_limit": 384}, {"giant_degree": 1024, "warp_limit": 32, "wide_weights": True}):
+        with lvb.Louvain(lvb.Graph(rp, cl, w), **kw) as e:
+            q = e.run(gain)
+            runs.append((kw, q, e.original_to_community()[0], e.stats()["sweeps"]))
+    for kw, q, m, sw in runs[1:]:
+        assert q == runs[0][1], kw
+        assert np.array_equal(m, runs[0][2]), kw
+        assert sw == runs[0][3], kw
+
+
+def test_work_mapping_knobs_are_checked(lvb):
+    g = lvb.gen_planted(500, 8, 10.0, 2.0, 1)
+    for kw in ({"giant_degree": 1000}, {"giant_degree": 70000}, {"warp_limit": 16}, {"warp_limit": 400}):
+        with pytest.raises(lvb.LouvainError) as ex:
+            lvb.Louvain(g, **kw)
+        assert ex.value.status == lvb.LV_ERR_INVALID

@@ -172,6 +172,22 @@ def test_csr_cache_roundtrip(lvb, tmp_path):
         assert ex.value.status == lvb.LV_ERR_IO
 
 
+def test_gen_planted_batch_equals_concatenated_graphs(lvb):
+    rng = np.random.default_rng(2)
+    params = []
+    for i in range(40):
+        V = int(rng.integers(1, 3000))
+        params.append((V, int(rng.integers(1, min(V, 256) + 1)), float(rng.uniform(0, 24)),
+                       float(rng.uniform(0, 4)), 77 + i))
+    for weights in ("unit", "uniform"):
+        got = lvb.gen_planted_batch(params, weights)
+        want = lvb.concat_graphs([lvb.gen_planted(*p[:4], seed=p[4], weights=weights) for p in params])
+        for x, y in zip(got, want):
+            assert np.array_equal(x, y)
+    with pytest.raises(lvb.LouvainError):
+        lvb.gen_planted_batch([(10, 20, 4.0, 1.0, 1)])   # more blocks than vertices
+
+
 def test_csr_cache_source_stamp(lvb, tmp_path):
     import ctypes as C
     g = lvb.gen_planted(500, 8, 10.0, 2.0, 3)
