@@ -682,12 +682,20 @@ def batch_summary(args, ranks: Ranks):
             es += st["edge_sweeps"]
             lat.append(b.graph_stats()["latency_ms"])
         ok = bool((b.results()["status"] == lvb.LV_OK).all())
+        gs = b.graph_stats()
+    # the graphs that bound the launch: the slowest five with their sizes
+    slow = np.argsort(-gs["latency_ms"])[:5]
+    vcount = np.diff(gptr)
+    ecount = np.diff(rp[gptr])
+    slowest = [{"graph": int(i), "V": int(vcount[i]), "E_csr": int(ecount[i]), "levels": int(gs["levels"][i]),
+                "sweeps": int(gs["sweeps"][i]), "ms": round(float(gs["latency_ms"][i]), 2)} for i in slow]
     lat = np.concatenate(lat)
     return {"workload": f"batch{G}_planted", "graphs_per_s": 2 * G / (dev_ms * 1e-3),
             "ms_per_launch": dev_ms / 2, "edge_sweeps_per_s": es / (dev_ms * 1e-3),
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "max": float(lat.max())},
             "all_ok": ok, "V_total": len(rp) - 1, "E_csr_total": len(cl), "generation_s": round(t_gen, 1),
+            "slowest": slowest,
             "note": "lv_batch_run, one persistent launch per run, device time (1 warm-up + 2 timed runs); "
                     "bench.py --workload batch gives the full line"}
 

@@ -505,6 +505,9 @@ void agg_merge_class(int acls, const AggBuffers &ab, const int32_t *P, const int
 void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *P, int32_t *vkey,
                       u64 *vw, uint32_t *vw32, int *err, int *hiflag, cudaStream_t s) {
     if (hg.nhubs <= 0) return;
+    // the per-community list lengths are zero between uses; cleared here too
+    // so that no earlier failure can leave an append offset behind
+    cudaMemsetAsync(hg.nocc, 0, sizeof(int32_t) * (size_t)hg.nhubs, s);
     mergeg_insert_kernel<<<hg.n_echunks, HG_INSERT_THREADS, HG_INSERT_SMEM, s>>>(hg, ab.mstart, P, ab.flag, vkey, vw, err); note_launches(1);
     mergeg_emit_kernel<<<hg.n_schunks, 256, 0, s>>>(hg, ab.mstart, P, ab.flag, vkey, vw, vw32, hiflag); note_launches(1);
     mergeg_finish_kernel<<<grid_for(hg.nhubs), 256, 0, s>>>(hg, ab.mstart, P, ab.flag, ab.newdeg, ab.epos_new); note_launches(1);

@@ -35,6 +35,11 @@
 #ifndef LV_U_STAGE
 #define LV_U_STAGE 8
 #endif
+// The narrow-weight warp kernel loads the home-slot keys of its U entries
+// together before inserting (1) or probes entry by entry (0).
+#ifndef LV_WARP_PREFETCH
+#define LV_WARP_PREFETCH 1
+#endif
 
 namespace lv {
 
@@ -243,9 +248,11 @@ __device__ __forceinline__ u64 piece_value(const PieceTable &t, uint32_t s) {
 
 // Insert (key, w) into a piece table (move-phase hash, linear probing,
 // bounded by the capacity); returns the slot newly claimed for key, or -1.
-__device__ __forceinline__ int32_t piece_insert(const PieceTable &t, int lg, int32_t key, u64 w, int *err) {
+// piece_insert_at starts at slot s = hash_slot(key, lg) (computed by the
+// caller, who may have loaded its key already to overlap the load latency).
+__device__ __forceinline__ int32_t piece_insert_at(const PieceTable &t, int lg, uint32_t s, int32_t key, u64 w,
+                                                   int *err) {
     const uint32_t mask = (1u << lg) - 1u;
-    uint32_t s = hash_slot(key, lg);
     for (uint32_t p = 0; p <= mask; ++p) {
         const int32_t k = ((volatile int32_t *)t.keys)[s];
         if (k == key) { piece_add(t, s, w); return -1; }
@@ -258,6 +265,10 @@ __device__ __forceinline__ int32_t piece_insert(const PieceTable &t, int lg, int
     }
     atomicOr(err, DEVERR_HASH_FULL);
     return -1;
+}
+
+__device__ __forceinline__ int32_t piece_insert(const PieceTable &t, int lg, int32_t key, u64 w, int *err) {
+    return piece_insert_at(t, lg, hash_slot(key, lg), key, w, err);
 }
 
 // Append the slots claimed by this warp's lanes (claimed >= 0) to occ[],

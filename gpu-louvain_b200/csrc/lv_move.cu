@@ -397,6 +397,33 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
             int32_t cc[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(st.comm + jj[u]) : -1;
+#if LV_WARP_PREFETCH
+            // the U first-probe slots and their keys are loaded together; a
+            // key already in its home slot (the common case once a row's few
+            // communities are in the table) is then added without probing
+            uint32_t hs[U];
+            int32_t kk[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                hs[u] = cc[u] >= 0 ? hash_slot(cc[u], lg) : 0u;
+                kk[u] = (cc[u] >= 0 && cc[u] != own) ? ((volatile int32_t *)t.keys)[hs[u]] : -2;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (cc[u] < 0) continue;
+                if (cc[u] == own) {
+                    e_own += ww[u];
+                } else if (kk[u] == cc[u]) {
+                    piece_add(t, hs[u], ww[u]);
+                } else {
+                    const int32_t claimed = piece_insert_at(t, lg, hs[u], cc[u], ww[u], st.err);
+                    if (claimed >= 0) {
+                        const int32_t i = atomicAdd(nocc, 1);
+                        if (i < WARP_OCC_CAP) occ[i] = claimed;
+                    }
+                }
+            }
+#else
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 if (cc[u] < 0) continue;
@@ -410,6 +437,7 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
                     }
                 }
             }
+#endif
             __syncwarp();
             if (*nocc > fs.warp_limit) { overflow = true; break; }
         }
@@ -1104,6 +1132,14 @@ void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGl
                         const FallbackSet &fs, const DeviceInfo &di, u64 *dE, cudaStream_t s, bool narrow) {
     if (hg.nhubs <= 0) return;
     cudaMemsetAsync(fs.q[NFBQ].count, 0, 2 * sizeof(int32_t), s);   // count, next
+    // The staging counters, the own-community sums and the partition done
+    // counters are returned to zero by the kernel that consumes them; they are
+    // cleared here as well, so that a sweep that ended early (a device error,
+    // an item the full large queue could not take) cannot leave a count that
+    // makes the next staging pass append beyond a giant's area.
+    cudaMemsetAsync(hg.nocc, 0, sizeof(int32_t) * (size_t)hg.nhubs, s);
+    cudaMemsetAsync(hg.eown, 0, sizeof(u64) * (size_t)hg.nhubs, s);
+    cudaMemsetAsync(fs.q[NFBQ].done, 0, sizeof(int32_t) * (size_t)fs.q[NFBQ].cap, s);
     if (narrow) giant_stage_narrow_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg);
     else giant_stage_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg);
     note_launches(1);
@@ -1128,8 +1164,11 @@ void launch_move_wide(const GraphView<WT> &g, const StateView &st, const int32_t
                       const FallbackSet &fs, const DeviceInfo &di, u64 *dE, cudaStream_t s,
                       int32_t max_degree, bool narrow) {
     if (n <= 0) return;
-    // the queues' (count, next) pairs are contiguous
+    // the queues' (count, next) pairs are contiguous; the large queue's done
+    // counters are cleared as in launch_move_giants
     cudaMemsetAsync(fs.q[0].count, 0, 2 * (NFBQ + 1) * sizeof(int32_t), s);
+    if (max_degree > fs.warp_limit)
+        cudaMemsetAsync(fs.q[NFBQ].done, 0, sizeof(int32_t) * (size_t)fs.q[NFBQ].cap, s);
     if (narrow) {
         const unsigned grid = (unsigned)imin64((n + 7) / 8, (int64_t)di.sms * di.occ_warp_narrow);
         move_warp_narrow_kernel<WT><<<grid, 256, WARP_NSMEM, s>>>(g, st, list, n, fs, dE);
