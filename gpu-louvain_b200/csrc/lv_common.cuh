@@ -138,6 +138,26 @@ __device__ __forceinline__ u64 wfix(const float *w, int64_t e, double scale) {
 __device__ __forceinline__ u64 wfix(const u64 *w, int64_t e, double) { return __ldg(w + e); }
 __device__ __forceinline__ u64 wfix(const uint32_t *w, int64_t e, double) { return (u64)__ldg(w + e); }
 
+// The same reads with the streaming (evict-first) cache hint, for row data
+// read once per sweep, so that it does not push the gathered per-vertex
+// arrays (communities, Sigma_tot) out of L2.
+#ifndef LV_STREAM_ROWS
+#define LV_STREAM_ROWS 1
+#endif
+template <typename T>
+__device__ __forceinline__ T ld_row(const T *p) {
+#if LV_STREAM_ROWS
+    return __ldcs(p);
+#else
+    return __ldg(p);
+#endif
+}
+__device__ __forceinline__ u64 wfix_row(const float *w, int64_t e, double scale) {
+    return (u64)__double2ll_rn(__dmul_rn((double)ld_row(w + e), scale));
+}
+__device__ __forceinline__ u64 wfix_row(const u64 *w, int64_t e, double) { return ld_row(w + e); }
+__device__ __forceinline__ u64 wfix_row(const uint32_t *w, int64_t e, double) { return (u64)ld_row(w + e); }
+
 // A level's graph: row v is col/w[rowptr[v] .. rowend[v]).  Level 0 is a
 // plain CSR (rowend = rowptr + 1); aggregated levels keep each merged row
 // where the merge wrote it, so rows need not be contiguous.

@@ -1085,7 +1085,9 @@ int optimise_level_learned(lv_handle *h, float min_gain, int32_t *changed) {
                 // recall over the movers whose features are current (evaluated
                 // since the last full sweep): what the predictor caught, not
                 // the moves it postponed
-                h->act_recall = fresh_movers > 0 ? (double)hits / (double)fresh_movers : 1.0;
+                // (no fresh mover while others moved: the proposals caught
+                // nothing, recall 0; nothing moved at all: recall 1)
+                h->act_recall = fresh_movers > 0 ? (double)hits / (double)fresh_movers : (movers > 0 ? 0.0 : 1.0);
                 if (h->act_recall < rmin) {
                     plain_rest = true;
                     h->act_fell_back = 1;

@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
                 const int32_t e = b0 + 32 * u;
                 jj[u] = -1;
                 ww[u] = 0;
-                if (e < r1) { jj[u] = __ldg(g.col + e); ww[u] = wfix(g.w, e, g.scale); }
+                if (e < r1) { jj[u] = ld_row(g.col + e); ww[u] = wfix_row(g.w, e, g.scale); }
             }
             int32_t cc[U];
 #pragma unroll
