@@ -298,6 +298,83 @@ __global__ void __launch_bounds__(T) merge_cta_kernel(const int32_t *__restrict_
     if (hi) atomicOr(hiflag, 1);
 }
 
+// merge_cta_kernel for a level whose non-self-loop weights are below 2^32:
+// the inter-community entries (the only ones that enter the table; the
+// community's own key is summed in registers, as a self-loop can be large)
+// are summed in 16-bit-piece counters with fire-and-forget adds, and the
+// self entry is appended to the merged row after the table's entries.
+template <int T, int CAPMAX>
+__global__ void __launch_bounds__(T) merge_cta_narrow_kernel(const int32_t *__restrict__ clist, int32_t n,
+                                                             const int32_t *__restrict__ mstart,
+                                                             const int32_t *__restrict__ P,
+                                                             const int32_t *__restrict__ newid,
+                                                             int32_t *vkey, u64 *vw, uint32_t *vw32,
+                                                             int32_t *newdeg, int32_t *epos_new, int *err,
+                                                             int *hiflag) {
+    static_assert(CAPMAX / 2 <= PIECE_MAX_ADDS, "a community's entries fit the piece counters");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PieceTable t;
+    t.lo = reinterpret_cast<uint32_t *>(smem_raw);
+    t.hi = t.lo + CAPMAX;
+    t.keys = reinterpret_cast<int32_t *>(t.hi + CAPMAX);
+    __shared__ int32_t cnt;
+    __shared__ u64 wpart[T / 32];
+    u64 hi = 0;
+    for (int s = threadIdx.x; s < CAPMAX; s += T) { t.keys[s] = -1; t.lo[s] = 0; t.hi[s] = 0; }
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    for (int32_t idx = blockIdx.x; idx < n; idx += gridDim.x) {
+        const int32_t c = clist[idx];
+        const int32_t a = P[mstart[c]], b = P[mstart[c + 1]];
+        int lg = ceil_log2_i(2 * (int64_t)(b - a));
+        lg = lg < 3 ? 3 : lg;
+        const int cap = 1 << lg;
+        const int32_t self = newid[c];
+        u64 w_self = 0;
+        for (int32_t i = a + threadIdx.x; i < b; i += T) {
+            const int32_t k = vkey[i];
+            if (k == self) w_self += vw[i];
+            else piece_insert_at(t, lg, hash_slot_agg(k, lg), k, vw[i], err);
+        }
+        w_self = warp_sum_u64(w_self);
+        if ((threadIdx.x & 31) == 0) wpart[threadIdx.x >> 5] = w_self;
+        __syncthreads();
+        for (int s = threadIdx.x; s < cap; s += T) {
+            const int32_t key = t.keys[s];
+            if (key >= 0) {
+                const int32_t pos = a + atomicAdd(&cnt, 1);
+                const u64 x = piece_value(t, (uint32_t)s);
+                vkey[pos] = key;
+                vw[pos] = x;
+                vw32[pos] = (uint32_t)x;
+                hi |= x >> 32;
+                t.keys[s] = -1;
+                t.lo[s] = 0;
+                t.hi[s] = 0;
+            }
+        }
+        if (threadIdx.x == 0) {
+            u64 ws = 0;
+            for (int i = 0; i < T / 32; ++i) ws += wpart[i];
+            if (ws) {
+                const int32_t pos = a + atomicAdd(&cnt, 1);
+                vkey[pos] = self;
+                vw[pos] = ws;
+                vw32[pos] = (uint32_t)ws;   // the self-loop is read as uint64 only
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int32_t nid = newid[c];
+            newdeg[nid] = cnt;
+            epos_new[nid] = a;
+            cnt = 0;
+        }
+        __syncthreads();
+    }
+    if (hi) atomicOr(hiflag, 1);
+}
+
 // Global-table merge for communities whose degree bound exceeds 4096: one CTA
 // per chunk of HG_EDGE_CHUNK entries, reduced first in a chunk-local shared
 // table (intra-community entries all carry the community's own key), then
@@ -339,6 +416,60 @@ __global__ void __launch_bounds__(HG_INSERT_THREADS) mergeg_insert_kernel(
     for (int s = threadIdx.x; s < LCAP; s += HG_INSERT_THREADS) {
         const int32_t k = lkeys[s];
         const int32_t claimed = k >= 0 ? table_insert_claim<0>(keys, vals, lg, k, lvals[s], err) : -1;
+        warp_append(claimed, occ, hg.nocc + h);
+    }
+}
+
+// mergeg_insert_kernel for a level whose non-self-loop weights are below
+// 2^32: the chunk-local table sums in 16-bit-piece counters (a chunk has
+// HG_EDGE_CHUNK entries); the chunk's weight to the community's own key (which
+// can be large) is summed over the CTA and added to the global table once.
+__global__ void __launch_bounds__(HG_INSERT_THREADS) mergeg_insert_narrow_kernel(
+    HubGlobal hg, const int32_t *__restrict__ mstart, const int32_t *__restrict__ P,
+    const int32_t *__restrict__ newid, const int32_t *__restrict__ vkey,
+    const u64 *__restrict__ vw, int *err) {
+    static_assert(HG_EDGE_CHUNK <= PIECE_MAX_ADDS, "chunks fit the piece counters");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int LCAP = 2 * HG_EDGE_CHUNK;
+    constexpr int LLG = ilog2_c(LCAP);
+    constexpr int NW = HG_INSERT_THREADS / 32;
+    PieceTable t;
+    t.lo = reinterpret_cast<uint32_t *>(smem_raw);
+    t.hi = t.lo + LCAP;
+    t.keys = reinterpret_cast<int32_t *>(t.hi + LCAP);
+    __shared__ u64 wpart[NW];
+    for (int s = threadIdx.x; s < LCAP; s += HG_INSERT_THREADS) { t.keys[s] = -1; t.lo[s] = 0; t.hi[s] = 0; }
+    __syncthreads();
+    const int32_t h = hg.echunk_hub[blockIdx.x];
+    const int32_t c = hg.hubs[h];
+    const int32_t b = P[mstart[c + 1]];
+    const int32_t i0 = P[mstart[c]] + hg.echunk_e0[blockIdx.x];
+    const int32_t i1 = min(i0 + HG_EDGE_CHUNK, b);
+    const int32_t self = newid[c];
+    u64 w_self = 0;
+    for (int32_t i = i0 + threadIdx.x; i < i1; i += HG_INSERT_THREADS) {
+        const int32_t k = vkey[i];
+        if (k == self) w_self += vw[i];
+        else piece_insert_at(t, LLG, hash_slot_agg(k, LLG), k, vw[i], err);
+    }
+    w_self = warp_sum_u64(w_self);
+    if ((threadIdx.x & 31) == 0) wpart[threadIdx.x >> 5] = w_self;
+    __syncthreads();
+    int32_t *keys = hg.keys + hg.tbl_off[h];
+    u64 *vals = hg.vals + hg.tbl_off[h];
+    int32_t *occ = hg.occ + hg.occ_off[h];
+    const int lg = hg.tbl_lg[h];
+    if (threadIdx.x < 32) {
+        u64 ws = 0;
+        if (threadIdx.x == 0)
+            for (int i = 0; i < NW; ++i) ws += wpart[i];
+        const int32_t claimed = ws ? table_insert_claim<0>(keys, vals, lg, self, ws, err) : -1;
+        warp_append(claimed, occ, hg.nocc + h);
+    }
+    // drained in the chunk table's slot order, as in mergeg_insert_kernel
+    for (int s = threadIdx.x; s < LCAP; s += HG_INSERT_THREADS) {
+        const int32_t k = t.keys[s];
+        const int32_t claimed = k >= 0 ? table_insert_claim<0>(keys, vals, lg, k, piece_value(t, (uint32_t)s), err) : -1;
         warp_append(claimed, occ, hg.nocc + h);
     }
 }
@@ -412,6 +543,11 @@ void init_agg_attributes() {
     cudaFuncSetAttribute(merge_cta_kernel<A4_T, A4_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          A4_CAP * 12);
     cudaFuncSetAttribute(mergeg_insert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HG_INSERT_SMEM);
+    cudaFuncSetAttribute(mergeg_insert_narrow_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HG_INSERT_SMEM);
+    cudaFuncSetAttribute(merge_cta_narrow_kernel<A3_T, A3_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         A3_CAP * 12);
+    cudaFuncSetAttribute(merge_cta_narrow_kernel<A4_T, A4_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         A4_CAP * 12);
     int o3 = 0, o4 = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, merge_cta_kernel<A3_T, A3_CAP>, A3_T, A3_CAP * 12);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o4, merge_cta_kernel<A4_T, A4_CAP>, A4_T, A4_CAP * 12);
@@ -477,7 +613,7 @@ void agg_new_vertices(const int32_t *size, const u64 *S, int32_t V, const AggBuf
 
 void agg_merge_class(int acls, const AggBuffers &ab, const int32_t *P, const int32_t *list,
                      int32_t n, int32_t *vkey, u64 *vw, uint32_t *vw32, int *err, int *hiflag, int sms,
-                     cudaStream_t s) {
+                     cudaStream_t s, bool narrow) {
     if (n <= 0) return;
     switch (acls) {
     case AC1:
@@ -489,26 +625,44 @@ void agg_merge_class(int acls, const AggBuffers &ab, const int32_t *P, const int
                                                                    vw, vw32, ab.newdeg, ab.epos_new, err, hiflag); note_launches(1);
         break;
     case AC3:
-        merge_cta_kernel<A3_T, A3_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a3), A3_T,
-                                         A3_CAP * 12, s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw, vw32,
-                                                           ab.newdeg, ab.epos_new, err, hiflag); note_launches(1);
+        if (narrow)
+            merge_cta_narrow_kernel<A3_T, A3_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a3), A3_T, A3_CAP * 12,
+                                                    s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw, vw32, ab.newdeg,
+                                                         ab.epos_new, err, hiflag);
+        else
+            merge_cta_kernel<A3_T, A3_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a3), A3_T,
+                                             A3_CAP * 12, s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw, vw32,
+                                                               ab.newdeg, ab.epos_new, err, hiflag);
+        note_launches(1);
         break;
     case AC4:
-        merge_cta_kernel<A4_T, A4_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a4), A4_T,
-                                         A4_CAP * 12, s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw, vw32,
-                                                           ab.newdeg, ab.epos_new, err, hiflag); note_launches(1);
+        if (narrow)
+            merge_cta_narrow_kernel<A4_T, A4_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a4), A4_T, A4_CAP * 12,
+                                                    s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw, vw32, ab.newdeg,
+                                                         ab.epos_new, err, hiflag);
+        else
+            merge_cta_kernel<A4_T, A4_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a4), A4_T,
+                                             A4_CAP * 12, s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw, vw32,
+                                                               ab.newdeg, ab.epos_new, err, hiflag);
+        note_launches(1);
         break;
     default: break;
     }
 }
 
 void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *P, int32_t *vkey,
-                      u64 *vw, uint32_t *vw32, int *err, int *hiflag, cudaStream_t s) {
+                      u64 *vw, uint32_t *vw32, int *err, int *hiflag, cudaStream_t s, bool narrow) {
     if (hg.nhubs <= 0) return;
     // the per-community list lengths are zero between uses; cleared here too
     // so that no earlier failure can leave an append offset behind
     cudaMemsetAsync(hg.nocc, 0, sizeof(int32_t) * (size_t)hg.nhubs, s);
-    mergeg_insert_kernel<<<hg.n_echunks, HG_INSERT_THREADS, HG_INSERT_SMEM, s>>>(hg, ab.mstart, P, ab.flag, vkey, vw, err); note_launches(1);
+    if (narrow)
+        mergeg_insert_narrow_kernel<<<hg.n_echunks, HG_INSERT_THREADS, HG_INSERT_SMEM, s>>>(hg, ab.mstart, P, ab.flag,
+                                                                                            vkey, vw, err);
+    else
+        mergeg_insert_kernel<<<hg.n_echunks, HG_INSERT_THREADS, HG_INSERT_SMEM, s>>>(hg, ab.mstart, P, ab.flag, vkey,
+                                                                                     vw, err);
+    note_launches(1);
     mergeg_emit_kernel<<<hg.n_schunks, 256, 0, s>>>(hg, ab.mstart, P, ab.flag, vkey, vw, vw32, hiflag); note_launches(1);
     mergeg_finish_kernel<<<grid_for(hg.nhubs), 256, 0, s>>>(hg, ab.mstart, P, ab.flag, ab.newdeg, ab.epos_new); note_launches(1);
 }

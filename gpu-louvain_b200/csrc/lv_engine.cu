@@ -33,9 +33,9 @@ void agg_new_vertices(const int32_t *size, const u64 *S, int32_t V, const AggBuf
                       const int32_t *P, u64 *knew, cudaStream_t s);
 void agg_merge_class(int acls, const AggBuffers &ab, const int32_t *P, const int32_t *list,
                      int32_t n, int32_t *vkey, u64 *vw, uint32_t *vw32, int *err, int *hiflag, int sms,
-                     cudaStream_t s);
+                     cudaStream_t s, bool narrow);
 void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *P, int32_t *vkey,
-                      u64 *vw, uint32_t *vw32, int *err, int *hiflag, cudaStream_t s);
+                      u64 *vw, uint32_t *vw32, int *err, int *hiflag, cudaStream_t s, bool narrow);
 void agg_row_bounds(const AggBuffers &ab, int32_t Vn, int32_t *start, int32_t *end, cudaStream_t s);
 void launch_gather_degrees(const int32_t *rowptr, const int32_t *rowend, const int32_t *list,
                            int32_t n, int32_t *out, cudaStream_t s);
@@ -1183,6 +1183,9 @@ int aggregate_t(lv_handle *h) {
     u64 *vw = h->lvl_w[nb];
     uint32_t *vw32 = h->lvl_w32[nb];
     int32_t *hiflag = ab.scalars + 12;   // set when a merged sum is 2^32 or more
+    // the permuted inter-community weights are the current level's
+    // non-self-loop weights: below 2^32 when the move phase reads them narrow
+    const bool narrow = h->cur_w32 ? !h->opts.wide_weights : narrow_weights<WT>(h);
     agg_prepare(h->cur_rowptr, h->cur_rowend, h->comm, h->size, V, ab, h->mslot, h->degm, h->P,
                 h->stream);
     LV_CUDA(h, cudaMemcpyAsync(h->small_h, ab.scalars, sizeof(int32_t) * (2 + NAC),
@@ -1212,8 +1215,8 @@ int aggregate_t(lv_handle *h) {
     LV_CUDA(h, cudaMemsetAsync(hiflag, 0, sizeof(int32_t), h->stream));
     for (int c = 0; c < NAC - 1; ++c)
         agg_merge_class(c, ab, h->P, ab.clist + aoff[c], aoff[c + 1] - aoff[c], vkey, vw, vw32,
-                        &h->tot_d->err, hiflag, h->di.sms, h->stream);
-    agg_merge_global(h->hub_agg.view, ab, h->P, vkey, vw, vw32, &h->tot_d->err, hiflag, h->stream);
+                        &h->tot_d->err, hiflag, h->di.sms, h->stream, narrow);
+    agg_merge_global(h->hub_agg.view, ab, h->P, vkey, vw, vw32, &h->tot_d->err, hiflag, h->stream, narrow);
     agg_row_bounds(ab, newV, h->lvl_start[nb], h->lvl_end[nb], h->stream);
     // E' = number of stored entries (P is free again after the merges)
     scan_exclusive_i32(ab.newdeg, h->P, newV, h->P + newV, ab.scan_tmp, h->stream);
