@@ -437,40 +437,66 @@ __global__ void __launch_bounds__(HG_INSERT_THREADS) mergeg_insert_narrow_kernel
     t.lo = reinterpret_cast<uint32_t *>(smem_raw);
     t.hi = t.lo + LCAP;
     t.keys = reinterpret_cast<int32_t *>(t.hi + LCAP);
+    int32_t *locc = t.keys + LCAP;   // claimed slots of the chunk table (at most HG_EDGE_CHUNK)
     __shared__ u64 wpart[NW];
+    __shared__ int32_t lnocc;
     for (int s = threadIdx.x; s < LCAP; s += HG_INSERT_THREADS) { t.keys[s] = -1; t.lo[s] = 0; t.hi[s] = 0; }
+    if (threadIdx.x == 0) lnocc = 0;
     __syncthreads();
-    const int32_t h = hg.echunk_hub[blockIdx.x];
-    const int32_t c = hg.hubs[h];
-    const int32_t b = P[mstart[c + 1]];
-    const int32_t i0 = P[mstart[c]] + hg.echunk_e0[blockIdx.x];
-    const int32_t i1 = min(i0 + HG_EDGE_CHUNK, b);
-    const int32_t self = newid[c];
-    u64 w_self = 0;
-    for (int32_t i = i0 + threadIdx.x; i < i1; i += HG_INSERT_THREADS) {
-        const int32_t k = vkey[i];
-        if (k == self) w_self += vw[i];
-        else piece_insert_at(t, LLG, hash_slot_agg(k, LLG), k, vw[i], err);
-    }
-    w_self = warp_sum_u64(w_self);
-    if ((threadIdx.x & 31) == 0) wpart[threadIdx.x >> 5] = w_self;
-    __syncthreads();
-    int32_t *keys = hg.keys + hg.tbl_off[h];
-    u64 *vals = hg.vals + hg.tbl_off[h];
-    int32_t *occ = hg.occ + hg.occ_off[h];
-    const int lg = hg.tbl_lg[h];
-    if (threadIdx.x < 32) {
-        u64 ws = 0;
-        if (threadIdx.x == 0)
-            for (int i = 0; i < NW; ++i) ws += wpart[i];
-        const int32_t claimed = ws ? table_insert_claim<0>(keys, vals, lg, self, ws, err) : -1;
-        warp_append(claimed, occ, hg.nocc + h);
-    }
-    // drained in the chunk table's slot order, as in mergeg_insert_kernel
-    for (int s = threadIdx.x; s < LCAP; s += HG_INSERT_THREADS) {
-        const int32_t k = t.keys[s];
-        const int32_t claimed = k >= 0 ? table_insert_claim<0>(keys, vals, lg, k, piece_value(t, (uint32_t)s), err) : -1;
-        warp_append(claimed, occ, hg.nocc + h);
+    // persistent over the chunks; after a chunk only its claimed slots are
+    // cleared
+    for (int32_t ch = blockIdx.x; ch < hg.n_echunks; ch += gridDim.x) {
+        const int32_t h = hg.echunk_hub[ch];
+        const int32_t c = hg.hubs[h];
+        const int32_t b = P[mstart[c + 1]];
+        const int32_t i0 = P[mstart[c]] + hg.echunk_e0[ch];
+        const int32_t i1 = min(i0 + HG_EDGE_CHUNK, b);
+        const int32_t self = newid[c];
+        u64 w_self = 0;
+        for (int32_t i = i0 + threadIdx.x; i < i1; i += HG_INSERT_THREADS) {
+            const int32_t k = vkey[i];
+            if (k == self) {
+                w_self += vw[i];
+            } else {
+                const int32_t claimed = piece_insert_at(t, LLG, hash_slot_agg(k, LLG), k, vw[i], err);
+                if (claimed >= 0) {
+                    const int32_t j = atomicAdd(&lnocc, 1);
+                    if (j < HG_EDGE_CHUNK) locc[j] = claimed;
+                }
+            }
+        }
+        w_self = warp_sum_u64(w_self);
+        if ((threadIdx.x & 31) == 0) wpart[threadIdx.x >> 5] = w_self;
+        __syncthreads();
+        int32_t *keys = hg.keys + hg.tbl_off[h];
+        u64 *vals = hg.vals + hg.tbl_off[h];
+        int32_t *occ = hg.occ + hg.occ_off[h];
+        const int lg = hg.tbl_lg[h];
+        if (threadIdx.x < 32) {
+            u64 ws = 0;
+            if (threadIdx.x == 0)
+                for (int i = 0; i < NW; ++i) ws += wpart[i];
+            const int32_t claimed = ws ? table_insert_claim<0>(keys, vals, lg, self, ws, err) : -1;
+            warp_append(claimed, occ, hg.nocc + h);
+        }
+        // drained in claim order into the community's global table (its
+        // move-phase hash is independent of the chunk table's)
+        const int32_t n = min(lnocc, HG_EDGE_CHUNK);
+        for (int32_t i0s = 0; i0s < n; i0s += HG_INSERT_THREADS) {
+            const int32_t i = i0s + threadIdx.x;
+            int32_t claimed = -1;
+            if (i < n) {
+                const uint32_t sl = (uint32_t)locc[i];
+                claimed = table_insert_claim<0>(keys, vals, lg, t.keys[sl], piece_value(t, sl), err);
+                t.keys[sl] = -1;
+                t.lo[sl] = 0;
+                t.hi[sl] = 0;
+            }
+            warp_append(claimed, occ, hg.nocc + h);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) lnocc = 0;
+        __syncthreads();
     }
 }
 
@@ -535,7 +561,9 @@ __global__ void row_bounds_kernel(const int32_t *__restrict__ epos_new,
 
 constexpr int A3_T = 256, A3_CAP = 2048;
 constexpr int A4_T = 512, A4_CAP = 8192;
-static int g_occ_a3 = 4, g_occ_a4 = 2;
+static int g_occ_a3 = 4, g_occ_a4 = 2, g_occ_mg = 2, g_sms = 148;
+// narrow global merge: chunk table + its claimed-slot list
+constexpr int HG_INSERT_NSMEM = 2 * HG_EDGE_CHUNK * 12 + HG_EDGE_CHUNK * 4;
 
 void init_agg_attributes() {
     cudaFuncSetAttribute(merge_cta_kernel<A3_T, A3_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -543,7 +571,15 @@ void init_agg_attributes() {
     cudaFuncSetAttribute(merge_cta_kernel<A4_T, A4_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          A4_CAP * 12);
     cudaFuncSetAttribute(mergeg_insert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HG_INSERT_SMEM);
-    cudaFuncSetAttribute(mergeg_insert_narrow_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HG_INSERT_SMEM);
+    cudaFuncSetAttribute(mergeg_insert_narrow_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HG_INSERT_NSMEM);
+    {
+        int o = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, mergeg_insert_narrow_kernel, HG_INSERT_THREADS, HG_INSERT_NSMEM);
+        g_occ_mg = o > 0 ? o : 1;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    }
     cudaFuncSetAttribute(merge_cta_narrow_kernel<A3_T, A3_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          A3_CAP * 12);
     cudaFuncSetAttribute(merge_cta_narrow_kernel<A4_T, A4_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -657,8 +693,8 @@ void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *
     // so that no earlier failure can leave an append offset behind
     cudaMemsetAsync(hg.nocc, 0, sizeof(int32_t) * (size_t)hg.nhubs, s);
     if (narrow)
-        mergeg_insert_narrow_kernel<<<hg.n_echunks, HG_INSERT_THREADS, HG_INSERT_SMEM, s>>>(hg, ab.mstart, P, ab.flag,
-                                                                                            vkey, vw, err);
+        mergeg_insert_narrow_kernel<<<(unsigned)imin64(hg.n_echunks, (int64_t)g_sms * g_occ_mg), HG_INSERT_THREADS,
+                                      HG_INSERT_NSMEM, s>>>(hg, ab.mstart, P, ab.flag, vkey, vw, err);
     else
         mergeg_insert_kernel<<<hg.n_echunks, HG_INSERT_THREADS, HG_INSERT_SMEM, s>>>(hg, ab.mstart, P, ab.flag, vkey,
                                                                                      vw, err);

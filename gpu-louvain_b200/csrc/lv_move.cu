@@ -704,25 +704,36 @@ __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_narrow_kernel(Graph
     for (int s = threadIdx.x; s < LCAP; s += STAGE_THREADS) { t.keys[s] = -1; t.lo[s] = 0; t.hi[s] = 0; }
     if (threadIdx.x == 0) lnocc = 0;
     __syncthreads();
-    const int32_t h = hg.echunk_hub[blockIdx.x];
-    const int32_t v = hg.hubs[h];
-    const int32_t r1 = g.rowend[v];
-    const int32_t e0 = g.rowptr[v] + hg.echunk_e0[blockIdx.x];
-    const int32_t e1 = min(e0 + STAGE_CHUNK, r1);
-    const int32_t own = __ldg(st.comm + v);
-    u64 e_own = 0;
-    insert_row_piece<LV_U_STAGE, true>(g, st.comm, v, own, e0, e1, threadIdx.x, STAGE_THREADS, t, LLG, st.err,
-                                       locc, &lnocc, STAGE_CHUNK, e_own);
-    block_add_total<STAGE_THREADS>(e_own, hg.eown + h);   // contains the barrier
-    const int32_t n = lnocc;
-    if (threadIdx.x == 0) base = atomicAdd(hg.nocc + h, n);
-    __syncthreads();
-    int32_t *sk = hg.stage_key + hg.occ_off[h] + base;
-    u64 *sv = hg.stage_val + hg.occ_off[h] + base;
-    for (int32_t i = threadIdx.x; i < n; i += STAGE_THREADS) {
-        const int32_t sl = locc[i];
-        sk[i] = t.keys[sl];
-        sv[i] = piece_value(t, (uint32_t)sl);
+    // persistent over the chunks: the table is initialised once and after
+    // each chunk only its claimed slots are cleared (a chunk of an aggregated
+    // level touches a few dozen of the 2 STAGE_CHUNK slots)
+    for (int32_t ch = blockIdx.x; ch < hg.n_echunks; ch += gridDim.x) {
+        const int32_t h = hg.echunk_hub[ch];
+        const int32_t v = hg.hubs[h];
+        const int32_t r1 = g.rowend[v];
+        const int32_t e0 = g.rowptr[v] + hg.echunk_e0[ch];
+        const int32_t e1 = min(e0 + STAGE_CHUNK, r1);
+        const int32_t own = __ldg(st.comm + v);
+        u64 e_own = 0;
+        insert_row_piece<LV_U_STAGE, true>(g, st.comm, v, own, e0, e1, threadIdx.x, STAGE_THREADS, t, LLG, st.err,
+                                           locc, &lnocc, STAGE_CHUNK, e_own);
+        block_add_total<STAGE_THREADS>(e_own, hg.eown + h);   // contains the barrier
+        const int32_t n = min(lnocc, STAGE_CHUNK);
+        if (threadIdx.x == 0) base = atomicAdd(hg.nocc + h, n);
+        __syncthreads();
+        int32_t *sk = hg.stage_key + hg.occ_off[h] + base;
+        u64 *sv = hg.stage_val + hg.occ_off[h] + base;
+        for (int32_t i = threadIdx.x; i < n; i += STAGE_THREADS) {
+            const uint32_t sl = (uint32_t)locc[i];
+            sk[i] = t.keys[sl];
+            sv[i] = piece_value(t, sl);
+            t.keys[sl] = -1;
+            t.lo[sl] = 0;
+            t.hi[sl] = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) lnocc = 0;
+        __syncthreads();
     }
 }
 
@@ -1072,6 +1083,11 @@ static void set_attrs_for(DeviceInfo &di) {
                          cudaFuncAttributeMaxDynamicSharedMemorySize, FB_SMEM);
     cudaFuncSetAttribute(giant_stage_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM);
     cudaFuncSetAttribute(giant_stage_narrow_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM);
+    {
+        int o2 = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, giant_stage_narrow_kernel<WT>, STAGE_THREADS, STAGE_SMEM);
+        di.occ_stage_narrow = o2 > 0 ? o2 : 1;
+    }
     cudaFuncSetAttribute(move_warp_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_SMEM);
     cudaFuncSetAttribute(move_warp_narrow_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_NSMEM);
     int o = 0;
@@ -1140,7 +1156,9 @@ void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGl
     cudaMemsetAsync(hg.nocc, 0, sizeof(int32_t) * (size_t)hg.nhubs, s);
     cudaMemsetAsync(hg.eown, 0, sizeof(u64) * (size_t)hg.nhubs, s);
     cudaMemsetAsync(fs.q[NFBQ].done, 0, sizeof(int32_t) * (size_t)fs.q[NFBQ].cap, s);
-    if (narrow) giant_stage_narrow_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg);
+    if (narrow)
+        giant_stage_narrow_kernel<WT><<<(unsigned)imin64(hg.n_echunks, (int64_t)di.sms * di.occ_stage_narrow),
+                                        STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg);
     else giant_stage_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg);
     note_launches(1);
 #if LV_MERGE_SMALL
