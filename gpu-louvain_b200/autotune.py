@@ -54,7 +54,7 @@ def _run_ms(lvb, graph, device_csr, device, min_gain, knobs) -> tuple[float, flo
 
 
 def tune(graph=None, *, device_csr=None, device: int = 0, min_gain: float = 1e-6, cache: str | None = None,
-         min_gain_frac: float = 0.01, giant_degrees=GIANT_DEGREES, warp_limits=WARP_LIMITS) -> dict:
+         min_gain_frac: float = 0.02, giant_degrees=GIANT_DEGREES, warp_limits=WARP_LIMITS) -> dict:
     """The fastest knob setting for this graph on this GPU:
     {"giant_degree", "warp_limit", "ms", "default_ms", "trials", "cached"}.
     Pass the returned giant_degree / warp_limit to Louvain(...)."""

@@ -304,6 +304,20 @@ __device__ __forceinline__ void warp_append(int32_t claimed, int32_t *occ, int32
     if (claimed >= 0) occ[base + __popc(bal & ((1u << lane) - 1u))] = claimed;
 }
 
+// warp_append for a list of occ_cap entries: *nocc counts every claim, the
+// first occ_cap of them are listed.  All 32 lanes must call it.
+__device__ __forceinline__ void warp_append_capped(int32_t claimed, int32_t *occ, int32_t *nocc, int32_t occ_cap) {
+    const unsigned bal = __ballot_sync(FULL, claimed >= 0);
+    if (!bal) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(bal) - 1;
+    int32_t base = 0;
+    if (lane == leader) base = atomicAdd(nocc, __popc(bal));
+    base = __shfl_sync(FULL, base, leader);
+    const int32_t i = base + __popc(bal & ((1u << lane) - 1u));
+    if (claimed >= 0 && i < occ_cap) occ[i] = claimed;
+}
+
 // table_insert that also appends every newly claimed slot to occ[] (count in
 // *nocc), so that evaluation and clearing visit only occupied slots.
 __device__ __forceinline__ void table_insert_occ(int32_t *keys, u64 *vals, int lg, int32_t key,

@@ -119,6 +119,9 @@ struct lv_handle {
     u64 *k = nullptr, *S = nullptr;
     int32_t *list = nullptr;
     int32_t *cls_scratch = nullptr;   // class counts, cursors, then V0 entries of scratch
+    int32_t *sort_buf = nullptr;      // 3 V0 int32: keys, keys and values of the degree sort
+    void *sort_temp = nullptr;
+    size_t sort_temp_bytes = 0;
     int32_t cls_off[NCLS + 1] = {0};
     int64_t cls_edges[NCLS] = {0};
 
@@ -588,6 +591,18 @@ int level_setup(lv_handle *h) {
     launch_class_scatter(h->cur_rowptr, h->cur_rowend, h->V, h->giant_degree, h->fb.warp_limit, h->cls_off,
                          cursors, h->list, h->fb.hint,
                          h->stream);
+    // the warp kernels' vertices by decreasing degree within each update
+    // bucket (bucket 6's warp part spans classes H1 and H2)
+    {
+        const int32_t V0 = h->V0;
+        int32_t *kb = h->sort_buf, *ka = h->sort_buf + V0, *va = h->sort_buf + 2 * (size_t)V0;
+        const int32_t seg[3][3] = {{CLS_B4, CLS_B5, 84}, {CLS_B5, CLS_H1, 319}, {CLS_H1, CLS_HG, h->giant_degree}};
+        for (const auto &sg : seg) {
+            const int32_t lo = h->cls_off[sg[0]], n = h->cls_off[sg[1]] - lo;
+            sort_by_degree_desc(h->cur_rowptr, h->cur_rowend, h->list + lo, n, sg[2], kb, ka, va, h->sort_temp,
+                                h->sort_temp_bytes, h->stream);
+        }
+    }
     if (h->level == 0) {
         LV_TRY(compute_k<float>(h));
     }
@@ -1282,6 +1297,13 @@ int finish_create(lv_handle *h) {
     LV_TRY(dalloc(h, &h->S, V + 1));
     LV_TRY(dalloc(h, &h->list, V + 1));
     LV_TRY(dalloc(h, &h->cls_scratch, V + SCRATCH_OFF + 16));
+    LV_TRY(dalloc(h, &h->sort_buf, 3 * V + 16));
+    h->sort_temp_bytes = sort_by_degree_temp_bytes((int32_t)V, HG_MIN_DEG_HI) + 256;
+    {
+        unsigned char *t = nullptr;
+        LV_TRY(dalloc(h, &t, h->sort_temp_bytes));
+        h->sort_temp = t;
+    }
     {
         // fallback work lists of the move phase.  Only vertices of degree
         // > warp_limit are queued (at most E / warp_limit of them at any
@@ -1289,7 +1311,8 @@ int finish_create(lv_handle *h) {
         // > FBQ_MAXDEG(NFBQ - 1), or as many staged pairs of a giant.
         FallbackSet &fs = h->fb;
         int32_t *counters = nullptr;
-        LV_TRY(dalloc(h, &counters, 2 * (NFBQ + 1)));
+        LV_TRY(dalloc(h, &counters, 2 * (NFBQ + 1) + 2));
+        fs.warp_next = counters + 2 * (NFBQ + 1);
         LV_TRY(dalloc(h, &fs.hint, V + 1));
         LV_CUDA(h, cudaMemsetAsync(fs.hint, 0, V + 1, h->stream));
         const size_t cap_row = (size_t)(h->E0 / fs.warp_limit) + 64;
@@ -1468,7 +1491,12 @@ int lv_destroy(lv_handle *h) {
         }
     }
     dfree(h, h->comm); dfree(h, h->newc); dfree(h, h->size); dfree(h, h->orig2comm);
-    dfree(h, h->k); dfree(h, h->S); dfree(h, h->list); dfree(h, h->cls_scratch);
+    dfree(h, h->k); dfree(h, h->S); dfree(h, h->list); dfree(h, h->cls_scratch); dfree(h, h->sort_buf);
+    {
+        unsigned char *t = (unsigned char *)h->sort_temp;
+        dfree(h, t);
+        h->sort_temp = nullptr;
+    }
     dfree(h, h->tbl_keys); dfree(h, h->tbl_vals); dfree(h, h->occ_buf); dfree(h, h->nocc_buf);
     dfree(h, h->stage_key); dfree(h, h->stage_val); dfree(h, h->eown_buf); dfree(h, h->ovf_buf);
     for (HubLayout *L : {&h->hub_move, &h->hub_agg}) {

@@ -128,6 +128,7 @@ constexpr int WARP_LIMIT_MIN = 32, WARP_LIMIT_MAX = 384;
 struct FallbackSet {
     Fallback q[NFBQ + 1];   // row queues by degree, then the large queue
     uint8_t *hint = nullptr;
+    int32_t *warp_next = nullptr;   // the warp kernels' vertex cursor (follows the queues' counters)
     int32_t warp_limit = 352;
     int32_t hint_set = 264;   // hint = distinct count above this
 };
@@ -189,6 +190,13 @@ void launch_class_count(const int32_t *rowptr, const int32_t *rowend, int32_t V,
 void launch_class_scatter(const int32_t *rowptr, const int32_t *rowend, int32_t V, int32_t giant_degree,
                           int32_t warp_limit, const int32_t *offsets, int32_t *cursors, int32_t *list,
                           uint8_t *hint, cudaStream_t s);
+// Reorder list[0, n) by decreasing row length (the warp kernels take their
+// vertices from a shared cursor, so the longest rows start first): keys,
+// keys_alt and vals_alt hold n int32 each, temp sort_by_degree_temp_bytes.
+size_t sort_by_degree_temp_bytes(int32_t n, int32_t maxdeg);
+void sort_by_degree_desc(const int32_t *rowptr, const int32_t *rowend, int32_t *list, int32_t n, int32_t maxdeg,
+                         int32_t *keys, int32_t *keys_alt, int32_t *vals_alt, void *temp, size_t temp_bytes,
+                         cudaStream_t s);
 void launch_fill_i32(int32_t *p, int64_t n, int32_t v, cudaStream_t s);
 void launch_iota_i32(int32_t *p, int64_t n, cudaStream_t s);
 void launch_level_init(int32_t *comm, int32_t *newc, int32_t *size, const u64 *k, u64 *S,

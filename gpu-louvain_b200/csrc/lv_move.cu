@@ -234,10 +234,15 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
     for (int s = lane; s < WARP_CAP; s += 32) { keys[s] = -1; vals[s] = 0; }
     __syncwarp();
     u64 delta_acc = 0;
-    const int32_t nwarps = gridDim.x * NW;
     // the next vertex's id, row bounds and community are loaded while the
     // current one is processed (none of them changes during the sub-round)
-    int32_t idx = blockIdx.x * NW + wid;
+    // vertices are taken one at a time from a shared cursor (the class lists
+    // are sorted by decreasing degree, so the longest rows go first and the
+    // warps finish together); the next vertex's id, row bounds and community
+    // are loaded while the current one is processed
+    int32_t idx = 0;
+    if (lane == 0) idx = atomicAdd(fs.warp_next, 1);
+    idx = __shfl_sync(FULL, idx, 0);
     int32_t nv = 0, nr0 = 0, nr1 = 0, nown = 0;
     if (idx < n) {
         nv = list[idx];
@@ -245,14 +250,18 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
         nr1 = g.rowend[nv];
         nown = __ldg(st.comm + nv);
     }
-    for (; idx < n; idx += nwarps) {
+    while (idx < n) {
         const int32_t v = nv, r0 = nr0, r1 = nr1, own = nown;
-        if (idx + nwarps < n) {
-            nv = list[idx + nwarps];
+        int32_t nidx = 0;
+        if (lane == 0) nidx = atomicAdd(fs.warp_next, 1);
+        nidx = __shfl_sync(FULL, nidx, 0);
+        if (nidx < n) {
+            nv = list[nidx];
             nr0 = g.rowptr[nv];
             nr1 = g.rowend[nv];
             nown = __ldg(st.comm + nv);
         }
+        idx = nidx;
         const int32_t d = r1 - r0;
         if (d > fs.warp_limit && fs.hint[v]) {
             if (lane == 0) enqueue_fallback(fs, v, d, st.err);
@@ -338,7 +347,6 @@ template <typename WT>
 __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, StateView st,
                                                                const int32_t *__restrict__ list, int32_t n,
                                                                FallbackSet fs, u64 *dE) {
-    constexpr int NW = 8;
     constexpr int LG = ilog2_c(WARP_CAP);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -353,8 +361,13 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
     if (lane == 0) *nocc = 0;
     __syncwarp();
     u64 delta_acc = 0;
-    const int32_t nwarps = gridDim.x * NW;
-    int32_t idx = blockIdx.x * NW + wid;
+    // vertices are taken one at a time from a shared cursor (the class lists
+    // are sorted by decreasing degree, so the longest rows go first and the
+    // warps finish together); the next vertex's id, row bounds and community
+    // are loaded while the current one is processed
+    int32_t idx = 0;
+    if (lane == 0) idx = atomicAdd(fs.warp_next, 1);
+    idx = __shfl_sync(FULL, idx, 0);
     int32_t nv = 0, nr0 = 0, nr1 = 0, nown = 0;
     if (idx < n) {
         nv = list[idx];
@@ -362,14 +375,18 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
         nr1 = g.rowend[nv];
         nown = __ldg(st.comm + nv);
     }
-    for (; idx < n; idx += nwarps) {
+    while (idx < n) {
         const int32_t v = nv, r0 = nr0, r1 = nr1, own = nown;
-        if (idx + nwarps < n) {
-            nv = list[idx + nwarps];
+        int32_t nidx = 0;
+        if (lane == 0) nidx = atomicAdd(fs.warp_next, 1);
+        nidx = __shfl_sync(FULL, nidx, 0);
+        if (nidx < n) {
+            nv = list[nidx];
             nr0 = g.rowptr[nv];
             nr1 = g.rowend[nv];
             nown = __ldg(st.comm + nv);
         }
+        idx = nidx;
         const int32_t d = r1 - r0;
         if (d > fs.warp_limit && fs.hint[v]) {
             if (lane == 0) enqueue_fallback(fs, v, d, st.err);
@@ -410,32 +427,24 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                if (cc[u] < 0) continue;
-                if (cc[u] == own) {
-                    e_own += ww[u];
-                } else if (kk[u] == cc[u]) {
-                    piece_add(t, hs[u], ww[u]);
-                } else {
-                    const int32_t claimed = piece_insert_at(t, lg, hs[u], cc[u], ww[u], st.err);
-                    if (claimed >= 0) {
-                        const int32_t i = atomicAdd(nocc, 1);
-                        if (i < WARP_OCC_CAP) occ[i] = claimed;
-                    }
+                int32_t claimed = -1;
+                if (cc[u] >= 0) {
+                    if (cc[u] == own) e_own += ww[u];
+                    else if (kk[u] == cc[u]) piece_add(t, hs[u], ww[u]);
+                    else claimed = piece_insert_at(t, lg, hs[u], cc[u], ww[u], st.err);
                 }
+                // one shared atomic per warp for the claims of this step
+                warp_append_capped(claimed, occ, nocc, WARP_OCC_CAP);
             }
 #else
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                if (cc[u] < 0) continue;
-                if (cc[u] == own) {
-                    e_own += ww[u];
-                } else {
-                    const int32_t claimed = piece_insert(t, lg, cc[u], ww[u], st.err);
-                    if (claimed >= 0) {
-                        const int32_t i = atomicAdd(nocc, 1);
-                        if (i < WARP_OCC_CAP) occ[i] = claimed;
-                    }
+                int32_t claimed = -1;
+                if (cc[u] >= 0) {
+                    if (cc[u] == own) e_own += ww[u];
+                    else claimed = piece_insert(t, lg, cc[u], ww[u], st.err);
                 }
+                warp_append_capped(claimed, occ, nocc, WARP_OCC_CAP);
             }
 #endif
             __syncwarp();
@@ -1184,7 +1193,7 @@ void launch_move_wide(const GraphView<WT> &g, const StateView &st, const int32_t
     if (n <= 0) return;
     // the queues' (count, next) pairs are contiguous; the large queue's done
     // counters are cleared as in launch_move_giants
-    cudaMemsetAsync(fs.q[0].count, 0, 2 * (NFBQ + 1) * sizeof(int32_t), s);
+    cudaMemsetAsync(fs.q[0].count, 0, (2 * (NFBQ + 1) + 1) * sizeof(int32_t), s);   // + the warp cursor
     if (max_degree > fs.warp_limit)
         cudaMemsetAsync(fs.q[NFBQ].done, 0, sizeof(int32_t) * (size_t)fs.q[NFBQ].cap, s);
     if (narrow) {

@@ -9,6 +9,8 @@
 // from pinned host memory).
 #include <atomic>
 
+#include <cub/cub.cuh>
+
 #include "lv_internal.h"
 
 namespace lv {
@@ -302,6 +304,41 @@ void launch_class_scatter(const int32_t *rowptr, const int32_t *rowend, int32_t 
     class_scatter_kernel<<<grid_for(V), 256, 0, s>>>(rowptr, rowend, V, giant_degree, warp_limit, o, cursors, list,
                                                      hint);
     note_launches(1);
+}
+
+namespace {
+__global__ void degree_key_kernel(const int32_t *__restrict__ rowptr, const int32_t *__restrict__ rowend,
+                                  const int32_t *__restrict__ list, int32_t n, int32_t maxdeg, int32_t *keys) {
+    for (int32_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
+        const int32_t v = list[i];
+        const int32_t d = rowend[v] - rowptr[v];
+        keys[i] = maxdeg - (d < maxdeg ? d : maxdeg);
+    }
+}
+
+int key_bits(int32_t maxdeg) {
+    int b = 1;
+    while (b < 31 && ((int64_t)1 << b) <= (int64_t)maxdeg) ++b;
+    return b;
+}
+}  // namespace
+
+size_t sort_by_degree_temp_bytes(int32_t n, int32_t maxdeg) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const int32_t *)nullptr, (int32_t *)nullptr,
+                                    (const int32_t *)nullptr, (int32_t *)nullptr, (int64_t)n, 0, key_bits(maxdeg));
+    return bytes;
+}
+
+void sort_by_degree_desc(const int32_t *rowptr, const int32_t *rowend, int32_t *list, int32_t n, int32_t maxdeg,
+                         int32_t *keys, int32_t *keys_alt, int32_t *vals_alt, void *temp, size_t temp_bytes,
+                         cudaStream_t s) {
+    if (n <= 1) return;
+    degree_key_kernel<<<grid_for(n), 256, 0, s>>>(rowptr, rowend, list, n, maxdeg, keys);
+    note_launches(1);
+    cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, keys_alt, list, vals_alt, (int64_t)n, 0, key_bits(maxdeg),
+                                    s);
+    cudaMemcpyAsync(list, vals_alt, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToDevice, s);
 }
 
 void launch_fill_i32(int32_t *p, int64_t n, int32_t v, cudaStream_t s) {
