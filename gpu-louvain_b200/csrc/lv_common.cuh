@@ -415,7 +415,11 @@ __device__ __forceinline__ void insert_row_piece(const GraphView<WT> &g, const i
                                                  int32_t v, int32_t own, int32_t r0, int32_t r1, int lane,
                                                  int stride, const PieceTable &t, int lg, int *err,
                                                  int32_t *occ, int32_t *nocc, int32_t occ_cap, u64 &e_own) {
-    for (int32_t base = r0 + lane; base < r1; base += U * stride) {
+    // OCC (CTA-wide callers: lane = threadIdx.x, stride a multiple of 32):
+    // the loop runs the same number of steps in every lane of a warp, so the
+    // claims of a step are listed with one shared atomic per warp
+    const int32_t wlane = OCC ? (lane & 31) : 0;
+    for (int32_t base = r0 + lane; base - wlane < r1; base += U * stride) {
         int32_t jj[U];
         u64 ww[U];
 #pragma unroll
@@ -433,16 +437,12 @@ __device__ __forceinline__ void insert_row_piece(const GraphView<WT> &g, const i
         for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(comm + jj[u]) : -1;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            if (cc[u] < 0) continue;
-            if (cc[u] == own) {
-                e_own += ww[u];
-            } else {
-                const int32_t claimed = piece_insert(t, lg, cc[u], ww[u], err);
-                if (OCC && claimed >= 0) {
-                    const int32_t i = atomicAdd(nocc, 1);
-                    if (i < occ_cap) occ[i] = claimed;
-                }
+            int32_t claimed = -1;
+            if (cc[u] >= 0) {
+                if (cc[u] == own) e_own += ww[u];
+                else claimed = piece_insert(t, lg, cc[u], ww[u], err);
             }
+            if (OCC) warp_append_capped(claimed, occ, nocc, occ_cap);
         }
     }
 }
