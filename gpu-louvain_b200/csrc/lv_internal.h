@@ -97,7 +97,10 @@ constexpr int WARP_CAP = 512;
 constexpr int WARP_LIMIT = 352;
 constexpr int NFBQ = 4;
 __host__ __device__ constexpr int FBQ_MAXDEG(int b) { return 512 << b; }                 // 512 .. 4096
-__host__ __device__ constexpr int FBQ_THREADS(int b) { return b == 0 ? 128 : (b == 3 ? 512 : 256); }
+// threads per CTA of each row queue: the two large bins hold one or two CTAs
+// per SM (their tables take 57 and 114 KB), so they get 512 and 1024 threads
+// to keep 32 warps per SM
+__host__ __device__ constexpr int FBQ_THREADS(int b) { return b == 0 ? 128 : (b == 1 ? 256 : (b == 2 ? 512 : 1024)); }
 constexpr int FB_THREADS = 1024, FB_CAP = 16384;
 constexpr int FB_KEYS = 7168;
 constexpr int FB_SMEM = FB_CAP * 14;   // table + occupied list
