@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(256) permute_group_kernel(GraphView<WT> g,
     const int32_t dst = P[mslot[v]] - r0;
     for (int32_t e = r0 + lane; e < r1; e += G) {
         vkey[dst + e] = lab[__ldg(g.col + e)];
-        vw[dst + e] = wfix(g.w, e, g.scale);
+        vw[dst + e] = gw(g, e);
     }
 }
 
@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(T) permute_cta_kernel(GraphView<WT> g,
         const int32_t dst = P[mslot[v]] - r0;
         for (int32_t e = r0 + threadIdx.x; e < r1; e += T) {
             vkey[dst + e] = lab[__ldg(g.col + e)];
-            vw[dst + e] = wfix(g.w, e, g.scale);
+            vw[dst + e] = gw(g, e);
         }
     }
 }
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(256) merge_group_kernel(const int32_t *__restr
                                                           const int32_t *__restrict__ newid,
                                                           int32_t *vkey, u64 *vw, uint32_t *vw32,
                                                           int32_t *newdeg, int32_t *epos_new, int *err,
-                                                          int *hiflag) {
+                                                          int *hiflag, uint8_t *wrow) {
     constexpr int GPB = 256 / G;
     constexpr int LG = (CAP == 64) ? 6 : (CAP == 128) ? 7 : 8;
     static_assert((1 << LG) == CAP, "CAP");
@@ -228,12 +228,15 @@ __global__ void __launch_bounds__(256) merge_group_kernel(const int32_t *__restr
             const u64 x = vals[s];
             vkey[pos] = keys[s];
             vw[pos] = x;
-            vw32[pos] = (uint32_t)x;
-            if (keys[s] != self) hi |= x >> 32;   // the self-loop is read as uint64 only
+            vw32[pos] = x < W32_ESC ? (uint32_t)x : W32_ESC;
+            if (keys[s] != self && x >= W32_ESC) hi = 1;   // the self-loop is read as uint64 only
         }
         cnt += __popc(bal);
     }
-    if (hi) atomicOr(hiflag, 1);
+    if (hi) {
+        atomicOr(hiflag, 1);
+        wrow[self] = 1;
+    }
     if (active && lane == 0) {
         const int32_t nid = newid[c];
         newdeg[nid] = cnt;
@@ -248,12 +251,11 @@ __global__ void __launch_bounds__(T) merge_cta_kernel(const int32_t *__restrict_
                                                       const int32_t *__restrict__ newid,
                                                       int32_t *vkey, u64 *vw, uint32_t *vw32,
                                                       int32_t *newdeg, int32_t *epos_new, int *err,
-                                                      int *hiflag) {
+                                                      int *hiflag, uint8_t *wrow) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     u64 *vals = reinterpret_cast<u64 *>(smem_raw);
     int32_t *keys = reinterpret_cast<int32_t *>(vals + CAPMAX);
     __shared__ int32_t cnt;
-    u64 hi = 0;
     for (int s = threadIdx.x; s < CAPMAX; s += T) { keys[s] = -1; vals[s] = 0; }
     if (threadIdx.x == 0) cnt = 0;
     __syncthreads();
@@ -280,8 +282,11 @@ __global__ void __launch_bounds__(T) merge_cta_kernel(const int32_t *__restrict_
                 const u64 x = vals[s];
                 vkey[pos] = key;
                 vw[pos] = x;
-                vw32[pos] = (uint32_t)x;
-                if (key != self) hi |= x >> 32;   // the self-loop is read as uint64 only
+                vw32[pos] = x < W32_ESC ? (uint32_t)x : W32_ESC;
+                if (key != self && x >= W32_ESC) {   // the self-loop is read as uint64 only
+                    atomicOr(hiflag, 1);
+                    wrow[self] = 1;
+                }
                 keys[s] = -1;
                 vals[s] = 0;
             }
@@ -295,7 +300,6 @@ __global__ void __launch_bounds__(T) merge_cta_kernel(const int32_t *__restrict_
         }
         __syncthreads();
     }
-    if (hi) atomicOr(hiflag, 1);
 }
 
 // merge_cta_kernel for a level whose non-self-loop weights are below 2^32:
@@ -310,7 +314,7 @@ __global__ void __launch_bounds__(T) merge_cta_narrow_kernel(const int32_t *__re
                                                              const int32_t *__restrict__ newid,
                                                              int32_t *vkey, u64 *vw, uint32_t *vw32,
                                                              int32_t *newdeg, int32_t *epos_new, int *err,
-                                                             int *hiflag) {
+                                                             int *hiflag, uint8_t *wrow) {
     static_assert(CAPMAX / 2 <= PIECE_MAX_ADDS, "a community's entries fit the piece counters");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PieceTable t;
@@ -319,7 +323,6 @@ __global__ void __launch_bounds__(T) merge_cta_narrow_kernel(const int32_t *__re
     t.keys = reinterpret_cast<int32_t *>(t.hi + CAPMAX);
     __shared__ int32_t cnt;
     __shared__ u64 wpart[T / 32];
-    u64 hi = 0;
     for (int s = threadIdx.x; s < CAPMAX; s += T) { t.keys[s] = -1; t.lo[s] = 0; t.hi[s] = 0; }
     if (threadIdx.x == 0) cnt = 0;
     __syncthreads();
@@ -346,8 +349,11 @@ __global__ void __launch_bounds__(T) merge_cta_narrow_kernel(const int32_t *__re
                 const u64 x = piece_value(t, (uint32_t)s);
                 vkey[pos] = key;
                 vw[pos] = x;
-                vw32[pos] = (uint32_t)x;
-                hi |= x >> 32;
+                vw32[pos] = x < W32_ESC ? (uint32_t)x : W32_ESC;
+                if (x >= W32_ESC) {
+                    atomicOr(hiflag, 1);
+                    wrow[self] = 1;
+                }
                 t.keys[s] = -1;
                 t.lo[s] = 0;
                 t.hi[s] = 0;
@@ -360,7 +366,7 @@ __global__ void __launch_bounds__(T) merge_cta_narrow_kernel(const int32_t *__re
                 const int32_t pos = a + atomicAdd(&cnt, 1);
                 vkey[pos] = self;
                 vw[pos] = ws;
-                vw32[pos] = (uint32_t)ws;   // the self-loop is read as uint64 only
+                vw32[pos] = ws < W32_ESC ? (uint32_t)ws : W32_ESC;   // the self-loop is read as uint64 only
             }
         }
         __syncthreads();
@@ -372,7 +378,6 @@ __global__ void __launch_bounds__(T) merge_cta_narrow_kernel(const int32_t *__re
         }
         __syncthreads();
     }
-    if (hi) atomicOr(hiflag, 1);
 }
 
 // Global-table merge for communities whose degree bound exceeds 4096: one CTA
@@ -506,7 +511,7 @@ __global__ void __launch_bounds__(256) mergeg_emit_kernel(HubGlobal hg,
                                                           const int32_t *__restrict__ P,
                                                           const int32_t *__restrict__ newid,
                                                           int32_t *vkey, u64 *vw, uint32_t *vw32,
-                                                          int *hiflag) {
+                                                          int *hiflag, uint8_t *wrow) {
     const int32_t bidx = blockIdx.x;
     const int32_t h = hg.schunk_hub[bidx];
     const int32_t c = hg.hubs[h];
@@ -524,12 +529,15 @@ __global__ void __launch_bounds__(256) mergeg_emit_kernel(HubGlobal hg,
         const u64 x = vals[sl];
         vkey[a + s0 + i] = key;
         vw[a + s0 + i] = x;
-        vw32[a + s0 + i] = (uint32_t)x;
-        if (key != self) hi |= x >> 32;   // the self-loop is read as uint64 only
+        vw32[a + s0 + i] = x < W32_ESC ? (uint32_t)x : W32_ESC;
+        if (key != self && x >= W32_ESC) hi = 1;   // the self-loop is read as uint64 only
         keys[sl] = -1;
         vals[sl] = 0;
     }
-    if (hi) atomicOr(hiflag, 1);
+    if (hi) {
+        atomicOr(hiflag, 1);
+        wrow[self] = 1;
+    }
 }
 
 __global__ void mergeg_finish_kernel(HubGlobal hg, const int32_t *__restrict__ mstart,
@@ -648,38 +656,38 @@ void agg_new_vertices(const int32_t *size, const u64 *S, int32_t V, const AggBuf
 }
 
 void agg_merge_class(int acls, const AggBuffers &ab, const int32_t *P, const int32_t *list,
-                     int32_t n, int32_t *vkey, u64 *vw, uint32_t *vw32, int *err, int *hiflag, int sms,
-                     cudaStream_t s, bool narrow) {
+                     int32_t n, int32_t *vkey, u64 *vw, uint32_t *vw32, int *err, int *hiflag, uint8_t *wrow,
+                     int sms, cudaStream_t s, bool narrow) {
     if (n <= 0) return;
     switch (acls) {
     case AC1:
         merge_group_kernel<8, 64><<<nblocks(n, 32), 256, 0, s>>>(list, n, ab.mstart, P, ab.flag, vkey,
-                                                                  vw, vw32, ab.newdeg, ab.epos_new, err, hiflag); note_launches(1);
+                                                                  vw, vw32, ab.newdeg, ab.epos_new, err, hiflag, wrow); note_launches(1);
         break;
     case AC2:
         merge_group_kernel<32, 256><<<nblocks(n, 8), 256, 0, s>>>(list, n, ab.mstart, P, ab.flag, vkey,
-                                                                   vw, vw32, ab.newdeg, ab.epos_new, err, hiflag); note_launches(1);
+                                                                   vw, vw32, ab.newdeg, ab.epos_new, err, hiflag, wrow); note_launches(1);
         break;
     case AC3:
         if (narrow)
             merge_cta_narrow_kernel<A3_T, A3_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a3), A3_T, A3_CAP * 12,
                                                     s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw, vw32, ab.newdeg,
-                                                         ab.epos_new, err, hiflag);
+                                                         ab.epos_new, err, hiflag, wrow);
         else
             merge_cta_kernel<A3_T, A3_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a3), A3_T,
                                              A3_CAP * 12, s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw, vw32,
-                                                               ab.newdeg, ab.epos_new, err, hiflag);
+                                                               ab.newdeg, ab.epos_new, err, hiflag, wrow);
         note_launches(1);
         break;
     case AC4:
         if (narrow)
             merge_cta_narrow_kernel<A4_T, A4_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a4), A4_T, A4_CAP * 12,
                                                     s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw, vw32, ab.newdeg,
-                                                         ab.epos_new, err, hiflag);
+                                                         ab.epos_new, err, hiflag, wrow);
         else
             merge_cta_kernel<A4_T, A4_CAP><<<(unsigned)imin64(n, (int64_t)sms * g_occ_a4), A4_T,
                                              A4_CAP * 12, s>>>(list, n, ab.mstart, P, ab.flag, vkey, vw, vw32,
-                                                               ab.newdeg, ab.epos_new, err, hiflag);
+                                                               ab.newdeg, ab.epos_new, err, hiflag, wrow);
         note_launches(1);
         break;
     default: break;
@@ -687,7 +695,8 @@ void agg_merge_class(int acls, const AggBuffers &ab, const int32_t *P, const int
 }
 
 void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *P, int32_t *vkey,
-                      u64 *vw, uint32_t *vw32, int *err, int *hiflag, cudaStream_t s, bool narrow) {
+                      u64 *vw, uint32_t *vw32, int *err, int *hiflag, uint8_t *wrow, cudaStream_t s,
+                      bool narrow) {
     if (hg.nhubs <= 0) return;
     // the per-community list lengths are zero between uses; cleared here too
     // so that no earlier failure can leave an append offset behind
@@ -699,7 +708,7 @@ void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *
         mergeg_insert_kernel<<<hg.n_echunks, HG_INSERT_THREADS, HG_INSERT_SMEM, s>>>(hg, ab.mstart, P, ab.flag, vkey,
                                                                                      vw, err);
     note_launches(1);
-    mergeg_emit_kernel<<<hg.n_schunks, 256, 0, s>>>(hg, ab.mstart, P, ab.flag, vkey, vw, vw32, hiflag); note_launches(1);
+    mergeg_emit_kernel<<<hg.n_schunks, 256, 0, s>>>(hg, ab.mstart, P, ab.flag, vkey, vw, vw32, hiflag, wrow); note_launches(1);
     mergeg_finish_kernel<<<grid_for(hg.nhubs), 256, 0, s>>>(hg, ab.mstart, P, ab.flag, ab.newdeg, ab.epos_new); note_launches(1);
 }
 

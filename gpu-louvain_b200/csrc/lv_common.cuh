@@ -167,8 +167,32 @@ struct GraphView {
     const int32_t *rowend;
     const int32_t *col;
     const WT *w;
-    double scale;   // 2^scale (used for float weights only)
+    double scale;     // 2^scale (used for float weights only)
+    const u64 *w64;   // 32-bit view of an aggregated level: the uint64 sums, read
+                      // where the 32-bit copy holds W32_ESC
 };
+
+// The 32-bit copy of an aggregated level holds each sum below W32_ESC as it
+// is and W32_ESC (an escape) for larger ones, whose exact value is read from
+// the uint64 sums.  A row with an escaped entry other than its self-loop is
+// marked (lv_handle::wrow) and decided by the 64-bit kernels, so the
+// piece-counter tables only ever see weights below 2^32.
+constexpr uint32_t W32_ESC = 0xFFFFFFFFu;
+
+// Exact weight of entry e of a level's row.
+__device__ __forceinline__ u64 gw(const GraphView<float> &g, int64_t e) { return gw(g, e); }
+__device__ __forceinline__ u64 gw(const GraphView<u64> &g, int64_t e) { return __ldg(g.w + e); }
+__device__ __forceinline__ u64 gw(const GraphView<uint32_t> &g, int64_t e) {
+    const uint32_t x = __ldg(g.w + e);
+    return x != W32_ESC ? (u64)x : __ldg(g.w64 + e);
+}
+// ... with the streaming cache hint (row data read once per sweep)
+__device__ __forceinline__ u64 gw_row(const GraphView<float> &g, int64_t e) { return wfix_row(g.w, e, g.scale); }
+__device__ __forceinline__ u64 gw_row(const GraphView<u64> &g, int64_t e) { return ld_row(g.w + e); }
+__device__ __forceinline__ u64 gw_row(const GraphView<uint32_t> &g, int64_t e) {
+    const uint32_t x = ld_row(g.w + e);
+    return x != W32_ESC ? (u64)x : __ldg(g.w64 + e);
+}
 
 struct StateView {
     int32_t *comm;
@@ -179,6 +203,8 @@ struct StateView {
     u64 T;
     int *err;
     float *feat;   // learned active set: 2 features per vertex, written when set
+    const uint8_t *wrow;   // rows with a weight of 2^32 or more (nullptr: none); such a
+                           // vertex is decided by the large fallback queue (64-bit sums)
 };
 
 // Exact 64-bit add to a table value.  In shared memory a 64-bit atomicAdd
@@ -387,7 +413,7 @@ __device__ __forceinline__ void insert_row(const GraphView<WT> &g, const int32_t
             ww[u] = 0;
             if (e < r1) {
                 jj[u] = __ldg(g.col + e);
-                ww[u] = wfix(g.w, e, g.scale);
+                ww[u] = gw(g, e);
             }
         }
         int32_t cc[U];
@@ -429,7 +455,7 @@ __device__ __forceinline__ void insert_row_piece(const GraphView<WT> &g, const i
             ww[u] = 0;
             if (e < r1) {
                 jj[u] = __ldg(g.col + e);
-                ww[u] = wfix(g.w, e, g.scale);
+                ww[u] = gw(g, e);
             }
         }
         int32_t cc[U];

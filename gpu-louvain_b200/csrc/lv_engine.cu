@@ -32,10 +32,11 @@ void agg_permute(int cls, const GraphView<WT> &g, const AggBuffers &ab, const in
 void agg_new_vertices(const int32_t *size, const u64 *S, int32_t V, const AggBuffers &ab,
                       const int32_t *P, u64 *knew, cudaStream_t s);
 void agg_merge_class(int acls, const AggBuffers &ab, const int32_t *P, const int32_t *list,
-                     int32_t n, int32_t *vkey, u64 *vw, uint32_t *vw32, int *err, int *hiflag, int sms,
-                     cudaStream_t s, bool narrow);
+                     int32_t n, int32_t *vkey, u64 *vw, uint32_t *vw32, int *err, int *hiflag, uint8_t *wrow,
+                     int sms, cudaStream_t s, bool narrow);
 void agg_merge_global(const HubGlobal &hg, const AggBuffers &ab, const int32_t *P, int32_t *vkey,
-                      u64 *vw, uint32_t *vw32, int *err, int *hiflag, cudaStream_t s, bool narrow);
+                      u64 *vw, uint32_t *vw32, int *err, int *hiflag, uint8_t *wrow, cudaStream_t s,
+                      bool narrow);
 void agg_row_bounds(const AggBuffers &ab, int32_t Vn, int32_t *start, int32_t *end, cudaStream_t s);
 void launch_gather_degrees(const int32_t *rowptr, const int32_t *rowend, const int32_t *list,
                            int32_t n, int32_t *out, cudaStream_t s);
@@ -102,10 +103,11 @@ struct lv_handle {
     // current level: row v = cur_col/cur_w[cur_rowptr[v] .. cur_rowend[v])
     int32_t *cur_rowptr = nullptr, *cur_rowend = nullptr, *cur_col = nullptr;
     u64 *cur_w = nullptr;   // nullptr at level 0 (float input weights)
-    uint32_t *cur_w32 = nullptr;   // 32-bit copy of cur_w when every sum other than the
-                                   // self-loops is below 2^32; the move kernels (which
-                                   // skip self-loops) then read it, the modularity pass
-                                   // and the aggregation read cur_w
+    uint32_t *cur_w32 = nullptr;   // 32-bit copy of cur_w (sums of 2^32 or more escaped to
+                                   // cur_w); the move kernels read it, the modularity
+                                   // pass and the aggregation read cur_w
+    uint8_t *wrow = nullptr;       // [V0] current level: row holds a non-self-loop sum >= 2^32
+    bool wrows_any = false;
 
     // aggregated levels, ping-pong: rows stay where the merge wrote them
     int32_t *lvl_start[2] = {nullptr, nullptr};
@@ -368,15 +370,15 @@ template <typename WT>
 GraphView<WT> view_of(lv_handle *h);
 template <>
 GraphView<float> view_of<float>(lv_handle *h) {
-    return GraphView<float>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->in_w, h->scale_d};
+    return GraphView<float>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->in_w, h->scale_d, nullptr};
 }
 template <>
 GraphView<u64> view_of<u64>(lv_handle *h) {
-    return GraphView<u64>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->cur_w, h->scale_d};
+    return GraphView<u64>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->cur_w, h->scale_d, nullptr};
 }
 template <>
 GraphView<uint32_t> view_of<uint32_t>(lv_handle *h) {
-    return GraphView<uint32_t>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->cur_w32, h->scale_d};
+    return GraphView<uint32_t>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->cur_w32, h->scale_d, h->cur_w};
 }
 
 // Calls F<WT>(args...) with the weight type the move phase reads at the
@@ -403,7 +405,8 @@ bool narrow_weights(const lv_handle *h) {
 }
 
 StateView state_of(lv_handle *h) {
-    return StateView{h->comm, h->newc, h->size, h->k, h->S, h->T, &h->tot_d->err, h->feat};
+    return StateView{h->comm, h->newc, h->size, h->k, h->S, h->T, &h->tot_d->err, h->feat,
+                     h->cur_w32 && h->wrows_any ? h->wrow : nullptr};
 }
 
 // ---------------------------------------------------------------------------
@@ -661,7 +664,8 @@ void enqueue_sweep(lv_handle *h) {
             tc->sbytes = (8.0 + wbytes) * (double)edges + 20.0 * (double)(hg0 - lo);
         }
         if (b < 4)
-            launch_move_class<WT>(b, g, st, h->list + lo, hi - lo, h->di, dE, h->stream, narrow_weights<WT>(h));
+            launch_move_class<WT>(b, g, st, h->list + lo, hi - lo, h->di, dE, h->stream, narrow_weights<WT>(h),
+                                  h->fb);
         else if (hg0 > lo)
             launch_move_wide<WT>(g, st, h->list + lo, hg0 - lo, h->fb, h->di, dE, h->stream,
                                  b == 6 ? h->giant_degree : (b == 4 ? 84 : 319), narrow_weights<WT>(h));
@@ -962,7 +966,7 @@ void enqueue_sweep_active(lv_handle *h, const int32_t *cnt) {
         if (!any) continue;
         if (b < 4) {
             launch_move_class<WT>(b, g, st, h->alist + h->cls_off[b], cnt[b], h->di, dE, h->stream,
-                                  narrow_weights<WT>(h));
+                                  narrow_weights<WT>(h), h->fb);
         } else {
             for (int c = c0; c < c1; ++c) {
                 if (c == CLS_HG || !cnt[c]) continue;
@@ -1183,6 +1187,7 @@ int ensure_agg(lv_handle *h) {
         LV_TRY(dalloc(h, &h->lvl_w[b], E));
         LV_TRY(dalloc(h, &h->lvl_w32[b], E));
     }
+    LV_TRY(dalloc(h, &h->wrow, V + 1));
     h->agg_ready = true;
     return LV_OK;
 }
@@ -1200,7 +1205,7 @@ int aggregate_t(lv_handle *h) {
     int32_t *hiflag = ab.scalars + 12;   // set when a merged sum is 2^32 or more
     // the permuted inter-community weights are the current level's
     // non-self-loop weights: below 2^32 when the move phase reads them narrow
-    const bool narrow = h->cur_w32 ? !h->opts.wide_weights : narrow_weights<WT>(h);
+    const bool narrow = h->cur_w32 ? !h->wrows_any : narrow_weights<WT>(h);
     agg_prepare(h->cur_rowptr, h->cur_rowend, h->comm, h->size, V, ab, h->mslot, h->degm, h->P,
                 h->stream);
     LV_CUDA(h, cudaMemcpyAsync(h->small_h, ab.scalars, sizeof(int32_t) * (2 + NAC),
@@ -1228,10 +1233,12 @@ int aggregate_t(lv_handle *h) {
                         h->cls_off[c + 1] - h->cls_off[c], vkey, vw, h->di.sms, h->stream);
     agg_new_vertices(h->size, h->S, V, ab, h->P, h->k, h->stream);
     LV_CUDA(h, cudaMemsetAsync(hiflag, 0, sizeof(int32_t), h->stream));
+    LV_CUDA(h, cudaMemsetAsync(h->wrow, 0, (size_t)newV + 1, h->stream));
     for (int c = 0; c < NAC - 1; ++c)
         agg_merge_class(c, ab, h->P, ab.clist + aoff[c], aoff[c + 1] - aoff[c], vkey, vw, vw32,
-                        &h->tot_d->err, hiflag, h->di.sms, h->stream, narrow);
-    agg_merge_global(h->hub_agg.view, ab, h->P, vkey, vw, vw32, &h->tot_d->err, hiflag, h->stream, narrow);
+                        &h->tot_d->err, hiflag, h->wrow, h->di.sms, h->stream, narrow);
+    agg_merge_global(h->hub_agg.view, ab, h->P, vkey, vw, vw32, &h->tot_d->err, hiflag, h->wrow, h->stream,
+                     narrow);
     agg_row_bounds(ab, newV, h->lvl_start[nb], h->lvl_end[nb], h->stream);
     // E' = number of stored entries (P is free again after the merges)
     scan_exclusive_i32(ab.newdeg, h->P, newV, h->P + newV, ab.scan_tmp, h->stream);
@@ -1247,13 +1254,13 @@ int aggregate_t(lv_handle *h) {
                      h->st.aggregate_ms);
     LV_TRY(check_device_error(h, h->tot_h->err));
     const int64_t newE = h->small_h[0];
-    const bool wide = h->small_h[1] != 0;
+    h->wrows_any = h->small_h[1] != 0;
     h->cur_buf = nb;
     h->cur_rowptr = h->lvl_start[nb];
     h->cur_rowend = h->lvl_end[nb];
     h->cur_col = h->lvl_col[nb];
     h->cur_w = h->lvl_w[nb];
-    h->cur_w32 = (wide || h->opts.wide_weights) ? nullptr : h->lvl_w32[nb];
+    h->cur_w32 = h->opts.wide_weights ? nullptr : h->lvl_w32[nb];
     h->V = newV;
     h->E = newE;
     h->level += 1;
@@ -1278,6 +1285,7 @@ int to_level0(lv_handle *h) {
     h->cur_col = h->in_col;
     h->cur_w = nullptr;
     h->cur_w32 = nullptr;
+    h->wrows_any = false;
     h->cur_buf = -1;
     h->e_own_valid = false;
     launch_iota_i32(h->orig2comm, h->V0, h->stream);
@@ -1513,6 +1521,7 @@ int lv_destroy(lv_handle *h) {
         dfree(h, h->lvl_start[b]); dfree(h, h->lvl_end[b]); dfree(h, h->lvl_col[b]); dfree(h, h->lvl_w[b]);
         dfree(h, h->lvl_w32[b]);
     }
+    dfree(h, h->wrow);
     dfree(h, h->tot_d);
     dfree(h, h->feat); dfree(h, h->moved); dfree(h, h->nmoved); dfree(h, h->pred); dfree(h, h->fresh);
     dfree(h, h->comm_prev); dfree(h, h->alist);

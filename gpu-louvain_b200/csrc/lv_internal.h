@@ -153,7 +153,8 @@ void init_kernel_attributes(DeviceInfo &di);
 // Classes B0..B3 (degree <= 32): group kernels.
 template <typename WT>
 void launch_move_class(int cls, const GraphView<WT> &g, const StateView &st, const int32_t *list,
-                       int32_t n, const DeviceInfo &di, u64 *dE, cudaStream_t s, bool narrow);
+                       int32_t n, const DeviceInfo &di, u64 *dE, cudaStream_t s, bool narrow,
+                       const FallbackSet &fb);
 // 32 < degree <= 8192 (the vertices of one update bucket): warp kernel +
 // fallback.  Degree > 8192: staged chunks + merge (hg describes the giants).
 // narrow: every weight the kernels read is below 2^32 (piece-counter tables).

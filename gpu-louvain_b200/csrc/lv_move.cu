@@ -35,6 +35,25 @@ __device__ __forceinline__ void block_add_total(u64 x, u64 *total) {
     __syncthreads();
 }
 
+// Queue vertex v (degree d) for the large queue only (64-bit sums, any row):
+// the vertices of a 32-bit-view level whose row holds a sum of 2^32 or more.
+// One lane calls it.
+__device__ __forceinline__ void enqueue_large(const Fallback &f, int32_t v, int32_t d, int *err) {
+    const int32_t P = d > FB_KEYS ? (d + FB_KEYS - 1) / FB_KEYS : 1;
+    const int32_t first = atomicAdd(f.count, P);
+    if (first + P <= f.cap) {
+        for (int32_t q = 0; q < P; ++q) {
+            f.v[first + q] = v;
+            f.p[first + q] = q;
+            f.P[first + q] = P;
+            f.first[first + q] = first;
+            f.src[first + q] = -1;
+        }
+    } else {
+        atomicOr(err, DEVERR_FALLBACK_FULL);
+    }
+}
+
 // ------------------------------------------------------------------------
 // group-per-vertex move kernel (degree <= 84)
 // ------------------------------------------------------------------------
@@ -84,7 +103,7 @@ __global__ void __launch_bounds__(256) move_group_kernel(GraphView<WT> g, StateV
 template <int G, int CAP, typename WT>
 __global__ void __launch_bounds__(256) move_group_narrow_kernel(GraphView<WT> g, StateView st,
                                                                 const int32_t *__restrict__ list,
-                                                                int32_t n, u64 *dE) {
+                                                                int32_t n, u64 *dE, Fallback fbl) {
     constexpr int GPB = 256 / G;
     constexpr int LG = ilog2_c(CAP);
     static_assert((1 << LG) == CAP, "CAP must be a power of two");
@@ -100,9 +119,14 @@ __global__ void __launch_bounds__(256) move_group_narrow_kernel(GraphView<WT> g,
 #pragma unroll
     for (int s = lane; s < CAP; s += G) { t.keys[s] = -1; t.lo[s] = 0; t.hi[s] = 0; }
     __syncwarp();
-    const bool active = idx < n;
+    bool active = idx < n;
     int32_t v = 0, own = 0;
     u64 e_own = 0;
+    if (active && st.wrow && st.wrow[list[idx]]) {
+        // a row with a sum of 2^32 or more: decided by the large queue
+        if (lane == 0) enqueue_large(fbl, list[idx], g.rowend[list[idx]] - g.rowptr[list[idx]], st.err);
+        active = false;
+    }
     if (active) {
         v = list[idx];
         own = __ldg(st.comm + v);
@@ -288,7 +312,7 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
                 const int32_t e = base + 32 * u;
                 jj[u] = -1;
                 ww[u] = 0;
-                if (e < r1) { jj[u] = __ldg(g.col + e); ww[u] = wfix(g.w, e, g.scale); }
+                if (e < r1) { jj[u] = __ldg(g.col + e); ww[u] = gw(g, e); }
             }
             int32_t cc[U];
 #pragma unroll
@@ -388,6 +412,10 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
         }
         idx = nidx;
         const int32_t d = r1 - r0;
+        if (st.wrow && st.wrow[v]) {   // a sum of 2^32 or more: 64-bit sums in the large queue
+            if (lane == 0) enqueue_large(fs.q[NFBQ], v, d, st.err);
+            continue;
+        }
         if (d > fs.warp_limit && fs.hint[v]) {
             if (lane == 0) enqueue_fallback(fs, v, d, st.err);
             continue;
@@ -409,7 +437,7 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
                 const int32_t e = b0 + 32 * u;
                 jj[u] = -1;
                 ww[u] = 0;
-                if (e < r1) { jj[u] = ld_row(g.col + e); ww[u] = wfix_row(g.w, e, g.scale); }
+                if (e < r1) { jj[u] = ld_row(g.col + e); ww[u] = gw_row(g, e); }
             }
             int32_t cc[U];
 #pragma unroll
@@ -540,9 +568,9 @@ __global__ void __launch_bounds__(THREADS) move_fallback_kernel(GraphView<WT> g,
                     if (j == v) continue;
                     const int32_t c = __ldg(st.comm + j);
                     if (c == own) {
-                        if (p == 0) e_own += wfix(g.w, e, g.scale);
+                        if (p == 0) e_own += gw(g, e);
                     } else if (P == 1 || (int32_t)part_of(c, P) == p) {
-                        table_insert_occ_capped(keys, vals, lg, c, wfix(g.w, e, g.scale), st.err, occ,
+                        table_insert_occ_capped(keys, vals, lg, c, gw(g, e), st.err, occ,
                                                 &nocc, OCC_CAP);
                     }
                 }
@@ -719,6 +747,7 @@ __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_narrow_kernel(Graph
     for (int32_t ch = blockIdx.x; ch < hg.n_echunks; ch += gridDim.x) {
         const int32_t h = hg.echunk_hub[ch];
         const int32_t v = hg.hubs[h];
+        if (st.wrow && st.wrow[v]) continue;   // staged by giant_stage_kernel (64-bit sums)
         const int32_t r1 = g.rowend[v];
         const int32_t e0 = g.rowptr[v] + hg.echunk_e0[ch];
         const int32_t e1 = min(e0 + STAGE_CHUNK, r1);
@@ -748,7 +777,10 @@ __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_narrow_kernel(Graph
 
 template <typename WT>
 __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_kernel(GraphView<WT> g, StateView st,
-                                                                    HubGlobal hg) {
+                                                                    HubGlobal hg, const uint8_t *only) {
+    // only != nullptr: just the giants marked there (the rest are staged by
+    // the narrow kernel)
+    if (only && !only[hg.hubs[hg.echunk_hub[blockIdx.x]]]) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int LCAP = 2 * STAGE_CHUNK;
     constexpr int LLG = ilog2_c(LCAP);
@@ -880,7 +912,7 @@ __global__ void __launch_bounds__(256) corr_group_kernel(GraphView<WT> g, const 
                 const int32_t j = __ldg(g.col + e);
                 if (j == u) continue;
                 const int32_t cj = comm[j], nj = newc[j];
-                if (cj != nj) acc += pair_correction(cu, nu, cj, nj, wfix(g.w, e, g.scale));
+                if (cj != nj) acc += pair_correction(cu, nu, cj, nj, gw(g, e));
             }
         }
     }
@@ -925,7 +957,7 @@ __global__ void __launch_bounds__(T) corr_cta_kernel(GraphView<WT> g, const int3
                 const int32_t j = __ldg(g.col + e);
                 if (j == u) continue;
                 const int32_t cj = comm[j], nj = newc[j];
-                if (cj != nj) acc += pair_correction(cu, nu, cj, nj, wfix(g.w, e, g.scale));
+                if (cj != nj) acc += pair_correction(cu, nu, cj, nj, gw(g, e));
             }
         }
         __syncthreads();   // movers / nm are rewritten by the next pass
@@ -976,9 +1008,9 @@ __global__ void __launch_bounds__(256) row_reduce_group_kernel(GraphView<WT> g,
         const int32_t r0 = g.rowptr[v], r1 = g.rowend[v];
         for (int32_t e = r0 + lane; e < r1; e += G) {
             if (MODE == 1) {
-                if (comm[__ldg(g.col + e)] == own) acc += wfix(g.w, e, g.scale);
+                if (comm[__ldg(g.col + e)] == own) acc += gw(g, e);
             } else {
-                acc += wfix(g.w, e, g.scale);
+                acc += gw(g, e);
             }
         }
     }
@@ -1005,9 +1037,9 @@ __global__ void __launch_bounds__(THREADS) row_reduce_cta_kernel(GraphView<WT> g
         u64 acc = 0;
         for (int32_t e = r0 + threadIdx.x; e < r1; e += THREADS) {
             if (MODE == 1) {
-                if (comm[__ldg(g.col + e)] == own) acc += wfix(g.w, e, g.scale);
+                if (comm[__ldg(g.col + e)] == own) acc += gw(g, e);
             } else {
-                acc += wfix(g.w, e, g.scale);
+                acc += gw(g, e);
             }
         }
         if (MODE == 0) {
@@ -1125,12 +1157,25 @@ void init_kernel_attributes(DeviceInfo &di) {
 }
 
 template <typename WT>
+static void launch_fallback_large(const GraphView<WT> &g, const StateView &st, const HubGlobal &hg,
+                                  const FallbackSet &fs, const DeviceInfo &di, u64 *dE, cudaStream_t s);
+
+template <typename WT>
 void launch_move_class(int cls, const GraphView<WT> &g, const StateView &st, const int32_t *list,
-                       int32_t n, const DeviceInfo &di, u64 *dE, cudaStream_t s, bool narrow) {
+                       int32_t n, const DeviceInfo &di, u64 *dE, cudaStream_t s, bool narrow,
+                       const FallbackSet &fs) {
     if (n <= 0) return;
+    // rows marked in st.wrow go to the large queue, decided right after
+    const bool large = narrow && st.wrow;
+    if (large) {
+        cudaMemsetAsync(fs.q[NFBQ].count, 0, 2 * sizeof(int32_t), s);   // count, next
+        cudaMemsetAsync(fs.q[NFBQ].done, 0, sizeof(int32_t) * (size_t)fs.q[NFBQ].cap, s);
+    }
 #define LV_GROUP(G, CAP)                                                                              \
     do {                                                                                              \
-        if (narrow) move_group_narrow_kernel<G, CAP, WT><<<nblocks(n, 256 / G), 256, 0, s>>>(g, st, list, n, dE); \
+        if (narrow)                                                                                   \
+            move_group_narrow_kernel<G, CAP, WT><<<nblocks(n, 256 / G), 256, 0, s>>>(g, st, list, n, dE, \
+                                                                                    fs.q[NFBQ]);     \
         else move_group_kernel<G, CAP, WT><<<nblocks(n, 256 / G), 256, 0, s>>>(g, st, list, n, dE);   \
         note_launches(1);                                                                             \
     } while (0)
@@ -1142,6 +1187,7 @@ void launch_move_class(int cls, const GraphView<WT> &g, const StateView &st, con
     default: break;
     }
 #undef LV_GROUP
+    if (large) launch_fallback_large<WT>(g, st, HubGlobal(), fs, di, dE, s);
 }
 
 template <typename WT>
@@ -1165,11 +1211,18 @@ void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGl
     cudaMemsetAsync(hg.nocc, 0, sizeof(int32_t) * (size_t)hg.nhubs, s);
     cudaMemsetAsync(hg.eown, 0, sizeof(u64) * (size_t)hg.nhubs, s);
     cudaMemsetAsync(fs.q[NFBQ].done, 0, sizeof(int32_t) * (size_t)fs.q[NFBQ].cap, s);
-    if (narrow)
+    if (narrow) {
         giant_stage_narrow_kernel<WT><<<(unsigned)imin64(hg.n_echunks, (int64_t)di.sms * di.occ_stage_narrow),
                                         STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg);
-    else giant_stage_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg);
-    note_launches(1);
+        note_launches(1);
+        if (st.wrow) {
+            giant_stage_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg, st.wrow);
+            note_launches(1);
+        }
+    } else {
+        giant_stage_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg, nullptr);
+        note_launches(1);
+    }
 #if LV_MERGE_SMALL
     giant_merge_kernel<MERGE_S_THREADS, MERGE_S_CAP>
         <<<(unsigned)imin64(hg.nhubs, (int64_t)di.sms * di.occ_merge_s), MERGE_S_THREADS, MERGE_S_CAP * 14, s>>>(
@@ -1194,7 +1247,7 @@ void launch_move_wide(const GraphView<WT> &g, const StateView &st, const int32_t
     // the queues' (count, next) pairs are contiguous; the large queue's done
     // counters are cleared as in launch_move_giants
     cudaMemsetAsync(fs.q[0].count, 0, (2 * (NFBQ + 1) + 1) * sizeof(int32_t), s);   // + the warp cursor
-    if (max_degree > fs.warp_limit)
+    if (max_degree > fs.warp_limit || (narrow && st.wrow))
         cudaMemsetAsync(fs.q[NFBQ].done, 0, sizeof(int32_t) * (size_t)fs.q[NFBQ].cap, s);
     if (narrow) {
         const unsigned grid = (unsigned)imin64((n + 7) / 8, (int64_t)di.sms * di.occ_warp_narrow);
@@ -1204,7 +1257,10 @@ void launch_move_wide(const GraphView<WT> &g, const StateView &st, const int32_t
         move_warp_kernel<WT><<<grid, 256, WARP_SMEM, s>>>(g, st, list, n, fs, dE);
     }
     note_launches(1);
-    if (max_degree <= fs.warp_limit) return;   // no vertex can overflow its warp table
+    if (max_degree <= fs.warp_limit) {   // no vertex can overflow its warp table
+        if (narrow && st.wrow) launch_fallback_large<WT>(g, st, HubGlobal(), fs, di, dE, s);
+        return;
+    }
     launch_fallback_large<WT>(g, st, HubGlobal(), fs, di, dE, s);
     launch_row_queue<WT, 3>(g, st, fs, di, dE, s, narrow);
     launch_row_queue<WT, 2>(g, st, fs, di, dE, s, narrow);
@@ -1284,10 +1340,10 @@ void launch_s2(const u64 *S, int32_t V, u64 *total_hi_lo, cudaStream_t s) {
 
 template void launch_move_class<float>(int, const GraphView<float> &, const StateView &,
                                        const int32_t *, int32_t, const DeviceInfo &, u64 *,
-                                       cudaStream_t, bool);
+                                       cudaStream_t, bool, const FallbackSet &);
 template void launch_move_class<u64>(int, const GraphView<u64> &, const StateView &,
                                      const int32_t *, int32_t, const DeviceInfo &, u64 *,
-                                     cudaStream_t, bool);
+                                     cudaStream_t, bool, const FallbackSet &);
 template void launch_move_wide<float>(const GraphView<float> &, const StateView &, const int32_t *,
                                       int32_t, const FallbackSet &, const DeviceInfo &, u64 *,
                                       cudaStream_t, int32_t, bool);
@@ -1314,7 +1370,7 @@ template void launch_row_reduce<u64>(int, int, const GraphView<u64> &, const int
 
 template void launch_move_class<uint32_t>(int, const GraphView<uint32_t> &, const StateView &,
                                      const int32_t *, int32_t, const DeviceInfo &, u64 *,
-                                     cudaStream_t, bool);
+                                     cudaStream_t, bool, const FallbackSet &);
 template void launch_move_wide<uint32_t>(const GraphView<uint32_t> &, const StateView &, const int32_t *,
                                     int32_t, const FallbackSet &, const DeviceInfo &, u64 *,
                                     cudaStream_t, int32_t, bool);
