@@ -140,6 +140,8 @@ struct lv_handle {
     u64 *eown_buf = nullptr;       // per hub, zero between uses (nocc_cap entries)
     int32_t *ovf_buf = nullptr;    // overflow list (nocc_cap entries) then its count
     bool capturing = false;        // a sweep is being captured into a graph (timers off)
+    bool destroying = false;       // lv_destroy: large buffers go to the per-device cache
+    std::vector<std::pair<void *, size_t>> big;   // live allocations of at least BIG_BYTES
     void *loop_d = nullptr;        // device state of the graph sweep loop
 
     bool agg_ready = false;
@@ -242,18 +244,83 @@ cudaMemPool_t device_pool(int dev) {
     return g_pool[dev];
 }
 
+// Large buffers (at least BIG_BYTES) of destroyed handles are kept per device
+// and handed to the next allocation of exactly the same size: handles of the
+// same graph ask for the same sizes, so a handle created again reuses its
+// predecessor's memory as it is, without the pool having to find or map room
+// for it (which, when its free blocks are fragmented, maps new memory and
+// costs hundreds of milliseconds for the ~20 GB of an R-MAT-24 handle).
+// lv_trim_device_memory releases them.
+constexpr size_t BIG_BYTES = size_t(16) << 20;
+std::mutex g_cache_mu;
+std::vector<std::pair<size_t, void *>> g_cache[LV_MAX_DEVICES];
+
+void *cache_take(int dev, size_t bytes) {
+    if (dev < 0 || dev >= LV_MAX_DEVICES) return nullptr;
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    auto &c = g_cache[dev];
+    for (size_t i = 0; i < c.size(); ++i)
+        if (c[i].first == bytes) {
+            void *p = c[i].second;
+            c[i] = c.back();
+            c.pop_back();
+            return p;
+        }
+    return nullptr;
+}
+
+// hands every cached buffer of the device back (to the pool, or to the driver
+// when the device has no pool); called by lv_trim_device_memory, by each
+// lv_destroy before it caches its own buffers (so the cache holds one
+// handle's worth at most), and by an allocation that failed
+void cache_release(int dev, cudaMemPool_t pool, cudaStream_t stream) {
+    if (dev < 0 || dev >= LV_MAX_DEVICES) return;
+    std::vector<std::pair<size_t, void *>> cached;
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mu);
+        cached.swap(g_cache[dev]);
+    }
+    for (auto &c : cached) {
+        if (pool) cudaFreeAsync(c.second, stream);
+        else cudaFree(c.second);
+    }
+}
+
+bool cache_put(int dev, size_t bytes, void *p) {
+    if (dev < 0 || dev >= LV_MAX_DEVICES) return false;
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    g_cache[dev].emplace_back(bytes, p);
+    return true;
+}
+
 template <typename T>
 int dalloc(lv_handle *h, T **p, size_t n) {
     *p = nullptr;
     if (n == 0) n = 1;
+    const size_t bytes = n * sizeof(T);
+    if (bytes >= BIG_BYTES) {
+        void *c = cache_take(h->device, bytes);
+        if (c) {
+            *p = (T *)c;
+            h->big.emplace_back(c, bytes);
+            return LV_OK;
+        }
+    }
     cudaMemPool_t pool = device_pool(h->device);
-    cudaError_t e = pool ? cudaMallocFromPoolAsync((void **)p, n * sizeof(T), pool, h->stream)
-                         : cudaMalloc((void **)p, n * sizeof(T));
+    cudaError_t e = pool ? cudaMallocFromPoolAsync((void **)p, bytes, pool, h->stream)
+                         : cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cache_release(h->device, pool, h->stream);
+        e = pool ? cudaMallocFromPoolAsync((void **)p, bytes, pool, h->stream)
+                 : cudaMalloc((void **)p, bytes);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         *p = nullptr;
         return fail(h, LV_ERR_NOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
     }
+    if (bytes >= BIG_BYTES) h->big.emplace_back((void *)*p, bytes);
     return LV_OK;
 }
 
@@ -285,8 +352,20 @@ namespace {
 template <typename T>
 void dfree(lv_handle *h, T *&p) {
     if (p) {
-        if (device_pool(h->device)) cudaFreeAsync((void *)p, h->stream);
-        else cudaFree((void *)p);
+        // a large buffer goes to the per-device cache when the handle is
+        // being destroyed (its stream has drained); otherwise to the pool
+        size_t big = 0;
+        for (size_t i = 0; i < h->big.size(); ++i)
+            if (h->big[i].first == (void *)p) {
+                big = h->big[i].second;
+                h->big[i] = h->big.back();
+                h->big.pop_back();
+                break;
+            }
+        if (!(big && h->destroying && cache_put(h->device, big, (void *)p))) {
+            if (device_pool(h->device)) cudaFreeAsync((void *)p, h->stream);
+            else cudaFree((void *)p);
+        }
     }
     p = nullptr;
 }
@@ -1474,6 +1553,12 @@ int lv_trim_device_memory(int32_t device) {
         std::lock_guard<std::mutex> lock(g_pool_mu);
         pool = g_pool[device];
     }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    cache_release(device, pool, 0);
+    cudaDeviceSynchronize();
+    cudaSetDevice(prev);
     if (!pool) return LV_OK;
     return cudaMemPoolTrimTo(pool, 0) == cudaSuccess ? LV_OK : LV_ERR_CUDA;
 }
@@ -1484,6 +1569,8 @@ int lv_destroy(lv_handle *h) {
     if (!h) return LV_OK;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    cache_release(h->device, device_pool(h->device), h->stream);
+    h->destroying = true;
     if (h->owns_input) {
         dfree(h, h->in_rowptr);
         dfree(h, h->in_col);

@@ -78,7 +78,7 @@ def main():
     ap.add_argument("--target-recall", type=float, default=0.99)
     ap.add_argument("--full-every", type=int, default=4, help="recommended lv_opts.active_full_every")
     ap.add_argument("--active-start", type=float, default=0.2, help="recommended lv_opts.active_start")
-    ap.add_argument("--min-recall", type=float, default=0.8, help="recommended lv_opts.active_min_recall")
+    ap.add_argument("--min-recall", type=float, default=0.5, help="recommended lv_opts.active_min_recall")
     ap.add_argument("--min-gain", type=float, default=1e-6)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--seed", type=int, default=7)
