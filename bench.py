@@ -229,6 +229,113 @@ def ncu_traffic(workload: str, cls_name: str):
         return None
 
 
+def ncu_class_split(csv_path: str) -> dict:
+    """Per-class device time and DRAM bytes of one --profile-only run, from
+    an ncu CSV of its launches (``--metrics gpu__time_duration.sum,
+    dram__bytes_read.sum,dram__bytes_write.sum --csv``, every launch).
+
+    Launches are attributed the way the engine issues a sweep: each degree
+    bucket's move kernels, then its correction kernels, then commit_kernel;
+    a bucket is named by its move kernel (move_group_*<G,...>: G = 4/8/16/32
+    -> buckets 0-3) or, for the warp buckets, by its correction kernel
+    (corr_group_kernel<32> -> bucket 4, corr_cta_kernel<128> -> bucket 5,
+    corr_cta_kernel<256|512> -> bucket 6).  In bucket 6 the giant kernels
+    (giant_stage_*, giant_merge_* and the large queue after them) form the
+    b6_giants class, as the engine's class events bracket them."""
+    import csv
+    import re
+    with open(csv_path) as f:
+        rows = list(csv.reader(f))
+    hi = next(i for i, r in enumerate(rows) if "Kernel Name" in r and "Metric Name" in r)
+    hdr = rows[hi]
+    c_id, c_name = hdr.index("ID"), hdr.index("Kernel Name")
+    c_metric, c_value = hdr.index("Metric Name"), hdr.index("Metric Value")
+    c_unit = hdr.index("Metric Unit") if "Metric Unit" in hdr else None
+    scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "nsecond": 1e-9, "usecond": 1e-6,
+             "msecond": 1e-3, "second": 1.0, "ns": 1e-9, "us": 1e-6, "ms": 1e-3}
+    launches = {}
+    order = []
+    for r in rows[hi + 1:]:
+        if len(r) <= max(c_id, c_name, c_metric, c_value):
+            continue
+        lid = int(r[c_id])
+        if lid not in launches:
+            launches[lid] = {"name": r[c_name], "s": 0.0, "bytes": 0.0}
+            order.append(lid)
+        v = float(r[c_value].replace(",", ""))
+        u = r[c_unit] if c_unit is not None else ""
+        v *= scale.get(u, 1.0)
+        m = r[c_metric]
+        if m.startswith("gpu__time_duration"):
+            launches[lid]["s"] += v
+        elif m.startswith("dram__bytes"):
+            launches[lid]["bytes"] += v
+
+    def short(n):
+        n = re.sub(r"\(.*", "", n)
+        return n.replace("void ", "").replace("lv::<unnamed>::", "").replace("<unnamed>::", "").strip()
+
+    out = {c: {"class_launches": 0, "kernel_launches": 0, "ms": 0.0, "dram_bytes": 0.0}
+           for c in CLASS_NAMES[:8]}
+    seg = []
+
+    def close(seg):
+        names = [short(launches[i]["name"]) for i in seg]
+        moves = [i for i, n in zip(seg, names) if not n.startswith(("corr_", "commit_kernel"))]
+        corr = [n for n in names if n.startswith("corr_")]
+        grp = [re.match(r"move_group\w*<(\d+),", n) for n in names]
+        grp = [int(m.group(1)) for m in grp if m]
+        if grp:
+            b = {4: 0, 8: 1, 16: 2, 32: 3}.get(grp[0])
+        elif any(n.startswith("corr_group_kernel<32") for n in corr):
+            b = 4
+        elif any(n.startswith("corr_cta_kernel<128") for n in corr):
+            b = 5
+        elif corr:
+            b = 6
+        else:
+            return
+        if b is None:
+            return
+        parts = {CLASS_NAMES[b]: []}
+        if b == 6:
+            parts["b6_giants"] = []
+            cur = CLASS_NAMES[6]
+            for i in moves:
+                if short(launches[i]["name"]).startswith("giant_stage"):
+                    cur = "b6_giants"
+                parts[cur].append(i)
+        else:
+            parts[CLASS_NAMES[b]] = moves
+        for c, ids in parts.items():
+            if not ids:
+                continue
+            o = out[c]
+            o["class_launches"] += 1
+            o["kernel_launches"] += len(ids)
+            o["ms"] += 1e3 * sum(launches[i]["s"] for i in ids)
+            o["dram_bytes"] += sum(launches[i]["bytes"] for i in ids)
+
+    in_sweep = False
+    for lid in order:
+        n = short(launches[lid]["name"])
+        if n.startswith(("move_", "giant_", "corr_")):
+            in_sweep = True
+        if in_sweep:
+            seg.append(lid)
+        if n.startswith("commit_kernel"):
+            close(seg)
+            seg, in_sweep = [], False
+    for c, o in out.items():
+        k = max(o["class_launches"], 1)
+        o["dram_bytes_per_launch"] = o["dram_bytes"] / k
+        o["ms_per_launch"] = o["ms"] / k
+        o["ms"] = round(o["ms"], 3)
+    return {"csv": os.path.basename(csv_path), "launches": len(order),
+            "total_ms": round(1e3 * sum(l["s"] for l in launches.values()), 3),
+            "total_dram_bytes": sum(l["bytes"] for l in launches.values()), "classes": out}
+
+
 def rmat_config(scale: int, V: int, E: int, world: int) -> dict:
     """The workload description shared by both arms (identical dicts)."""
     return {"workload": f"rmat{scale}_plain", "scale": scale, "edge_factor": EDGE_FACTOR,
@@ -313,9 +420,10 @@ def run_profile_only(args, ranks: Ranks):
     dev = ranks.local
     torch.cuda.set_device(dev)
     dg = lvb.gen_rmat_device(args.scale, EDGE_FACTOR, SEED, device=dev)
-    cs, pst, _ = profiled_run(lvb, dg, dev, args.wide_weights)
+    knobs = {k: v for k, v in (("giant_degree", args.giant_degree), ("warp_limit", args.warp_limit)) if v}
+    cs, pst, _ = profiled_run(lvb, dg, dev, args.wide_weights, knobs)
     dg.free()
-    return {"profile_only": True, "wide_weights": args.wide_weights,
+    return {"profile_only": True, "wide_weights": args.wide_weights, "knobs": knobs,
             "config": rmat_config(args.scale, dg.V, dg.E, ranks.world),
             "phases_ms": {k: round(pst[k], 3) for k in ("move_ms", "modularity_ms", "aggregate_ms", "setup_ms")},
             "classes": class_table_of(cs), "sweeps": pst["sweeps"], "levels": pst["levels"]}
@@ -932,7 +1040,17 @@ def main():
                     help="default workload: skip the learned and batched summaries added to the line")
     ap.add_argument("--wide-weights", action="store_true",
                     help="with --profile-only: 64-bit table sums and weights at every level (lv_opts.wide_weights)")
+    ap.add_argument("--giant-degree", type=int, default=0,
+                    help="with --profile-only: lv_opts.giant_degree (0 = library default)")
+    ap.add_argument("--warp-limit", type=int, default=0,
+                    help="with --profile-only: lv_opts.warp_limit (0 = library default)")
+    ap.add_argument("--ncu-classes", default=None, metavar="CSV",
+                    help="no GPU work: split an ncu CSV of a --profile-only run (time and DRAM "
+                         "bytes per launch) into the engine's kernel classes and print it")
     args = ap.parse_args()
+    if args.ncu_classes:
+        print(json.dumps(ncu_class_split(args.ncu_classes)))
+        return
     if args.impl == "reference":
         ranks = Ranks(backend="gloo")
         line = run_reference_batch(args, ranks) if args.workload == "batch" else run_reference(args, ranks)
