@@ -180,7 +180,7 @@ struct GraphView {
 constexpr uint32_t W32_ESC = 0xFFFFFFFFu;
 
 // Exact weight of entry e of a level's row.
-__device__ __forceinline__ u64 gw(const GraphView<float> &g, int64_t e) { return gw(g, e); }
+__device__ __forceinline__ u64 gw(const GraphView<float> &g, int64_t e) { return wfix(g.w, e, g.scale); }
 __device__ __forceinline__ u64 gw(const GraphView<u64> &g, int64_t e) { return __ldg(g.w + e); }
 __device__ __forceinline__ u64 gw(const GraphView<uint32_t> &g, int64_t e) {
     const uint32_t x = __ldg(g.w + e);
