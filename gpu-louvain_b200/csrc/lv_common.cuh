@@ -35,6 +35,12 @@
 #ifndef LV_U_STAGE
 #define LV_U_STAGE 8
 #endif
+// The narrow-weight warp kernel issues the next chunk's column and weight
+// loads before inserting the current chunk (1), or loads each chunk when it
+// gets to it (0).
+#ifndef LV_WARP_PIPE
+#define LV_WARP_PIPE 1
+#endif
 // The narrow-weight warp kernel loads the home-slot keys of its U entries
 // together before inserting (1) or probes entry by entry (0).
 #ifndef LV_WARP_PREFETCH
@@ -191,6 +197,26 @@ __device__ __forceinline__ u64 gw_row(const GraphView<float> &g, int64_t e) { re
 __device__ __forceinline__ u64 gw_row(const GraphView<u64> &g, int64_t e) { return ld_row(g.w + e); }
 __device__ __forceinline__ u64 gw_row(const GraphView<uint32_t> &g, int64_t e) {
     const uint32_t x = ld_row(g.w + e);
+    return x != W32_ESC ? (u64)x : __ldg(g.w64 + e);
+}
+
+// Row weights as loaded (32 bits for float and the 32-bit view) and their
+// exact value: a chunk's weights can be loaded one step ahead of their use
+// while holding one register each.
+template <typename WT>
+struct RawOf { typedef uint32_t T; };
+template <>
+struct RawOf<u64> { typedef u64 T; };
+__device__ __forceinline__ u64 raw_row(const GraphView<u64> &g, int64_t e) { return ld_row(g.w + e); }
+__device__ __forceinline__ u64 raw_value(const GraphView<u64> &, int64_t, u64 x) { return x; }
+__device__ __forceinline__ uint32_t raw_row(const GraphView<float> &g, int64_t e) {
+    return __float_as_uint(ld_row(g.w + e));
+}
+__device__ __forceinline__ uint32_t raw_row(const GraphView<uint32_t> &g, int64_t e) { return ld_row(g.w + e); }
+__device__ __forceinline__ u64 raw_value(const GraphView<float> &g, int64_t, uint32_t x) {
+    return (u64)__double2ll_rn(__dmul_rn((double)__uint_as_float(x), g.scale));
+}
+__device__ __forceinline__ u64 raw_value(const GraphView<uint32_t> &g, int64_t e, uint32_t x) {
     return x != W32_ESC ? (u64)x : __ldg(g.w64 + e);
 }
 

@@ -46,6 +46,10 @@ void launch_gather_cdeg(const int32_t *mstart, const int32_t *P, const int32_t *
 
 using namespace lv;
 
+#ifndef LV_NARROW_ESCAPES
+#define LV_NARROW_ESCAPES 1
+#endif
+
 namespace {
 
 constexpr int NAC = 5;   // aggregation merge classes (lv_agg.cu)
@@ -1339,7 +1343,9 @@ int aggregate_t(lv_handle *h) {
     h->cur_rowend = h->lvl_end[nb];
     h->cur_col = h->lvl_col[nb];
     h->cur_w = h->lvl_w[nb];
-    h->cur_w32 = h->opts.wide_weights ? nullptr : h->lvl_w32[nb];
+    // LV_NARROW_ESCAPES = 0: a level with escaped sums is swept with the
+    // 64-bit kernels throughout instead of the 32-bit view
+    h->cur_w32 = (h->opts.wide_weights || (!LV_NARROW_ESCAPES && h->wrows_any)) ? nullptr : h->lvl_w32[nb];
     h->V = newV;
     h->E = newE;
     h->level += 1;

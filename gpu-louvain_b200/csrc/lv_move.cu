@@ -120,20 +120,24 @@ __global__ void __launch_bounds__(256) move_group_narrow_kernel(GraphView<WT> g,
     for (int s = lane; s < CAP; s += G) { t.keys[s] = -1; t.lo[s] = 0; t.hi[s] = 0; }
     __syncwarp();
     bool active = idx < n;
-    int32_t v = 0, own = 0;
+    int32_t v = 0, own = 0, r0 = 0, r1 = 0;
     u64 e_own = 0;
-    if (active && st.wrow && st.wrow[list[idx]]) {
-        // a row with a sum of 2^32 or more: decided by the large queue
-        if (lane == 0) enqueue_large(fbl, list[idx], g.rowend[list[idx]] - g.rowptr[list[idx]], st.err);
-        active = false;
-    }
     if (active) {
+        // the row bounds, the community and the wide-row flag are loaded
+        // together (none depends on another)
         v = list[idx];
+        r0 = g.rowptr[v];
+        r1 = g.rowend[v];
         own = __ldg(st.comm + v);
-        insert_row_piece<(CAP > 32 ? LV_U_CTA : LV_U_GROUP), false>(g, st.comm, v, own, g.rowptr[v], g.rowend[v],
-                                                                     lane, G, t, LG, st.err, nullptr, nullptr, 0,
-                                                                     e_own);
+        if (st.wrow && st.wrow[v]) {
+            // a row with a sum of 2^32 or more: decided by the large queue
+            if (lane == 0) enqueue_large(fbl, v, r1 - r0, st.err);
+            active = false;
+        }
     }
+    if (active)
+        insert_row_piece<(CAP > 32 ? LV_U_CTA : LV_U_GROUP), false>(g, st.comm, v, own, r0, r1, lane, G, t, LG,
+                                                                     st.err, nullptr, nullptr, 0, e_own);
     __syncwarp();
     const MoveCtx m = move_ctx(own, active ? __ldg(st.size + own) == 1 : false, st.T,
                                active ? __ldg(st.k + v) : 0, active ? __ldg(st.S + own) : 0);
@@ -393,14 +397,17 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
     if (lane == 0) idx = atomicAdd(fs.warp_next, 1);
     idx = __shfl_sync(FULL, idx, 0);
     int32_t nv = 0, nr0 = 0, nr1 = 0, nown = 0;
+    bool nwide = false;
     if (idx < n) {
         nv = list[idx];
         nr0 = g.rowptr[nv];
         nr1 = g.rowend[nv];
         nown = __ldg(st.comm + nv);
+        nwide = st.wrow && st.wrow[nv];
     }
     while (idx < n) {
         const int32_t v = nv, r0 = nr0, r1 = nr1, own = nown;
+        const bool wide = nwide;
         int32_t nidx = 0;
         if (lane == 0) nidx = atomicAdd(fs.warp_next, 1);
         nidx = __shfl_sync(FULL, nidx, 0);
@@ -409,10 +416,11 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
             nr0 = g.rowptr[nv];
             nr1 = g.rowend[nv];
             nown = __ldg(st.comm + nv);
+            nwide = st.wrow && st.wrow[nv];
         }
         idx = nidx;
         const int32_t d = r1 - r0;
-        if (st.wrow && st.wrow[v]) {   // a sum of 2^32 or more: 64-bit sums in the large queue
+        if (wide) {   // a sum of 2^32 or more: 64-bit sums in the large queue
             if (lane == 0) enqueue_large(fs.q[NFBQ], v, d, st.err);
             continue;
         }
@@ -429,9 +437,26 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
         // U chunks of 32 edges per step; the claim count is read after every
         // step, so at most WARP_LIMIT + 32 U slots are ever claimed
         constexpr int U = LV_U_WARP;
+#if LV_WARP_PIPE
+        // the step's column and raw weight loads were issued one step ahead
+        int32_t jn[U];
+        typename RawOf<WT>::T xn[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int32_t e = r0 + lane + 32 * u;
+            jn[u] = -1;
+            xn[u] = 0;
+            if (e < r1) { jn[u] = ld_row(g.col + e); xn[u] = raw_row(g, e); }
+        }
+#endif
         for (int32_t b0 = r0 + lane; b0 < r1 + lane; b0 += 32 * U) {
             int32_t jj[U];
             u64 ww[U];
+#if LV_WARP_PIPE
+            typename RawOf<WT>::T xx[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) { jj[u] = jn[u]; xx[u] = xn[u]; }
+#else
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int32_t e = b0 + 32 * u;
@@ -439,9 +464,22 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
                 ww[u] = 0;
                 if (e < r1) { jj[u] = ld_row(g.col + e); ww[u] = gw_row(g, e); }
             }
+#endif
             int32_t cc[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(st.comm + jj[u]) : -1;
+#if LV_WARP_PIPE
+            // the next step's loads go out before this step's inserts
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int32_t e = b0 + 32 * (U + u);
+                jn[u] = -1;
+                xn[u] = 0;
+                if (e < r1) { jn[u] = ld_row(g.col + e); xn[u] = raw_row(g, e); }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) ww[u] = jj[u] >= 0 ? raw_value(g, b0 + 32 * u, xx[u]) : 0;
+#endif
 #if LV_WARP_PREFETCH
             // the U first-probe slots and their keys are loaded together; a
             // key already in its home slot (the common case once a row's few
