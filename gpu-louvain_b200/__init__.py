@@ -572,12 +572,21 @@ class Louvain:
         self._c(lib().lv_set_active_model(self._h, _ptr(m, C.c_uint16), len(m), logit_threshold))
 
     def traces(self):
-        """(features [n, ACTIVE_FEATURES] float32, labels [n] uint8) recorded with trace_sample > 0."""
+        """(features [n, ACTIVE_FEATURES] float32, labels [n] uint8) recorded with trace_sample > 0.
+
+        The device appends the sampled rows in whatever order its threads get
+        to them; the rows are returned sorted (by label, then feature bits),
+        so that the same run gives the same arrays and a model trained on
+        them is reproducible across processes."""
         n = C.c_int64()
         self._c(lib().lv_get_traces(self._h, None, None, 0, C.byref(n)))
         x = np.empty((n.value, ACTIVE_FEATURES), np.float32)
         y = np.empty(n.value, np.uint8)
         self._c(lib().lv_get_traces(self._h, _ptr(x, C.c_float), _ptr(y, C.c_uint8), n.value, C.byref(n)))
+        if len(y) > 1:
+            bits = x.view(np.uint32)
+            order = np.lexsort(tuple(bits[:, j] for j in range(ACTIVE_FEATURES - 1, -1, -1)) + (y,))
+            x, y = np.ascontiguousarray(x[order]), np.ascontiguousarray(y[order])
         return x, y
 
     def active_stats(self) -> dict:

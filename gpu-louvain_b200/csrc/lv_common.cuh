@@ -39,7 +39,7 @@
 // loads before inserting the current chunk (1), or loads each chunk when it
 // gets to it (0).
 #ifndef LV_WARP_PIPE
-#define LV_WARP_PIPE 1
+#define LV_WARP_PIPE 0
 #endif
 // The narrow-weight warp kernel loads the home-slot keys of its U entries
 // together before inserting (1) or probes entry by entry (0).
@@ -231,6 +231,8 @@ struct StateView {
     float *feat;   // learned active set: 2 features per vertex, written when set
     const uint8_t *wrow;   // rows with a weight of 2^32 or more (nullptr: none); such a
                            // vertex is decided by the large fallback queue (64-bit sums)
+    int dedup;             // aggregated level: the narrow insert loops combine a warp's
+                           // equal keys before their shared atomics (key_peers)
 };
 
 // Exact 64-bit add to a table value.  In shared memory a 64-bit atomicAdd
@@ -343,6 +345,62 @@ __device__ __forceinline__ int32_t piece_insert(const PieceTable &t, int lg, int
     return piece_insert_at(t, lg, hash_slot(key, lg), key, w, err);
 }
 
+// Warp-level combining of equal keys before the shared atomics.  On
+// aggregated levels a row's entries fall into a few communities, so many
+// lanes of a warp add to the same slot and their atomics serialise.
+// key_peers gives the lanes of the warp holding the same valid key (an
+// invalid lane groups alone); the group's weights are summed piecewise with
+// redux.sync (a group has at most 32 lanes, so each 16-bit-piece sum stays
+// below 2^21), and only the group's lowest lane touches the table.  All 32
+// lanes must call these together.
+__device__ __forceinline__ unsigned key_peers(int32_t key, bool valid) {
+    return __match_any_sync(FULL, valid ? key : (int32_t)(0x80000000u | (threadIdx.x & 31u)));
+}
+struct Pieces {
+    uint32_t lo, hi;   // sum of (w & 0xFFFF) and of (w >> 16) over the group
+};
+__device__ __forceinline__ Pieces group_pieces(unsigned peers, u64 w) {
+    Pieces p;
+    p.lo = __reduce_add_sync(peers, (uint32_t)w & 0xFFFFu);
+    p.hi = __reduce_add_sync(peers, (uint32_t)(w >> 16));
+    return p;
+}
+// Exact uint64 sum over the group: four 16-bit-piece sums (each below 2^21)
+// recombined modulo 2^64, which is the exact sum while that stays below 2^64
+// (as every weight sum of a level does).
+__device__ __forceinline__ u64 group_sum_u64(unsigned peers, u64 w) {
+    const u64 p0 = __reduce_add_sync(peers, (uint32_t)w & 0xFFFFu);
+    const u64 p1 = __reduce_add_sync(peers, (uint32_t)(w >> 16) & 0xFFFFu);
+    const u64 p2 = __reduce_add_sync(peers, (uint32_t)(w >> 32) & 0xFFFFu);
+    const u64 p3 = __reduce_add_sync(peers, (uint32_t)(w >> 48));
+    return p0 + (p1 << 16) + (p2 << 32) + (p3 << 48);
+}
+__device__ __forceinline__ bool group_leader(unsigned peers) {
+    return (threadIdx.x & 31u) == (unsigned)(__ffs(peers) - 1);
+}
+__device__ __forceinline__ void piece_add_p(const PieceTable &t, uint32_t s, Pieces p) {
+    atomicAdd(t.lo + s, p.lo);
+    atomicAdd(t.hi + s, p.hi);
+}
+// piece_insert_at for a group's combined pieces (the group counts as one
+// add per member towards PIECE_MAX_ADDS, as before combining).
+__device__ __forceinline__ int32_t piece_insert_at_p(const PieceTable &t, int lg, uint32_t s, int32_t key, Pieces p,
+                                                     int *err) {
+    const uint32_t mask = (1u << lg) - 1u;
+    for (uint32_t q = 0; q <= mask; ++q) {
+        const int32_t k = ((volatile int32_t *)t.keys)[s];
+        if (k == key) { piece_add_p(t, s, p); return -1; }
+        if (k < 0) {
+            const int32_t prev = atomicCAS(t.keys + s, -1, key);
+            if (prev < 0) { piece_add_p(t, s, p); return (int32_t)s; }
+            if (prev == key) { piece_add_p(t, s, p); return -1; }
+        }
+        s = (s + 1u) & mask;
+    }
+    atomicOr(err, DEVERR_HASH_FULL);
+    return -1;
+}
+
 // Append the slots claimed by this warp's lanes (claimed >= 0) to occ[],
 // reserving space with one atomic per warp.  All 32 lanes must call it.
 __device__ __forceinline__ void warp_append(int32_t claimed, int32_t *occ, int32_t *nocc) {
@@ -428,8 +486,12 @@ template <int U, bool OCC, typename WT>
 __device__ __forceinline__ void insert_row(const GraphView<WT> &g, const int32_t *__restrict__ comm,
                                            int32_t v, int32_t own, int32_t r0, int32_t r1, int lane,
                                            int stride, int32_t *keys, u64 *vals, int lg, int *err,
-                                           int32_t *occ, int32_t *nocc, u64 &e_own) {
-    for (int32_t base = r0 + lane; base < r1; base += U * stride) {
+                                           int32_t *occ, int32_t *nocc, u64 &e_own, bool dedup = false) {
+    // dedup (CTA-wide OCC callers only: lane = threadIdx.x, stride a multiple
+    // of 32): the loop then runs the same steps in every lane of a warp and a
+    // warp's equal keys are combined before the atomics (key_peers)
+    const int32_t wlane = (OCC && dedup) ? (lane & 31) : 0;
+    for (int32_t base = r0 + lane; base - wlane < r1; base += U * stride) {
         int32_t jj[U];
         u64 ww[U];
 #pragma unroll
@@ -447,6 +509,14 @@ __device__ __forceinline__ void insert_row(const GraphView<WT> &g, const int32_t
         for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(comm + jj[u]) : -1;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
+            if (OCC && dedup) {
+                const bool valid = cc[u] >= 0 && cc[u] != own;
+                if (cc[u] >= 0 && cc[u] == own) e_own += ww[u];
+                const unsigned peers = key_peers(cc[u], valid);
+                const u64 ws = group_sum_u64(peers, valid ? ww[u] : 0);
+                if (valid && group_leader(peers)) table_insert_occ(keys, vals, lg, cc[u], ws, err, occ, nocc);
+                continue;
+            }
             if (cc[u] < 0) continue;
             if (cc[u] == own) {
                 e_own += ww[u];
@@ -466,7 +536,8 @@ template <int U, bool OCC, typename WT>
 __device__ __forceinline__ void insert_row_piece(const GraphView<WT> &g, const int32_t *__restrict__ comm,
                                                  int32_t v, int32_t own, int32_t r0, int32_t r1, int lane,
                                                  int stride, const PieceTable &t, int lg, int *err,
-                                                 int32_t *occ, int32_t *nocc, int32_t occ_cap, u64 &e_own) {
+                                                 int32_t *occ, int32_t *nocc, int32_t occ_cap, u64 &e_own,
+                                                 bool dedup = false) {
     // OCC (CTA-wide callers: lane = threadIdx.x, stride a multiple of 32):
     // the loop runs the same number of steps in every lane of a warp, so the
     // claims of a step are listed with one shared atomic per warp
@@ -490,7 +561,15 @@ __device__ __forceinline__ void insert_row_piece(const GraphView<WT> &g, const i
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             int32_t claimed = -1;
-            if (cc[u] >= 0) {
+            if (OCC && dedup) {
+                // equal keys of the warp combined first (see key_peers)
+                const bool valid = cc[u] >= 0 && cc[u] != own;
+                if (cc[u] >= 0 && cc[u] == own) e_own += ww[u];
+                const unsigned peers = key_peers(cc[u], valid);
+                const Pieces pc = group_pieces(peers, valid ? ww[u] : 0);
+                if (valid && group_leader(peers))
+                    claimed = piece_insert_at_p(t, lg, hash_slot(cc[u], lg), cc[u], pc, err);
+            } else if (cc[u] >= 0) {
                 if (cc[u] == own) e_own += ww[u];
                 else claimed = piece_insert(t, lg, cc[u], ww[u], err);
             }

@@ -49,6 +49,10 @@ using namespace lv;
 #ifndef LV_NARROW_ESCAPES
 #define LV_NARROW_ESCAPES 1
 #endif
+// the insert loops combine a warp's equal keys: 1 on aggregated levels, 2 at every level, 0 never
+#ifndef LV_DEDUP
+#define LV_DEDUP 1
+#endif
 
 namespace {
 
@@ -489,7 +493,8 @@ bool narrow_weights(const lv_handle *h) {
 
 StateView state_of(lv_handle *h) {
     return StateView{h->comm, h->newc, h->size, h->k, h->S, h->T, &h->tot_d->err, h->feat,
-                     h->cur_w32 && h->wrows_any ? h->wrow : nullptr};
+                     h->cur_w32 && h->wrows_any ? h->wrow : nullptr,
+                     (LV_DEDUP == 2 || (LV_DEDUP && h->level > 0)) ? 1 : 0};
 }
 
 // ---------------------------------------------------------------------------

@@ -324,7 +324,14 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 int32_t claimed = -1;
-                if (cc[u] >= 0) {
+                if (st.dedup) {
+                    // equal keys of the warp combined before the atomics
+                    const bool valid = cc[u] >= 0 && cc[u] != own;
+                    if (cc[u] >= 0 && cc[u] == own) e_own += ww[u];
+                    const unsigned peers = key_peers(cc[u], valid);
+                    const u64 ws = group_sum_u64(peers, valid ? ww[u] : 0);
+                    if (valid && group_leader(peers)) claimed = table_insert_claim(keys, vals, lg, cc[u], ws, st.err);
+                } else if (cc[u] >= 0) {
                     if (cc[u] == own) e_own += ww[u];
                     else claimed = table_insert_claim(keys, vals, lg, cc[u], ww[u], st.err);
                 }
@@ -491,16 +498,33 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
                 hs[u] = cc[u] >= 0 ? hash_slot(cc[u], lg) : 0u;
                 kk[u] = (cc[u] >= 0 && cc[u] != own) ? ((volatile int32_t *)t.keys)[hs[u]] : -2;
             }
+            if (st.dedup) {
+                // equal keys of the warp combined before the atomics
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                int32_t claimed = -1;
-                if (cc[u] >= 0) {
-                    if (cc[u] == own) e_own += ww[u];
-                    else if (kk[u] == cc[u]) piece_add(t, hs[u], ww[u]);
-                    else claimed = piece_insert_at(t, lg, hs[u], cc[u], ww[u], st.err);
+                for (int u = 0; u < U; ++u) {
+                    int32_t claimed = -1;
+                    const bool valid = cc[u] >= 0 && cc[u] != own;
+                    if (cc[u] >= 0 && cc[u] == own) e_own += ww[u];
+                    const unsigned peers = key_peers(cc[u], valid);
+                    const Pieces pc = group_pieces(peers, valid ? ww[u] : 0);
+                    if (valid && group_leader(peers)) {
+                        if (kk[u] == cc[u]) piece_add_p(t, hs[u], pc);
+                        else claimed = piece_insert_at_p(t, lg, hs[u], cc[u], pc, st.err);
+                    }
+                    warp_append_capped(claimed, occ, nocc, WARP_OCC_CAP);
                 }
-                // one shared atomic per warp for the claims of this step
-                warp_append_capped(claimed, occ, nocc, WARP_OCC_CAP);
+            } else {
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    int32_t claimed = -1;
+                    if (cc[u] >= 0) {
+                        if (cc[u] == own) e_own += ww[u];
+                        else if (kk[u] == cc[u]) piece_add(t, hs[u], ww[u]);
+                        else claimed = piece_insert_at(t, lg, hs[u], cc[u], ww[u], st.err);
+                    }
+                    // one shared atomic per warp for the claims of this step
+                    warp_append_capped(claimed, occ, nocc, WARP_OCC_CAP);
+                }
             }
 #else
 #pragma unroll
@@ -599,7 +623,28 @@ __global__ void __launch_bounds__(THREADS) move_fallback_kernel(GraphView<WT> g,
             lg = lg < 3 ? 3 : lg;
             if (!PART) {
                 insert_row<LV_U_FB, true>(g, st.comm, v, own, r0, r1, threadIdx.x, THREADS, keys, vals,
-                                          lg, st.err, occ, &nocc, e_own);
+                                          lg, st.err, occ, &nocc, e_own, st.dedup != 0);
+            } else if (st.dedup) {
+                // warp-uniform steps; a warp's equal keys combined first
+                const int lane = threadIdx.x & 31;
+                for (int32_t b = r0 + threadIdx.x - lane; b < r1; b += THREADS) {
+                    const int32_t e = b + lane;
+                    int32_t c = -1;
+                    u64 w = 0;
+                    if (e < r1) {
+                        const int32_t j = __ldg(g.col + e);
+                        if (j != v) {
+                            c = __ldg(st.comm + j);
+                            w = gw(g, e);
+                        }
+                    }
+                    if (c >= 0 && c == own && p == 0) e_own += w;
+                    const bool valid = c >= 0 && c != own && (P == 1 || (int32_t)part_of(c, P) == p);
+                    const unsigned peers = key_peers(c, valid);
+                    const u64 ws = group_sum_u64(peers, valid ? w : 0);
+                    if (valid && group_leader(peers))
+                        table_insert_occ_capped(keys, vals, lg, c, ws, st.err, occ, &nocc, OCC_CAP);
+                }
             } else {
                 for (int32_t e = r0 + threadIdx.x; e < r1; e += THREADS) {
                     const int32_t j = __ldg(g.col + e);
@@ -717,7 +762,7 @@ __global__ void __launch_bounds__(THREADS) move_rowq_narrow_kernel(GraphView<WT>
         lg = lg < 3 ? 3 : lg;
         u64 e_own = 0;
         insert_row_piece<LV_U_FB, true>(g, st.comm, v, own, r0, r1, threadIdx.x, THREADS, t, lg, st.err, occ,
-                                        &nocc, OCC_CAP, e_own);
+                                        &nocc, OCC_CAP, e_own, st.dedup != 0);
         __syncthreads();
         const int32_t nd = min(nocc, OCC_CAP);
         const MoveCtx m = move_ctx(own, __ldg(st.size + own) == 1, st.T, __ldg(st.k + v), __ldg(st.S + own));
@@ -792,7 +837,7 @@ __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_narrow_kernel(Graph
         const int32_t own = __ldg(st.comm + v);
         u64 e_own = 0;
         insert_row_piece<LV_U_STAGE, true>(g, st.comm, v, own, e0, e1, threadIdx.x, STAGE_THREADS, t, LLG, st.err,
-                                           locc, &lnocc, STAGE_CHUNK, e_own);
+                                           locc, &lnocc, STAGE_CHUNK, e_own, st.dedup != 0);
         block_add_total<STAGE_THREADS>(e_own, hg.eown + h);   // contains the barrier
         const int32_t n = min(lnocc, STAGE_CHUNK);
         if (threadIdx.x == 0) base = atomicAdd(hg.nocc + h, n);
@@ -837,7 +882,7 @@ __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_kernel(GraphView<WT
     const int32_t own = __ldg(st.comm + v);
     u64 e_own = 0;
     insert_row<LV_U_STAGE, true>(g, st.comm, v, own, e0, e1, threadIdx.x, STAGE_THREADS, lkeys, lvals, LLG,
-                                 st.err, locc, &lnocc, e_own);
+                                 st.err, locc, &lnocc, e_own, st.dedup != 0);
     block_add_total<STAGE_THREADS>(e_own, hg.eown + h);   // contains the barrier
     const int32_t n = lnocc;
     if (threadIdx.x == 0) base = atomicAdd(hg.nocc + h, n);
