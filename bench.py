@@ -798,10 +798,15 @@ def batch_summary(args, ranks: Ranks):
     slowest = [{"graph": int(i), "V": int(vcount[i]), "E_csr": int(ecount[i]), "levels": int(gs["levels"][i]),
                 "sweeps": int(gs["sweeps"][i]), "ms": round(float(gs["latency_ms"][i]), 2)} for i in slow]
     lat = np.concatenate(lat)
+    # the launch against its load: the summed per-graph latencies spread over
+    # the CTAs (the launch time with perfect balancing) and the longest graph
+    ctas = int(st.get("ctas", 0) or 0)
+    busy = float(lat.sum()) / 2 / ctas if ctas else None
     return {"workload": f"batch{G}_planted", "graphs_per_s": 2 * G / (dev_ms * 1e-3),
             "ms_per_launch": dev_ms / 2, "edge_sweeps_per_s": es / (dev_ms * 1e-3),
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "max": float(lat.max())},
+            "ctas": ctas, "balanced_ms_per_launch": busy,
             "all_ok": ok, "V_total": len(rp) - 1, "E_csr_total": len(cl), "generation_s": round(t_gen, 1),
             "slowest": slowest,
             "note": "lv_batch_run, one persistent launch per run, device time (1 warm-up + 2 timed runs); "

@@ -176,6 +176,7 @@ struct GraphView {
     double scale;     // 2^scale (used for float weights only)
     const u64 *w64;   // 32-bit view of an aggregated level: the uint64 sums, read
                       // where the 32-bit copy holds W32_ESC
+    int64_t nent;     // entries allocated in col / w (bulk copies stay below it)
 };
 
 // The 32-bit copy of an aggregated level holds each sum below W32_ESC as it
@@ -219,6 +220,53 @@ __device__ __forceinline__ u64 raw_value(const GraphView<float> &g, int64_t, uin
 __device__ __forceinline__ u64 raw_value(const GraphView<uint32_t> &g, int64_t e, uint32_t x) {
     return x != W32_ESC ? (u64)x : __ldg(g.w64 + e);
 }
+
+// ---------------------------------------------------------------------------
+// 1-D bulk copies (TMA, no tensor map) into shared memory, completed on an
+// mbarrier.  Addresses and sizes are multiples of 16 bytes; a CTA launched
+// without a cluster is its own cluster of one, so its shared::cta addresses
+// are valid shared::cluster destinations.  Waits are bounded: a wait that runs
+// out reports false and the caller records a device error.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// one arrival that also announces `bytes` of transfers still to complete
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// generic-proxy accesses of shared memory ordered before later bulk copies
+// into it
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_wait_parity(uint64_t *bar, uint32_t parity, uint32_t max_polls) {
+    const uint32_t a = smem_u32(bar);
+    for (uint32_t i = 0; i < max_polls; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+constexpr uint32_t MBAR_MAX_POLLS = 1u << 22;   // each try_wait may itself suspend for a while
 
 struct StateView {
     int32_t *comm;

@@ -457,15 +457,16 @@ template <typename WT>
 GraphView<WT> view_of(lv_handle *h);
 template <>
 GraphView<float> view_of<float>(lv_handle *h) {
-    return GraphView<float>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->in_w, h->scale_d, nullptr};
+    return GraphView<float>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->in_w, h->scale_d, nullptr, h->E0};
 }
 template <>
 GraphView<u64> view_of<u64>(lv_handle *h) {
-    return GraphView<u64>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->cur_w, h->scale_d, nullptr};
+    return GraphView<u64>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->cur_w, h->scale_d, nullptr, h->E0};
 }
 template <>
 GraphView<uint32_t> view_of<uint32_t>(lv_handle *h) {
-    return GraphView<uint32_t>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->cur_w32, h->scale_d, h->cur_w};
+    return GraphView<uint32_t>{h->cur_rowptr, h->cur_rowend, h->cur_col, h->cur_w32, h->scale_d, h->cur_w,
+                               h->E0};
 }
 
 // Calls F<WT>(args...) with the weight type the move phase reads at the

@@ -143,6 +143,7 @@ struct DeviceInfo {
     int occ_warp_narrow = 4;   // ... of its narrow-weight form
     int occ_fbq[NFBQ] = {1, 1, 1, 1};   // ... of the row fallback kernels
     int occ_fbq_narrow[NFBQ] = {1, 1, 1, 1};   // ... and of their narrow-weight form
+    int occ_fbq_staged[NFBQ] = {1, 1, 1, 1};   // ... and of its bulk-copy row-staging form
     int occ_merge_s = 1;                 // ... of the small giant-merge kernel
     int occ_stage_narrow = 1;            // ... of the persistent narrow staging kernel
 };

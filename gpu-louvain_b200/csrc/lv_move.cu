@@ -794,6 +794,181 @@ __global__ void __launch_bounds__(THREADS) move_rowq_narrow_kernel(GraphView<WT>
     if (threadIdx.x == 0 && delta_acc) atomicAdd(dE, delta_acc);
 }
 
+// move_rowq_narrow_kernel with the rows staged in shared memory by 1-D bulk
+// copies (TMA): while the CTA decides one row, the next item's columns and
+// weights are already on their way into the other of two staging buffers, so
+// the insert loop reads them from shared memory and only the community
+// gathers go to global memory.  A bulk copy covers the row rounded out to
+// 16-byte boundaries (entries [r0 & ~3, (r1 + 3) & ~3)), clipped to the last
+// whole 16 bytes of the arrays; entries past the clip are read from global
+// memory.  The host uses this form only for 4-byte weights whose column and
+// weight arrays start on 16-byte boundaries.
+template <int THREADS, int CAP>
+struct RowqStage {
+    static constexpr int SB = CAP / 2 + 4;   // staged entries per buffer (row + alignment)
+    static constexpr int TABLE = CAP * 12 + (CAP / 2) * 4;
+    static constexpr int BYTES = TABLE + 2 * SB * 8 + 2 * 8 + 8 * 4;
+};
+
+template <typename WT, int THREADS, int CAP>
+__global__ void __launch_bounds__(THREADS) move_rowq_staged_kernel(GraphView<WT> g, StateView st, Fallback fb,
+                                                                   uint8_t *hint, int32_t hint_set, u64 *dE) {
+    static_assert(sizeof(WT) == 4, "staged rows hold 4-byte weights");
+    constexpr int OCC_CAP = CAP / 2;
+    constexpr int SB = RowqStage<THREADS, CAP>::SB;
+    constexpr int U = LV_U_FB;
+    static_assert(OCC_CAP <= PIECE_MAX_ADDS, "rows of the queue fit the piece counters");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PieceTable t;
+    t.lo = reinterpret_cast<uint32_t *>(smem_raw);
+    t.hi = t.lo + CAP;
+    t.keys = reinterpret_cast<int32_t *>(t.hi + CAP);
+    int32_t *occ = t.keys + CAP;
+    int32_t *scol = reinterpret_cast<int32_t *>(smem_raw + RowqStage<THREADS, CAP>::TABLE);   // [2][SB]
+    uint32_t *sw = reinterpret_cast<uint32_t *>(scol + 2 * SB);                               // [2][SB]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sw + 2 * SB);                                // [2]
+    int32_t *info = reinterpret_cast<int32_t *>(bar + 2);   // [2][4]: item, r0, r1, staged count
+    __shared__ int32_t nocc;
+    __shared__ int timed_out;
+    for (int s = threadIdx.x; s < CAP; s += THREADS) { t.keys[s] = -1; t.lo[s] = 0; t.hi[s] = 0; }
+    const int32_t count = min(*fb.count, fb.cap);
+    const int64_t clip = g.nent & ~(int64_t)3;   // bulk copies end at or before this entry
+    // thread 0 takes the next item and starts its row's bulk copy into buffer b
+    auto fetch = [&](int b) {
+        const int32_t item = atomicAdd(fb.next, 1);
+        int32_t r0 = 0, r1 = 0, nst = 0;
+        if (item < count) {
+            const int32_t v = fb.v[item];
+            r0 = g.rowptr[v];
+            r1 = g.rowend[v];
+            const int64_t a0 = (int64_t)(r0 & ~3);
+            int64_t a1 = ((int64_t)r1 + 3) & ~(int64_t)3;
+            if (a1 > clip) a1 = clip;
+            nst = a1 > a0 ? (int32_t)(a1 - a0) : 0;
+            if (nst > SB) nst = 0;   // cannot happen for rows of this queue; read them from global memory
+            fence_proxy_async_smem();
+            mbar_arrive_expect(bar + b, (uint32_t)nst * 8u);
+            if (nst > 0) {
+                bulk_g2s(scol + b * SB, g.col + a0, (uint32_t)nst * 4u, bar + b);
+                bulk_g2s(sw + b * SB, g.w + a0, (uint32_t)nst * 4u, bar + b);
+            }
+        }
+        info[4 * b] = item;
+        info[4 * b + 1] = r0;
+        info[4 * b + 2] = r1;
+        info[4 * b + 3] = nst;
+    };
+    if (threadIdx.x == 0) {
+        nocc = 0;
+        timed_out = 0;
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) fetch(0);
+    __syncthreads();
+    u64 delta_acc = 0;
+    uint32_t phase = 0;   // bit b: parity of buffer b's next completion
+    int b = 0;
+    for (;;) {
+        const int32_t item = info[4 * b];
+        if (item >= count) break;
+        const int32_t r0 = info[4 * b + 1], r1 = info[4 * b + 2], nst = info[4 * b + 3];
+        // the next item's copy goes out before this row is waited for
+        if (threadIdx.x == 0) fetch(b ^ 1);
+        if (!mbar_wait_parity(bar + b, (phase >> b) & 1u, MBAR_MAX_POLLS)) timed_out = 1;
+        __syncthreads();
+        if (timed_out) break;
+        phase ^= 1u << b;
+        const int32_t v = fb.v[item];
+        const int32_t own = __ldg(st.comm + v);
+        const int32_t a0 = r0 & ~3;                        // staged entry i is entry a0 + i
+        const int32_t *rc = scol + b * SB;
+        const uint32_t *rw = sw + b * SB;
+        const int32_t send = a0 + nst;                     // first entry not staged
+        int lg = ceil_log2_i(2 * (int64_t)(r1 - r0));
+        lg = lg < 3 ? 3 : lg;
+        u64 e_own = 0;
+        const int lane = threadIdx.x & 31;
+        for (int32_t base = r0 + threadIdx.x; base - lane < r1; base += U * THREADS) {
+            int32_t jj[U];
+            uint32_t xx[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int32_t e = base + u * THREADS;
+                jj[u] = -1;
+                xx[u] = 0;
+                if (e < r1) {
+                    if (e < send) { jj[u] = rc[e - a0]; xx[u] = rw[e - a0]; }
+                    else { jj[u] = __ldg(g.col + e); xx[u] = raw_row(g, e); }
+                }
+            }
+            int32_t cc[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(st.comm + jj[u]) : -1;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const u64 w = cc[u] >= 0 ? raw_value(g, base + u * THREADS, xx[u]) : 0;
+                int32_t claimed = -1;
+                if (st.dedup) {
+                    const bool valid = cc[u] >= 0 && cc[u] != own;
+                    if (cc[u] >= 0 && cc[u] == own) e_own += w;
+                    const unsigned peers = key_peers(cc[u], valid);
+                    const Pieces pc = group_pieces(peers, valid ? w : 0);
+                    if (valid && group_leader(peers))
+                        claimed = piece_insert_at_p(t, lg, hash_slot(cc[u], lg), cc[u], pc, st.err);
+                } else if (cc[u] >= 0) {
+                    if (cc[u] == own) e_own += w;
+                    else claimed = piece_insert(t, lg, cc[u], w, st.err);
+                }
+                warp_append_capped(claimed, occ, &nocc, OCC_CAP);
+            }
+        }
+        __syncthreads();
+        const int32_t nd = min(nocc, OCC_CAP);
+        const MoveCtx m = move_ctx(own, __ldg(st.size + own) == 1, st.T, __ldg(st.k + v), __ldg(st.S + own));
+        Best bb = best_init(own);
+        bb.eo = e_own;
+        for (int32_t i = threadIdx.x; i < nd; i += THREADS) {
+            const int32_t sl = occ[i];
+            const int32_t c = t.keys[sl];
+            const u64 ec = piece_value(t, (uint32_t)sl);
+            t.keys[sl] = -1;
+            t.lo[sl] = 0;
+            t.hi[sl] = 0;
+            const bool cand = c != own;
+            const u64 Sc = cand ? __ldg(st.S + c) : 0;
+            const int32_t szc = (cand && guard_needs_size(m, c)) ? __ldg(st.size + c) : 0;
+            eval_loaded(c, ec, Sc, szc, m, bb);
+        }
+        cta_reduce_best<THREADS>(m, bb);
+        if (threadIdx.x == 0) {
+            nocc = 0;
+            u64 delta = 0;
+            st.newc[v] = move_decision(m, bb, &delta);
+            record_features(st, v, m, bb);
+            delta_acc += delta;
+            hint[v] = nd > hint_set ? 1 : 0;
+        }
+        __syncthreads();
+        b ^= 1;
+    }
+    if (timed_out) {
+        // a copy that did not complete in time: report it, and give the
+        // copies still in flight (buffer b's and, when the next item was
+        // valid, the other buffer's) a bounded time to land before the CTA's
+        // shared memory is released
+        if (threadIdx.x == 0) {
+            atomicOr(st.err, DEVERR_BAD_STATE);
+            mbar_wait_parity(bar + b, (phase >> b) & 1u, MBAR_MAX_POLLS);
+            if (info[4 * (b ^ 1)] < count) mbar_wait_parity(bar + (b ^ 1), (phase >> (b ^ 1)) & 1u, MBAR_MAX_POLLS);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && delta_acc) atomicAdd(dE, delta_acc);
+}
+
 // ------------------------------------------------------------------------
 // giants (degree > 8192): staged two-level reduction
 // ------------------------------------------------------------------------
@@ -1171,6 +1346,12 @@ inline unsigned nblocks(int64_t items, int per_block) {
 
 __host__ __device__ constexpr int FBQ_SMEM(int b) { return 2 * FBQ_MAXDEG(b) * 14; }
 
+// Rows of the narrow row queues staged by bulk copies (1) or read with
+// plain loads (0).
+#ifndef LV_ROWQ_STAGE
+#define LV_ROWQ_STAGE 1
+#endif
+
 template <typename WT, int B>
 static void set_row_queue_attrs(DeviceInfo &di) {
     constexpr int T = FBQ_THREADS(B), CAP = 2 * FBQ_MAXDEG(B), SM = FBQ_SMEM(B);
@@ -1182,12 +1363,29 @@ static void set_row_queue_attrs(DeviceInfo &di) {
     o = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_rowq_narrow_kernel<WT, T, CAP>, T, SM);
     di.occ_fbq_narrow[B] = o > 0 ? o : 1;
+    if constexpr (sizeof(WT) == 4) {
+        constexpr int SS = RowqStage<T, CAP>::BYTES;
+        cudaFuncSetAttribute(move_rowq_staged_kernel<WT, T, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, SS);
+        o = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_rowq_staged_kernel<WT, T, CAP>, T, SS);
+        di.occ_fbq_staged[B] = o > 0 ? o : 1;
+    }
 }
 
 template <typename WT, int B>
 static void launch_row_queue(const GraphView<WT> &g, const StateView &st, const FallbackSet &fs,
                              const DeviceInfo &di, u64 *dE, cudaStream_t s, bool narrow) {
     constexpr int T = FBQ_THREADS(B), CAP = 2 * FBQ_MAXDEG(B), SM = FBQ_SMEM(B);
+    if constexpr (sizeof(WT) == 4) {
+        // bulk copies need 16-byte aligned arrays
+        const bool aligned = (((uintptr_t)g.col | (uintptr_t)g.w) & 15u) == 0;
+        if (LV_ROWQ_STAGE && narrow && aligned) {
+            move_rowq_staged_kernel<WT, T, CAP><<<di.sms * di.occ_fbq_staged[B], T, RowqStage<T, CAP>::BYTES, s>>>(
+                g, st, fs.q[B], fs.hint, fs.hint_set, dE);
+            note_launches(1);
+            return;
+        }
+    }
     if (narrow)
         move_rowq_narrow_kernel<WT, T, CAP><<<di.sms * di.occ_fbq_narrow[B], T, SM, s>>>(g, st, fs.q[B], fs.hint,
                                                                                         fs.hint_set, dE);
