@@ -46,12 +46,21 @@ void launch_gather_cdeg(const int32_t *mstart, const int32_t *P, const int32_t *
 
 using namespace lv;
 
+// Aggregated levels holding a sum of 2^32 or more: swept with the 64-bit
+// kernels throughout (0), or through the 32-bit view with those rows sent to
+// the large queue (1).  0 is the default: on R-MAT-24 the 32-bit view's piece
+// tables were slower on these levels (298 vs 257 ms of move phase per run),
+// their two atomics per add serialising where many lanes add to one
+// community.
 #ifndef LV_NARROW_ESCAPES
-#define LV_NARROW_ESCAPES 1
+#define LV_NARROW_ESCAPES 0
 #endif
-// the insert loops combine a warp's equal keys: 1 on aggregated levels, 2 at every level, 0 never
+// The insert loops combine a warp's equal keys before their atomics
+// (key_peers: __match_any_sync + __reduce_add_sync): 1 on aggregated levels,
+// 2 at every level, 0 never.  0 is the default: with 1 the move phase of an
+// R-MAT-24 run took 620 ms instead of 306 ms.
 #ifndef LV_DEDUP
-#define LV_DEDUP 1
+#define LV_DEDUP 0
 #endif
 
 namespace {

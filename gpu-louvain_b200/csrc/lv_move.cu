@@ -1347,9 +1347,12 @@ inline unsigned nblocks(int64_t items, int per_block) {
 __host__ __device__ constexpr int FBQ_SMEM(int b) { return 2 * FBQ_MAXDEG(b) * 14; }
 
 // Rows of the narrow row queues staged by bulk copies (1) or read with
-// plain loads (0).
+// plain loads (0).  0 is the default: on R-MAT-22's first level-0 sweep the
+// staged 256-thread queue kernel took 595 us against 474 us (its rows are
+// already read by coalesced loads; the staging adds barrier and
+// shared-memory waits, issue-active 43 % against 53 %).
 #ifndef LV_ROWQ_STAGE
-#define LV_ROWQ_STAGE 1
+#define LV_ROWQ_STAGE 0
 #endif
 
 template <typename WT, int B>
