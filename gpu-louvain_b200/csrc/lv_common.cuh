@@ -35,6 +35,11 @@
 #ifndef LV_U_STAGE
 #define LV_U_STAGE 8
 #endif
+// The 64-bit warp kernel sums runs of one community per lane in registers
+// before its table adds (1) or adds every entry (0).
+#ifndef LV_WARP_COMBINE
+#define LV_WARP_COMBINE 0
+#endif
 // The narrow-weight warp kernel issues the next chunk's column and weight
 // loads before inserting the current chunk (1), or loads each chunk when it
 // gets to it (0, the default: 1 made the degree > 319 class of an R-MAT-24

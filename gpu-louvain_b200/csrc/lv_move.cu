@@ -303,10 +303,17 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
         u64 e_own = 0;
         int32_t nclaim = 0;
         bool overflow = false;
+        // LV_WARP_COMBINE: each lane holds its last community and the weight
+        // summed to it in registers and adds them to the table only when the
+        // community changes (and at the end of the row), so runs of one
+        // community in a lane's entries cost one shared add
+        int32_t ck = -1;
+        u64 cw = 0;
         // U chunks of 32 edges per step: U column and weight loads, then U
         // community gathers, are in flight together.  The claim count is
         // checked after every chunk, so at most WARP_LIMIT + 32 slots of
-        // the WARP_CAP-slot table are ever claimed.
+        // the WARP_CAP-slot table are ever claimed (+ 32 held in registers
+        // with LV_WARP_COMBINE, added at the end of the row).
         constexpr int U = LV_U_WARP;
         for (int32_t base = r0 + lane; base < r1 + lane && !overflow; base += 32 * U) {
             int32_t jj[U];
@@ -332,12 +339,29 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
                     const u64 ws = group_sum_u64(peers, valid ? ww[u] : 0);
                     if (valid && group_leader(peers)) claimed = table_insert_claim(keys, vals, lg, cc[u], ws, st.err);
                 } else if (cc[u] >= 0) {
-                    if (cc[u] == own) e_own += ww[u];
-                    else claimed = table_insert_claim(keys, vals, lg, cc[u], ww[u], st.err);
+                    if (cc[u] == own) {
+                        e_own += ww[u];
+                    } else if (LV_WARP_COMBINE) {
+                        if (cc[u] == ck) {
+                            cw += ww[u];
+                        } else {
+                            if (ck >= 0) claimed = table_insert_claim(keys, vals, lg, ck, cw, st.err);
+                            ck = cc[u];
+                            cw = ww[u];
+                        }
+                    } else {
+                        claimed = table_insert_claim(keys, vals, lg, cc[u], ww[u], st.err);
+                    }
                 }
                 nclaim += __popc(__ballot_sync(FULL, claimed >= 0));
                 if (nclaim > fs.warp_limit) { overflow = true; break; }
             }
+        }
+        if (LV_WARP_COMBINE && !overflow) {
+            // the communities still held in registers
+            const int32_t claimed = ck >= 0 ? table_insert_claim(keys, vals, lg, ck, cw, st.err) : -1;
+            nclaim += __popc(__ballot_sync(FULL, claimed >= 0));
+            if (nclaim > fs.warp_limit) overflow = true;
         }
         __syncwarp();
         const int nslots = 1 << lg;
