@@ -511,6 +511,40 @@ StateView state_of(lv_handle *h) {
 // global hash-table layouts (hub vertices in the move phase, very large
 // communities in aggregation)
 // ---------------------------------------------------------------------------
+// Pinned host scratch (the totals block and the class counts a handle reads
+// back) comes from a process-wide free list: page-locking memory is a slow
+// driver call, and a handle created per run should not pay it.
+struct PinnedBlock {
+    Totals tot;
+    int32_t small[128];
+};
+std::mutex g_pinned_mu;
+std::vector<PinnedBlock *> g_pinned_free;
+
+int pinned_take(lv_handle *h) {
+    PinnedBlock *b = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_mu);
+        if (!g_pinned_free.empty()) {
+            b = g_pinned_free.back();
+            g_pinned_free.pop_back();
+        }
+    }
+    if (!b) LV_CUDA(h, cudaMallocHost((void **)&b, sizeof(PinnedBlock)));
+    h->tot_h = &b->tot;
+    h->small_h = b->small;
+    return LV_OK;
+}
+
+void pinned_give(lv_handle *h) {
+    if (!h->tot_h) return;
+    PinnedBlock *b = reinterpret_cast<PinnedBlock *>(h->tot_h);
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    g_pinned_free.push_back(b);
+    h->tot_h = nullptr;
+    h->small_h = nullptr;
+}
+
 int ensure_tables(lv_handle *h, size_t slots) {
     if (slots <= h->tbl_slots) return LV_OK;
     size_t want = slots + slots / 4;
@@ -1449,8 +1483,7 @@ int finish_create(lv_handle *h) {
     }
     LV_TRY(dalloc(h, &h->tot_d, 1));
     LV_CUDA(h, cudaMemsetAsync(h->tot_d, 0, sizeof(Totals), h->stream));
-    LV_CUDA(h, cudaMallocHost((void **)&h->tot_h, sizeof(Totals)));
-    LV_CUDA(h, cudaMallocHost((void **)&h->small_h, sizeof(int32_t) * 128));
+    LV_TRY(pinned_take(h));
     // CSR validation
     launch_validate_csr(h->in_rowptr, h->in_col, h->V0, h->E0, &h->tot_d->err, h->stream);
     LV_CUDA(h, cudaMemcpyAsync(h->tot_h, h->tot_d, sizeof(Totals), cudaMemcpyDeviceToHost, h->stream));
@@ -1640,8 +1673,7 @@ int lv_destroy(lv_handle *h) {
         dfree(h, ld);
         h->loop_d = nullptr;
     }
-    if (h->tot_h) cudaFreeHost(h->tot_h);
-    if (h->small_h) cudaFreeHost(h->small_h);
+    pinned_give(h);
     for (const Pending &p : h->pend) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     for (cudaEvent_t e : h->ev_free) cudaEventDestroy(e);
     if (h->stream) {
