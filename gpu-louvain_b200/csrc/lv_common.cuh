@@ -36,7 +36,8 @@
 #define LV_U_STAGE 8
 #endif
 // The 64-bit warp kernel sums runs of one community per lane in registers
-// before its table adds (1) or adds every entry (0).
+// before its table adds (1) or adds every entry (0, the default: 1 measured
+// no faster on R-MAT-24, 121 against 120 ms for the degree > 319 class).
 #ifndef LV_WARP_COMBINE
 #define LV_WARP_COMBINE 0
 #endif
