@@ -146,6 +146,7 @@ struct DeviceInfo {
     int occ_fbq_staged[NFBQ] = {1, 1, 1, 1};   // ... and of its bulk-copy row-staging form
     int occ_merge_s = 1;                 // ... of the small giant-merge kernel
     int occ_stage_narrow = 1;            // ... of the persistent narrow staging kernel
+    int occ_stage = 1;                   // ... and of the persistent 64-bit one
 };
 void init_kernel_attributes(DeviceInfo &di);
 

@@ -1061,37 +1061,46 @@ template <typename WT>
 __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_kernel(GraphView<WT> g, StateView st,
                                                                     HubGlobal hg, const uint8_t *only) {
     // only != nullptr: just the giants marked there (the rest are staged by
-    // the narrow kernel)
-    if (only && !only[hg.hubs[hg.echunk_hub[blockIdx.x]]]) return;
+    // the narrow kernel).  Persistent over the chunks, as the narrow kernel:
+    // the table is initialised once and after each chunk only its claimed
+    // slots are cleared.
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int LCAP = 2 * STAGE_CHUNK;
     constexpr int LLG = ilog2_c(LCAP);
     u64 *lvals = reinterpret_cast<u64 *>(smem_raw);
     int32_t *lkeys = reinterpret_cast<int32_t *>(lvals + LCAP);
-    int32_t *locc = lkeys + LCAP;
+    int32_t *locc = lkeys + LCAP;   // claimed slots of the chunk (at most STAGE_CHUNK)
     __shared__ int32_t lnocc, base;
     for (int s = threadIdx.x; s < LCAP; s += STAGE_THREADS) { lkeys[s] = -1; lvals[s] = 0; }
     if (threadIdx.x == 0) lnocc = 0;
     __syncthreads();
-    const int32_t h = hg.echunk_hub[blockIdx.x];
-    const int32_t v = hg.hubs[h];
-    const int32_t r1 = g.rowend[v];
-    const int32_t e0 = g.rowptr[v] + hg.echunk_e0[blockIdx.x];
-    const int32_t e1 = min(e0 + STAGE_CHUNK, r1);
-    const int32_t own = __ldg(st.comm + v);
-    u64 e_own = 0;
-    insert_row<LV_U_STAGE, true>(g, st.comm, v, own, e0, e1, threadIdx.x, STAGE_THREADS, lkeys, lvals, LLG,
-                                 st.err, locc, &lnocc, e_own, st.dedup != 0);
-    block_add_total<STAGE_THREADS>(e_own, hg.eown + h);   // contains the barrier
-    const int32_t n = lnocc;
-    if (threadIdx.x == 0) base = atomicAdd(hg.nocc + h, n);
-    __syncthreads();
-    int32_t *sk = hg.stage_key + hg.occ_off[h] + base;
-    u64 *sv = hg.stage_val + hg.occ_off[h] + base;
-    for (int32_t i = threadIdx.x; i < n; i += STAGE_THREADS) {
-        const int32_t sl = locc[i];
-        sk[i] = lkeys[sl];
-        sv[i] = lvals[sl];
+    for (int32_t ch = blockIdx.x; ch < hg.n_echunks; ch += gridDim.x) {
+        const int32_t h = hg.echunk_hub[ch];
+        const int32_t v = hg.hubs[h];
+        if (only && !only[v]) continue;
+        const int32_t r1 = g.rowend[v];
+        const int32_t e0 = g.rowptr[v] + hg.echunk_e0[ch];
+        const int32_t e1 = min(e0 + STAGE_CHUNK, r1);
+        const int32_t own = __ldg(st.comm + v);
+        u64 e_own = 0;
+        insert_row<LV_U_STAGE, true>(g, st.comm, v, own, e0, e1, threadIdx.x, STAGE_THREADS, lkeys, lvals, LLG,
+                                     st.err, locc, &lnocc, e_own, st.dedup != 0);
+        block_add_total<STAGE_THREADS>(e_own, hg.eown + h);   // contains the barrier
+        const int32_t n = min(lnocc, STAGE_CHUNK);
+        if (threadIdx.x == 0) base = atomicAdd(hg.nocc + h, n);
+        __syncthreads();
+        int32_t *sk = hg.stage_key + hg.occ_off[h] + base;
+        u64 *sv = hg.stage_val + hg.occ_off[h] + base;
+        for (int32_t i = threadIdx.x; i < n; i += STAGE_THREADS) {
+            const int32_t sl = locc[i];
+            sk[i] = lkeys[sl];
+            sv[i] = lvals[sl];
+            lkeys[sl] = -1;
+            lvals[sl] = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) lnocc = 0;
+        __syncthreads();
     }
 }
 
@@ -1436,6 +1445,9 @@ static void set_attrs_for(DeviceInfo &di) {
         int o2 = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, giant_stage_narrow_kernel<WT>, STAGE_THREADS, STAGE_SMEM);
         di.occ_stage_narrow = o2 > 0 ? o2 : 1;
+        o2 = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, giant_stage_kernel<WT>, STAGE_THREADS, STAGE_SMEM);
+        di.occ_stage = o2 > 0 ? o2 : 1;
     }
     cudaFuncSetAttribute(move_warp_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_SMEM);
     cudaFuncSetAttribute(move_warp_narrow_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_NSMEM);
@@ -1524,11 +1536,13 @@ void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGl
                                         STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg);
         note_launches(1);
         if (st.wrow) {
-            giant_stage_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg, st.wrow);
+            giant_stage_kernel<WT><<<(unsigned)imin64(hg.n_echunks, (int64_t)di.sms * di.occ_stage), STAGE_THREADS,
+                                     STAGE_SMEM, s>>>(g, st, hg, st.wrow);
             note_launches(1);
         }
     } else {
-        giant_stage_kernel<WT><<<hg.n_echunks, STAGE_THREADS, STAGE_SMEM, s>>>(g, st, hg, nullptr);
+        giant_stage_kernel<WT><<<(unsigned)imin64(hg.n_echunks, (int64_t)di.sms * di.occ_stage), STAGE_THREADS,
+                                 STAGE_SMEM, s>>>(g, st, hg, nullptr);
         note_launches(1);
     }
 #if LV_MERGE_SMALL
