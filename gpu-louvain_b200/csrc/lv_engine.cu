@@ -154,6 +154,10 @@ struct lv_handle {
     size_t nocc_cap = 0;
     int32_t *stage_key = nullptr;  // staging area of the hub path (entries = occ_cap)
     u64 *stage_val = nullptr;
+    int32_t *stage2_key = nullptr; // the staged pairs regrouped by key partition (occ_cap)
+    u64 *stage2_val = nullptr;
+    int32_t *poff_buf = nullptr;   // partition offsets of the regrouped pairs
+    size_t poff_cap = 0;
     u64 *eown_buf = nullptr;       // per hub, zero between uses (nocc_cap entries)
     int32_t *ovf_buf = nullptr;    // overflow list (nocc_cap entries) then its count
     bool capturing = false;        // a sweep is being captured into a graph (timers off)
@@ -564,11 +568,15 @@ int ensure_occ(lv_handle *h, size_t entries, size_t hubs) {
         dfree(h, h->occ_buf);
         dfree(h, h->stage_key);
         dfree(h, h->stage_val);
+        dfree(h, h->stage2_key);
+        dfree(h, h->stage2_val);
         h->occ_cap = 0;
         size_t want = entries + entries / 4 + 1;
         LV_TRY(dalloc(h, &h->occ_buf, want));
         LV_TRY(dalloc(h, &h->stage_key, want));
         LV_TRY(dalloc(h, &h->stage_val, want));
+        LV_TRY(dalloc(h, &h->stage2_key, want));
+        LV_TRY(dalloc(h, &h->stage2_val, want));
         h->occ_cap = want;
     }
     if (hubs > h->nocc_cap) {
@@ -596,7 +604,7 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
     const int32_t n = (int32_t)ids.size();
     std::vector<int64_t> off(n), occ_off(n);
     int64_t occ_total = 0;
-    std::vector<int32_t> lg(n), ech_hub, ech_e0, sch_hub, sch_s0, hub_s0(n + 1);
+    std::vector<int32_t> lg(n), ech_hub, ech_e0, sch_hub, sch_s0, hub_s0(n + 1), hub_cap(n), pbase(n + 1, 0);
     int64_t total = 0;
     for (int32_t i = 0; i < n; ++i) {
         int64_t distinct = deg[i];
@@ -615,6 +623,8 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
         hub_s0[i] = (int32_t)sch_hub.size();
         occ_off[i] = occ_total;
         occ_total += deg[i];
+        hub_cap[i] = deg[i];
+        pbase[i + 1] = pbase[i] + (deg[i] + FB_KEYS - 1) / FB_KEYS + 2;
         const int64_t span = occ_lists ? (int64_t)deg[i] : (int64_t(1) << l);
         for (int64_t s0 = 0; s0 < span; s0 += HG_SLOT_CHUNK) {
             sch_hub.push_back(i);
@@ -631,7 +641,7 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
     const size_t ne = ech_hub.size(), ns = sch_hub.size();
     // packed: ids | lg | ech_hub | ech_e0 | sch_hub | sch_s0 | hub_s0 | res_c | (8-aligned) off |
     // res_g | res_e | res_b | occ_off
-    size_t i32_count = (size_t)n + n + ne + ne + ns + ns + (n + 1) + ns;
+    size_t i32_count = (size_t)n + n + ne + ne + ns + ns + (n + 1) + ns + n + (n + 1);
     size_t i32_bytes = ((i32_count * 4 + 15) / 16) * 16;
     size_t bytes = i32_bytes + (size_t)n * 8 + ns * 16 + ns * 8 + ns * 8 + (size_t)n * 8 + 64;
     if (bytes > L.dev_bytes) {
@@ -659,6 +669,7 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
     size_t o_hs = put(hub_s0.data(), n + 1);
     size_t o_rc = at;
     at += ns;
+    size_t o_cap = put(hub_cap.data(), n), o_pb = put(pbase.data(), n + 1);
     unsigned char *base8 = host.data() + i32_bytes;
     if (n) std::memcpy(base8, off.data(), (size_t)n * 8);
     if (n) std::memcpy(base8 + (size_t)n * 8 + ns * 32, occ_off.data(), (size_t)n * 8);
@@ -679,6 +690,8 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
     v.schunk_s0 = d32 + o_s0;
     v.hub_schunk0 = d32 + o_hs;
     v.res_c = d32 + o_rc;
+    v.hub_cap = d32 + o_cap;
+    v.pbase = d32 + o_pb;
     v.tbl_off = (const int64_t *)d8;
     v.res_g = (u64 *)(d8 + (size_t)n * 8);
     v.res_e = (u64 *)(d8 + (size_t)n * 8 + ns * 16);
@@ -688,6 +701,15 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
     v.nocc = h->nocc_buf;
     v.stage_key = h->stage_key;
     v.stage_val = h->stage_val;
+    v.stage2_key = h->stage2_key;
+    v.stage2_val = h->stage2_val;
+    if ((size_t)pbase[n] > h->poff_cap) {
+        dfree(h, h->poff_buf);
+        h->poff_cap = 0;
+        LV_TRY(dalloc(h, &h->poff_buf, (size_t)pbase[n] + 1));
+        h->poff_cap = (size_t)pbase[n];
+    }
+    v.poff = h->poff_buf;
     v.eown = h->eown_buf;
     v.ovf_list = h->ovf_buf;
     v.ovf_count = h->ovf_buf + h->nocc_cap;
@@ -1648,6 +1670,7 @@ int lv_destroy(lv_handle *h) {
     }
     dfree(h, h->tbl_keys); dfree(h, h->tbl_vals); dfree(h, h->occ_buf); dfree(h, h->nocc_buf);
     dfree(h, h->stage_key); dfree(h, h->stage_val); dfree(h, h->eown_buf); dfree(h, h->ovf_buf);
+    dfree(h, h->stage2_key); dfree(h, h->stage2_val); dfree(h, h->poff_buf);
     for (HubLayout *L : {&h->hub_move, &h->hub_agg}) {
         unsigned char *d = (unsigned char *)L->dev;
         dfree(h, d);

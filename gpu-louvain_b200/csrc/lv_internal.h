@@ -57,6 +57,16 @@ struct HubGlobal {
     u64 *eown = nullptr;                  // [nhubs] weight to the own community (zero between uses)
     int32_t *ovf_list = nullptr;          // hubs whose staged pairs overflow shared memory
     int32_t *ovf_count = nullptr;         // length of ovf_list (reset by the host per use)
+    // staged pairs regrouped by large-queue key partition (move phase): hub h
+    // owns poff[pbase[h] .. pbase[h + 1]) = its Pmax + 2 words, Pmax =
+    // ceil(hub_cap[h] / FB_KEYS): poff[pbase[h] + p] is the first regrouped
+    // pair of partition p (p = 0 .. P), poff[pbase[h + 1] - 1] the P used, and
+    // poff[pbase[h]] = -1 when the hub's pairs were not regrouped
+    const int32_t *hub_cap = nullptr;     // [nhubs] staging room (the hub's degree)
+    const int32_t *pbase = nullptr;       // [nhubs + 1]
+    int32_t *poff = nullptr;
+    int32_t *stage2_key = nullptr;        // regrouped pairs, same layout as stage_key
+    u64 *stage2_val = nullptr;
 };
 
 // Device memory from the library's per-device stream-ordered pool (freed

@@ -687,12 +687,24 @@ __global__ void __launch_bounds__(THREADS) move_fallback_kernel(GraphView<WT> g,
             const int32_t n = hg.nocc[src];
             int lg = P > 1 ? ilog2_c(CAP) : ceil_log2_i(2 * (int64_t)n);
             lg = lg < 3 ? 3 : lg;
-            const int32_t *sk = hg.stage_key + hg.occ_off[src];
-            const u64 *sv = hg.stage_val + hg.occ_off[src];
-            for (int32_t i = threadIdx.x; i < n; i += THREADS) {
-                const int32_t c = sk[i];
-                if (P == 1 || (int32_t)part_of(c, P) == p)
-                    table_insert_occ_capped(keys, vals, lg, c, sv[i], st.err, occ, &nocc, OCC_CAP);
+            const int32_t pb = hg.pbase[src], pe = hg.pbase[src + 1];
+            const bool regrouped = hg.poff && P > 1 && P + 2 <= pe - pb && hg.poff[pb] >= 0 && hg.poff[pe - 1] == P &&
+                                   hg.poff[pb + P] == n;
+            if (regrouped) {
+                // partition p's pairs only (giant_regroup_kernel)
+                const int32_t i0 = hg.poff[pb + p], i1 = min(hg.poff[pb + p + 1], n);
+                const int32_t *sk = hg.stage2_key + hg.occ_off[src];
+                const u64 *sv = hg.stage2_val + hg.occ_off[src];
+                for (int32_t i = i0 + threadIdx.x; i < i1; i += THREADS)
+                    table_insert_occ_capped(keys, vals, lg, sk[i], sv[i], st.err, occ, &nocc, OCC_CAP);
+            } else {
+                const int32_t *sk = hg.stage_key + hg.occ_off[src];
+                const u64 *sv = hg.stage_val + hg.occ_off[src];
+                for (int32_t i = threadIdx.x; i < n; i += THREADS) {
+                    const int32_t c = sk[i];
+                    if (P == 1 || (int32_t)part_of(c, P) == p)
+                        table_insert_occ_capped(keys, vals, lg, c, sv[i], st.err, occ, &nocc, OCC_CAP);
+                }
             }
             if (p == 0 && threadIdx.x == 0) e_own = hg.eown[src];
         }
@@ -1104,6 +1116,58 @@ __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_kernel(GraphView<WT
     }
 }
 
+// Giants with more staged pairs than the merge table holds are decided by
+// P = ceil(n / FB_KEYS) large-queue items, item p keeping the pairs whose
+// key falls in partition p.  Before the merges, one CTA per such giant
+// regroups its n staged pairs by partition (a counting sort: partition
+// sizes, their offsets, then a scatter into stage2), so that each item reads
+// its own n / P pairs instead of all n.  A giant whose P would exceed
+// REGROUP_PMAX keeps the filtering path (poff[pbase] = -1).
+constexpr int REGROUP_THREADS = 1024;
+constexpr int REGROUP_PMAX = 4096;
+
+__global__ void __launch_bounds__(REGROUP_THREADS) giant_regroup_kernel(HubGlobal hg) {
+    __shared__ int32_t cnt[REGROUP_PMAX];
+    const int32_t h = blockIdx.x;
+    const int32_t pb = hg.pbase[h], pe = hg.pbase[h + 1];   // pe - pb = Pmax + 2
+    const int32_t cap = hg.hub_cap[h];
+    const int32_t n = min(hg.nocc[h], cap);
+    if (2 * (int64_t)n <= HG_MERGE_CAP) return;   // merged in shared memory; no items
+    const int32_t P = (n + FB_KEYS - 1) / FB_KEYS;
+    if (P > REGROUP_PMAX || P + 2 > pe - pb) {
+        if (threadIdx.x == 0) hg.poff[pb] = -1;
+        return;
+    }
+    for (int32_t p = threadIdx.x; p < P; p += REGROUP_THREADS) cnt[p] = 0;
+    __syncthreads();
+    const int64_t o = hg.occ_off[h];
+    const int32_t *sk = hg.stage_key + o;
+    const u64 *sv = hg.stage_val + o;
+    for (int32_t i = threadIdx.x; i < n; i += REGROUP_THREADS) atomicAdd(&cnt[part_of(sk[i], P)], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // exclusive offsets; cnt[p] becomes partition p's write cursor
+        int32_t run = 0;
+        for (int32_t p = 0; p < P; ++p) {
+            const int32_t c = cnt[p];
+            hg.poff[pb + p] = run;
+            cnt[p] = run;
+            run += c;
+        }
+        hg.poff[pb + P] = run;        // = n
+        hg.poff[pe - 1] = P;
+    }
+    __syncthreads();
+    int32_t *dk = hg.stage2_key + o;
+    u64 *dv = hg.stage2_val + o;
+    for (int32_t i = threadIdx.x; i < n; i += REGROUP_THREADS) {
+        const int32_t c = sk[i];
+        const int32_t pos = atomicAdd(&cnt[part_of(c, P)], 1);   // < n: the cursors stay in their partitions
+        dk[pos] = c;
+        dv[pos] = sv[i];
+    }
+}
+
 // Two instances: CAP = HG_MERGE_CAP decides the giants with
 // n_min < n <= HG_MERGE_CAP / 2 staged pairs and queues the larger ones; a
 // smaller instance (more CTAs per SM) runs first and takes n <= CAP / 2.
@@ -1379,6 +1443,13 @@ inline unsigned nblocks(int64_t items, int per_block) {
 
 __host__ __device__ constexpr int FBQ_SMEM(int b) { return 2 * FBQ_MAXDEG(b) * 14; }
 
+// Giants decided by several large-queue items have their staged pairs
+// regrouped by key partition first (1), or every item filters all of the
+// giant's pairs (0).
+#ifndef LV_GIANT_REGROUP
+#define LV_GIANT_REGROUP 1
+#endif
+
 // Rows of the narrow row queues staged by bulk copies (1) or read with
 // plain loads (0).  0 is the default: on R-MAT-22's first level-0 sweep the
 // staged 256-thread queue kernel took 595 us against 474 us (its rows are
@@ -1543,6 +1614,10 @@ void launch_move_giants(const GraphView<WT> &g, const StateView &st, const HubGl
     } else {
         giant_stage_kernel<WT><<<(unsigned)imin64(hg.n_echunks, (int64_t)di.sms * di.occ_stage), STAGE_THREADS,
                                  STAGE_SMEM, s>>>(g, st, hg, nullptr);
+        note_launches(1);
+    }
+    if (LV_GIANT_REGROUP && hg.poff) {
+        giant_regroup_kernel<<<hg.nhubs, REGROUP_THREADS, 0, s>>>(hg);
         note_launches(1);
     }
 #if LV_MERGE_SMALL
