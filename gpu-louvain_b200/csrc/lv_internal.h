@@ -114,11 +114,7 @@ __host__ __device__ constexpr int FBQ_THREADS(int b) { return b == 0 ? 128 : (b 
 constexpr int FB_THREADS = 1024, FB_CAP = 16384;
 constexpr int FB_KEYS = 7168;
 constexpr int FB_SMEM = FB_CAP * 14;   // table + occupied list
-// claimed slots listed per warp table of the 64-bit warp kernel (a vertex
-// with at most this many distinct neighbour communities is evaluated and
-// cleared over the list, not over the whole table)
-constexpr int WIDE_OCC_CAP = 128;
-constexpr int WARP_SMEM = 8 * (WARP_CAP * 12 + WIDE_OCC_CAP * 4);   // 8 warp tables per CTA
+constexpr int WARP_SMEM = 8 * WARP_CAP * 12;   // 8 warp tables per CTA
 
 // A fallback work list (device memory; count and next are adjacent).
 struct Fallback {

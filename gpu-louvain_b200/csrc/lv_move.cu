@@ -247,12 +247,6 @@ __device__ __forceinline__ void enqueue_fallback(const FallbackSet &fs, int32_t 
     }
 }
 
-// The 64-bit warp kernel evaluates a vertex over its listed claims when
-// they fit the list (1) or always over the whole table (0).
-#ifndef LV_WIDE_OCC
-#define LV_WIDE_OCC 1
-#endif
-
 template <typename WT>
 __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateView st,
                                                         const int32_t *__restrict__ list, int32_t n,
@@ -262,12 +256,9 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
     extern __shared__ __align__(16) unsigned char smem_raw[];
     u64 *svals = reinterpret_cast<u64 *>(smem_raw);
     int32_t *skeys = reinterpret_cast<int32_t *>(svals + NW * WARP_CAP);
-    int32_t *socc = skeys + NW * WARP_CAP;
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int32_t *keys = skeys + wid * WARP_CAP;
     u64 *vals = svals + wid * WARP_CAP;
-    int32_t *occ = socc + wid * WIDE_OCC_CAP;   // the vertex's claimed slots (the first WIDE_OCC_CAP)
-    const unsigned lt_mask = (1u << lane) - 1u;
     for (int s = lane; s < WARP_CAP; s += 32) { keys[s] = -1; vals[s] = 0; }
     __syncwarp();
     u64 delta_acc = 0;
@@ -362,24 +353,14 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
                         claimed = table_insert_claim(keys, vals, lg, cc[u], ww[u], st.err);
                     }
                 }
-                {
-                    // the claim count is warp-uniform: the ballot also gives
-                    // each claim its place in the list
-                    const unsigned bal = __ballot_sync(FULL, claimed >= 0);
-                    const int32_t pos = nclaim + __popc(bal & lt_mask);
-                    if (claimed >= 0 && pos < WIDE_OCC_CAP) occ[pos] = claimed;
-                    nclaim += __popc(bal);
-                }
+                nclaim += __popc(__ballot_sync(FULL, claimed >= 0));
                 if (nclaim > fs.warp_limit) { overflow = true; break; }
             }
         }
         if (LV_WARP_COMBINE && !overflow) {
             // the communities still held in registers
             const int32_t claimed = ck >= 0 ? table_insert_claim(keys, vals, lg, ck, cw, st.err) : -1;
-            const unsigned bal = __ballot_sync(FULL, claimed >= 0);
-            const int32_t pos = nclaim + __popc(bal & lt_mask);
-            if (claimed >= 0 && pos < WIDE_OCC_CAP) occ[pos] = claimed;
-            nclaim += __popc(bal);
+            nclaim += __popc(__ballot_sync(FULL, claimed >= 0));
             if (nclaim > fs.warp_limit) overflow = true;
         }
         __syncwarp();
@@ -398,11 +379,7 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
         const MoveCtx m = move_ctx(own, sz_own == 1, st.T, k_v, s_own);
         Best b = best_init(own);
         b.eo = e_own;
-        // evaluation (and clearing) over the listed claims when they all fit
-        // the list, else over the whole table
-        if (LV_WIDE_OCC && nclaim <= WIDE_OCC_CAP)
-            eval_slots<1, true, true>(keys, vals, occ, nclaim, lane, 32, m, st.S, st.size, b);
-        else eval_slots<1, false, true>(keys, vals, nullptr, nslots, lane, 32, m, st.S, st.size, b);
+        eval_slots<1, false, true>(keys, vals, nullptr, nslots, lane, 32, m, st.S, st.size, b);
         group_reduce_best(m, b, 32);
         if (lane == 0) {
             u64 delta = 0;
