@@ -114,7 +114,12 @@ __host__ __device__ constexpr int FBQ_THREADS(int b) { return b == 0 ? 128 : (b 
 constexpr int FB_THREADS = 1024, FB_CAP = 16384;
 constexpr int FB_KEYS = 7168;
 constexpr int FB_SMEM = FB_CAP * 14;   // table + occupied list
-constexpr int WARP_SMEM = 8 * WARP_CAP * 12;   // 8 warp tables per CTA
+// LV_WARP_PAD: extra shared bytes per CTA of the 64-bit warp kernel (0; a
+// measurement knob for the shared-memory / L1 split)
+#ifndef LV_WARP_PAD
+#define LV_WARP_PAD 0
+#endif
+constexpr int WARP_SMEM = 8 * WARP_CAP * 12 + LV_WARP_PAD;   // 8 warp tables per CTA
 
 // A fallback work list (device memory; count and next are adjacent).
 struct Fallback {

@@ -1522,6 +1522,12 @@ static void set_attrs_for(DeviceInfo &di) {
     }
     cudaFuncSetAttribute(move_warp_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_SMEM);
     cudaFuncSetAttribute(move_warp_narrow_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_NSMEM);
+#ifdef LV_NARROW_CARVEOUT
+    // measurement knob: the shared-memory share of the SM's L1/shared split
+    // (percent) preferred for the narrow warp kernel
+    cudaFuncSetAttribute(move_warp_narrow_kernel<WT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         LV_NARROW_CARVEOUT);
+#endif
     int o = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_warp_kernel<WT>, 256, WARP_SMEM);
     di.occ_warp = o > 0 ? o : 1;
