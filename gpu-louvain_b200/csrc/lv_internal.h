@@ -111,8 +111,14 @@ __host__ __device__ constexpr int FBQ_MAXDEG(int b) { return 512 << b; }        
 // per SM (their tables take 57 and 114 KB), so they get 512 and 1024 threads
 // to keep 32 warps per SM
 __host__ __device__ constexpr int FBQ_THREADS(int b) { return b == 0 ? 128 : (b == 1 ? 256 : (b == 2 ? 512 : 1024)); }
-constexpr int FB_THREADS = 1024, FB_CAP = 16384;
-constexpr int FB_KEYS = 7168;
+// large queue: CTA threads, table slots and keys per partition (the
+// partition bound stays below the occupied list's CAP / 2 with room for the
+// hash's imbalance)
+#ifndef LV_FB_CAP
+#define LV_FB_CAP 16384
+#endif
+constexpr int FB_THREADS = 1024, FB_CAP = LV_FB_CAP;
+constexpr int FB_KEYS = FB_CAP / 16 * 7;
 constexpr int FB_SMEM = FB_CAP * 14;   // table + occupied list
 // LV_WARP_PAD: extra shared bytes per CTA of the 64-bit warp kernel (0; a
 // measurement knob for the shared-memory / L1 split)

@@ -1521,13 +1521,24 @@ static void set_attrs_for(DeviceInfo &di) {
         di.occ_stage = o2 > 0 ? o2 : 1;
     }
     cudaFuncSetAttribute(move_warp_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_SMEM);
-    cudaFuncSetAttribute(move_warp_narrow_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_NSMEM);
-#ifdef LV_NARROW_CARVEOUT
-    // measurement knob: the shared-memory share of the SM's L1/shared split
-    // (percent) preferred for the narrow warp kernel
-    cudaFuncSetAttribute(move_warp_narrow_kernel<WT>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         LV_NARROW_CARVEOUT);
+#ifdef LV_WIDE_CARVEOUT
+    // measurement knob: preferred shared-memory share of the 64-bit warp kernel
+    cudaFuncSetAttribute(move_warp_kernel<WT>, cudaFuncAttributePreferredSharedMemoryCarveout, LV_WIDE_CARVEOUT);
 #endif
+    cudaFuncSetAttribute(move_warp_narrow_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_NSMEM);
+    // The SM's L1 / shared-memory split follows the shared memory its
+    // resident CTAs need, in steps (…, 132, 164, 196, 228 KB of shared
+    // memory; L1 gets the rest of 256 KB).  Four narrow warp CTAs (53 KB
+    // each) would take the 228 KB step and leave 28 KB of L1 for the
+    // community and Sigma_tot gathers; preferring the 164 KB step runs three
+    // CTAs per SM with 92 KB of L1, which measured faster (degrees 33-84 at
+    // level 0: 9.45 against 10.05 ms per R-MAT-24 run).
+#ifndef LV_NARROW_CARVEOUT
+#define LV_NARROW_CARVEOUT 72
+#endif
+    if (LV_NARROW_CARVEOUT > 0)
+        cudaFuncSetAttribute(move_warp_narrow_kernel<WT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             LV_NARROW_CARVEOUT);
     int o = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, move_warp_kernel<WT>, 256, WARP_SMEM);
     di.occ_warp = o > 0 ? o : 1;
