@@ -380,6 +380,27 @@ __global__ void __launch_bounds__(T) merge_cta_narrow_kernel(const int32_t *__re
     }
 }
 
+// Insert (key, w) into a community's global table (GSlot layout, move-phase
+// hash, linear probing bounded by the capacity); returns the slot newly
+// claimed for key, or -1.
+__device__ __forceinline__ int32_t gslot_insert_claim(GSlot *t, int lg, int32_t key, u64 w, int *err) {
+    const uint32_t mask = (1u << lg) - 1u;
+    const uint32_t k1 = (uint32_t)key + 1u;
+    uint32_t s = hash_slot(key, lg);
+    for (uint32_t p = 0; p <= mask; ++p) {
+        const uint32_t cur = ((volatile uint32_t *)&t[s].key1)[0];
+        if (cur == k1) { atomicAdd(&t[s].val, w); return -1; }
+        if (cur == 0) {
+            const uint32_t prev = atomicCAS(&t[s].key1, 0u, k1);
+            if (prev == 0) { atomicAdd(&t[s].val, w); return (int32_t)s; }
+            if (prev == k1) { atomicAdd(&t[s].val, w); return -1; }
+        }
+        s = (s + 1u) & mask;
+    }
+    atomicOr(err, DEVERR_HASH_FULL);
+    return -1;
+}
+
 // Global-table merge for communities whose degree bound exceeds 4096: one CTA
 // per chunk of HG_EDGE_CHUNK entries, reduced first in a chunk-local shared
 // table (intra-community entries all carry the community's own key), then
@@ -414,13 +435,12 @@ __global__ void __launch_bounds__(HG_INSERT_THREADS) mergeg_insert_kernel(
     // community's global table (move-phase hash), so consecutive inserts land
     // far apart; the merged row comes out in claim order, i.e. in the chunk
     // table's slot order, which is independent of the move phase's hash
-    int32_t *keys = hg.keys + hg.tbl_off[h];
-    u64 *vals = hg.vals + hg.tbl_off[h];
+    GSlot *tbl = hg.slots + hg.tbl_off[h];
     int32_t *occ = hg.occ + hg.occ_off[h];
     const int lg = hg.tbl_lg[h];
     for (int s = threadIdx.x; s < LCAP; s += HG_INSERT_THREADS) {
         const int32_t k = lkeys[s];
-        const int32_t claimed = k >= 0 ? table_insert_claim<0>(keys, vals, lg, k, lvals[s], err) : -1;
+        const int32_t claimed = k >= 0 ? gslot_insert_claim(tbl, lg, k, lvals[s], err) : -1;
         warp_append(claimed, occ, hg.nocc + h);
     }
 }
@@ -473,15 +493,14 @@ __global__ void __launch_bounds__(HG_INSERT_THREADS) mergeg_insert_narrow_kernel
         w_self = warp_sum_u64(w_self);
         if ((threadIdx.x & 31) == 0) wpart[threadIdx.x >> 5] = w_self;
         __syncthreads();
-        int32_t *keys = hg.keys + hg.tbl_off[h];
-        u64 *vals = hg.vals + hg.tbl_off[h];
+        GSlot *tbl = hg.slots + hg.tbl_off[h];
         int32_t *occ = hg.occ + hg.occ_off[h];
         const int lg = hg.tbl_lg[h];
         if (threadIdx.x < 32) {
             u64 ws = 0;
             if (threadIdx.x == 0)
                 for (int i = 0; i < NW; ++i) ws += wpart[i];
-            const int32_t claimed = ws ? table_insert_claim<0>(keys, vals, lg, self, ws, err) : -1;
+            const int32_t claimed = ws ? gslot_insert_claim(tbl, lg, self, ws, err) : -1;
             warp_append(claimed, occ, hg.nocc + h);
         }
         // drained in claim order into the community's global table (its
@@ -492,7 +511,7 @@ __global__ void __launch_bounds__(HG_INSERT_THREADS) mergeg_insert_narrow_kernel
             int32_t claimed = -1;
             if (i < n) {
                 const uint32_t sl = (uint32_t)locc[i];
-                claimed = table_insert_claim<0>(keys, vals, lg, t.keys[sl], piece_value(t, sl), err);
+                claimed = gslot_insert_claim(tbl, lg, t.keys[sl], piece_value(t, sl), err);
                 t.keys[sl] = -1;
                 t.lo[sl] = 0;
                 t.hi[sl] = 0;
@@ -517,22 +536,21 @@ __global__ void __launch_bounds__(256) mergeg_emit_kernel(HubGlobal hg,
     const int32_t c = hg.hubs[h];
     const int32_t a = P[mstart[c]];
     const int32_t self = newid[c];
-    int32_t *keys = hg.keys + hg.tbl_off[h];
-    u64 *vals = hg.vals + hg.tbl_off[h];
+    GSlot *tbl = hg.slots + hg.tbl_off[h];
     const int32_t *occ = hg.occ + hg.occ_off[h];
     const int32_t s0 = hg.schunk_s0[bidx];
     const int32_t n = min(hg.nocc[h] - s0, HG_SLOT_CHUNK);
     u64 hi = 0;
     for (int32_t i = threadIdx.x; i < n; i += 256) {
         const int32_t sl = occ[s0 + i];
-        const int32_t key = keys[sl];
-        const u64 x = vals[sl];
+        const GSlot g = tbl[sl];
+        const int32_t key = (int32_t)(g.key1 - 1u);
+        const u64 x = g.val;
         vkey[a + s0 + i] = key;
         vw[a + s0 + i] = x;
         vw32[a + s0 + i] = x < W32_ESC ? (uint32_t)x : W32_ESC;
         if (key != self && x >= W32_ESC) hi = 1;   // the self-loop is read as uint64 only
-        keys[sl] = -1;
-        vals[sl] = 0;
+        tbl[sl] = GSlot{0u, 0u, 0};
     }
     if (hi) {
         atomicOr(hiflag, 1);

@@ -145,8 +145,7 @@ struct lv_handle {
     int64_t cls_edges[NCLS] = {0};
 
     HubLayout hub_move, hub_agg;
-    int32_t *tbl_keys = nullptr;
-    u64 *tbl_vals = nullptr;
+    GSlot *tbl_buf = nullptr;
     size_t tbl_slots = 0;
     int32_t *occ_buf = nullptr;    // occupied-slot lists of the global tables
     size_t occ_cap = 0;
@@ -552,13 +551,10 @@ void pinned_give(lv_handle *h) {
 int ensure_tables(lv_handle *h, size_t slots) {
     if (slots <= h->tbl_slots) return LV_OK;
     size_t want = slots + slots / 4;
-    dfree(h, h->tbl_keys);
-    dfree(h, h->tbl_vals);
+    dfree(h, h->tbl_buf);
     h->tbl_slots = 0;
-    LV_TRY(dalloc(h, &h->tbl_keys, want));
-    LV_TRY(dalloc(h, &h->tbl_vals, want));
-    LV_CUDA(h, cudaMemsetAsync(h->tbl_keys, 0xFF, want * sizeof(int32_t), h->stream));
-    LV_CUDA(h, cudaMemsetAsync(h->tbl_vals, 0, want * sizeof(u64), h->stream));
+    LV_TRY(dalloc(h, &h->tbl_buf, want));
+    LV_CUDA(h, cudaMemsetAsync(h->tbl_buf, 0, want * sizeof(GSlot), h->stream));
     h->tbl_slots = want;
     return LV_OK;
 }
@@ -713,8 +709,7 @@ int build_layout(lv_handle *h, HubLayout &L, const std::vector<int32_t> &ids,
     v.eown = h->eown_buf;
     v.ovf_list = h->ovf_buf;
     v.ovf_count = h->ovf_buf + h->nocc_cap;
-    v.keys = h->tbl_keys;
-    v.vals = h->tbl_vals;
+    v.slots = h->tbl_buf;
     L.ids = ids;
     return LV_OK;
 }
@@ -1668,7 +1663,7 @@ int lv_destroy(lv_handle *h) {
         dfree(h, t);
         h->sort_temp = nullptr;
     }
-    dfree(h, h->tbl_keys); dfree(h, h->tbl_vals); dfree(h, h->occ_buf); dfree(h, h->nocc_buf);
+    dfree(h, h->tbl_buf); dfree(h, h->occ_buf); dfree(h, h->nocc_buf);
     dfree(h, h->stage_key); dfree(h, h->stage_val); dfree(h, h->eown_buf); dfree(h, h->ovf_buf);
     dfree(h, h->stage2_key); dfree(h, h->stage2_val); dfree(h, h->poff_buf);
     for (HubLayout *L : {&h->hub_move, &h->hub_agg}) {

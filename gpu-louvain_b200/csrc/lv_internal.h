@@ -30,6 +30,16 @@ constexpr int MERGE_S_THREADS = 256, MERGE_S_CAP = 2048;
 #endif
 
 
+// Slot of the aggregation's global hash tables: the key (stored plus one, so
+// that an all-zero slot is empty) and its sum share one 16-byte slot, so an
+// insert's compare-and-swap and add touch one 32-byte DRAM sector instead of
+// one in a key array and one in a value array.
+struct GSlot {
+    uint32_t key1;   // key + 1; 0 = empty
+    uint32_t pad;
+    u64 val;
+};
+
 struct HubGlobal {
     int32_t nhubs = 0;
     int32_t n_echunks = 0;
@@ -42,8 +52,7 @@ struct HubGlobal {
     const int32_t *schunk_hub = nullptr;  // [n_schunks]
     const int32_t *schunk_s0 = nullptr;   // [n_schunks] first slot
     const int32_t *hub_schunk0 = nullptr; // [nhubs + 1]
-    int32_t *keys = nullptr;              // table keys (-1 = empty)
-    u64 *vals = nullptr;                  // table sums
+    GSlot *slots = nullptr;               // global tables (all-zero between uses)
     u64 *res_g = nullptr;                 // [2 * n_schunks] best gain (lo, hi)
     int32_t *res_c = nullptr;             // [n_schunks] best community
     u64 *res_e = nullptr;                 // [n_schunks] e_own contribution
