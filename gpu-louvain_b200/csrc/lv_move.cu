@@ -1522,7 +1522,9 @@ static void set_attrs_for(DeviceInfo &di) {
     }
     cudaFuncSetAttribute(move_warp_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_SMEM);
 #ifdef LV_WIDE_CARVEOUT
-    // measurement knob: preferred shared-memory share of the 64-bit warp kernel
+    // measurement knob: preferred shared-memory share of the 64-bit warp
+    // kernel (72: three CTAs per SM with 92 KB of L1 instead of four with
+    // 60 KB measured the same, 119.7 ms for the degree > 319 class)
     cudaFuncSetAttribute(move_warp_kernel<WT>, cudaFuncAttributePreferredSharedMemoryCarveout, LV_WIDE_CARVEOUT);
 #endif
     cudaFuncSetAttribute(move_warp_narrow_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, WARP_NSMEM);
