@@ -533,8 +533,9 @@ def run_ours(args, ranks: Ranks):
     ranks.barrier()
     torch.cuda.synchronize()
     # the interpreter's cyclic garbage collector stays out of the timed steps
+    # (disabled, not run first: a full collection here leaves the GPU idle
+    # long enough for its clocks to drop before the first timed step)
     import gc
-    gc.collect()
     gc.disable()
     t0 = time.perf_counter()
     e2e_units = 0
