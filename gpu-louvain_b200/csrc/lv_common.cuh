@@ -35,6 +35,15 @@
 #ifndef LV_U_STAGE
 #define LV_U_STAGE 8
 #endif
+// The insert loops combine a warp's equal keys before their atomics
+// (key_peers: __match_any_sync + __reduce_add_sync): 1 on aggregated levels,
+// 2 at every level, 0 never (the code compiled out), 3 never (the code
+// compiled in, switched off at run time; for measurement).  0 is the
+// default: with 1 the move phase of an R-MAT-24 run took 620 ms instead of
+// 306 ms.
+#ifndef LV_DEDUP
+#define LV_DEDUP 0
+#endif
 // The 64-bit warp kernel sums runs of one community per lane in registers
 // before its table adds (1) or adds every entry (0, the default: 1 measured
 // no faster on R-MAT-24, 121 against 120 ms for the degree > 319 class).
@@ -545,7 +554,7 @@ __device__ __forceinline__ void insert_row(const GraphView<WT> &g, const int32_t
     // dedup (CTA-wide OCC callers only: lane = threadIdx.x, stride a multiple
     // of 32): the loop then runs the same steps in every lane of a warp and a
     // warp's equal keys are combined before the atomics (key_peers)
-    const int32_t wlane = (OCC && dedup) ? (lane & 31) : 0;
+    const int32_t wlane = (LV_DEDUP && OCC && dedup) ? (lane & 31) : 0;
     for (int32_t base = r0 + lane; base - wlane < r1; base += U * stride) {
         int32_t jj[U];
         u64 ww[U];
@@ -564,7 +573,7 @@ __device__ __forceinline__ void insert_row(const GraphView<WT> &g, const int32_t
         for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(comm + jj[u]) : -1;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            if (OCC && dedup) {
+            if (LV_DEDUP && OCC && dedup) {
                 const bool valid = cc[u] >= 0 && cc[u] != own;
                 if (cc[u] >= 0 && cc[u] == own) e_own += ww[u];
                 const unsigned peers = key_peers(cc[u], valid);
@@ -616,7 +625,7 @@ __device__ __forceinline__ void insert_row_piece(const GraphView<WT> &g, const i
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             int32_t claimed = -1;
-            if (OCC && dedup) {
+            if (LV_DEDUP && OCC && dedup) {
                 // equal keys of the warp combined first (see key_peers)
                 const bool valid = cc[u] >= 0 && cc[u] != own;
                 if (cc[u] >= 0 && cc[u] == own) e_own += ww[u];

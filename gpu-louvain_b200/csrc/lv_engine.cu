@@ -55,13 +55,6 @@ using namespace lv;
 #ifndef LV_NARROW_ESCAPES
 #define LV_NARROW_ESCAPES 0
 #endif
-// The insert loops combine a warp's equal keys before their atomics
-// (key_peers: __match_any_sync + __reduce_add_sync): 1 on aggregated levels,
-// 2 at every level, 0 never.  0 is the default: with 1 the move phase of an
-// R-MAT-24 run took 620 ms instead of 306 ms.
-#ifndef LV_DEDUP
-#define LV_DEDUP 0
-#endif
 
 namespace {
 
@@ -507,7 +500,7 @@ bool narrow_weights(const lv_handle *h) {
 StateView state_of(lv_handle *h) {
     return StateView{h->comm, h->newc, h->size, h->k, h->S, h->T, &h->tot_d->err, h->feat,
                      h->cur_w32 && h->wrows_any ? h->wrow : nullptr,
-                     (LV_DEDUP == 2 || (LV_DEDUP && h->level > 0)) ? 1 : 0};
+                     (LV_DEDUP == 2 || (LV_DEDUP == 1 && h->level > 0)) ? 1 : 0};
 }
 
 // ---------------------------------------------------------------------------

@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 int32_t claimed = -1;
-                if (st.dedup) {
+                if (LV_DEDUP && st.dedup) {
                     // equal keys of the warp combined before the atomics
                     const bool valid = cc[u] >= 0 && cc[u] != own;
                     if (cc[u] >= 0 && cc[u] == own) e_own += ww[u];
@@ -522,7 +522,7 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
                 hs[u] = cc[u] >= 0 ? hash_slot(cc[u], lg) : 0u;
                 kk[u] = (cc[u] >= 0 && cc[u] != own) ? ((volatile int32_t *)t.keys)[hs[u]] : -2;
             }
-            if (st.dedup) {
+            if (LV_DEDUP && st.dedup) {
                 // equal keys of the warp combined before the atomics
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
@@ -647,8 +647,8 @@ __global__ void __launch_bounds__(THREADS) move_fallback_kernel(GraphView<WT> g,
             lg = lg < 3 ? 3 : lg;
             if (!PART) {
                 insert_row<LV_U_FB, true>(g, st.comm, v, own, r0, r1, threadIdx.x, THREADS, keys, vals,
-                                          lg, st.err, occ, &nocc, e_own, st.dedup != 0);
-            } else if (st.dedup) {
+                                          lg, st.err, occ, &nocc, e_own, (LV_DEDUP && st.dedup != 0));
+            } else if (LV_DEDUP && st.dedup) {
                 // warp-uniform steps; a warp's equal keys combined first
                 const int lane = threadIdx.x & 31;
                 for (int32_t b = r0 + threadIdx.x - lane; b < r1; b += THREADS) {
@@ -798,7 +798,7 @@ __global__ void __launch_bounds__(THREADS) move_rowq_narrow_kernel(GraphView<WT>
         lg = lg < 3 ? 3 : lg;
         u64 e_own = 0;
         insert_row_piece<LV_U_FB, true>(g, st.comm, v, own, r0, r1, threadIdx.x, THREADS, t, lg, st.err, occ,
-                                        &nocc, OCC_CAP, e_own, st.dedup != 0);
+                                        &nocc, OCC_CAP, e_own, (LV_DEDUP && st.dedup != 0));
         __syncthreads();
         const int32_t nd = min(nocc, OCC_CAP);
         const MoveCtx m = move_ctx(own, __ldg(st.size + own) == 1, st.T, __ldg(st.k + v), __ldg(st.S + own));
@@ -947,7 +947,7 @@ __global__ void __launch_bounds__(THREADS) move_rowq_staged_kernel(GraphView<WT>
             for (int u = 0; u < U; ++u) {
                 const u64 w = cc[u] >= 0 ? raw_value(g, base + u * THREADS, xx[u]) : 0;
                 int32_t claimed = -1;
-                if (st.dedup) {
+                if (LV_DEDUP && st.dedup) {
                     const bool valid = cc[u] >= 0 && cc[u] != own;
                     if (cc[u] >= 0 && cc[u] == own) e_own += w;
                     const unsigned peers = key_peers(cc[u], valid);
@@ -1048,7 +1048,7 @@ __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_narrow_kernel(Graph
         const int32_t own = __ldg(st.comm + v);
         u64 e_own = 0;
         insert_row_piece<LV_U_STAGE, true>(g, st.comm, v, own, e0, e1, threadIdx.x, STAGE_THREADS, t, LLG, st.err,
-                                           locc, &lnocc, STAGE_CHUNK, e_own, st.dedup != 0);
+                                           locc, &lnocc, STAGE_CHUNK, e_own, (LV_DEDUP && st.dedup != 0));
         block_add_total<STAGE_THREADS>(e_own, hg.eown + h);   // contains the barrier
         const int32_t n = min(lnocc, STAGE_CHUNK);
         if (threadIdx.x == 0) base = atomicAdd(hg.nocc + h, n);
@@ -1096,7 +1096,7 @@ __global__ void __launch_bounds__(STAGE_THREADS) giant_stage_kernel(GraphView<WT
         const int32_t own = __ldg(st.comm + v);
         u64 e_own = 0;
         insert_row<LV_U_STAGE, true>(g, st.comm, v, own, e0, e1, threadIdx.x, STAGE_THREADS, lkeys, lvals, LLG,
-                                     st.err, locc, &lnocc, e_own, st.dedup != 0);
+                                     st.err, locc, &lnocc, e_own, (LV_DEDUP && st.dedup != 0));
         block_add_total<STAGE_THREADS>(e_own, hg.eown + h);   // contains the barrier
         const int32_t n = min(lnocc, STAGE_CHUNK);
         if (threadIdx.x == 0) base = atomicAdd(hg.nocc + h, n);
