@@ -40,7 +40,8 @@
 // 2 at every level, 0 never (the code compiled out), 3 never (the code
 // compiled in, switched off at run time; for measurement).  0 is the
 // default: with 1 the move phase of an R-MAT-24 run took 620 ms instead of
-// 306 ms.
+// 306 ms, and merely compiling the code in (3) costs 5 % (256 against 243 ms
+// of move phase: the degree > 319 class 119.8 against 111.6 ms).
 #ifndef LV_DEDUP
 #define LV_DEDUP 0
 #endif
