@@ -306,8 +306,14 @@ struct StateView {
 // gives the carry into the high word.  The final hi:lo equals the 64-bit sum
 // whatever the order of the adds (read it only after they have all
 // completed).  Global tables use the native 64-bit atomic.
+// LV_TABLE_SPACE_CHECK = 0: every table add takes the split form, which is
+// exact in global memory too (a global table then pays two atomics instead
+// of one) and saves the address-space test in the move kernels' inner loops.
+#ifndef LV_TABLE_SPACE_CHECK
+#define LV_TABLE_SPACE_CHECK 1
+#endif
 __device__ __forceinline__ void table_add(u64 *p, u64 w) {
-    if (__isShared(p)) {
+    if (!LV_TABLE_SPACE_CHECK || __isShared(p)) {
         unsigned *q = reinterpret_cast<unsigned *>(p);
         const unsigned lo = (unsigned)w, hi = (unsigned)(w >> 32);
         const unsigned old = atomicAdd(q, lo);
