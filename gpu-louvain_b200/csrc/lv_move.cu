@@ -247,6 +247,14 @@ __device__ __forceinline__ void enqueue_fallback(const FallbackSet &fs, int32_t 
     }
 }
 
+// The 64-bit warp kernel counts its claims after every chunk of 32 entries
+// (0) or once per step of U chunks (1).
+#ifndef LV_CLAIM_PER_STEP
+#define LV_CLAIM_PER_STEP 0
+#endif
+static_assert(!LV_CLAIM_PER_STEP || WARP_LIMIT_MAX + 32 * LV_U_WARP <= WARP_CAP,
+              "claims counted per step fit the warp table");
+
 template <typename WT>
 __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateView st,
                                                         const int32_t *__restrict__ list, int32_t n,
@@ -318,6 +326,7 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
         for (int32_t base = r0 + lane; base < r1 + lane && !overflow; base += 32 * U) {
             int32_t jj[U];
             u64 ww[U];
+            int32_t lclaims = 0;   // LV_CLAIM_PER_STEP: this lane's claims in the step
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int32_t e = base + 32 * u;
@@ -353,8 +362,18 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
                         claimed = table_insert_claim(keys, vals, lg, cc[u], ww[u], st.err);
                     }
                 }
-                nclaim += __popc(__ballot_sync(FULL, claimed >= 0));
-                if (nclaim > fs.warp_limit) { overflow = true; break; }
+                if (LV_CLAIM_PER_STEP) {
+                    lclaims += claimed >= 0 ? 1 : 0;
+                } else {
+                    nclaim += __popc(__ballot_sync(FULL, claimed >= 0));
+                    if (nclaim > fs.warp_limit) { overflow = true; break; }
+                }
+            }
+            if (LV_CLAIM_PER_STEP) {
+                // claims counted once per step: at most warp_limit + 32 U
+                // (<= 512 = WARP_CAP) distinct keys are ever claimed
+                nclaim += (int32_t)__reduce_add_sync(FULL, (unsigned)lclaims);
+                if (nclaim > fs.warp_limit) overflow = true;
             }
         }
         if (LV_WARP_COMBINE && !overflow) {
