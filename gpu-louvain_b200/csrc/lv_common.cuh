@@ -308,7 +308,8 @@ struct StateView {
 // completed).  Global tables use the native 64-bit atomic.
 // LV_TABLE_SPACE_CHECK = 0: every table add takes the split form, which is
 // exact in global memory too (a global table then pays two atomics instead
-// of one) and saves the address-space test in the move kernels' inner loops.
+// of one) and drops the address-space test; it measured no faster (the
+// compiler already resolves the test where the table is known to be shared).
 #ifndef LV_TABLE_SPACE_CHECK
 #define LV_TABLE_SPACE_CHECK 1
 #endif

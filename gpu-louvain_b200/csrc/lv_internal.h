@@ -17,7 +17,10 @@ constexpr int HG_INSERT_THREADS = 512;
 constexpr int HG_INSERT_SMEM = 2 * HG_EDGE_CHUNK * 12;   // chunk-local table
 // move phase, giant vertices: chunks of STAGE_CHUNK edges reduced by
 // STAGE_THREADS-thread CTAs in a 2*STAGE_CHUNK-slot table
-constexpr int STAGE_CHUNK = 2048;
+#ifndef LV_STAGE_CHUNK
+#define LV_STAGE_CHUNK 2048
+#endif
+constexpr int STAGE_CHUNK = LV_STAGE_CHUNK;
 constexpr int STAGE_THREADS = 256;
 constexpr int STAGE_SMEM = 2 * STAGE_CHUNK * 14;
 constexpr int HG_MERGE_THREADS = 1024;
