@@ -17,8 +17,11 @@ constexpr int HG_INSERT_THREADS = 512;
 constexpr int HG_INSERT_SMEM = 2 * HG_EDGE_CHUNK * 12;   // chunk-local table
 // move phase, giant vertices: chunks of STAGE_CHUNK edges reduced by
 // STAGE_THREADS-thread CTAs in a 2*STAGE_CHUNK-slot table
+// entries per staging chunk: 1024 (the persistent staging kernels then hold
+// twice as many CTAs per SM; the giants of an R-MAT-24 run took 50.4 against
+// 51.8 ms with 2048)
 #ifndef LV_STAGE_CHUNK
-#define LV_STAGE_CHUNK 2048
+#define LV_STAGE_CHUNK 1024
 #endif
 constexpr int STAGE_CHUNK = LV_STAGE_CHUNK;
 constexpr int STAGE_THREADS = 256;
