@@ -47,11 +47,12 @@ void launch_gather_cdeg(const int32_t *mstart, const int32_t *P, const int32_t *
 using namespace lv;
 
 // Aggregated levels holding a sum of 2^32 or more: swept with the 64-bit
-// kernels throughout (0), or through the 32-bit view with those rows sent to
-// the large queue (1).  0 is the default: on R-MAT-24 the 32-bit view's piece
-// tables were slower on these levels (298 vs 257 ms of move phase per run),
-// their two atomics per add serialising where many lanes add to one
-// community.
+// kernels on the uint64 sums (0), through the 32-bit view with the narrow
+// (piece-table) kernels and those rows sent to the large queue (1), or
+// through the 32-bit view with the 64-bit-table kernels, escaped sums read
+// from the uint64 copy (2).  0 is the default: on R-MAT-24 mode 1 was slower
+// (298 vs 257 ms of move phase per run), the piece tables' two atomics per
+// add serialising where many lanes add to one community.
 #ifndef LV_NARROW_ESCAPES
 #define LV_NARROW_ESCAPES 0
 #endif
@@ -492,14 +493,16 @@ GraphView<uint32_t> view_of<uint32_t>(lv_handle *h) {
 template <typename WT>
 bool narrow_weights(const lv_handle *h) {
     if (h->opts.wide_weights) return false;
-    if (std::is_same<WT, uint32_t>::value) return true;
+    // the 32-bit view of a level holding escaped sums: narrow kernels (with
+    // the marked rows sent to the large queue) only in mode 1
+    if (std::is_same<WT, uint32_t>::value) return LV_NARROW_ESCAPES == 1 || !h->wrows_any;
     if (std::is_same<WT, float>::value) return h->w0_narrow;
     return false;
 }
 
 StateView state_of(lv_handle *h) {
     return StateView{h->comm, h->newc, h->size, h->k, h->S, h->T, &h->tot_d->err, h->feat,
-                     h->cur_w32 && h->wrows_any ? h->wrow : nullptr,
+                     (LV_NARROW_ESCAPES == 1 && h->cur_w32 && h->wrows_any) ? h->wrow : nullptr,
                      (LV_DEDUP == 2 || (LV_DEDUP == 1 && h->level > 0)) ? 1 : 0};
 }
 
@@ -1402,9 +1405,8 @@ int aggregate_t(lv_handle *h) {
     h->cur_rowend = h->lvl_end[nb];
     h->cur_col = h->lvl_col[nb];
     h->cur_w = h->lvl_w[nb];
-    // LV_NARROW_ESCAPES = 0: a level with escaped sums is swept with the
-    // 64-bit kernels throughout instead of the 32-bit view
-    h->cur_w32 = (h->opts.wide_weights || (!LV_NARROW_ESCAPES && h->wrows_any)) ? nullptr : h->lvl_w32[nb];
+    // mode 0: a level with escaped sums is swept on its uint64 sums
+    h->cur_w32 = (h->opts.wide_weights || (LV_NARROW_ESCAPES == 0 && h->wrows_any)) ? nullptr : h->lvl_w32[nb];
     h->V = newV;
     h->E = newE;
     h->level += 1;
