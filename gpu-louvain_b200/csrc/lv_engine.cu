@@ -50,9 +50,11 @@ using namespace lv;
 // kernels on the uint64 sums (0), through the 32-bit view with the narrow
 // (piece-table) kernels and those rows sent to the large queue (1), or
 // through the 32-bit view with the 64-bit-table kernels, escaped sums read
-// from the uint64 copy (2).  0 is the default: on R-MAT-24 mode 1 was slower
-// (298 vs 257 ms of move phase per run), the piece tables' two atomics per
-// add serialising where many lanes add to one community.
+// from the uint64 copy (2).  0 is the default: on R-MAT-24 the move phase of
+// a run took 241 ms in mode 0, 262 ms in mode 1 (the piece tables' two
+// atomics per add serialise where many lanes add to one community) and
+// 256 ms in mode 2 (the escape test per entry costs more than the 4 bytes
+// per entry it saves).
 #ifndef LV_NARROW_ESCAPES
 #define LV_NARROW_ESCAPES 0
 #endif
