@@ -247,6 +247,11 @@ __device__ __forceinline__ void enqueue_fallback(const FallbackSet &fs, int32_t 
     }
 }
 
+// The 64-bit warp kernel loads a step that lies wholly inside the row
+// without per-entry bound tests (1) or tests every entry (0).
+#ifndef LV_WARP_FULLSTEP
+#define LV_WARP_FULLSTEP 1
+#endif
 // The 64-bit warp kernel counts its claims after every chunk of 32 entries
 // (0) or once per step of U chunks (1, the default: 0.6 ms less per R-MAT-24
 // run, 111.4 against 111.8 ms for the degree > 319 class).
@@ -328,16 +333,28 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
             int32_t jj[U];
             u64 ww[U];
             int32_t lclaims = 0;   // LV_CLAIM_PER_STEP: this lane's claims in the step
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int32_t e = base + 32 * u;
-                jj[u] = -1;
-                ww[u] = 0;
-                if (e < r1) { jj[u] = __ldg(g.col + e); ww[u] = gw(g, e); }
-            }
             int32_t cc[U];
+            if (LV_WARP_FULLSTEP && base - lane + 32 * U <= r1) {
+                // a whole step inside the row (warp-uniform): no bound tests
 #pragma unroll
-            for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(st.comm + jj[u]) : -1;
+                for (int u = 0; u < U; ++u) {
+                    const int32_t e = base + 32 * u;
+                    jj[u] = __ldg(g.col + e);
+                    ww[u] = gw(g, e);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) cc[u] = jj[u] != v ? __ldg(st.comm + jj[u]) : -1;
+            } else {
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int32_t e = base + 32 * u;
+                    jj[u] = -1;
+                    ww[u] = 0;
+                    if (e < r1) { jj[u] = __ldg(g.col + e); ww[u] = gw(g, e); }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(st.comm + jj[u]) : -1;
+            }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 int32_t claimed = -1;
@@ -507,18 +524,33 @@ __global__ void __launch_bounds__(256) move_warp_narrow_kernel(GraphView<WT> g, 
             typename RawOf<WT>::T xx[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) { jj[u] = jn[u]; xx[u] = xn[u]; }
-#else
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int32_t e = b0 + 32 * u;
-                jj[u] = -1;
-                ww[u] = 0;
-                if (e < r1) { jj[u] = ld_row(g.col + e); ww[u] = gw_row(g, e); }
-            }
-#endif
             int32_t cc[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(st.comm + jj[u]) : -1;
+#else
+            int32_t cc[U];
+            if (LV_WARP_FULLSTEP && b0 - lane + 32 * U <= r1) {
+                // a whole step inside the row (warp-uniform): no bound tests
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int32_t e = b0 + 32 * u;
+                    jj[u] = ld_row(g.col + e);
+                    ww[u] = gw_row(g, e);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) cc[u] = jj[u] != v ? __ldg(st.comm + jj[u]) : -1;
+            } else {
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int32_t e = b0 + 32 * u;
+                    jj[u] = -1;
+                    ww[u] = 0;
+                    if (e < r1) { jj[u] = ld_row(g.col + e); ww[u] = gw_row(g, e); }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(st.comm + jj[u]) : -1;
+            }
+#endif
 #if LV_WARP_PIPE
             // the next step's loads go out before this step's inserts
 #pragma unroll
