@@ -51,6 +51,11 @@
 #ifndef LV_WARP_COMBINE
 #define LV_WARP_COMBINE 0
 #endif
+// The row insert loops of the CTA and group kernels load U entries that all
+// lie inside the row without per-entry bound tests (1) or test each (0).
+#ifndef LV_ROW_FULLSTEP
+#define LV_ROW_FULLSTEP 1
+#endif
 // The narrow-weight warp kernel issues the next chunk's column and weight
 // loads before inserting the current chunk (1), or loads each chunk when it
 // gets to it (0, the default: 1 made the degree > 319 class of an R-MAT-24
@@ -566,19 +571,31 @@ __device__ __forceinline__ void insert_row(const GraphView<WT> &g, const int32_t
     for (int32_t base = r0 + lane; base - wlane < r1; base += U * stride) {
         int32_t jj[U];
         u64 ww[U];
+        int32_t cc[U];
+        if (LV_ROW_FULLSTEP && base + (U - 1) * stride < r1) {
+            // all U entries inside the row: no bound tests
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int32_t e = base + u * stride;
-            jj[u] = -1;
-            ww[u] = 0;
-            if (e < r1) {
+            for (int u = 0; u < U; ++u) {
+                const int32_t e = base + u * stride;
                 jj[u] = __ldg(g.col + e);
                 ww[u] = gw(g, e);
             }
-        }
-        int32_t cc[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(comm + jj[u]) : -1;
+            for (int u = 0; u < U; ++u) cc[u] = jj[u] != v ? __ldg(comm + jj[u]) : -1;
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int32_t e = base + u * stride;
+                jj[u] = -1;
+                ww[u] = 0;
+                if (e < r1) {
+                    jj[u] = __ldg(g.col + e);
+                    ww[u] = gw(g, e);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(comm + jj[u]) : -1;
+        }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             if (LV_DEDUP && OCC && dedup) {
@@ -617,19 +634,31 @@ __device__ __forceinline__ void insert_row_piece(const GraphView<WT> &g, const i
     for (int32_t base = r0 + lane; base - wlane < r1; base += U * stride) {
         int32_t jj[U];
         u64 ww[U];
+        int32_t cc[U];
+        if (LV_ROW_FULLSTEP && base + (U - 1) * stride < r1) {
+            // all U entries inside the row: no bound tests
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int32_t e = base + u * stride;
-            jj[u] = -1;
-            ww[u] = 0;
-            if (e < r1) {
+            for (int u = 0; u < U; ++u) {
+                const int32_t e = base + u * stride;
                 jj[u] = __ldg(g.col + e);
                 ww[u] = gw(g, e);
             }
-        }
-        int32_t cc[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(comm + jj[u]) : -1;
+            for (int u = 0; u < U; ++u) cc[u] = jj[u] != v ? __ldg(comm + jj[u]) : -1;
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int32_t e = base + u * stride;
+                jj[u] = -1;
+                ww[u] = 0;
+                if (e < r1) {
+                    jj[u] = __ldg(g.col + e);
+                    ww[u] = gw(g, e);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(comm + jj[u]) : -1;
+        }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             int32_t claimed = -1;
