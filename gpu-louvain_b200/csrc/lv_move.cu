@@ -247,8 +247,9 @@ __device__ __forceinline__ void enqueue_fallback(const FallbackSet &fs, int32_t 
     }
 }
 
-// The 64-bit warp kernel loads a step that lies wholly inside the row
-// without per-entry bound tests (1) or tests every entry (0).
+// The warp kernels load a step that lies wholly inside the row without
+// per-entry bound tests (1, the default: the degree > 319 class of an
+// R-MAT-24 run 107.1 against 111.5 ms) or test every entry (0).
 #ifndef LV_WARP_FULLSTEP
 #define LV_WARP_FULLSTEP 1
 #endif
