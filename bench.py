@@ -559,7 +559,10 @@ def run_ours(args, ranks: Ranks):
             "modularity": qs[-1], "communities": int(ncomm), "levels": levels_run, "sweeps": sweeps_run,
             "edge_sweeps": es_run})
     ms_per_step = secs * 1e3 / args.steps
-    traffic = ncu_traffic(f"rmat{scale}", CLASS_NAMES[dom])
+    # the class sizes depend on giant_degree: the traffic of a tuned setting
+    # is looked up under its own key
+    gd = int(knobs.get("giant_degree", 8192) or 8192)
+    traffic = ncu_traffic(f"rmat{scale}" if gd == 8192 else f"rmat{scale}_g{gd}", CLASS_NAMES[dom])
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
