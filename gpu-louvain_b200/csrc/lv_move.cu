@@ -247,6 +247,11 @@ __device__ __forceinline__ void enqueue_fallback(const FallbackSet &fs, int32_t 
     }
 }
 
+// The 64-bit warp kernel loads the home-slot keys of a step's U entries
+// together before its inserts (1) or probes entry by entry (0).
+#ifndef LV_WIDE_PREFETCH
+#define LV_WIDE_PREFETCH 1
+#endif
 // The warp kernels load a step that lies wholly inside the row without
 // per-entry bound tests (1, the default: the degree > 319 class of an
 // R-MAT-24 run 107.1 against 111.5 ms) or test every entry (0).
@@ -356,6 +361,15 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
 #pragma unroll
                 for (int u = 0; u < U; ++u) cc[u] = (jj[u] >= 0 && jj[u] != v) ? __ldg(st.comm + jj[u]) : -1;
             }
+            // LV_WIDE_PREFETCH: the U home slots and their keys are loaded
+            // together; a key already in its home slot is added without probing
+            uint32_t hs[U];
+            int32_t kk[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                hs[u] = cc[u] >= 0 ? hash_slot(cc[u], lg) : 0u;
+                kk[u] = (LV_WIDE_PREFETCH && cc[u] >= 0 && cc[u] != own) ? ((volatile int32_t *)keys)[hs[u]] : -2;
+            }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 int32_t claimed = -1;
@@ -366,6 +380,13 @@ __global__ void __launch_bounds__(256) move_warp_kernel(GraphView<WT> g, StateVi
                     const unsigned peers = key_peers(cc[u], valid);
                     const u64 ws = group_sum_u64(peers, valid ? ww[u] : 0);
                     if (valid && group_leader(peers)) claimed = table_insert_claim(keys, vals, lg, cc[u], ws, st.err);
+                } else if (LV_WIDE_PREFETCH && !LV_WARP_COMBINE) {
+                    // home-slot key loaded with the step's other U (below)
+                    if (cc[u] >= 0) {
+                        if (cc[u] == own) e_own += ww[u];
+                        else if (kk[u] == cc[u]) table_add(vals + hs[u], ww[u]);
+                        else claimed = table_insert_claim(keys, vals, lg, cc[u], ww[u], st.err);
+                    }
                 } else if (cc[u] >= 0) {
                     if (cc[u] == own) {
                         e_own += ww[u];
