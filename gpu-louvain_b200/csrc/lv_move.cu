@@ -248,9 +248,11 @@ __device__ __forceinline__ void enqueue_fallback(const FallbackSet &fs, int32_t 
 }
 
 // The 64-bit warp kernel loads the home-slot keys of a step's U entries
-// together before its inserts (1) or probes entry by entry (0).
+// together before its inserts (1) or probes entry by entry (0, the default:
+// 1 measured 0.3 ms slower per R-MAT-24 run, the degree > 319 class 0.4 ms
+// faster and degrees 33-319 0.5 ms slower).
 #ifndef LV_WIDE_PREFETCH
-#define LV_WIDE_PREFETCH 1
+#define LV_WIDE_PREFETCH 0
 #endif
 // The warp kernels load a step that lies wholly inside the row without
 // per-entry bound tests (1, the default: the degree > 319 class of an
