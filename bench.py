@@ -272,6 +272,9 @@ def ncu_class_split(csv_path: str) -> dict:
             launches[lid]["bytes"] += v
 
     def short(n):
+        # names as ncu prints them by default or with --kernel-name-base
+        # demangled (template arguments then carry casts such as "(int)4")
+        n = re.sub(r"\((int|bool|unsigned int)\)", "", n)
         n = re.sub(r"\(.*", "", n)
         return n.replace("void ", "").replace("lv::<unnamed>::", "").replace("<unnamed>::", "").strip()
 
