@@ -837,7 +837,12 @@ def learned_summary(args, ranks: Ranks):
             "max_abs_dq": line["max_abs_dq"], "target": "speed-up >= 1.5 at |dQ| <= 1e-3",
             "per_graph": [{"mu": r["mu"], "plain_ms": round(r["plain_ms"], 2), "learned_ms": round(r["learned_ms"], 2),
                            "speedup": round(r["speedup"], 3), "dq": r["dq"],
-                           "recall": r["learned"]["recall"], "fell_back": r["learned"]["fell_back"]}
+                           "recall": r["learned"]["recall"], "fell_back": r["learned"]["fell_back"],
+                           "sweeps": {"plain": r["plain"]["sweeps"], "learned": r["learned"]["sweeps"],
+                                      "learned_full": r["learned"]["full_sweeps"],
+                                      "learned_active": r["learned"]["active_sweeps"]},
+                           "move_ms": {"plain": r["plain"]["device_ms_per_run"]["move_ms"],
+                                       "learned": r["learned"]["device_ms_per_run"]["move_ms"]}}
                           for r in line["per_graph"]],
             "settings": {k: line["config"][k] for k in ("full_every", "active_start", "min_recall")},
             "note": "plain vs learned on the same handle options, best of 2 timed runs each; "
@@ -952,8 +957,15 @@ def run_lfr(args, ranks: Ranks):
                 st = e.stats()
                 a = e.active_stats()
                 m, nc = e.original_to_community()
+            # device time per run by phase (the engine's coarse CUDA-event
+            # counters): in learned mode move_ms also holds the active sweeps
+            per_run = {k: round(st[k] / args.steps, 3)
+                       for k in ("move_ms", "modularity_ms", "aggregate_ms", "setup_ms")}
             res[mode] = {"s": min(ts), "q": q, "communities": int(nc),
                          "levels": st["levels"] // args.steps, "sweeps": st["sweeps"] // args.steps,
+                         "device_ms_per_run": per_run,
+                         "kernel_launches_per_run": st["kernel_launches"] // args.steps,
+                         "active_sweeps": a["active_sweeps"] // args.steps if mode == "learned" else None,
                          "evaluated_per_run": a["evaluated"] // args.steps if mode == "learned" else None,
                          "full_sweeps": a["full_sweeps"] // args.steps if mode == "learned" else None,
                          "recall": a["last_recall"] if mode == "learned" else None,
