@@ -81,17 +81,23 @@ def tune(graph=None, *, device_csr=None, device: int = 0, min_gain: float = 1e-6
 
     best = dict(DEFAULT)
     best_ms = default_ms = measure(best)
+    # every setting is timed once: the warp-limit pass skips the setting the
+    # giant-degree pass already timed (the chosen giant degree at the
+    # default warp limit), also after another warp limit has been kept
+    seen = {(best["giant_degree"], best["warp_limit"])}
     for gd in giant_degrees:
-        if gd == best["giant_degree"]:
+        if (gd, best["warp_limit"]) in seen:
             continue
         k = {"giant_degree": gd, "warp_limit": best["warp_limit"]}
+        seen.add((gd, k["warp_limit"]))
         ms = measure(k)
         if ms < best_ms * (1.0 - min_gain_frac):
             best, best_ms = k, ms
     for wl in warp_limits:
-        if wl == best["warp_limit"]:
+        if (best["giant_degree"], wl) in seen:
             continue
         k = {"giant_degree": best["giant_degree"], "warp_limit": wl}
+        seen.add((k["giant_degree"], wl))
         ms = measure(k)
         if ms < best_ms * (1.0 - min_gain_frac):
             best, best_ms = k, ms
@@ -102,8 +108,25 @@ def tune(graph=None, *, device_csr=None, device: int = 0, min_gain: float = 1e-6
            "default_ms": round(default_ms, 3), "trials": trials, "key": key, "cached": False}
     if cache:
         store[key] = {k: v for k, v in out.items() if k != "cached"}
-        tmp = cache + ".tmp"
-        with open(tmp, "w") as f:
+        _write_cache(cache, store)
+    return out
+
+
+def _write_cache(cache: str, store: dict) -> None:
+    """Replace the cache file atomically.  Each writer uses its own temporary
+    file in the cache's directory, so ranks that tune at the same time (one
+    process per GPU) never rename each other's half-written file; the last
+    complete write wins."""
+    import tempfile
+    d = os.path.dirname(os.path.abspath(cache))
+    fd, tmp = tempfile.mkstemp(prefix=os.path.basename(cache) + ".", suffix=".tmp", dir=d)
+    try:
+        with os.fdopen(fd, "w") as f:
             json.dump(store, f, indent=1)
         os.replace(tmp, cache)
-    return out
+    except BaseException:
+        try:
+            os.unlink(tmp)
+        except OSError:
+            pass
+        raise
