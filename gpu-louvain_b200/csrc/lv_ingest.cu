@@ -121,9 +121,14 @@ extern "C" int lv_csr_from_entries_device(int32_t device, int32_t V, int64_t nnz
         ING_CHECK(cudaMemcpyAsync(ww, w, sizeof(float) * n, cudaMemcpyHostToDevice, s));
         ING_CHECK(cudaMemsetAsync(cnt + n, 0, sizeof(int32_t), s));
         entry_count_kernel<<<grid, 256, 0, s>>>(a, b, nnz, V, cnt, err);
-        ING_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt, pos, (int64_t)nnz + 1, s));
+        // the directed total reaches 2 nnz, beyond int32 for nnz >= 2^30: the
+        // scan accumulates in int64 (an ExclusiveSum would accumulate in the
+        // int32 input type and wrap before the E check below)
+        ING_CHECK(cub::DeviceScan::ExclusiveScan(nullptr, tmp_bytes, cnt, pos, ::cuda::std::plus<>{}, (int64_t)0,
+                                                 (int64_t)nnz + 1, s));
         ING_CHECK(cudaMalloc(&tmp, tmp_bytes));
-        ING_CHECK(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, pos, (int64_t)nnz + 1, s));
+        ING_CHECK(cub::DeviceScan::ExclusiveScan(tmp, tmp_bytes, cnt, pos, ::cuda::std::plus<>{}, (int64_t)0,
+                                                 (int64_t)nnz + 1, s));
         ING_CHECK(cudaMemcpyAsync(&E, pos + nnz, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
         ING_CHECK(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s));
         ING_CHECK(cudaStreamSynchronize(s));
