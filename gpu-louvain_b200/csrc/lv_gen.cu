@@ -93,12 +93,14 @@ int lv_gen_rmat_device(int32_t scale, int32_t edge_factor, uint64_t seed, double
     const lvrng::RmatParams p = lvrng::rmat_params(scale, a, b, c, seed);
     u64 *k1 = nullptr, *k2 = nullptr;
     void *tmp = nullptr;
-    int32_t *dlo = nullptr, *dhi = nullptr, *rp = nullptr, *cl = nullptr, *nsel = nullptr;
+    int32_t *dlo = nullptr, *dhi = nullptr, *rp = nullptr, *cl = nullptr;
+    // the distinct-key count is 64-bit: edge_factor << scale reaches 2^31 and more
+    int64_t *nsel = nullptr;
     float *wt = nullptr;
     size_t tmp_bytes = 0, t1 = 0, t2 = 0, t3 = 0;
     int rc = LV_OK;
     int64_t nk = 0;
-    int h_nsel = 0;
+    int64_t h_nsel = 0;
     const unsigned grid = 148 * 16;
 #define GEN_CHECK(x)                                  \
     do {                                              \
@@ -106,7 +108,7 @@ int lv_gen_rmat_device(int32_t scale, int32_t edge_factor, uint64_t seed, double
     } while (0)
     GEN_CHECK(cudaMalloc(&k1, sizeof(u64) * (size_t)n));
     GEN_CHECK(cudaMalloc(&k2, sizeof(u64) * (size_t)n));
-    GEN_CHECK(cudaMalloc(&nsel, sizeof(int) * 2));
+    GEN_CHECK(cudaMalloc(&nsel, sizeof(int64_t) * 2));
     rmat_draw_kernel<<<grid, 256>>>(p, n, k1);
     cub::DeviceRadixSort::SortKeys(nullptr, t1, k1, k2, (int64_t)n, 0, bits);
     cub::DeviceSelect::Unique(nullptr, t2, k2, k1, nsel, (int64_t)n);
@@ -116,7 +118,7 @@ int lv_gen_rmat_device(int32_t scale, int32_t edge_factor, uint64_t seed, double
     GEN_CHECK(cudaMalloc(&tmp, tmp_bytes));
     GEN_CHECK(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, k1, k2, (int64_t)n, 0, bits));
     GEN_CHECK(cub::DeviceSelect::Unique(tmp, tmp_bytes, k2, k1, nsel, (int64_t)n));
-    GEN_CHECK(cudaMemcpy(&h_nsel, nsel, sizeof(int), cudaMemcpyDeviceToHost));
+    GEN_CHECK(cudaMemcpy(&h_nsel, nsel, sizeof(int64_t), cudaMemcpyDeviceToHost));
     nk = h_nsel;
     {
         // drop the self-loop marker (the largest key) if present
