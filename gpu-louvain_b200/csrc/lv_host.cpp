@@ -334,6 +334,11 @@ int read_mtx_entries(const char *path, int32_t *Vout, std::vector<int32_t> &ea, 
         return LV_ERR_IO;
     if (cols < 0 || nnz < 0) return LV_ERR_IO;
     if (cols > 0x7ffffffeLL) return LV_ERR_TOO_LARGE;
+    // an entry takes at least 4 bytes ("1 2" and a line break; the last may
+    // lack the break), so a size line that promises more entries than the
+    // rest of the file can hold is a short file: rejected before the entry
+    // arrays are sized by it
+    if (nnz > (long long)((size_t)(end - p) / 4) + 1) return LV_ERR_IO;
     const int32_t V = (int32_t)cols;
     ea.resize((size_t)nnz);
     eb.resize((size_t)nnz);
@@ -356,6 +361,9 @@ float reference_m(const std::vector<int32_t> &ea, const std::vector<int32_t> &eb
     return M / 2;
 }
 
+int read_mtx_host_csr(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr_out, int32_t **col_out,
+                      float **w_out, float *m_ref);
+
 }  // namespace
 
 extern "C" {
@@ -363,6 +371,21 @@ extern "C" {
 int lv_read_mtx(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr_out,
                 int32_t **col_out, float **w_out, float *m_ref) {
     if (!path || !Vout || !Eout || !rowptr_out || !col_out || !w_out) return LV_ERR_INVALID;
+    try {
+        return read_mtx_host_csr(path, Vout, Eout, rowptr_out, col_out, w_out, m_ref);
+    } catch (const std::bad_alloc &) {
+        return LV_ERR_NOMEM;
+    }
+}
+
+}  // extern "C"
+
+namespace {
+
+// lv_read_mtx's body; its vectors may throw std::bad_alloc, which the entry
+// point turns into LV_ERR_NOMEM
+int read_mtx_host_csr(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr_out, int32_t **col_out,
+                      float **w_out, float *m_ref) {
     int32_t V = 0;
     std::vector<int32_t> ea, eb;
     std::vector<float> ew;
@@ -386,6 +409,7 @@ int lv_read_mtx(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr
     }
     M /= 2;
     if (E > 0x7fffffffLL) return LV_ERR_TOO_LARGE;
+    std::vector<int64_t> cur((size_t)V);   // before the mallocs: a throw here leaks nothing
     int32_t *rp = (int32_t *)std::malloc(sizeof(int32_t) * ((size_t)V + 1));
     int32_t *cl = (int32_t *)std::malloc(sizeof(int32_t) * (size_t)(E > 0 ? E : 1));
     float *wt = (float *)std::malloc(sizeof(float) * (size_t)(E > 0 ? E : 1));
@@ -399,7 +423,6 @@ int lv_read_mtx(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr
         acc += deg[(size_t)v];
     }
     rp[V] = (int32_t)acc;
-    std::vector<int64_t> cur((size_t)V);
     for (int32_t v = 0; v < V; ++v) cur[(size_t)v] = rp[v];
     // rows keep file order (utils.cu:50-59)
     for (long long i = 0; i < nnz; ++i) {
@@ -422,6 +445,10 @@ int lv_read_mtx(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr
     if (m_ref) *m_ref = M;
     return LV_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int lv_read_mtx_entries(const char *path, int32_t *Vout, int64_t *nnz_out, int32_t **v1, int32_t **v2, float **w) {
     if (!path || !Vout || !nnz_out || !v1 || !v2 || !w) return LV_ERR_INVALID;

@@ -70,6 +70,47 @@ def test_reader_edge_cases(lvb, orc, tmp_path):
     assert r5.V == 0 and r5.E == 0
 
 
+HDR = "%%MatrixMarket matrix coordinate real symmetric\n"
+
+
+@pytest.mark.parametrize("name,text,status", [
+    # a size line promising more entries than the file can hold: an I/O error,
+    # not an attempt to size the entry arrays by it
+    ("huge_nnz", HDR + "3 3 99999999999999\n1 2 1.0\n", 7),
+    ("short_file", HDR + "3 3 5\n1 2 1.0\n", 7),
+    ("truncated_entry", HDR + "3 3 2\n1 2 1.0\n2", 7),
+    ("missing_weight", HDR + "3 3 1\n1 2\n", 7),
+    ("bad_weight", HDR + "3 3 1\n1 2 abc\n", 7),
+    ("negative_size", HDR + "3 -5 1\n1 2 1.0\n", 7),
+    ("no_size_line", HDR, 7),
+    ("zero_index", HDR + "3 3 1\n0 2 1.0\n", 1),
+    ("negative_index", HDR + "3 3 1\n-1 2 1.0\n", 1),
+    ("index_past_v", HDR + "3 3 1\n1 4 1.0\n", 1),
+    ("index_overflows_int64", HDR + "3 3 1\n1 99999999999999999999 1.0\n", 1),
+    ("entries_without_vertices", HDR + "0 0 1\n1 1 1.0\n", 1),
+    ("vertices_past_int32", HDR + "3 2147483648 1\n1 2 1.0\n", 3),
+])
+def test_reader_rejects_malformed_files(lvb, tmp_path, name, text, status):
+    p = tmp_path / (name + ".mtx")
+    p.write_text(text)
+    with pytest.raises(lvb.LouvainError) as ei:
+        lvb.read_mtx(str(p))
+    assert ei.value.status == status
+
+
+def test_reader_line_endings_and_separators(lvb, tmp_path):
+    ref = None
+    for name, text in (("lf", HDR + "3 3 2\n1 2 1.0\n2 3 2.0\n"),
+                       ("crlf", HDR.replace("\n", "\r\n") + "3 3 2\r\n1 2 1.0\r\n2 3 2.0\r\n"),
+                       ("tabs", HDR + "3\t3\t2\n1\t2\t1.0\n2\t3\t2.0\n"),
+                       ("no_final_break", HDR + "3 3 2\n1 2 1.0\n2 3 2.0")):
+        p = tmp_path / (name + ".mtx")
+        p.write_text(text)
+        g = lvb.read_mtx(str(p))
+        got = (list(g.rowptr), list(g.col), list(g.w))
+        assert got == ([0, 1, 3, 4], [1, 0, 2, 1], [1.0, 1.0, 2.0, 2.0]), name
+
+
 def test_print_communities_format(lvb, tmp_path):
     # printOriginalToCommunity: V_final, then "c+1 members+1..." for every
     # community id (empty ones included), members in increasing id
