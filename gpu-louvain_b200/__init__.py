@@ -292,13 +292,22 @@ def write_mtx(path: str, g: Graph) -> None:
                               _ptr(w, C.c_float)))
 
 
+def _weight_mode(weights: str) -> int:
+    """Generator weight mode: "unit" (every weight 1) or "uniform" (uniform in
+    [0.5, 1.5) on a 2^-24 grid)."""
+    modes = {"unit": 0, "uniform": 1}
+    if weights not in modes:
+        raise ValueError(f"weights must be 'unit' or 'uniform', not {weights!r}")
+    return modes[weights]
+
+
 def gen_rmat(scale: int, edge_factor: int = 16, seed: int = 1, a: float = 0.57, b: float = 0.19,
              c: float = 0.19, weights: str = "uniform") -> Graph:
     L = lib()
     V = C.c_int32()
     E = C.c_int64()
     rp, cl, w = P32(), P32(), PF()
-    _check(L.lv_gen_rmat(scale, edge_factor, seed, a, b, c, 1 if weights == "uniform" else 0,
+    _check(L.lv_gen_rmat(scale, edge_factor, seed, a, b, c, _weight_mode(weights),
                          C.byref(V), C.byref(E), C.byref(rp), C.byref(cl), C.byref(w)))
     return Graph(_take_host(rp, V.value + 1, np.int32), _take_host(cl, E.value, np.int32),
                  _take_host(w, E.value, np.float32))
@@ -309,7 +318,7 @@ def gen_planted(V: int = 10000, blocks: int = 64, d_in: float = 16.0, d_out: flo
     L = lib()
     E = C.c_int64()
     rp, cl, w = P32(), P32(), PF()
-    _check(L.lv_gen_planted(V, blocks, d_in, d_out, seed, 1 if weights == "uniform" else 0,
+    _check(L.lv_gen_planted(V, blocks, d_in, d_out, seed, _weight_mode(weights),
                             C.byref(E), C.byref(rp), C.byref(cl), C.byref(w)))
     return Graph(_take_host(rp, V + 1, np.int32), _take_host(cl, E.value, np.int32),
                  _take_host(w, E.value, np.float32))
@@ -330,7 +339,7 @@ def gen_planted_batch(params, weights: str = "unit"):
     rp, cl, w, gp = P32(), P32(), PF(), P32()
     _check(lib().lv_gen_planted_batch(G, _ptr(Vs, C.c_int32), _ptr(Bs, C.c_int32), _ptr(di, C.c_double),
                                       _ptr(do, C.c_double), _ptr(sd, C.c_uint64),
-                                      1 if weights == "uniform" else 0, C.byref(Vt), C.byref(Et), C.byref(rp),
+                                      _weight_mode(weights), C.byref(Vt), C.byref(Et), C.byref(rp),
                                       C.byref(cl), C.byref(w), C.byref(gp)))
     return (_take_host(rp, Vt.value + 1, np.int32), _take_host(cl, Et.value, np.int32),
             _take_host(w, Et.value, np.float32), _take_host(gp, G + 1, np.int32))
@@ -373,7 +382,7 @@ def gen_rmat_device(scale: int, edge_factor: int = 16, seed: int = 1, a: float =
     V = C.c_int32()
     E = C.c_int64()
     rp, cl, w = C.c_void_p(), C.c_void_p(), C.c_void_p()
-    _check(L.lv_gen_rmat_device(scale, edge_factor, seed, a, b, c, 1 if weights == "uniform" else 0,
+    _check(L.lv_gen_rmat_device(scale, edge_factor, seed, a, b, c, _weight_mode(weights),
                                 device, C.byref(V), C.byref(E), C.byref(rp), C.byref(cl), C.byref(w)))
     return DeviceGraph(V.value, E.value, rp.value, cl.value, w.value, device)
 

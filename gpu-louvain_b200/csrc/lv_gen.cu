@@ -84,7 +84,8 @@ void lv_free_device(void *p) {
 int lv_gen_rmat_device(int32_t scale, int32_t edge_factor, uint64_t seed, double a, double b,
                        double c, int32_t weight_mode, int32_t device, int32_t *Vout, int64_t *Eout,
                        int32_t **d_rowptr, int32_t **d_col, float **d_w) {
-    if (scale < 1 || scale > 30 || edge_factor < 1 || !Vout || !Eout || !d_rowptr || !d_col || !d_w)
+    if (scale < 1 || scale > 30 || edge_factor < 1 || !Vout || !Eout || !d_rowptr || !d_col || !d_w ||
+        !lvrng::rmat_probabilities_ok(a, b, c))
         return LV_ERR_INVALID;
     if (cudaSetDevice(device) != cudaSuccess) return LV_ERR_NO_DEVICE;
     const int64_t n = (int64_t)edge_factor << scale;

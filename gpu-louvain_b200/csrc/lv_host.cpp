@@ -704,11 +704,9 @@ int keys_to_csr(const std::vector<uint64_t> &keys, int sh, int32_t V, int32_t we
 
 extern "C" {
 
-int lv_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed, double a, double b, double c,
-                int32_t weight_mode, int32_t *Vout, int64_t *Eout, int32_t **rowptr, int32_t **col,
-                float **w) {
-    if (scale < 1 || scale > 30 || edge_factor < 1 || !Vout || !Eout || !rowptr || !col || !w)
-        return LV_ERR_INVALID;
+static int gen_rmat_body(int32_t scale, int32_t edge_factor, uint64_t seed, double a, double b, double c,
+                         int32_t weight_mode, int32_t *Vout, int64_t *Eout, int32_t **rowptr, int32_t **col,
+                         float **w) {
     const int64_t n = (int64_t)edge_factor << scale;
     const lvrng::RmatParams rp = lvrng::rmat_params(scale, a, b, c, seed);
     std::vector<uint64_t> keys((size_t)n);
@@ -748,6 +746,19 @@ int lv_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed, double a, dou
     return rc;
 }
 
+int lv_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed, double a, double b, double c,
+                int32_t weight_mode, int32_t *Vout, int64_t *Eout, int32_t **rowptr, int32_t **col,
+                float **w) {
+    if (scale < 1 || scale > 30 || edge_factor < 1 || !Vout || !Eout || !rowptr || !col || !w ||
+        !lvrng::rmat_probabilities_ok(a, b, c))
+        return LV_ERR_INVALID;
+    try {
+        return gen_rmat_body(scale, edge_factor, seed, a, b, c, weight_mode, Vout, Eout, rowptr, col, w);
+    } catch (const std::bad_alloc &) {
+        return LV_ERR_NOMEM;
+    }
+}
+
 }  // extern "C"
 
 namespace {
@@ -756,7 +767,10 @@ namespace {
 // draw; false for invalid arguments.
 bool planted_keys(int32_t V, int32_t blocks, double d_in, double d_out, uint64_t seed,
                   std::vector<uint64_t> &keys) {
-    if (V < 1 || blocks < 1 || blocks > V || d_in < 0 || d_out < 0) return false;
+    if (V < 1 || blocks < 1 || blocks > V || !(d_in >= 0.0) || !(d_out >= 0.0)) return false;
+    // the draws of a graph whose CSR could hold int32 offsets at most
+    // (2 entries per pair); NaN and infinite degrees fail here too
+    if (!((double)V * (d_in + d_out) / 2.0 <= (double)(1ll << 30))) return false;
     const int64_t m_in = (int64_t)std::llround((double)V * d_in / 2.0);
     const int64_t m_out = (int64_t)std::llround((double)V * d_out / 2.0);
     keys.clear();
@@ -782,9 +796,13 @@ extern "C" {
 int lv_gen_planted(int32_t V, int32_t blocks, double d_in, double d_out, uint64_t seed,
                    int32_t weight_mode, int64_t *Eout, int32_t **rowptr, int32_t **col, float **w) {
     if (!Eout || !rowptr || !col || !w) return LV_ERR_INVALID;
-    std::vector<uint64_t> keys;
-    if (!planted_keys(V, blocks, d_in, d_out, seed, keys)) return LV_ERR_INVALID;
-    return keys_to_csr(keys, 32, V, weight_mode, seed, Eout, rowptr, col, w);
+    try {
+        std::vector<uint64_t> keys;
+        if (!planted_keys(V, blocks, d_in, d_out, seed, keys)) return LV_ERR_INVALID;
+        return keys_to_csr(keys, 32, V, weight_mode, seed, Eout, rowptr, col, w);
+    } catch (const std::bad_alloc &) {
+        return LV_ERR_NOMEM;
+    }
 }
 
 int lv_gen_planted_batch(int32_t G, const int32_t *V, const int32_t *blocks, const double *d_in,
@@ -879,13 +897,32 @@ int lv_gen_planted_batch(int32_t G, const int32_t *V, const int32_t *blocks, con
 // pairs are dropped, and vertex ids are a random permutation of the
 // community order.  Unit weights.  comm_out (may be NULL) receives each
 // vertex's planted community (malloc'd, V entries).
+static int gen_lfr_body(int32_t V, double tau1, double mean_degree, int32_t kmax, double tau2, int32_t cmin,
+                        int32_t cmax, double mu, uint64_t seed, int64_t *Eout, int32_t **rowptr, int32_t **col,
+                        float **w, int32_t **comm_out);
+
 int lv_gen_lfr(int32_t V, double tau1, double mean_degree, int32_t kmax, double tau2, int32_t cmin,
                int32_t cmax, double mu, uint64_t seed, int64_t *Eout, int32_t **rowptr, int32_t **col,
                float **w, int32_t **comm_out) {
-    if (V < 2 || tau1 <= 1.0 || tau2 <= 1.0 || mean_degree < 1.0 || kmax < 2 || cmin < 2 || cmax < cmin ||
-        mu < 0.0 || mu > 1.0 || !Eout || !rowptr || !col || !w)
+    // the comparisons are written so that NaN fails them
+    if (V < 2 || !(tau1 > 1.0 && tau1 < 1e3) || !(tau2 > 1.0 && tau2 < 1e3) || !(mean_degree >= 1.0) ||
+        kmax < 2 || cmin < 2 || cmax < cmin || !(mu >= 0.0 && mu <= 1.0) || !Eout || !rowptr || !col || !w)
         return LV_ERR_INVALID;
     if (V >= (1 << 26)) return LV_ERR_TOO_LARGE;
+    // about V * mean_degree stubs, one CSR entry each: more than an int32 CSR
+    // holds is too large (and a huge mean would only exhaust host memory)
+    if ((double)V * mean_degree > (double)(1ll << 30)) return LV_ERR_TOO_LARGE;
+    try {
+        return gen_lfr_body(V, tau1, mean_degree, kmax, tau2, cmin, cmax, mu, seed, Eout, rowptr, col, w,
+                            comm_out);
+    } catch (const std::bad_alloc &) {
+        return LV_ERR_NOMEM;
+    }
+}
+
+static int gen_lfr_body(int32_t V, double tau1, double mean_degree, int32_t kmax, double tau2, int32_t cmin,
+                        int32_t cmax, double mu, uint64_t seed, int64_t *Eout, int32_t **rowptr, int32_t **col,
+                        float **w, int32_t **comm_out) {
     // continuous power-law sample on [a, b] with exponent t from u in [0, 1)
     auto plaw = [](double u, double a, double b, double t) {
         const double e = 1.0 - t;

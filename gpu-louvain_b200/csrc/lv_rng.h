@@ -41,6 +41,13 @@ struct RmatParams {
     uint64_t keys[16];
 };
 
+// Valid quadrant probabilities: a, b, c >= 0 and d = 1 - a - b - c > 0 (the
+// thresholds below are 32-bit fixed-point cumulative sums, so a + b + c must
+// stay below 1); NaN fails every comparison.
+inline bool rmat_probabilities_ok(double a, double b, double c) {
+    return a >= 0.0 && b >= 0.0 && c >= 0.0 && a + b + c < 1.0;
+}
+
 inline RmatParams rmat_params(int scale, double a, double b, double c, uint64_t seed) {
     RmatParams p;
     p.scale = scale;

@@ -265,3 +265,35 @@ def test_print_communities_large_matches_python(lvb, tmp_path):
         mem = order[bounds[c]:bounds[c + 1]] + 1
         lines.append(" ".join([str(c + 1)] + [str(x) for x in mem]))
     assert open(p).read() == "\n".join(lines) + "\n"
+
+
+@pytest.mark.parametrize("name,call,status", [
+    ("rmat_scale_0", lambda L: L.gen_rmat(0), 1),
+    ("rmat_scale_31", lambda L: L.gen_rmat(31), 1),
+    ("rmat_edge_factor_0", lambda L: L.gen_rmat(5, 0), 1),
+    ("rmat_probabilities_over_1", lambda L: L.gen_rmat(5, a=0.5, b=0.3, c=0.3), 1),
+    ("rmat_probability_negative", lambda L: L.gen_rmat(5, a=0.7, b=-0.1, c=0.2), 1),
+    ("rmat_probability_nan", lambda L: L.gen_rmat(5, a=float("nan")), 1),
+    ("planted_no_vertices", lambda L: L.gen_planted(0, 1, 1.0, 1.0, 0, "unit"), 1),
+    ("planted_more_blocks_than_vertices", lambda L: L.gen_planted(10, 100, 1.0, 1.0, 0, "unit"), 1),
+    ("planted_negative_degree", lambda L: L.gen_planted(100, 4, -1.0, 1.0, 0, "unit"), 1),
+    ("planted_nan_degree", lambda L: L.gen_planted(100, 4, float("nan"), 1.0, 0, "unit"), 1),
+    # more draws than an int32 CSR can hold: refused before any array is sized
+    ("planted_huge_degree", lambda L: L.gen_planted(100, 4, 1e9, 1.0, 0, "unit"), 1),
+    ("lfr_mu_above_1", lambda L: L.gen_lfr(1000, 1.5), 1),
+    ("lfr_mu_nan", lambda L: L.gen_lfr(1000, float("nan")), 1),
+    ("lfr_tau1_1", lambda L: L.gen_lfr(1000, 0.3, tau1=1.0), 1),
+    ("lfr_cmin_above_cmax", lambda L: L.gen_lfr(1000, 0.3, cmin=500, cmax=50), 1),
+    ("lfr_vertices_past_2_26", lambda L: L.gen_lfr(1 << 26, 0.3), 3),
+    ("lfr_stubs_past_int32", lambda L: L.gen_lfr(1 << 20, 0.3, mean_degree=5000.0, kmax=10000), 3),
+])
+def test_generators_reject_bad_arguments(lvb, name, call, status):
+    with pytest.raises(lvb.LouvainError) as ei:
+        call(lvb)
+    assert ei.value.status == status
+
+
+def test_generator_weight_names(lvb):
+    with pytest.raises(ValueError):
+        lvb.gen_planted(100, 4, 4.0, 1.0, 0, "uniformly")
+    assert set(lvb.gen_planted(100, 4, 4.0, 1.0, 0, "unit").w.tolist()) == {1.0}
