@@ -108,3 +108,92 @@ def test_committed_traffic_is_keyed_by_threshold():
         d = json.load(f)
     for key in ("rmat24", "rmat24_g16384"):
         assert d[key]["b6_deg8192"]["class_launches"] == 34
+
+
+class _FakeEngine:
+    """Stands in for the Louvain handle: the counters run_lfr reads, with the
+    learned mode taking fewer, cheaper sweeps."""
+
+    def __init__(self, graph, device=0, **kw):
+        self.learned = bool(kw.get("active_set"))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+    def set_active_model(self, model, thr):
+        pass
+
+    def reset(self):
+        pass
+
+    def clear_stats(self):
+        pass
+
+    def run(self, min_gain):
+        return 0.5 if not self.learned else 0.4999
+
+    def stats(self):
+        f = 0.5 if self.learned else 1.0
+        return {"levels": 2 * 2, "sweeps": 2 * (30 if self.learned else 20), "move_ms": 2 * 60.0 * f,
+                "modularity_ms": 2.0, "aggregate_ms": 8.0, "setup_ms": 0.4, "kernel_launches": 1600}
+
+    def active_stats(self):
+        return {"evaluated": 2 * 1000, "full_sweeps": 2 * 10, "active_sweeps": 2 * 18, "last_recall": 0.97,
+                "fell_back": False}
+
+    def original_to_community(self):
+        import numpy as np
+        return np.zeros(4, np.int32), 1
+
+
+class _FakePkg:
+    Louvain = _FakeEngine
+
+    @staticmethod
+    def load_active_model(path=None):
+        import numpy as np
+        return np.zeros(113, np.uint16), -2.7
+
+    @staticmethod
+    def gen_lfr(V, mu, seed=0, **kw):
+        class G:
+            pass
+        g = G()
+        g.V, g.E = V, 20 * V
+        return g, None
+
+
+def test_learned_summary_schema(monkeypatch):
+    """The default bench line's `learned` block (built from run_lfr's records)
+    carries per graph the speed-up, modularity difference, recall, sweep
+    counts and move-phase times."""
+    import types
+    import torch
+    b = load_bench()
+    monkeypatch.setattr(b, "load_pkg", lambda: _FakePkg)
+    monkeypatch.setattr(torch.cuda, "set_device", lambda d: None)
+
+    class _Clock:
+        def __init__(self, gpu):
+            pass
+
+        def start(self):
+            pass
+
+        def stop(self):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+
+    monkeypatch.setattr(b, "ClockSampler", _Clock)
+    args = types.SimpleNamespace(active_model=None, lfr_vertices=1000, steps=3, warmup=3)
+    s = b.learned_summary(args, b.Ranks())
+    assert s["target"] == "speed-up >= 1.5 at |dQ| <= 1e-3"
+    assert len(s["per_graph"]) == 3
+    for r in s["per_graph"]:
+        assert r["speedup"] > 0 and abs(r["dq"]) < 1e-3
+        assert r["sweeps"] == {"plain": 20, "learned": 30, "learned_full": 10, "learned_active": 18}
+        assert r["move_ms"] == {"plain": 60.0, "learned": 30.0}
+        assert r["recall"] == 0.97 and r["fell_back"] is False
+    assert set(s["settings"]) == {"full_every", "active_start", "min_recall"}
