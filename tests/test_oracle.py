@@ -52,6 +52,69 @@ def test_isolated_and_self_loops(orc, gnp):
     assert orc.modularity_f64(rp, cl, w, o2c) == pytest.approx(q, abs=1e-12)
 
 
+def ring_of_cliques(k, s, gnp):
+    """k cliques of s vertices (unit weights), clique c's last vertex joined to
+    clique c+1's first (mod k)."""
+    edges = []
+    for c in range(k):
+        b = c * s
+        edges += [(b + i, b + j, 1.0) for i in range(s) for j in range(i + 1, s)]
+        edges.append((b + s - 1, ((c + 1) % k) * s, 1.0))
+    return csr(k * s, edges, gnp)
+
+
+def test_ring_of_cliques(orc, gnp):
+    # 6 cliques of 5: one community per clique, Q = sum over cliques of
+    # l/m - (d/2m)^2 with l = 10 internal edges, d = 22, m = 66
+    rp, cl, w = ring_of_cliques(6, 5, gnp)
+    o = orc.Oracle(rp, cl, w, 1)
+    q, _ = o.run(1e-6)
+    m = o.original_to_community()
+    assert [len(set(m[c * 5:(c + 1) * 5])) for c in range(6)] == [1] * 6
+    assert len(set(m.tolist())) == 6
+    assert q == pytest.approx(6 * (10 / 66 - (22 / 132) ** 2), abs=1e-15)
+    # 8 cliques of 4: the synchronous sub-rounds end in a local optimum that
+    # keeps every clique whole but merges one adjacent pair: 7 communities,
+    # Q = 13/56 - (28/112)^2 + 6 (6/56 - (14/112)^2) = 23/32 (one community per
+    # clique would give 41/56)
+    rp, cl, w = ring_of_cliques(8, 4, gnp)
+    o = orc.Oracle(rp, cl, w, 1)
+    q, _ = o.run(1e-6)
+    m = o.original_to_community()
+    assert all(len(set(m[c * 4:(c + 1) * 4])) == 1 for c in range(8))
+    labels = [m[c * 4] for c in range(8)]
+    assert len(set(labels)) == 7
+    pair = [c for c in range(8) if labels.count(labels[c]) == 2]
+    assert len(pair) == 2 and (pair[1] - pair[0]) % 8 in (1, 7)
+    assert q == pytest.approx(23 / 32, abs=1e-15)
+    # 30 triangles: past the resolution limit (k > s(s-1) + 2) merging
+    # adjacent cliques raises Q above one community per clique
+    rp, cl, w = ring_of_cliques(30, 3, gnp)
+    o = orc.Oracle(rp, cl, w, 1)
+    q, _ = o.run(1e-6)
+    m = o.original_to_community()
+    assert all(len(set(m[c * 3:(c + 1) * 3])) == 1 for c in range(30))
+    assert len(set(m.tolist())) < 30
+    assert q > 30 * (3 / 120 - (8 / 240) ** 2)
+
+
+def test_duplicate_edge_mtx(orc, lvb, tmp_path):
+    """A repeated entry is kept twice, as the reference's reader appends every
+    line (utils.cu:50-59): it counts twice in k, in T and in e_own."""
+    p = tmp_path / "dup.mtx"
+    p.write_text("%%MatrixMarket matrix coordinate real symmetric\n3 3 3\n2 1 1\n2 1 1\n3 2 1\n")
+    rp, cl, w, _ = orc.read_mtx(str(p))
+    assert list(rp) == [0, 2, 5, 6] and list(cl) == [1, 1, 0, 0, 2, 1]
+    r = lvb.read_mtx(str(p))
+    assert np.array_equal(r.rowptr, rp) and np.array_equal(r.col, cl) and np.array_equal(r.w, w)
+    # partition {0, 1}, {2}: T = 6, e_own = 4, S = (2 + 3, 1)
+    q = orc.modularity_f64(rp, cl, w, np.array([0, 0, 2], np.int32))
+    assert q == pytest.approx(4 / 6 - (25 + 1) / 36, abs=1e-15)
+    o = orc.Oracle(rp, cl, w, 1)
+    o.set_communities(np.array([0, 0, 2], np.int32))
+    assert o.modularity() == q
+
+
 def test_scale_rule(orc):
     rc, s, ex = orc.choose_scale(np.array([1.0, 2.0, 3.0], np.float32))
     assert (rc, s, ex) == (0, 0, True)
