@@ -523,21 +523,77 @@ int lv_write_mtx(const char *path, int32_t V, int64_t n_edges, const int32_t *u,
 // threads into their own buffers (ranges of about equal member counts), then
 // written in order.  Every buffer is allocated before the threads start, so
 // an allocation failure returns LV_ERR_NOMEM instead of ending the process.
+// Stable LSD radix sort of n 64-bit keys on bits [lo, hi), 8 bits per pass,
+// all host threads.  The buffers are left uninitialised so that the threads
+// that fill them also fault their pages in (a zero-filled std::vector would
+// touch every page from one thread first).
+static void radix_sort_key_bits(std::unique_ptr<uint64_t[]> &a, size_t n, int lo, int hi) {
+    if (n < 2 || hi <= lo) return;
+    std::unique_ptr<uint64_t[]> b(new uint64_t[n]);
+    const int nt = omp_get_max_threads() > 0 ? omp_get_max_threads() : 1;
+    std::vector<size_t> hist((size_t)nt * 256);
+    for (int shift = lo; shift < hi; shift += 8) {
+        std::fill(hist.begin(), hist.end(), 0);
+#pragma omp parallel num_threads(nt)
+        {
+            const int t = omp_get_thread_num();
+            const size_t i0 = n * t / nt, i1 = n * (t + 1) / nt;
+            size_t *h = hist.data() + (size_t)t * 256;
+            for (size_t i = i0; i < i1; ++i) h[(a[i] >> shift) & 255]++;
+        }
+        size_t run = 0;
+        for (int d = 0; d < 256; ++d)
+            for (int t = 0; t < nt; ++t) {
+                const size_t c = hist[(size_t)t * 256 + d];
+                hist[(size_t)t * 256 + d] = run;
+                run += c;
+            }
+#pragma omp parallel num_threads(nt)
+        {
+            const int t = omp_get_thread_num();
+            const size_t i0 = n * t / nt, i1 = n * (t + 1) / nt;
+            size_t *h = hist.data() + (size_t)t * 256;
+            for (size_t i = i0; i < i1; ++i) b[h[(a[i] >> shift) & 255]++] = a[i];
+        }
+        a.swap(b);
+    }
+}
+
 static int print_communities_impl(const char *path, const int32_t *orig2comm, int32_t V0,
                                   int32_t num_communities) {
-    // counting sort of the vertices by community (members in increasing id)
-    std::vector<int64_t> start((size_t)num_communities + 1, 0);
+    // vertices grouped by community with members in increasing id: keys
+    // (community << 32 | vertex) in vertex order, stably sorted on the
+    // community bits only (the same order as a counting sort, built by all
+    // host threads)
+    const size_t nv = V0 > 0 ? (size_t)V0 : 1;
+    std::unique_ptr<uint64_t[]> key(new uint64_t[nv]);
+    int bad = 0;
+#pragma omp parallel for reduction(| : bad) schedule(static)
     for (int32_t v = 0; v < V0; ++v) {
         const int32_t c = orig2comm[v];
-        if (c < 0 || c >= num_communities) return LV_ERR_INVALID;
-        start[(size_t)c + 1]++;
+        if (c < 0 || c >= num_communities) bad = 1;
+        key[(size_t)v] = ((uint64_t)(uint32_t)c << 32) | (uint32_t)v;
     }
-    for (int32_t c = 0; c < num_communities; ++c) start[(size_t)c + 1] += start[(size_t)c];
-    std::vector<int32_t> mem((size_t)V0);
+    if (bad) return LV_ERR_INVALID;
+    int cbits = 0;
+    while (cbits < 31 && ((int64_t)1 << cbits) < (int64_t)num_communities) ++cbits;
+    radix_sort_key_bits(key, (size_t)V0, 32, 32 + cbits);
+    // start[c] = first position whose community is >= c (empty communities
+    // get an empty range); mem = the members in that order
+    std::unique_ptr<int64_t[]> start(new int64_t[(size_t)num_communities + 1]);
+    std::unique_ptr<int32_t[]> mem(new int32_t[nv]);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)V0; ++i) {
+        const int32_t c = (int32_t)(key[(size_t)i] >> 32);
+        mem[(size_t)i] = (int32_t)(uint32_t)key[(size_t)i];
+        const int32_t prev = i > 0 ? (int32_t)(key[(size_t)i - 1] >> 32) : -1;
+        for (int32_t x = prev + 1; x <= c; ++x) start[(size_t)x] = i;
+    }
     {
-        std::vector<int64_t> pos(start.begin(), start.end() - 1);
-        for (int32_t v = 0; v < V0; ++v) mem[(size_t)pos[(size_t)orig2comm[v]]++] = v;
+        const int32_t last = V0 > 0 ? (int32_t)(key[(size_t)V0 - 1] >> 32) : -1;
+        for (int32_t x = last + 1; x <= num_communities; ++x) start[(size_t)x] = V0;
     }
+    key.reset();
     const int T = omp_get_max_threads() > 0 ? omp_get_max_threads() : 1;
     const int64_t per = ((int64_t)V0 + num_communities) / T + 1;
     std::vector<int32_t> cut((size_t)T + 1, num_communities);
@@ -555,16 +611,33 @@ static int print_communities_impl(const char *path, const int32_t *orig2comm, in
                                  char[(size_t)(start[(size_t)c1] - start[(size_t)c0] + (c1 - c0)) * 12]);
         if (!buf[(size_t)t]) return LV_ERR_NOMEM;
     }
-    // decimal digits of x >= 0 at p; returns the end
+    // decimal digits of x >= 0 at p, two per division from a table of
+    // "00".."99"; returns the end
+    static const char kPairs[201] =
+        "00010203040506070809101112131415161718192021222324252627282930313233343536373839"
+        "40414243444546474849505152535455565758596061626364656667686970717273747576777879"
+        "8081828384858687888990919293949596979899";
     auto put_int = [](char *p, int64_t x) {
-        char tmp[24];
-        int n = 0;
-        do {
-            tmp[n++] = (char)('0' + x % 10);
-            x /= 10;
-        } while (x > 0);
-        while (n > 0) *p++ = tmp[--n];
-        return p;
+        uint64_t u = (uint64_t)x;
+        int n = 1;
+        for (uint64_t t = u; t >= 10; t /= 10) ++n;
+        char *const e = p + n;
+        char *q = e;
+        while (u >= 100) {
+            const unsigned r = (unsigned)(u % 100);
+            u /= 100;
+            q -= 2;
+            q[0] = kPairs[2 * r];
+            q[1] = kPairs[2 * r + 1];
+        }
+        if (u >= 10) {
+            q -= 2;
+            q[0] = kPairs[2 * u];
+            q[1] = kPairs[2 * u + 1];
+        } else {
+            *--q = (char)('0' + u);
+        }
+        return e;
     };
     std::vector<size_t> len((size_t)T, 0);
 #pragma omp parallel for num_threads(T) schedule(static, 1)
@@ -667,6 +740,7 @@ int keys_to_csr(const std::vector<uint64_t> &keys, int sh, int32_t V, int32_t we
         dhi[(size_t)a]++;   // a's larger neighbours
         dlo[(size_t)b]++;   // b's smaller neighbours
     }
+    std::vector<int64_t> clo((size_t)V), chi((size_t)V);   // before the mallocs: a throw leaks nothing
     int32_t *rp = (int32_t *)std::malloc(sizeof(int32_t) * ((size_t)V + 1));
     int32_t *cl = (int32_t *)std::malloc(sizeof(int32_t) * (size_t)(E > 0 ? E : 1));
     float *wt = (float *)std::malloc(sizeof(float) * (size_t)(E > 0 ? E : 1));
@@ -675,7 +749,6 @@ int keys_to_csr(const std::vector<uint64_t> &keys, int sh, int32_t V, int32_t we
         return LV_ERR_NOMEM;
     }
     int64_t acc = 0;
-    std::vector<int64_t> clo((size_t)V), chi((size_t)V);
     for (int32_t v = 0; v < V; ++v) {
         rp[v] = (int32_t)acc;
         clo[(size_t)v] = acc;
