@@ -57,14 +57,81 @@ inline bool parse_i64(const char *&p, const char *end, long long *out) {
     return true;
 }
 
+// Fast path of the decimal -> float conversion: a token of the form
+// [+-]digits[.digits][(e|E)[+-]digits] with at most 19 significant digits
+// whose value m * 10^k has m < 2^53 and |k| <= 22.  Then m and 10^|k| are
+// exact doubles and one multiplication or division gives d, the double
+// nearest the decimal value x (Clinger's fast path).  Rounding d to float
+// gives the float nearest x unless d is exactly halfway between two
+// adjacent floats (a boundary that d can reach by rounding while x lies on
+// one side of it): every midpoint is a double, so for any other d, x and d
+// lie on the same side of every midpoint.  Returns false (the caller uses
+// strtof) for every other token, a midpoint d, or a d outside the normal
+// float range.
+inline bool fast_f32(const char *p, const char *q, float *out) {
+    static const double kPow10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,  1e8,  1e9,  1e10, 1e11,
+                                      1e12, 1e13, 1e14, 1e15, 1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
+    bool neg = false;
+    if (p < q && (*p == '+' || *p == '-')) { neg = *p == '-'; ++p; }
+    uint64_t m = 0;
+    int sig = 0, frac = 0, digits = 0;
+    for (; p < q && *p >= '0' && *p <= '9'; ++p, ++digits) {
+        if (m == 0 && *p == '0') continue;   // leading zeros
+        if (++sig > 19) return false;
+        m = m * 10 + (uint64_t)(*p - '0');
+    }
+    if (p < q && *p == '.') {
+        for (++p; p < q && *p >= '0' && *p <= '9'; ++p, ++digits) {
+            ++frac;
+            if (m == 0 && *p == '0') continue;
+            if (++sig > 19) return false;
+            m = m * 10 + (uint64_t)(*p - '0');
+        }
+    }
+    if (digits == 0) return false;
+    int ex = 0;
+    if (p < q && (*p == 'e' || *p == 'E')) {
+        ++p;
+        bool eneg = false;
+        if (p < q && (*p == '+' || *p == '-')) { eneg = *p == '-'; ++p; }
+        if (p >= q || *p < '0' || *p > '9') return false;
+        for (; p < q && *p >= '0' && *p <= '9'; ++p) {
+            if (ex > 1000) return false;
+            ex = ex * 10 + (*p - '0');
+        }
+        if (eneg) ex = -ex;
+    }
+    if (p != q) return false;
+    if (m == 0) {
+        *out = neg ? -0.0f : 0.0f;
+        return true;
+    }
+    const int k = ex - frac;
+    if (m >= (1ull << 53) || k < -22 || k > 22) return false;
+    const double d = k >= 0 ? (double)m * kPow10[k] : (double)m / kPow10[-k];
+    uint64_t bits;
+    std::memcpy(&bits, &d, sizeof bits);
+    const int e2 = (int)((bits >> 52) & 0x7ff) - 1023;
+    if (e2 < -126 || e2 > 127) return false;                 // subnormal or overflowing float
+    if ((bits & 0x1fffffffull) == 0x10000000ull) return false;   // a float midpoint
+    const float f = (float)d;
+    *out = neg ? -f : f;
+    return true;
+}
+
 // Decimal -> float with the rounding of strtof (the reference reads with
-// `file >> w` into a float).  The token is copied to a NUL-terminated buffer.
+// `file >> w` into a float): the fast path above, else strtof on the token
+// copied to a NUL-terminated buffer.
 inline bool parse_f32(const char *&p, const char *end, float *out) {
     p = skip_ws(p, end);
     const char *q = p;
     while (q < end && !(*q == ' ' || *q == '\t' || *q == '\r' || *q == '\n')) ++q;
     size_t len = (size_t)(q - p);
     if (len == 0 || len > 120) return false;
+    if (fast_f32(p, q, out)) {
+        p = q;
+        return true;
+    }
     char buf[128];
     std::memcpy(buf, p, len);
     buf[len] = 0;
@@ -292,10 +359,31 @@ int lv_read_csr(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr
 
 namespace {
 
+// The entries of a Matrix Market file in malloc'd arrays, freed with the
+// object unless released to a caller.  They are not initialised when
+// allocated: the parsing threads fault their pages in as they fill them.
+struct Entries {
+    int32_t *a = nullptr, *b = nullptr;
+    float *w = nullptr;
+    size_t n = 0;
+    Entries() = default;
+    Entries(const Entries &) = delete;
+    Entries &operator=(const Entries &) = delete;
+    ~Entries() { std::free(a); std::free(b); std::free(w); }
+    bool alloc(size_t k) {
+        const size_t c = k > 0 ? k : 1;
+        a = (int32_t *)std::malloc(sizeof(int32_t) * c);
+        b = (int32_t *)std::malloc(sizeof(int32_t) * c);
+        w = (float *)std::malloc(sizeof(float) * c);
+        n = k;
+        return a && b && w;
+    }
+    void release() { a = b = nullptr; w = nullptr; }
+};
+
 // The header and the entries of a Matrix Market file, in file order
 // (0-based): the vertex count is the size line's second number.
-int read_mtx_entries(const char *path, int32_t *Vout, std::vector<int32_t> &ea, std::vector<int32_t> &eb,
-                     std::vector<float> &ew) {
+int read_mtx_entries(const char *path, int32_t *Vout, Entries &en) {
     Mapped m;
     m.fd = open(path, O_RDONLY);
     if (m.fd < 0) return LV_ERR_IO;
@@ -340,11 +428,9 @@ int read_mtx_entries(const char *path, int32_t *Vout, std::vector<int32_t> &ea, 
     // arrays are sized by it
     if (nnz > (long long)((size_t)(end - p) / 4) + 1) return LV_ERR_IO;
     const int32_t V = (int32_t)cols;
-    ea.resize((size_t)nnz);
-    eb.resize((size_t)nnz);
-    ew.resize((size_t)nnz);
-    int prc = parse_entries_parallel(p, end, nnz, pattern, V, ea.data(), eb.data(), ew.data());
-    if (prc == PARSE_SEQUENTIAL) prc = parse_entries(p, end, nnz, pattern, V, ea.data(), eb.data(), ew.data());
+    if (!en.alloc((size_t)nnz)) return LV_ERR_NOMEM;
+    int prc = parse_entries_parallel(p, end, nnz, pattern, V, en.a, en.b, en.w);
+    if (prc == PARSE_SEQUENTIAL) prc = parse_entries(p, end, nnz, pattern, V, en.a, en.b, en.w);
     if (prc != LV_OK) return prc;
     *Vout = V;
     return LV_OK;
@@ -352,11 +438,11 @@ int read_mtx_entries(const char *path, int32_t *Vout, std::vector<int32_t> &ea, 
 
 // M as the reference accumulates it: a sequential float sum of every entry's
 // weight, counted twice for off-diagonal entries, halved (utils.cu:36-46).
-float reference_m(const std::vector<int32_t> &ea, const std::vector<int32_t> &eb, const std::vector<float> &ew) {
+float reference_m(const Entries &en) {
     float M = 0;
-    for (size_t i = 0; i < ea.size(); ++i) {
-        if (ea[i] != eb[i]) M += ew[i];
-        M += ew[i];
+    for (size_t i = 0; i < en.n; ++i) {
+        if (en.a[i] != en.b[i]) M += en.w[i];
+        M += en.w[i];
     }
     return M / 2;
 }
@@ -387,11 +473,12 @@ namespace {
 int read_mtx_host_csr(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr_out, int32_t **col_out,
                       float **w_out, float *m_ref) {
     int32_t V = 0;
-    std::vector<int32_t> ea, eb;
-    std::vector<float> ew;
-    const int prc = read_mtx_entries(path, &V, ea, eb, ew);
+    Entries en;
+    const int prc = read_mtx_entries(path, &V, en);
     if (prc != LV_OK) return prc;
-    const long long nnz = (long long)ea.size();
+    const long long nnz = (long long)en.n;
+    const int32_t *ea = en.a, *eb = en.b;
+    const float *ew = en.w;
     // degrees: v1 gets (v2,w); v2 gets (v1,w) unless self-loop (utils.cu:32-46)
     std::vector<int64_t> deg((size_t)V + 1, 0);
     int64_t E = 0;
@@ -453,31 +540,19 @@ extern "C" {
 int lv_read_mtx_entries(const char *path, int32_t *Vout, int64_t *nnz_out, int32_t **v1, int32_t **v2, float **w) {
     if (!path || !Vout || !nnz_out || !v1 || !v2 || !w) return LV_ERR_INVALID;
     int32_t V = 0;
-    std::vector<int32_t> ea, eb;
-    std::vector<float> ew;
+    Entries en;
     try {
-        const int prc = read_mtx_entries(path, &V, ea, eb, ew);
+        const int prc = read_mtx_entries(path, &V, en);
         if (prc != LV_OK) return prc;
     } catch (const std::bad_alloc &) {
         return LV_ERR_NOMEM;
     }
-    const size_t n = ea.size() > 0 ? ea.size() : 1;
-    int32_t *a = (int32_t *)std::malloc(sizeof(int32_t) * n), *b = (int32_t *)std::malloc(sizeof(int32_t) * n);
-    float *x = (float *)std::malloc(sizeof(float) * n);
-    if (!a || !b || !x) {
-        std::free(a); std::free(b); std::free(x);
-        return LV_ERR_NOMEM;
-    }
-    if (!ea.empty()) {
-        std::memcpy(a, ea.data(), sizeof(int32_t) * ea.size());
-        std::memcpy(b, eb.data(), sizeof(int32_t) * eb.size());
-        std::memcpy(x, ew.data(), sizeof(float) * ew.size());
-    }
     *Vout = V;
-    *nnz_out = (int64_t)ea.size();
-    *v1 = a;
-    *v2 = b;
-    *w = x;
+    *nnz_out = (int64_t)en.n;
+    *v1 = en.a;
+    *v2 = en.b;
+    *w = en.w;
+    en.release();   // the caller frees them (lv_free_host)
     return LV_OK;
 }
 
@@ -485,19 +560,18 @@ int lv_read_mtx_device(const char *path, int32_t device, int32_t *Vout, int64_t 
                        int32_t **d_col, float **d_w, float *m_ref) {
     if (!path || !Vout || !Eout || !d_rowptr || !d_col || !d_w) return LV_ERR_INVALID;
     int32_t V = 0;
-    std::vector<int32_t> ea, eb;
-    std::vector<float> ew;
+    Entries en;
     try {
-        const int prc = read_mtx_entries(path, &V, ea, eb, ew);
+        const int prc = read_mtx_entries(path, &V, en);
         if (prc != LV_OK) return prc;
     } catch (const std::bad_alloc &) {
         return LV_ERR_NOMEM;
     }
-    const int rc = lv_csr_from_entries_device(device, V, (int64_t)ea.size(), ea.data(), eb.data(), ew.data(), Eout,
-                                              d_rowptr, d_col, d_w);
+    const int rc = lv_csr_from_entries_device(device, V, (int64_t)en.n, en.a, en.b, en.w, Eout, d_rowptr, d_col,
+                                              d_w);
     if (rc != LV_OK) return rc;
     *Vout = V;
-    if (m_ref) *m_ref = reference_m(ea, eb, ew);
+    if (m_ref) *m_ref = reference_m(en);
     return LV_OK;
 }
 

@@ -297,3 +297,72 @@ def test_generator_weight_names(lvb):
     with pytest.raises(ValueError):
         lvb.gen_planted(100, 4, 4.0, 1.0, 0, "uniformly")
     assert set(lvb.gen_planted(100, 4, 4.0, 1.0, 0, "unit").w.tolist()) == {1.0}
+
+
+def _weight_tokens(n_random=120000, seed=3):
+    """Decimal tokens of many shapes: printed float32 values, random digit
+    strings with exponents, decimal forms of values next to float midpoints,
+    and edge forms (signs, bare points, subnormal and overflowing values)."""
+    rng = np.random.default_rng(seed)
+    toks = []
+    f = rng.uniform(-1.0, 1.0, n_random // 4).astype(np.float32) * np.float32(10.0) ** rng.integers(-12, 12, n_random // 4)
+    for i, x in enumerate(f.tolist()):
+        toks.append(("%.9g", "%.8g", "%.17g", "%e")[i % 4] % x)
+    for _ in range(n_random // 4):
+        nd = int(rng.integers(1, 21))
+        digits = "".join(str(int(d)) for d in rng.integers(0, 10, nd))
+        cut = int(rng.integers(0, nd + 1))
+        tok = digits[:cut] + "." + digits[cut:] if cut < nd else digits
+        if rng.random() < 0.5:
+            tok += "e%d" % int(rng.integers(-30, 31))
+        toks.append(tok)
+    # values at and next to float midpoints (the halfway points are exact doubles)
+    base = rng.uniform(0.5, 2.0, n_random // 8).astype(np.float32) * np.float32(2.0) ** rng.integers(-100, 100, n_random // 8)
+    up = np.nextafter(base, np.float32(np.inf))
+    mid = (base.astype(np.float64) + up.astype(np.float64)) / 2.0
+    for x in mid.tolist():
+        toks.append("%.17g" % x)
+        toks.append("%.16g" % x)
+        toks.append("%.25g" % x)
+        toks.append(repr(float(np.nextafter(x, np.inf))))
+    toks += ["0", "-0", "0.0", "-0.000", ".5", "5.", "+1", "1e0", "1E+2", "2.5e-3", "1e-45", "1.4e-45",
+             "1.17549435e-38", "1.1754942e-38", "3.4028235e38", "3.4028236e38", "1e39", "123456789012345678",
+             "1234567890123456789012", "0.000000000000000000000000001", "9007199254740993", "16777217",
+             "0.1", "0.2", "0.3", "1.23782778", "1.5abc", "inf", "nan", "0x1p3"]
+    return toks
+
+
+def _strtof(tokens):
+    import ctypes as C
+    libc = C.CDLL("libc.so.6")
+    libc.strtof.restype = C.c_float
+    libc.strtof.argtypes = [C.c_char_p, C.c_void_p]
+    return np.array([libc.strtof(t.encode(), None) for t in tokens], np.float32)
+
+
+@pytest.mark.parametrize("parallel", [False, True])
+def test_reader_weights_round_like_strtof(lvb, tmp_path, parallel):
+    """Every weight token reads as the float strtof gives (the reference reads
+    weights with `>>` into a float): the reader's fast decimal path and its
+    strtof fall-back together, on the sequential reading (small file) and on
+    the multi-threaded one (over 4 MB and 100,000 entries)."""
+    import ctypes as C
+    toks = _weight_tokens(200000 if parallel else 4000)
+    n = len(toks)
+    p = tmp_path / "w.mtx"
+    with open(p, "w") as f:
+        f.write("%%%%MatrixMarket matrix coordinate real symmetric\n5 5 %d\n" % n)
+        for i, t in enumerate(toks):
+            f.write("%d %d %s\n" % (1 + i % 5, 1 + (i * 7 + 1) % 5, t))
+    if parallel:
+        assert os.path.getsize(p) > (1 << 22)
+    L = lvb.lib()
+    V, m = C.c_int32(), C.c_int64()
+    a, b, w = C.POINTER(C.c_int32)(), C.POINTER(C.c_int32)(), C.POINTER(C.c_float)()
+    assert L.lv_read_mtx_entries(str(p).encode(), C.byref(V), C.byref(m), C.byref(a), C.byref(b), C.byref(w)) == 0
+    assert m.value == n
+    got = np.ctypeslib.as_array(w, shape=(n,)).copy()
+    for x in (a, b, w):
+        L.lv_free_host(C.cast(x, C.c_void_p))
+    want = _strtof(toks)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
