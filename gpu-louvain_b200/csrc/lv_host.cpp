@@ -479,25 +479,57 @@ int read_mtx_host_csr(const char *path, int32_t *Vout, int64_t *Eout, int32_t **
     const long long nnz = (long long)en.n;
     const int32_t *ea = en.a, *eb = en.b;
     const float *ew = en.w;
-    // degrees: v1 gets (v2,w); v2 gets (v1,w) unless self-loop (utils.cu:32-46)
-    std::vector<int64_t> deg((size_t)V + 1, 0);
-    int64_t E = 0;
-    float M = 0;
-    for (long long i = 0; i < nnz; ++i) {
-        const int32_t a = ea[(size_t)i], b = eb[(size_t)i];
-        deg[(size_t)a]++;
-        E++;
-        if (a != b) {
-            deg[(size_t)b]++;
-            E++;
-            M += ew[(size_t)i];
+    // entry "v1 v2 w" gives row v1 the pair (v2, w) and, unless it is a
+    // self-loop, row v2 the pair (v1, w); each row keeps file order
+    // (utils.cu:32-59).  T threads take contiguous ranges of entries: each
+    // counts its pairs per row, the counts become per-thread offsets inside
+    // each row (thread t's pairs of a row follow those of threads < t), and
+    // each thread writes its range in order.  Fewer threads when the
+    // per-thread counts would pass 1 GB.
+    const float M = reference_m(en);
+    int T = omp_get_max_threads() > 0 ? omp_get_max_threads() : 1;
+    if (T > 32) T = 32;
+    if (nnz < (1 << 16)) T = 1;
+    while (T > 1 && (double)T * (double)V * 4.0 > (double)(1ll << 30)) T /= 2;
+    const size_t Vs = (size_t)V;
+    std::unique_ptr<uint32_t[]> cnt(new uint32_t[(size_t)T * Vs + 1]);
+    std::unique_ptr<int64_t[]> deg(new int64_t[Vs + 1]);
+    auto range = [&](int t, long long *lo, long long *hi) {
+        *lo = nnz * t / T;
+        *hi = nnz * (t + 1) / T;
+    };
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+    for (int t = 0; t < T; ++t) {
+        uint32_t *c = cnt.get() + (size_t)t * Vs;
+        std::fill(c, c + Vs, 0u);
+        long long lo, hi;
+        range(t, &lo, &hi);
+        for (long long i = lo; i < hi; ++i) {
+            const int32_t a = ea[(size_t)i], b = eb[(size_t)i];
+            c[(size_t)a]++;
+            if (a != b) c[(size_t)b]++;
         }
-        M += ew[(size_t)i];
     }
-    M /= 2;
+    int64_t E = 0;
+#pragma omp parallel for num_threads(T) schedule(static) reduction(+ : E)
+    for (int64_t v = 0; v < (int64_t)V; ++v) {
+        int64_t d = 0;
+        for (int t = 0; t < T; ++t) d += cnt[(size_t)t * Vs + (size_t)v];
+        deg[(size_t)v] = d;
+        E += d;
+    }
     if (E > 0x7fffffffLL) return LV_ERR_TOO_LARGE;
-    std::vector<int64_t> cur((size_t)V);   // before the mallocs: a throw here leaks nothing
-    int32_t *rp = (int32_t *)std::malloc(sizeof(int32_t) * ((size_t)V + 1));
+    // per-thread offsets inside each row (every partial sum is <= E < 2^31)
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (int64_t v = 0; v < (int64_t)V; ++v) {
+        uint32_t run = 0;
+        for (int t = 0; t < T; ++t) {
+            const uint32_t c = cnt[(size_t)t * Vs + (size_t)v];
+            cnt[(size_t)t * Vs + (size_t)v] = run;
+            run += c;
+        }
+    }
+    int32_t *rp = (int32_t *)std::malloc(sizeof(int32_t) * (Vs + 1));
     int32_t *cl = (int32_t *)std::malloc(sizeof(int32_t) * (size_t)(E > 0 ? E : 1));
     float *wt = (float *)std::malloc(sizeof(float) * (size_t)(E > 0 ? E : 1));
     if (!rp || !cl || !wt) {
@@ -510,18 +542,22 @@ int read_mtx_host_csr(const char *path, int32_t *Vout, int64_t *Eout, int32_t **
         acc += deg[(size_t)v];
     }
     rp[V] = (int32_t)acc;
-    for (int32_t v = 0; v < V; ++v) cur[(size_t)v] = rp[v];
-    // rows keep file order (utils.cu:50-59)
-    for (long long i = 0; i < nnz; ++i) {
-        const int32_t a = ea[(size_t)i], b = eb[(size_t)i];
-        const float wv = ew[(size_t)i];
-        int64_t pa = cur[(size_t)a]++;
-        cl[pa] = b;
-        wt[pa] = wv;
-        if (a != b) {
-            int64_t pb = cur[(size_t)b]++;
-            cl[pb] = a;
-            wt[pb] = wv;
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+    for (int t = 0; t < T; ++t) {
+        uint32_t *c = cnt.get() + (size_t)t * Vs;
+        long long lo, hi;
+        range(t, &lo, &hi);
+        for (long long i = lo; i < hi; ++i) {
+            const int32_t a = ea[(size_t)i], b = eb[(size_t)i];
+            const float wv = ew[(size_t)i];
+            const int64_t pa = (int64_t)rp[a] + c[(size_t)a]++;
+            cl[pa] = b;
+            wt[pa] = wv;
+            if (a != b) {
+                const int64_t pb = (int64_t)rp[b] + c[(size_t)b]++;
+                cl[pb] = a;
+                wt[pb] = wv;
+            }
         }
     }
     *Vout = V;
