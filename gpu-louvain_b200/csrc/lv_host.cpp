@@ -620,19 +620,43 @@ int lv_write_mtx(const char *path, int32_t V, int64_t n_edges, const int32_t *u,
     std::setvbuf(f, buf.data(), _IOFBF, buf.size());
     std::fprintf(f, "%%%%MatrixMarket matrix coordinate real symmetric\n");
     std::fprintf(f, "%d %d %lld\n", V, V, (long long)n_edges);
-    for (int64_t i = 0; i < n_edges; ++i) {
-        int32_t a = u[i], b = v[i];
-        if (a < b) std::swap(a, b);
-        std::fprintf(f, "%d %d %.9g\n", a + 1, b + 1, w ? (double)w[i] : 1.0);
+    // lines "a b w" (larger id first, 1-based, %.9g: the float reads back
+    // exactly) formatted by all host threads, a block of entries at a time,
+    // each thread into its own buffer; the buffers are written in order
+    constexpr int64_t BLOCK = 1 << 20;
+    constexpr size_t LINE_MAX_BYTES = 64;   // two ints, a %.9g float, 2 blanks and a break
+    const int T = omp_get_max_threads() > 0 ? omp_get_max_threads() : 1;
+    const int64_t per = (BLOCK + T - 1) / T;
+    std::unique_ptr<char[]> out(new (std::nothrow) char[(size_t)T * (size_t)per * LINE_MAX_BYTES]);
+    if (!out) {
+        std::fclose(f);
+        return LV_ERR_NOMEM;
     }
-    int rc = std::fclose(f);
-    return rc == 0 ? LV_OK : LV_ERR_IO;
+    std::vector<size_t> len((size_t)T);
+    bool ok = true;
+    for (int64_t b0 = 0; b0 < n_edges && ok; b0 += BLOCK) {
+        const int64_t b1 = b0 + BLOCK < n_edges ? b0 + BLOCK : n_edges;
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+        for (int t = 0; t < T; ++t) {
+            const int64_t i0 = b0 + per * t, i1 = i0 + per < b1 ? i0 + per : b1;
+            char *const o = out.get() + (size_t)t * (size_t)per * LINE_MAX_BYTES;
+            char *q = o;
+            for (int64_t i = i0; i < i1; ++i) {
+                int32_t a = u[i], b = v[i];
+                if (a < b) std::swap(a, b);
+                q += std::snprintf(q, LINE_MAX_BYTES, "%d %d %.9g\n", a + 1, b + 1, w ? (double)w[i] : 1.0);
+            }
+            len[(size_t)t] = i1 > i0 ? (size_t)(q - o) : 0;
+        }
+        for (int t = 0; t < T && ok; ++t)
+            ok = len[(size_t)t] == 0 ||
+                 std::fwrite(out.get() + (size_t)t * (size_t)per * LINE_MAX_BYTES, 1, len[(size_t)t], f) ==
+                     len[(size_t)t];
+    }
+    const int rc = std::fclose(f);
+    return rc == 0 && ok ? LV_OK : LV_ERR_IO;
 }
 
-// The lines of consecutive community ranges are formatted by all host
-// threads into their own buffers (ranges of about equal member counts), then
-// written in order.  Every buffer is allocated before the threads start, so
-// an allocation failure returns LV_ERR_NOMEM instead of ending the process.
 // Stable LSD radix sort of n 64-bit keys on bits [lo, hi), 8 bits per pass,
 // all host threads.  The buffers are left uninitialised so that the threads
 // that fill them also fault their pages in (a zero-filled std::vector would
@@ -669,6 +693,10 @@ static void radix_sort_key_bits(std::unique_ptr<uint64_t[]> &a, size_t n, int lo
     }
 }
 
+// The lines of consecutive community ranges are formatted by all host
+// threads into their own buffers (ranges of about equal member counts), then
+// written in order.  Every buffer is allocated before the threads start, so
+// an allocation failure returns LV_ERR_NOMEM instead of ending the process.
 static int print_communities_impl(const char *path, const int32_t *orig2comm, int32_t V0,
                                   int32_t num_communities) {
     // vertices grouped by community with members in increasing id: keys
