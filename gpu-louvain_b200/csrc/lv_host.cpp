@@ -333,16 +333,30 @@ int lv_read_csr(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr
         std::free(rp); std::free(cl); std::free(wt);
         return LV_ERR_NOMEM;
     }
-    const char *q = m.p + sizeof h;
-    std::memcpy(rp, q, 4 * ((size_t)h.V + 1));
-    q += 4 * ((size_t)h.V + 1);
-    std::memcpy(cl, q, 4 * (size_t)h.E);
-    q += 4 * (size_t)h.E;
-    std::memcpy(wt, q, 4 * (size_t)h.E);
-    bool okp = rp[0] == 0 && (int64_t)rp[h.V] == h.E;
-    for (int64_t v = 0; okp && v < h.V; ++v) okp = rp[v + 1] >= rp[v];
-    for (int64_t e = 0; okp && e < h.E; ++e) okp = cl[e] >= 0 && cl[e] < h.V;
-    if (!okp) {
+    // copied and checked (offsets non-decreasing from 0 to E, columns in
+    // [0, V)) by all host threads, in 1 MB-sized pieces
+    const char *const q0 = m.p + sizeof h;
+    const char *const q1 = q0 + 4 * ((size_t)h.V + 1);
+    const char *const q2 = q1 + 4 * (size_t)h.E;
+    constexpr int64_t PIECE = 1 << 18;   // 4-byte words
+    const int64_t nrp = h.V + 1, ne = h.E;
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t s0 = 0; s0 < nrp; s0 += PIECE) {
+        const int64_t s1 = s0 + PIECE < nrp ? s0 + PIECE : nrp;
+        std::memcpy(rp + s0, q0 + 4 * s0, 4 * (size_t)(s1 - s0));
+    }
+#pragma omp parallel for schedule(dynamic, 4) reduction(| : bad)
+    for (int64_t s0 = 0; s0 < ne; s0 += PIECE) {
+        const int64_t s1 = s0 + PIECE < ne ? s0 + PIECE : ne;
+        std::memcpy(cl + s0, q1 + 4 * s0, 4 * (size_t)(s1 - s0));
+        std::memcpy(wt + s0, q2 + 4 * s0, 4 * (size_t)(s1 - s0));
+        for (int64_t e = s0; e < s1; ++e) bad |= (cl[e] < 0 || cl[e] >= h.V) ? 1 : 0;
+    }
+    bad |= (rp[0] != 0 || (int64_t)rp[h.V] != h.E) ? 1 : 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (int64_t v = 0; v < h.V; ++v) bad |= rp[v + 1] < rp[v] ? 1 : 0;
+    if (bad) {
         std::free(rp); std::free(cl); std::free(wt);
         return LV_ERR_IO;
     }

@@ -205,7 +205,14 @@ def test_csr_cache_roundtrip(lvb, tmp_path):
     assert np.array_equal(r.rowptr, g.rowptr) and np.array_equal(r.col, g.col) and np.array_equal(r.w, g.w)
     assert r.m_ref == np.float32(1234.5)
     raw = open(p, "rb").read()
-    for broken in (raw[:-4], b"XXXXXXXX" + raw[8:], raw[:64] + (b"\xff" * 4) + raw[68:]):
+    hdr = 48                                   # magic, V, E, m_ref, pad, source size, source mtime
+    c0 = hdr + 4 * (g.V + 1)                   # first column word
+    last = c0 + 4 * (g.E - 1)                  # last column word
+    for broken in (raw[:-4], b"XXXXXXXX" + raw[8:], raw[:64] + (b"\xff" * 4) + raw[68:],
+                   raw[:c0] + np.int32(-1).tobytes() + raw[c0 + 4:],            # column below 0
+                   raw[:last] + np.int32(g.V).tobytes() + raw[last + 4:],       # column past V
+                   raw[:hdr] + np.int32(1).tobytes() + raw[hdr + 4:],           # rowptr[0] != 0
+                   raw[:c0 - 4] + np.int32(g.E - 1).tobytes() + raw[c0:]):      # rowptr[V] != E
         q = str(tmp_path / "broken.lvcsr")
         open(q, "wb").write(broken)
         with pytest.raises(lvb.LouvainError) as ex:
