@@ -482,8 +482,8 @@ int lv_read_mtx(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr
 
 namespace {
 
-// lv_read_mtx's body; its vectors may throw std::bad_alloc, which the entry
-// point turns into LV_ERR_NOMEM
+// lv_read_mtx's body; its allocations may throw std::bad_alloc, which the
+// entry point turns into LV_ERR_NOMEM
 int read_mtx_host_csr(const char *path, int32_t *Vout, int64_t *Eout, int32_t **rowptr_out, int32_t **col_out,
                       float **w_out, float *m_ref) {
     int32_t V = 0;
