@@ -91,6 +91,7 @@ EXPORTED = [
     "lv_gen_lfr", "lv_set_active_model", "lv_get_traces", "lv_get_active_stats", "lv_active_train",
     "lv_active_predict", "lv_write_csr", "lv_read_csr", "lv_write_csr_stamped", "lv_read_csr_stamp", "lv_gen_planted_batch", "lv_read_mtx_device",
     "lv_csr_from_entries_device", "lv_read_mtx_entries", "lv_get_level_classes", "lv_get_device_name",
+    "lv_read_active_model",
 ]
 
 _lib = None
@@ -189,6 +190,7 @@ def lib() -> C.CDLL:
     PU16 = C.POINTER(C.c_uint16)
     PU8 = C.POINTER(C.c_uint8)
     L.lv_set_active_model.argtypes = [C.c_void_p, PU16, C.c_int32, C.c_float]
+    L.lv_read_active_model.argtypes = [C.c_char_p, PU16, C.c_int32, P32, PF, C.POINTER(_Opts)]
     L.lv_get_traces.argtypes = [C.c_void_p, PF, PU8, C.c_int64, P64]
     L.lv_get_active_stats.argtypes = [C.c_void_p, P64, P64, P64, C.POINTER(C.c_double), P32]
     L.lv_active_train.argtypes = [PF, PU8, C.c_int64, C.c_int32, C.c_int32, C.c_float, C.c_float,
@@ -635,6 +637,23 @@ def active_predict(model, x, device: int = 0) -> np.ndarray:
     _check(lib().lv_active_predict(_ptr(m, C.c_uint16), _ptr(xx, C.c_float), len(xx), device,
                                    _ptr(out, C.c_float)))
     return out
+
+
+def read_active_model(path: str | None = None):
+    """The predictor file read by the library (lv_read_active_model, as the
+    CLI's --mode learned reads it): (model uint16[ACTIVE_MODEL_SIZE], logit
+    threshold, {"full_every", "active_start", "min_recall"} as they land in
+    lv_opts)."""
+    L = lib()
+    path = path or os.path.join(_HERE, "active_set_lfr.json")
+    m = np.zeros(ACTIVE_MODEL_SIZE, np.uint16)
+    n, thr = C.c_int32(), C.c_float()
+    opts = _Opts()
+    L.lv_default_opts(C.byref(opts))
+    _check(L.lv_read_active_model(path.encode(), _ptr(m, C.c_uint16), len(m), C.byref(n), C.byref(thr),
+                                  C.byref(opts)))
+    return m[:n.value], thr.value, {"full_every": opts.active_full_every, "active_start": opts.active_start,
+                                    "min_recall": opts.active_min_recall, "active_set": opts.active_set}
 
 
 def load_active_model(path: str | None = None):

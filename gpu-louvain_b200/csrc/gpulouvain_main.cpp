@@ -14,14 +14,20 @@
 // read instead of the text only while both still match the file.  Without
 // -c the parsed entries are copied to the device and the CSR is built there
 // (lv_csr_from_entries_device; the same CSR as the host build), timed as the
-// reference times its host->device copy.
+// reference times its host->device copy.  --mode learned runs the learned
+// active-set sweeps with a predictor file (--model FILE; default: the
+// packaged active_set_lfr.json beside the bin/ directory) and the settings
+// stored in it; the partition is then no longer the plain rule's.
 #include <getopt.h>
 #include <sys/stat.h>
+#include <unistd.h>
 
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/louvain_b200.h"
 
@@ -51,23 +57,62 @@ static void usage() {
     std::exit(1);
 }
 
+// The packaged predictor: ../active_set_lfr.json relative to this binary.
+static std::string packaged_model() {
+    char exe[4096];
+    const ssize_t n = readlink("/proc/self/exe", exe, sizeof exe - 1);
+    if (n <= 0) return "active_set_lfr.json";
+    exe[n] = 0;
+    std::string dir(exe);
+    const size_t slash = dir.rfind('/');
+    dir = slash == std::string::npos ? std::string(".") : dir.substr(0, slash);
+    return dir + "/../active_set_lfr.json";
+}
+
 int main(int argc, char *argv[]) {
     const char *file = nullptr;
     float min_gain = 0;
     bool have_f = false, have_g = false, verbose = false, use_cache = false;
     int device = 0;
+    bool learned = false;
+    std::string model_path;
+    static const struct option long_opts[] = {{"mode", required_argument, nullptr, 'm'},
+                                              {"model", required_argument, nullptr, 'M'},
+                                              {nullptr, 0, nullptr, 0}};
     int opt;
-    while ((opt = getopt(argc, argv, "f:g:vd:c")) != -1) {
+    while ((opt = getopt_long(argc, argv, "f:g:vd:c", long_opts, nullptr)) != -1) {
         switch (opt) {
         case 'g': have_g = true; min_gain = std::strtof(optarg, nullptr); break;
         case 'v': verbose = true; break;
         case 'f': have_f = true; file = optarg; break;
         case 'd': device = std::atoi(optarg); break;
         case 'c': use_cache = true; break;
+        case 'm':
+            if (std::strcmp(optarg, "learned") == 0) learned = true;
+            else if (std::strcmp(optarg, "plain") != 0) usage();
+            break;
+        case 'M': model_path = optarg; break;
         default: usage();
         }
     }
     if (!have_f || !have_g) usage();
+
+    lv_opts opts;
+    lv_default_opts(&opts);
+    opts.device = device;
+    std::vector<uint16_t> model(LV_ACTIVE_MODEL_SIZE);
+    int32_t n_params = 0;
+    float logit_thr = 0;
+    if (learned) {
+        if (model_path.empty()) model_path = packaged_model();
+        const int mrc = lv_read_active_model(model_path.c_str(), model.data(), (int32_t)model.size(), &n_params,
+                                             &logit_thr, &opts);
+        if (mrc != LV_OK) {
+            std::fprintf(stderr, "gpulouvain: cannot read the predictor %s: %s\n", model_path.c_str(),
+                         lv_status_string(mrc));
+            return EXIT_FAILURE;
+        }
+    }
 
     int32_t V = 0;
     int64_t E = 0;
@@ -82,9 +127,6 @@ int main(int argc, char *argv[]) {
         std::fprintf(stderr, "gpulouvain: cannot read %s: %s\n", file, lv_status_string(rc));
         return EXIT_FAILURE;
     }
-    lv_opts opts;
-    lv_default_opts(&opts);
-    opts.device = device;
     using clk = std::chrono::steady_clock;
     lv_handle *h = nullptr;
     auto t0 = clk::now();
@@ -94,6 +136,7 @@ int main(int argc, char *argv[]) {
         rc = lv_csr_from_entries_device(device, V, nnz, ea, eb, ew, &E, &rowptr, &col, &w);
         if (rc == LV_OK) rc = lv_create_device(rowptr, col, w, V, E, &opts, &h);
     }
+    if (rc == LV_OK && learned) rc = lv_set_active_model(h, model.data(), n_params, logit_thr);
     auto t1 = clk::now();
     if (rc != LV_OK) {
         std::fprintf(stderr, "gpulouvain: %s\n", lv_status_string(rc));

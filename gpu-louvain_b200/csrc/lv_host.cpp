@@ -625,6 +625,99 @@ int lv_read_mtx_device(const char *path, int32_t device, int32_t *Vout, int64_t 
     return LV_OK;
 }
 
+// ---------------------------------------------------------------------------
+// predictor files of the learned active-set mode
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+// The value after `"key"` and a colon in the JSON text, or nullptr.  The
+// files are the flat objects train_active_set.py writes; a key is matched
+// only where it is followed by a colon (a key name inside a string value is
+// not).
+const char *json_value(const std::string &text, const char *key) {
+    const std::string k = std::string("\"") + key + "\"";
+    for (size_t at = text.find(k); at != std::string::npos; at = text.find(k, at + 1)) {
+        size_t i = at + k.size();
+        while (i < text.size() && (text[i] == ' ' || text[i] == '\t' || text[i] == '\r' || text[i] == '\n')) ++i;
+        if (i < text.size() && text[i] == ':') {
+            ++i;
+            while (i < text.size() && (text[i] == ' ' || text[i] == '\t' || text[i] == '\r' || text[i] == '\n'))
+                ++i;
+            return text.c_str() + i;
+        }
+    }
+    return nullptr;
+}
+
+bool json_number(const std::string &text, const char *key, double *out) {
+    const char *v = json_value(text, key);
+    if (!v) return false;
+    char *e = nullptr;
+    const double x = std::strtod(v, &e);
+    if (e == v || !std::isfinite(x)) return false;
+    *out = x;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lv_read_active_model(const char *path, uint16_t *model, int32_t cap, int32_t *n_params,
+                         float *logit_threshold, lv_opts *opts) {
+    if (!path || !model || !n_params || !logit_threshold || cap < 0) return LV_ERR_INVALID;
+    std::string text;
+    {
+        FILE *f = std::fopen(path, "rb");
+        if (!f) return LV_ERR_IO;
+        char buf[1 << 16];
+        size_t got;
+        while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) {
+            text.append(buf, got);
+            if (text.size() > ((size_t)1 << 24)) {   // far beyond any predictor file
+                std::fclose(f);
+                return LV_ERR_IO;
+            }
+        }
+        std::fclose(f);
+    }
+    const char *v = json_value(text, "model_bf16");
+    if (!v || *v != '[') return LV_ERR_IO;
+    ++v;
+    int32_t n = 0;
+    for (;;) {
+        while (*v == ' ' || *v == '\t' || *v == '\r' || *v == '\n') ++v;
+        if (*v == ']') break;
+        if (*v < '0' || *v > '9') return LV_ERR_IO;
+        char *e = nullptr;
+        const long x = std::strtol(v, &e, 10);
+        if (x < 0 || x > 65535) return LV_ERR_IO;
+        if (n >= LV_ACTIVE_MODEL_SIZE) return LV_ERR_INVALID;   // more parameters than the model has
+        if (n < cap) model[n] = (uint16_t)x;
+        ++n;
+        v = e;
+        while (*v == ' ' || *v == '\t' || *v == '\r' || *v == '\n') ++v;
+        if (*v == ',') ++v;
+        else if (*v != ']') return LV_ERR_IO;
+    }
+    if (n != LV_ACTIVE_MODEL_SIZE) return LV_ERR_INVALID;
+    if (cap < n) return LV_ERR_INVALID;
+    double thr = 0;
+    if (!json_number(text, "logit_threshold", &thr)) return LV_ERR_IO;
+    *n_params = n;
+    *logit_threshold = (float)thr;
+    if (opts) {
+        double x = 0;
+        opts->active_set = 1;
+        if (json_number(text, "full_every", &x) && x >= 1 && x <= 1e6) opts->active_full_every = (int32_t)x;
+        if (json_number(text, "active_start", &x) && x >= 0 && x <= 1) opts->active_start = (float)x;
+        if (json_number(text, "min_recall", &x) && x >= 0 && x <= 1) opts->active_min_recall = (float)x;
+    }
+    return LV_OK;
+}
+
 int lv_write_mtx(const char *path, int32_t V, int64_t n_edges, const int32_t *u, const int32_t *v,
                  const float *w) {
     if (!path || V < 0 || n_edges < 0 || (n_edges > 0 && (!u || !v))) return LV_ERR_INVALID;

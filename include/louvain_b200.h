@@ -329,6 +329,17 @@ int lv_modularity_noalloc(const int32_t *d_rowptr, const int32_t *d_col, const f
 /* Model for lv_opts.active_set = 1; a vertex is proposed when its logit
  * exceeds logit_threshold. */
 int lv_set_active_model(lv_handle *h, const uint16_t *model, int32_t n_params, float logit_threshold);
+/* Read a predictor file as train_active_set.py writes it (JSON with
+ * "model_bf16": [LV_ACTIVE_MODEL_SIZE bit patterns], "logit_threshold" and
+ * the settings it was measured with, "full_every", "active_start",
+ * "min_recall").  model receives the parameters (cap >= LV_ACTIVE_MODEL_SIZE),
+ * *n_params their count, *logit_threshold the threshold; when opts is not
+ * NULL, active_set is set to 1 and the three settings present in the file
+ * are copied into it.  Host only (no device is touched).  LV_ERR_IO for a
+ * missing or malformed file, LV_ERR_INVALID for a parameter count other than
+ * LV_ACTIVE_MODEL_SIZE. */
+int lv_read_active_model(const char *path, uint16_t *model, int32_t cap, int32_t *n_params,
+                         float *logit_threshold, lv_opts *opts);
 /* Move traces recorded with lv_opts.trace_sample > 0: features[n][FEATURES]
  * and labels[n] (1 = moved in the sweep after sampling); up to cap rows are
  * copied, *n receives the number of complete rows available. */

@@ -164,3 +164,52 @@ def test_packaged_model_and_threshold_rule(lvb):
     for target in (0.9, 0.97, 0.99):
         t = T.pick_threshold(z, y, target)
         assert ((z > t) & (y == 1)).sum() >= target * (y == 1).sum()
+
+
+def test_library_reads_the_predictor_file(lvb, tmp_path):
+    """lv_read_active_model (what the CLI's --mode learned uses) reads the
+    packaged file to the same parameters, threshold and settings as the
+    Python loader, and refuses files that are not predictor files."""
+    import json
+    import os
+    m, thr, st = lvb.read_active_model()
+    m2, thr2 = lvb.load_active_model()
+    assert np.array_equal(m, m2) and np.float32(thr) == np.float32(thr2)
+    with open(os.path.join(os.path.dirname(lvb.__file__), "active_set_lfr.json")) as f:
+        meta = json.load(f)
+    assert st["active_set"] == 1 and st["full_every"] == meta["full_every"]
+    assert np.float32(st["active_start"]) == np.float32(meta["active_start"])
+    assert np.float32(st["min_recall"]) == np.float32(meta["min_recall"])
+    good = {"model_bf16": [int(x) for x in m2], "logit_threshold": -1.5, "full_every": 6,
+            "settings_note": "a note that names \"model_bf16\" inside a string"}
+    p = tmp_path / "m.json"
+    p.write_text(json.dumps(good))
+    m3, thr3, st3 = lvb.read_active_model(str(p))
+    assert np.array_equal(m3, m2) and thr3 == -1.5 and st3["full_every"] == 6
+    bad = [("missing_model", {k: v for k, v in good.items() if k != "model_bf16"}, lvb.LV_ERR_IO),
+           ("missing_threshold", {k: v for k, v in good.items() if k != "logit_threshold"}, lvb.LV_ERR_IO),
+           ("short_model", dict(good, model_bf16=good["model_bf16"][:-1]), lvb.LV_ERR_INVALID),
+           ("long_model", dict(good, model_bf16=good["model_bf16"] + [0]), lvb.LV_ERR_INVALID),
+           ("value_past_16_bits", dict(good, model_bf16=[70000] + good["model_bf16"][1:]), lvb.LV_ERR_IO),
+           ("negative_value", dict(good, model_bf16=[-1] + good["model_bf16"][1:]), lvb.LV_ERR_IO),
+           ("text_value", dict(good, model_bf16=["x"] + good["model_bf16"][1:]), lvb.LV_ERR_IO)]
+    for name, d, status in bad:
+        q = tmp_path / (name + ".json")
+        q.write_text(json.dumps(d))
+        with pytest.raises(lvb.LouvainError) as ei:
+            lvb.read_active_model(str(q))
+        assert ei.value.status == status, name
+    with pytest.raises(lvb.LouvainError):
+        lvb.read_active_model(str(tmp_path / "absent.json"))
+
+
+def test_cli_learned_mode_arguments(lvb, tmp_path):
+    """--mode takes plain or learned; a predictor that cannot be read ends the
+    CLI with a message before any graph or device work."""
+    import subprocess
+    r = subprocess.run([lvb.CLI_PATH, "--mode", "fast", "-f", "x.mtx", "-g", "0.1"], capture_output=True,
+                       text=True)
+    assert r.returncode == 1 and r.stdout.startswith("Usage:")
+    r = subprocess.run([lvb.CLI_PATH, "--mode", "learned", "--model", str(tmp_path / "none.json"), "-f",
+                        "x.mtx", "-g", "0.1"], capture_output=True, text=True)
+    assert r.returncode == 1 and "cannot read the predictor" in r.stderr
