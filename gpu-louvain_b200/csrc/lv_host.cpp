@@ -665,9 +665,21 @@ bool json_number(const std::string &text, const char *key, double *out) {
 
 extern "C" {
 
+static int read_active_model_body(const char *path, uint16_t *model, int32_t cap, int32_t *n_params,
+                                  float *logit_threshold, lv_opts *opts);
+
 int lv_read_active_model(const char *path, uint16_t *model, int32_t cap, int32_t *n_params,
                          float *logit_threshold, lv_opts *opts) {
     if (!path || !model || !n_params || !logit_threshold || cap < 0) return LV_ERR_INVALID;
+    try {
+        return read_active_model_body(path, model, cap, n_params, logit_threshold, opts);
+    } catch (const std::bad_alloc &) {
+        return LV_ERR_NOMEM;
+    }
+}
+
+static int read_active_model_body(const char *path, uint16_t *model, int32_t cap, int32_t *n_params,
+                                  float *logit_threshold, lv_opts *opts) {
     std::string text;
     {
         FILE *f = std::fopen(path, "rb");
